@@ -1,0 +1,329 @@
+"""Benchmark: batched 3D eikonal travel-time tables on one B200.
+
+Workload (the batched-tables configuration): 64 surface sources (seeded
+uniform x, y; z = 0, which takes the reference's on-node nudge) solved on 4
+grids of uneven size, all h = 50 m, nx x ny x nz = 96x96x64, 128x128x80,
+160x160x96, 200x120x100, cell velocity v(z) = 3000 + 0.5 z (cell centre).
+Every (grid, source) pair is one work item: 256 solves per step, one kernel
+launch replayed from a CUDA graph.  A step = the whole batch: field
+initialisation, the 8 initialisation sweeps and nsweep = 2 Gauss-Seidel
+passes of 8 sweeps (the reference's default, no convergence test in 3D).
+
+metric: node updates per second, counted as the reference evaluates them:
+per source and grid, the masked initialisation sweeps plus nsweep x 8 x
+(nz-1)(nx-1)(ny-1).  Inputs are synthetic and seeded.
+
+--impl reference runs the CPU restatement of the reference's OpenMP
+level-set solver (oracle/, FP64, 32-node chunks, a barrier per level) on
+the host cores with the same metric, on a bounded sample of the workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+GRIDS = [(96, 96, 64), (128, 128, 80), (160, 160, 96), (200, 120, 100)]  # nx, ny, nz
+H = 50.0
+NSRC = 64
+NSWEEP = 2
+EPS = 5.0
+METRIC = "3D eikonal node-updates/s (64-src batch)"
+
+
+def workload():
+    rng = np.random.default_rng(4)
+    srcxy = rng.uniform(0.0, 1.0, size=(NSRC, 2))
+    grids = []
+    for nx, ny, nz in GRIDS:
+        zc = (np.arange(nz - 1) + 0.5) * H
+        vel = np.broadcast_to(3000.0 + 0.5 * zc, (ny - 1, nx - 1, nz - 1)).copy()
+        xs = srcxy[:, 0] * (nx - 1) * H
+        ys = srcxy[:, 1] * (ny - 1) * H
+        zs = np.zeros(NSRC)
+        grids.append(dict(nx=nx, ny=ny, nz=nz, vel=vel, xs=xs, ys=ys, zs=zs))
+    return grids
+
+
+def snap1(n, h, v):
+    """source.F90:150-168 for one coordinate -> 1-based cell index."""
+    a = v / h + 1.0
+    if abs(a - 1.0) < 2.220446049250313e-16:
+        a += 1e-4
+    if a >= n:
+        a -= 1e-4
+    return int(a)
+
+
+def node_updates(g):
+    """Node updates the reference evaluates for one grid's sources
+    (solver3D.F90:493-565 boxes, init boxes clamped to the grid)."""
+    nz, nx, ny = g["nz"], g["nx"], g["ny"]
+    per_pass = 8 * (nz - 1) * (nx - 1) * (ny - 1)
+    total = 0
+    for k in range(NSRC):
+        si = (snap1(nz, H, g["zs"][k]), snap1(nx, H, g["xs"][k]), snap1(ny, H, g["ys"][k]))
+        init = 0
+        for s in range(8):
+            signs = (1 if s < 4 else -1, 1 if s % 2 == 0 else -1, 1 if (s // 2) % 2 == 0 else -1)
+            cnt = 1
+            for sgn, n, i in zip(signs, (nz, nx, ny), si):
+                if sgn > 0:
+                    lo, hi = max(2, i), n
+                else:
+                    lo, hi = 1, min(i + 1, n - 1)
+                cnt *= max(0, hi - lo + 1)
+            init += cnt
+        total += init + NSWEEP * per_pass
+    return total
+
+
+def algorithmic_bytes(grids, upd_total):
+    """FP32 travel time read + write per node update, plus the slowness
+    read once per grid per sweep (shared by the grid's sources)."""
+    slow = sum(4 * (g["nz"] - 1) * (g["nx"] - 1) * (g["ny"] - 1) * 8 * (1 + NSWEEP) for g in grids)
+    return 8 * upd_total + slow
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons}
+
+
+def cpu_reference(grids, steps, warmup, nthreads, sample_src=1):
+    """CPU restatement of the reference (oracle/), timed on a bounded sample:
+    `sample_src` sources on the largest grid per step."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    g = grids[2]
+    n = (g["nz"], g["nx"], g["ny"])
+    slow = (1.0 / g["vel"]).ravel()
+    upd = 0
+    si_sa = []
+    for k in range(sample_src):
+        si, sa = O.source_snap(True, n, (0, 0, 0), (H, H, H), (g["zs"][k], g["xs"][k], g["ys"][k]))
+        si_sa.append((si, sa))
+        ni, npass = O.count_updates3d(n, si)
+        upd += ni + NSWEEP * npass
+    for _ in range(warmup):
+        O.solve3d(n, (H, H, H), slow, *si_sa[0], EPS, NSWEEP, level_set=True, nthreads=nthreads)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for si, sa in si_sa:
+            O.solve3d(n, (H, H, H), slow, si, sa, EPS, NSWEEP, level_set=True, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return upd * steps / dt, dt, "%d source(s) on the %dx%dx%d grid per step, %d step(s)" % (
+        sample_src, g["nx"], g["ny"], g["nz"], steps)
+
+
+def run_reference(args, rank, world):
+    grids = workload()
+    nth = os.cpu_count() or 1
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    value, dt, sample = cpu_reference(grids, steps=min(steps, 3), warmup=min(args.warmup, 1), nthreads=nth)
+    line = {"metric": METRIC, "value": value, "unit": "node-updates/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": min(steps, 3), "warmup": min(args.warmup, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "batched tables: 64 surface sources x 4 grids, h=50 m", "nsweep": NSWEEP},
+            "cpu_baseline": {"value": value, "unit": "node-updates/s", "cores": nth, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "node-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    import fteik_b200 as fk
+    if not os.path.exists(fk.LIB_PATH):
+        fk.build()
+
+    grids = workload()
+    upd_total = sum(node_updates(g) for g in grids)
+    bytes_step = algorithmic_bytes(grids, upd_total)
+
+    b = fk.Batch3D([(g["nz"], g["nx"], g["ny"], H, H, H) for g in grids], nsweep=NSWEEP, eps=EPS,
+                   precision=4)
+    for i, g in enumerate(grids, start=1):
+        b.setVelocityModel(i, g["vel"])
+        b.setSources(i, g["zs"], g["xs"], g["ys"])
+    b.solve()  # builds and captures the graph
+    stream = torch.cuda.ExternalStream(fk.lib().fteik_b200_stream())
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-resident timing: K graph replays on the library stream ----
+    for _ in range(args.warmup):
+        b.solveAsync()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            rc = b.solveAsync()
+            assert rc == 0, rc
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = upd_total * world / (ms * 1e-3)
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        outs = []
+        for g in grids:
+            n = NSRC * g["nz"] * g["nx"] * g["ny"]
+            outs.append(torch.empty(n, dtype=torch.float32, pin_memory=True).numpy())
+        vels = [torch.from_numpy(np.ascontiguousarray(g["vel"].ravel())).pin_memory().numpy() for g in grids]
+        h2d = sum(v.nbytes for v in vels) + sum(3 * 8 * NSRC for _ in grids)
+        d2h = sum(o.nbytes for o in outs)
+
+        def e2e_step():
+            for i, g in enumerate(grids, start=1):
+                b.setVelocityModel(i, vels[i - 1])
+                b.setSources(i, g["zs"], g["xs"], g["ys"])
+            b.solve()
+            for i in range(1, len(grids) + 1):
+                b.fields32(i, outs[i - 1])
+
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        ke = max(1, min(args.steps, 3))
+        for _ in range(ke):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        te = (time.perf_counter() - t0) / ke
+        if dist is not None:
+            t = torch.tensor([te], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": upd_total * world / te, "unit": "node-updates/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": te * 1e3}
+
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6651.0, "fallback"
+    if os.path.exists(peaks_path):
+        peak = json.load(open(peaks_path))["hbm_gbs"]
+        peak_src = "measured"
+    achieved = bytes_step / (ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src, "traffic": None,
+                "algorithmic_bytes_per_launch": bytes_step}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, dt, sample = cpu_reference(grids, steps=1, warmup=0, nthreads=os.cpu_count() or 1)
+        cpu = {"value": v, "unit": "node-updates/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": sample}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "node-updates/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": "batched tables: 64 surface sources x 4 grids "
+                           "(96x96x64, 128x128x80, 160x160x96, 200x120x100), h=50 m, v(z)=3000+0.5z",
+                           "nsweep": NSWEEP, "eps": EPS, "work_items": NSRC * len(GRIDS),
+                           "node_updates_per_step": upd_total,
+                           "l2": "fields 1.73 GB > L2 (inputs larger than L2)",
+                           "parallelism": "replicas (one batch per GPU)" if world > 1 else "1 GPU"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": args.steps, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    b.finalize()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,525 @@
+"""fteik_b200 -- B200 (sm_100a) implementation of fteik's eikonal solver and
+grid-search locator behind the reference's C ABI.
+
+The product is the shared library ``fteik_b200/lib/libfteik_shared.so``
+(C host layer + CUDA kernels); its entry points are declared in
+``include/fteik_b200.h``.  This module binds it with ctypes and mirrors the
+reference's Python wrappers (python/fteik3d.py, python/fteik2d.py) so that
+existing callers read the same.  There is no CPU fallback: if the library
+or a CUDA device is missing, calls raise.
+"""
+import ctypes
+import os
+import subprocess
+from ctypes import POINTER, byref, c_bool, c_double, c_float, c_int, c_longlong
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libfteik_shared.so")
+CSRC = os.path.join(_HERE, "csrc")
+
+FTEIK_NATURAL_ORDERING = 0
+FTEIK_ZXY_ORDERING = 0
+FTEIK_ZX_ORDERING = 0
+FTEIK_XYZ_ORDERING = 1
+FTEIK_XZ_ORDERING = 1
+FTEIK_ZYX_ORDERING = 2
+FTEIK_HUGE = 99999.0
+
+_lib = None
+
+_PD = POINTER(c_double)
+_PF = POINTER(c_float)
+_PI = POINTER(c_int)
+
+# name -> argtypes (restype void unless listed in _RESTYPES)
+_SIGS = {
+    # model.F90
+    "fteik_model_initializeGeometry": [c_bool, c_int, c_int, c_int] + [c_double] * 6 + [_PI],
+    "fteik_model_setGridSize": [c_bool, c_int, c_int, c_int, _PI],
+    "fteik_model_setGridSpacing": [c_bool, c_double, c_double, c_double, _PI],
+    "fteik_model_setOrigin3D": [c_double, c_double, c_double],
+    "fteik_model_setOrigin2D": [c_double, c_double],
+    "fteik_model_getGridSize": [_PI, _PI, _PI, _PI, _PI, _PI],
+    "fteik_model_setVelocityModel64f": [c_int, _PD, _PI],
+    "fteik_model_setNodalVelocityModel64f": [c_int, c_int, _PD, _PI],
+    "fteik_model_setCellVelocityModel64f": [c_int, c_int, _PD, _PI],
+    "fteik_model_grid2indexF": [c_int] * 5,
+    "fteik_model_grid2index": [c_int] * 5,
+    "fteik_model_index2gridF": [c_int, _PI, _PI, _PI, _PI],
+    "fteik_model_velGrid2indexF": [c_int] * 5,
+    "fteik_model_free": [],
+    # source.F90
+    "fteik_source_initialize64f": [c_int, _PD, _PD, _PD, c_int, _PI],
+    "fteik_source_getSolverInfo64fF": [c_int, _PI, _PI, _PI, _PD, _PD, _PD, _PD, _PD, _PI],
+    "fteik_source_getNumberOfSources": [_PI, _PI],
+    "fteik_source_free": [],
+    # receiver.F90
+    "fteik_receiver_initialize64f": [c_int, _PD, _PD, _PD, c_int, _PI],
+    "fteik_receiver_getTravelTimes64f": [c_int, c_int, _PD, _PD, _PI],
+    "fteik_receiver_getNumberOfReceivers": [_PI, _PI],
+    "fteik_receiver_free": [],
+    # solver3D.F90
+    "fteik_solver3d_initialize": [c_int, c_int, c_int] + [c_double] * 6 + [c_int, c_double, c_double, c_int, _PI],
+    "fteik_solver3d_free": [],
+    "fteik_solver3d_setVerbosity": [c_int],
+    "fteik_solver3d_setConvergenceTolerance": [c_double],
+    "fteik_solver3d_setNumberOfSweeps": [c_int, _PI],
+    "fteik_solver3d_setSphereToCartEpsilon": [c_double, _PI],
+    "fteik_solver3d_setVelocityModel64f": [c_int, _PD, _PI],
+    "fteik_solver3d_setCellVelocityModel64f": [c_int, c_int, _PD, _PI],
+    "fteik_solver3d_setNodalVelocityModel64f": [c_int, c_int, _PD, _PI],
+    "fteik_solver3d_setSources64f": [c_int, _PD, _PD, _PD, _PI],
+    "fteik_solver3d_getNumberOfSources": [_PI, _PI],
+    "fteik_solver3d_setReceivers64f": [c_int, _PD, _PD, _PD, _PI],
+    "fteik_solver3d_getNumberOfReceivers": [_PI, _PI],
+    "fteik_solver3d_solveSourceLSM": [c_int, _PI],
+    "fteik_solver3d_getTravelTimeField64f": [c_int, c_int, _PD, _PI],
+    "fteik_solver3d_getTravelTimeFieldCell64f": [c_int, c_int, _PD, _PI],
+    "fteik_solver3d_getTravelTimes64f": [c_int, _PD, _PI],
+    "fteik_solver3d_traceRaysToReceivers": [_PI],
+    # solver2D.F90
+    "fteik_solver2d_initialize": [c_int, c_int] + [c_double] * 4 + [c_int, c_double, c_double, c_int, _PI],
+    "fteik_solver2d_free": [],
+    "fteik_solver2d_setVelocityModel64f": [c_int, _PD, _PI],
+    "fteik_solver2d_setCellVelocityModel64f": [c_int, c_int, _PD, _PI],
+    "fteik_solver2d_setNodalVelocityModel64f": [c_int, c_int, _PD, _PI],
+    "fteik_solver2d_setSources64f": [c_int, _PD, _PD, _PI],
+    "fteik_solver2d_setReceivers64f": [c_int, _PD, _PD, _PI],
+    "fteik_solver2d_getNumberOfReceivers": [_PI, _PI],
+    "fteik_solver2d_solveSourceLSM": [c_int, _PI],
+    "fteik_solver2d_solveSourceFSM": [c_int, _PI],
+    "fteik_solver2d_solveLSM": [_PI],
+    "fteik_solver2d_getTravelTimeField64f": [c_int, c_int, _PD, _PI],
+    "fteik_solver2d_getTravelTimeFieldCell64f": [c_int, c_int, _PD, _PI],
+    "fteik_solver2d_getTravelTimes64f": [c_int, _PD, _PI],
+    # analytic.F90
+    "fteik_analytic_initialize64f": [c_int, c_int, c_int] + [c_double] * 6 + [c_int, _PI],
+    "fteik_analytic_setSources64f": [c_int, _PD, _PD, _PD, _PI],
+    "fteik_analytic_setReceivers64f": [c_int, _PD, _PD, _PD, _PI],
+    "fteik_analytic_setConstantVelocity64f": [c_double, _PI],
+    "fteik_analytic_setLinearVelocityGradient64f": [c_double, c_double, _PI],
+    "fteik_analytic_solveSourceConstantVelocity64f": [c_int, _PI],
+    "fteik_analytic_solveSourceLinearVelocityGradient64f": [c_int, _PI],
+    "fteik_analytic_getTravelTimeField64f": [c_int, c_int, _PD, _PI],
+    "fteik_analytic_getTravelTimesConstantVel64f": [c_int, _PD, _PI],
+    "fteik_analytic_getTravelTimesGradientVel64f": [c_int, _PD, _PI],
+    "fteik_analytic_free": [],
+    # locate.F90
+    "locate_initialize": [c_int, c_int, c_int, _PI],
+    "locate_finalize": [],
+    "locate_setTravelTimeField64f": [c_int, c_int, _PD, _PI],
+    "locate_setTravelTimeField32f": [c_int, c_int, _PF, _PI],
+    "locate_setObservation64f": [c_int, c_int, c_bool, c_double, _PI, _PD, _PD, _PI],
+    "locate_setObservation64fC": [c_int, c_int, c_bool, c_double, _PI, _PD, _PD, _PI],
+    "locate_locateEvent": [c_int, _PI, _PD, _PD],
+    # additions
+    "fteik_b200_version": [],
+    "fteik_b200_device": [],
+    "fteik_b200_stream": [],
+    "fteik_b200_solver3d_setPrecision": [c_int, _PI],
+    "fteik_b200_solver3d_getSolveInfo": [_PD, _PI, _PI],
+    "fteik_b200_batch3d_initialize": [c_int, _PI, _PI, _PI, _PD, _PD, _PD, c_int, c_double, c_double,
+                                      c_int, c_int, _PI],
+    "fteik_b200_batch3d_setVelocityModel64f": [c_int, c_int, _PD, _PI],
+    "fteik_b200_batch3d_setSources64f": [c_int, c_int, _PD, _PD, _PD, _PI],
+    "fteik_b200_batch3d_setReceivers64f": [c_int, c_int, _PD, _PD, _PD, _PI],
+    "fteik_b200_batch3d_solve": [_PI],
+    "fteik_b200_batch3d_solveAsync": [],
+    "fteik_b200_batch3d_getTravelTimeField64f": [c_int, c_int, c_int, c_int, _PD, _PI],
+    "fteik_b200_batch3d_getTravelTimeFields32f": [c_int, c_longlong, _PF, _PI],
+    "fteik_b200_batch3d_getTravelTimes64f": [c_int, c_int, _PD, _PI],
+    "fteik_b200_batch3d_getSolveInfo": [c_int, c_int, _PD, _PI, _PI],
+    "fteik_b200_batch3d_exportToLocator": [c_int, c_int, _PI],
+    "fteik_b200_batch3d_finalize": [],
+    "fteik_b200_locate_locateEvents": [c_int, _PI, _PI, _PD, _PD, _PI],
+    "fteik_h5io_initializeF": [ctypes.c_char_p],
+    "fteik_h5io_finalizeF": [],
+    "fteik_h5io_writeLevelSchedulesF": [],
+    "fteik_h5io_writeVelocityModelF": [ctypes.c_char_p],
+    "fteik_h5io_writeTravelTimesF": [ctypes.c_char_p],
+}
+_RESTYPES = {
+    "fteik_model_grid2indexF": c_int,
+    "fteik_model_grid2index": c_int,
+    "fteik_model_velGrid2indexF": c_int,
+    "fteik_b200_version": ctypes.c_char_p,
+    "fteik_b200_device": c_int,
+    "fteik_b200_stream": ctypes.c_void_p,
+    "fteik_b200_batch3d_solveAsync": c_int,
+    "fteik_h5io_initializeF": c_int,
+    "fteik_h5io_finalizeF": c_int,
+    "fteik_h5io_writeLevelSchedulesF": c_int,
+    "fteik_h5io_writeVelocityModelF": c_int,
+    "fteik_h5io_writeTravelTimesF": c_int,
+}
+
+
+def build(quiet=True):
+    """Compile libfteik_shared.so for sm_100a in-tree (nvcc + gcc)."""
+    out = subprocess.DEVNULL if quiet else None
+    subprocess.check_call(["make", "-C", CSRC, "-j8"], stdout=out)
+    return LIB_PATH
+
+
+def lib():
+    """The loaded product library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libfteik_shared.so is not built; run fteik_b200.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, args in _SIGS.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = _RESTYPES.get(name, None)
+    _lib = L
+    return L
+
+
+def exported_symbols():
+    return sorted(_SIGS)
+
+
+def _d(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(_PD)
+
+
+def _i(a):
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data_as(_PI)
+
+
+class FteikError(RuntimeError):
+    pass
+
+
+def _check(ierr, what):
+    if ierr.value != 0:
+        raise FteikError("%s failed (ierr=%d)" % (what, ierr.value))
+
+
+class fteik3d:
+    """Mirror of the reference's python/fteik3d.py class over this library."""
+
+    def __init__(self):
+        self.lib = lib()
+        self.nx = self.ny = self.nz = 0
+        self.nsrc = 0
+        self.nrec = 0
+
+    def free(self):
+        self.lib.fteik_solver3d_free()
+
+    def initialize(self, nx, ny, nz, dx, dy, dz, x0=0.0, y0=0.0, z0=0.0,
+                   nsweep=2, eps=5.0, convTol=0.0, verbose=0, precision=4):
+        ierr = c_int(1)
+        self.lib.fteik_b200_solver3d_setPrecision(int(precision), byref(ierr))
+        _check(ierr, "setPrecision")
+        self.lib.fteik_solver3d_initialize(nz, nx, ny, z0, x0, y0, dz, dx, dy, nsweep,
+                                           float(eps), float(convTol), verbose, byref(ierr))
+        _check(ierr, "fteik_solver3d_initialize")
+        self.nx, self.ny, self.nz = nx, ny, nz
+        return 0
+
+    def setCellSlownessNatural(self, vel_natural):
+        """Cell velocities in the solver's natural order (z fastest)."""
+        v, p = _d(np.ravel(vel_natural))
+        ierr = c_int(1)
+        self.lib.fteik_solver3d_setCellVelocityModel64f(v.size, FTEIK_NATURAL_ORDERING, p, byref(ierr))
+        _check(ierr, "setCellVelocityModel64f")
+
+    def setVelocityModel(self, vel):
+        """[nz-1, ny-1, nx-1] cell or [nz, ny, nx] nodal velocities (python/fteik3d.py)."""
+        vel = np.asarray(vel)
+        v, p = _d(np.reshape(vel, vel.size, order="F"))
+        ierr = c_int(1)
+        if v.size == (self.nx - 1) * (self.ny - 1) * (self.nz - 1):
+            self.lib.fteik_solver3d_setCellVelocityModel64f(v.size, FTEIK_ZYX_ORDERING, p, byref(ierr))
+        else:
+            self.lib.fteik_solver3d_setNodalVelocityModel64f(v.size, FTEIK_ZYX_ORDERING, p, byref(ierr))
+        _check(ierr, "setVelocityModel")
+        return 0
+
+    def setSources(self, xsrc, ysrc, zsrc):
+        x, px = _d(np.atleast_1d(xsrc))
+        y, py = _d(np.atleast_1d(ysrc))
+        z, pz = _d(np.atleast_1d(zsrc))
+        ierr = c_int(1)
+        self.lib.fteik_solver3d_setSources64f(x.size, pz, px, py, byref(ierr))
+        _check(ierr, "setSources64f")
+        self.nsrc = x.size
+        return 0
+
+    def setReceivers(self, xrec, yrec, zrec):
+        x, px = _d(np.atleast_1d(xrec))
+        y, py = _d(np.atleast_1d(yrec))
+        z, pz = _d(np.atleast_1d(zrec))
+        ierr = c_int(1)
+        self.lib.fteik_solver3d_setReceivers64f(x.size, pz, px, py, byref(ierr))
+        _check(ierr, "setReceivers64f")
+        self.nrec = x.size
+        return 0
+
+    def solveSourceLSM(self, isrc):
+        ierr = c_int(1)
+        self.lib.fteik_solver3d_solveSourceLSM(int(isrc), byref(ierr))
+        _check(ierr, "solveSourceLSM")
+
+    def solveLSM(self):
+        errorAll = 0
+        for i in range(self.nsrc):
+            ierr = c_int(1)
+            self.lib.fteik_solver3d_solveSourceLSM(i + 1, byref(ierr))
+            errorAll += int(ierr.value != 0)
+        return errorAll
+
+    def getTravelTimeField(self, wantCell=False, order=FTEIK_NATURAL_ORDERING):
+        """Natural-order (z fastest) FP64 field as a flat array."""
+        ierr = c_int(1)
+        if wantCell:
+            n = (self.nx - 1) * (self.ny - 1) * (self.nz - 1)
+            out = np.zeros(n)
+            self.lib.fteik_solver3d_getTravelTimeFieldCell64f(n, order, out.ctypes.data_as(_PD), byref(ierr))
+        else:
+            n = self.nx * self.ny * self.nz
+            out = np.zeros(n)
+            self.lib.fteik_solver3d_getTravelTimeField64f(n, order, out.ctypes.data_as(_PD), byref(ierr))
+        _check(ierr, "getTravelTimeField")
+        return out
+
+    def getTravelTimes(self):
+        out = np.zeros(max(self.nrec, 1))
+        ierr = c_int(1)
+        self.lib.fteik_solver3d_getTravelTimes64f(self.nrec, out.ctypes.data_as(_PD), byref(ierr))
+        _check(ierr, "getTravelTimes64f")
+        return out[: self.nrec]
+
+    def getSolveInfo(self):
+        r, n, ierr = c_double(), c_int(), c_int(1)
+        self.lib.fteik_b200_solver3d_getSolveInfo(byref(r), byref(n), byref(ierr))
+        return r.value, n.value
+
+
+class fteik2d:
+    """Mirror of the reference's python/fteik2d.py class over this library."""
+
+    def __init__(self):
+        self.lib = lib()
+        self.nx = self.nz = 0
+        self.nsrc = self.nrec = 0
+
+    def free(self):
+        self.lib.fteik_solver2d_free()
+
+    def initialize(self, nx, nz, dx, dz, x0=0.0, z0=0.0, nsweep=2, eps=5.0,
+                   convTol=0.0, verbose=0):
+        ierr = c_int(1)
+        self.lib.fteik_solver2d_initialize(nz, nx, z0, x0, dz, dx, nsweep, float(eps),
+                                           float(convTol), verbose, byref(ierr))
+        _check(ierr, "fteik_solver2d_initialize")
+        self.nx, self.nz = nx, nz
+        return 0
+
+    def setCellVelocityNatural(self, vel_natural):
+        v, p = _d(np.ravel(vel_natural))
+        ierr = c_int(1)
+        self.lib.fteik_solver2d_setCellVelocityModel64f(v.size, FTEIK_NATURAL_ORDERING, p, byref(ierr))
+        _check(ierr, "setCellVelocityModel64f")
+
+    def setSources(self, xsrc, zsrc):
+        x, px = _d(np.atleast_1d(xsrc))
+        z, pz = _d(np.atleast_1d(zsrc))
+        ierr = c_int(1)
+        self.lib.fteik_solver2d_setSources64f(x.size, pz, px, byref(ierr))
+        _check(ierr, "setSources64f")
+        self.nsrc = x.size
+
+    def setReceivers(self, xrec, zrec):
+        x, px = _d(np.atleast_1d(xrec))
+        z, pz = _d(np.atleast_1d(zrec))
+        ierr = c_int(1)
+        self.lib.fteik_solver2d_setReceivers64f(x.size, pz, px, byref(ierr))
+        _check(ierr, "setReceivers64f")
+        self.nrec = x.size
+
+    def solveSourceLSM(self, isrc):
+        ierr = c_int(1)
+        self.lib.fteik_solver2d_solveSourceLSM(int(isrc), byref(ierr))
+        _check(ierr, "solveSourceLSM")
+
+    def solveSourceFSM(self, isrc):
+        ierr = c_int(1)
+        self.lib.fteik_solver2d_solveSourceFSM(int(isrc), byref(ierr))
+        _check(ierr, "solveSourceFSM")
+
+    def solveLSM(self):
+        ierr = c_int(1)
+        self.lib.fteik_solver2d_solveLSM(byref(ierr))
+        _check(ierr, "solveLSM")
+
+    def getTravelTimeField(self, order=FTEIK_NATURAL_ORDERING):
+        n = self.nx * self.nz
+        out = np.zeros(n)
+        ierr = c_int(1)
+        self.lib.fteik_solver2d_getTravelTimeField64f(n, order, out.ctypes.data_as(_PD), byref(ierr))
+        _check(ierr, "getTravelTimeField64f")
+        return out
+
+    def getTravelTimes(self):
+        out = np.zeros(max(self.nrec * self.nsrc, 1))
+        ierr = c_int(1)
+        self.lib.fteik_solver2d_getTravelTimes64f(self.nrec, out.ctypes.data_as(_PD), byref(ierr))
+        _check(ierr, "getTravelTimes64f")
+        return out[: self.nrec * self.nsrc].reshape(self.nsrc, self.nrec)
+
+
+class Locator:
+    """locate.F90's C ABI (locate_initialize ... locate_locateEvent)."""
+
+    def __init__(self, nEvents, ntf, ngrd):
+        self.lib = lib()
+        ierr = c_int(1)
+        self.lib.locate_initialize(nEvents, ntf, ngrd, byref(ierr))
+        _check(ierr, "locate_initialize")
+        self.nev, self.ntf, self.ngrd = nEvents, ntf, ngrd
+
+    def finalize(self):
+        self.lib.locate_finalize()
+
+    def setTravelTimeField64f(self, itf, tt):
+        t, p = _d(tt)
+        ierr = c_int(1)
+        self.lib.locate_setTravelTimeField64f(t.size, int(itf), p, byref(ierr))
+        _check(ierr, "locate_setTravelTimeField64f")
+
+    def setTravelTimeField32f(self, itf, tt):
+        t = np.ascontiguousarray(tt, dtype=np.float32)
+        ierr = c_int(1)
+        self.lib.locate_setTravelTimeField32f(t.size, int(itf), t.ctypes.data_as(_PF), byref(ierr))
+        _check(ierr, "locate_setTravelTimeField32f")
+
+    def setObservation(self, ev, obs2tf, picks, wts, lhaveOT=False, t0=0.0):
+        o, po = _i(obs2tf)
+        p_, pp = _d(picks)
+        w, pw = _d(wts)
+        ierr = c_int(1)
+        self.lib.locate_setObservation64f(int(ev), o.size, bool(lhaveOT), float(t0), po, pp, pw,
+                                          byref(ierr))
+        _check(ierr, "locate_setObservation64f")
+
+    def locateEvent(self, ev):
+        oi, t0, ob = c_int(), c_double(), c_double()
+        self.lib.locate_locateEvent(int(ev), byref(oi), byref(t0), byref(ob))
+        return oi.value, t0.value, ob.value
+
+    def locateEvents(self, events):
+        ev, pev = _i(events)
+        n = ev.size
+        oi = np.zeros(n, np.int32)
+        t0 = np.zeros(n)
+        ob = np.zeros(n)
+        ierr = c_int(1)
+        self.lib.fteik_b200_locate_locateEvents(n, pev, oi.ctypes.data_as(_PI), t0.ctypes.data_as(_PD),
+                                                ob.ctypes.data_as(_PD), byref(ierr))
+        _check(ierr, "fteik_b200_locate_locateEvents")
+        return oi, t0, ob
+
+
+class Batch3D:
+    """Batched multi-source, multi-grid 3D solve (fteik_b200_batch3d_*)."""
+
+    def __init__(self, grids, nsweep=2, eps=5.0, convTol=-1.0, maxPass=0, precision=4):
+        """grids: list of (nz, nx, ny, dz, dx, dy)."""
+        self.lib = lib()
+        g = np.asarray(grids, dtype=np.float64)
+        nz, pnz = _i(g[:, 0])
+        nx, pnx = _i(g[:, 1])
+        ny, pny = _i(g[:, 2])
+        dz, pdz = _d(g[:, 3])
+        dx, pdx = _d(g[:, 4])
+        dy, pdy = _d(g[:, 5])
+        ierr = c_int(1)
+        self.lib.fteik_b200_batch3d_initialize(len(grids), pnz, pnx, pny, pdz, pdx, pdy, nsweep,
+                                               float(eps), float(convTol), maxPass, precision,
+                                               byref(ierr))
+        _check(ierr, "fteik_b200_batch3d_initialize")
+        self.grids = [tuple(int(v) for v in r[:3]) for r in g]
+        self.nsrc = [0] * len(grids)
+        self.precision = precision
+
+    def finalize(self):
+        self.lib.fteik_b200_batch3d_finalize()
+
+    def setVelocityModel(self, igrid, vel_natural):
+        v, p = _d(np.ravel(vel_natural))
+        ierr = c_int(1)
+        self.lib.fteik_b200_batch3d_setVelocityModel64f(igrid, v.size, p, byref(ierr))
+        _check(ierr, "batch3d_setVelocityModel64f")
+
+    def setSources(self, igrid, zsrc, xsrc, ysrc):
+        z, pz = _d(zsrc)
+        x, px = _d(xsrc)
+        y, py = _d(ysrc)
+        ierr = c_int(1)
+        self.lib.fteik_b200_batch3d_setSources64f(igrid, z.size, pz, px, py, byref(ierr))
+        _check(ierr, "batch3d_setSources64f")
+        self.nsrc[igrid - 1] = z.size
+
+    def setReceivers(self, igrid, zrec, xrec, yrec):
+        z, pz = _d(zrec)
+        x, px = _d(xrec)
+        y, py = _d(yrec)
+        ierr = c_int(1)
+        self.lib.fteik_b200_batch3d_setReceivers64f(igrid, z.size, pz, px, py, byref(ierr))
+        _check(ierr, "batch3d_setReceivers64f")
+        self.nrec = z.size
+
+    def solve(self):
+        ierr = c_int(1)
+        self.lib.fteik_b200_batch3d_solve(byref(ierr))
+        _check(ierr, "batch3d_solve")
+
+    def solveAsync(self):
+        return self.lib.fteik_b200_batch3d_solveAsync()
+
+    def field(self, igrid, isrc, order=FTEIK_NATURAL_ORDERING):
+        nz, nx, ny = self.grids[igrid - 1]
+        out = np.zeros(nz * nx * ny)
+        ierr = c_int(1)
+        self.lib.fteik_b200_batch3d_getTravelTimeField64f(igrid, isrc, out.size, order,
+                                                          out.ctypes.data_as(_PD), byref(ierr))
+        _check(ierr, "batch3d_getTravelTimeField64f")
+        return out
+
+    def fields32(self, igrid, out=None):
+        nz, nx, ny = self.grids[igrid - 1]
+        n = self.nsrc[igrid - 1] * nz * nx * ny
+        if out is None:
+            out = np.empty(n, np.float32)
+        ierr = c_int(1)
+        self.lib.fteik_b200_batch3d_getTravelTimeFields32f(igrid, n, out.ctypes.data_as(_PF), byref(ierr))
+        _check(ierr, "batch3d_getTravelTimeFields32f")
+        return out
+
+    def travelTimes(self, igrid):
+        n = self.nsrc[igrid - 1] * self.nrec
+        out = np.zeros(n)
+        ierr = c_int(1)
+        self.lib.fteik_b200_batch3d_getTravelTimes64f(igrid, n, out.ctypes.data_as(_PD), byref(ierr))
+        _check(ierr, "batch3d_getTravelTimes64f")
+        return out.reshape(self.nsrc[igrid - 1], self.nrec)
+
+    def solveInfo(self, igrid, isrc):
+        r, n, ierr = c_double(), c_int(), c_int(1)
+        self.lib.fteik_b200_batch3d_getSolveInfo(igrid, isrc, byref(r), byref(n), byref(ierr))
+        _check(ierr, "batch3d_getSolveInfo")
+        return r.value, n.value
+
+    def exportToLocator(self, igrid, itf0=1):
+        ierr = c_int(1)
+        self.lib.fteik_b200_batch3d_exportToLocator(igrid, itf0, byref(ierr))
+        _check(ierr, "batch3d_exportToLocator")

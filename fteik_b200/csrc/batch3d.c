@@ -1,0 +1,430 @@
+/*
+ * batch3d.c -- batched multi-source, multi-grid 3D solve (no reference
+ * counterpart; the reference solves one source at a time,
+ * solver3D.F90:1156-1243, and callers loop over sources,
+ * python/fteik3d.py:258-263).
+ *
+ * Every (grid, source) pair becomes one work item; one kernel launch solves
+ * them all, one CTA per item, largest grids first.  The launch is captured
+ * once into a CUDA graph and replayed while the work list is unchanged.
+ * Fields stay on the device until exported.
+ */
+#include "host_common.h"
+#include "fteik_b200.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+    int nz, nx, ny, ngrd, ncell, zp, zcp;
+    double dz, dx, dy;
+    double *slow;           /* host FP64 natural */
+    void *slow_dev;         /* device padded, batch precision */
+    bool have_model;
+    int nsrc;
+    int *zsi, *xsi, *ysi;
+    double *zsa, *xsa, *ysa;
+    void *fields;           /* device [nsrc][ny][nx][zp] */
+    int nrec;
+    int *ri_dev;
+    double *rd_dev;
+    int work0;              /* index of this grid's first work item */
+} bgrid_t;
+
+static struct {
+    bool init, solved;
+    int ngrid, precision, nsweep, max_pass;
+    double eps, conv_tol;
+    bgrid_t *g;
+    fk_grid3d_t *grids_dev;
+    fk_work3d_t *work_dev;
+    fk_result3d_t *res_dev;
+    fk_result3d_t *res_host;
+    int nwork, max_nx, max_nz;
+    int *work_order;        /* work item -> (grid, src) packed as grid<<20|src */
+    cudaGraphExec_t graph;
+    bool graph_ok;
+    double *export_buf;
+    size_t export_cap;
+} SB;
+
+static void free_grid(bgrid_t *g)
+{
+    free(g->slow); free(g->zsi); free(g->xsi); free(g->ysi);
+    free(g->zsa); free(g->xsa); free(g->ysa);
+    fk_dfree(g->slow_dev); fk_dfree(g->fields); fk_dfree(g->ri_dev); fk_dfree(g->rd_dev);
+    memset(g, 0, sizeof(*g));
+}
+
+static void invalidate(void)
+{
+    if (SB.graph_ok) cudaGraphExecDestroy(SB.graph);
+    SB.graph_ok = false;
+    SB.solved = false;
+}
+
+void fteik_b200_batch3d_finalize(void)
+{
+    invalidate();
+    for (int i = 0; i < SB.ngrid; i++) free_grid(&SB.g[i]);
+    free(SB.g);
+    fk_dfree(SB.grids_dev); fk_dfree(SB.work_dev); fk_dfree(SB.res_dev); fk_dfree(SB.export_buf);
+    free(SB.res_host); free(SB.work_order);
+    memset(&SB, 0, sizeof(SB));
+}
+
+void fteik_b200_batch3d_initialize(int ngrid, const int nz[], const int nx[], const int ny[],
+                                   const double dz[], const double dx[], const double dy[],
+                                   int nsweep, double eps, double convTol, int maxPass,
+                                   int precision, int *ierr)
+{
+    *ierr = 0;
+    fteik_b200_batch3d_finalize();
+    if (ngrid < 1) { FK_ERR("fteik_b200_batch3d_initialize: ngrid must be positive"); *ierr = 1; return; }
+    if (precision != 4 && precision != 8) { FK_ERR("fteik_b200_batch3d_initialize: precision must be 4 or 8"); *ierr = 1; return; }
+    if (nsweep < 0) { FK_ERR("fteik_b200_batch3d_initialize: nsweep must be non-negative"); *ierr = 1; return; }
+    if (fk_dev_ready("fteik_b200_batch3d_initialize")) { *ierr = 1; return; }
+    SB.g = (bgrid_t *)calloc((size_t)ngrid, sizeof(bgrid_t));
+    SB.ngrid = ngrid;
+    for (int i = 0; i < ngrid; i++) {
+        bgrid_t *g = &SB.g[i];
+        if (nz[i] < 3 || nx[i] < 3 || ny[i] < 3 || dz[i] <= 0 || dx[i] <= 0 || dy[i] <= 0) {
+            FK_ERR("fteik_b200_batch3d_initialize: grid %d needs n >= 3 and h > 0", i + 1);
+            *ierr = 1;
+            return;
+        }
+        if (nx[i] > 1024) {
+            FK_ERR("fteik_b200_batch3d_initialize: grid %d has nx=%d > 1024", i + 1, nx[i]);
+            *ierr = 1;
+            return;
+        }
+        if ((int)eps > nz[i] || (int)eps > nx[i] || (int)eps > ny[i]) {
+            FK_ERR("fteik_b200_batch3d_initialize: eps=%d bigger than grid %d", (int)eps, i + 1);
+            *ierr = 1;
+            return;
+        }
+        g->nz = nz[i]; g->nx = nx[i]; g->ny = ny[i];
+        g->ngrd = nz[i] * nx[i] * ny[i];
+        g->ncell = (nz[i] - 1) * (nx[i] - 1) * (ny[i] - 1);
+        g->zp = FK_PITCH(nz[i]); g->zcp = FK_PITCH(nz[i] - 1);
+        g->dz = dz[i]; g->dx = dx[i]; g->dy = dy[i];
+        g->slow = (double *)calloc((size_t)g->ncell, sizeof(double));
+    }
+    SB.precision = precision;
+    SB.nsweep = nsweep;
+    SB.eps = eps;
+    SB.conv_tol = convTol;
+    SB.max_pass = maxPass;
+    SB.init = true;
+}
+
+static bgrid_t *grid_of(int igrid, const char *who)
+{
+    if (!SB.init) { FK_ERR("%s: batch not initialized", who); return NULL; }
+    if (igrid < 1 || igrid > SB.ngrid) { FK_ERR("%s: grid %d out of range [1,%d]", who, igrid, SB.ngrid); return NULL; }
+    return &SB.g[igrid - 1];
+}
+
+void fteik_b200_batch3d_setVelocityModel64f(int igrid, int ncell, const double vel[], int *ierr)
+{
+    const char *who = "fteik_b200_batch3d_setVelocityModel64f";
+    *ierr = 1;
+    bgrid_t *g = grid_of(igrid, who);
+    if (!g) return;
+    if (ncell != g->ncell) { FK_ERR("%s: ncell=%d, grid has %d cells", who, ncell, g->ncell); return; }
+    for (int i = 0; i < ncell; i++)
+        if (!(vel[i] > 0.0)) { FK_ERR("%s: velocities must be positive", who); return; }
+    for (int i = 0; i < ncell; i++) g->slow[i] = 1.0 / vel[i];
+    const size_t nelem = (size_t)g->zcp * (g->nx - 1) * (g->ny - 1);
+    if (!g->slow_dev) g->slow_dev = fk_dalloc(nelem * (size_t)SB.precision, who);
+    double *tmp = (double *)fk_dalloc(sizeof(double) * (size_t)ncell, who);
+    if (!g->slow_dev || !tmp) { fk_dfree(tmp); return; }
+    cudaStream_t s = fk_stream();
+    int e = (int)cudaMemsetAsync(g->slow_dev, 0, nelem * (size_t)SB.precision, s);
+    if (!e) e = (int)cudaMemcpyAsync(tmp, g->slow, sizeof(double) * (size_t)ncell, cudaMemcpyHostToDevice, s);
+    if (!e) e = fk_pack_slowness(SB.precision, 1, g->nz, g->nx, g->ny, g->zcp, tmp, g->slow_dev, s);
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    fk_dfree(tmp);
+    if (fk_check(e, who)) return;
+    g->have_model = true;
+    SB.solved = false;
+    *ierr = 0;
+}
+
+void fteik_b200_batch3d_setSources64f(int igrid, int nsrc, const double zsrc[],
+                                      const double xsrc[], const double ysrc[], int *ierr)
+{
+    const char *who = "fteik_b200_batch3d_setSources64f";
+    *ierr = 1;
+    bgrid_t *g = grid_of(igrid, who);
+    if (!g) return;
+    if (nsrc < 1) { FK_ERR("%s: No sources", who); return; }
+    free(g->zsi); free(g->xsi); free(g->ysi); free(g->zsa); free(g->xsa); free(g->ysa);
+    fk_dfree(g->fields); g->fields = NULL;
+    g->nsrc = 0;
+    g->zsi = (int *)malloc(sizeof(int) * (size_t)nsrc);
+    g->xsi = (int *)malloc(sizeof(int) * (size_t)nsrc);
+    g->ysi = (int *)malloc(sizeof(int) * (size_t)nsrc);
+    g->zsa = (double *)malloc(sizeof(double) * (size_t)nsrc);
+    g->xsa = (double *)malloc(sizeof(double) * (size_t)nsrc);
+    g->ysa = (double *)malloc(sizeof(double) * (size_t)nsrc);
+    for (int i = 0; i < nsrc; i++)
+        if (fk_snap_source(true, g->nz, g->nx, g->ny, 0.0, 0.0, 0.0, g->dz, g->dx, g->dy, zsrc[i],
+                           xsrc[i], ysrc[i], i + 1, &g->zsi[i], &g->xsi[i], &g->ysi[i], &g->zsa[i],
+                           &g->xsa[i], &g->ysa[i]))
+            return;
+    const size_t fbytes = (size_t)g->zp * g->nx * g->ny * (size_t)SB.precision;
+    g->fields = fk_dalloc(fbytes * (size_t)nsrc, who);
+    if (!g->fields) return;
+    g->nsrc = nsrc;
+    invalidate();
+    *ierr = 0;
+}
+
+void fteik_b200_batch3d_setReceivers64f(int igrid, int nrec, const double zrec[],
+                                        const double xrec[], const double yrec[], int *ierr)
+{
+    const char *who = "fteik_b200_batch3d_setReceivers64f";
+    *ierr = 1;
+    bgrid_t *g = grid_of(igrid, who);
+    if (!g) return;
+    if (nrec < 1) { FK_ERR("%s: No receivers", who); return; }
+    int *ri = (int *)malloc(3 * sizeof(int) * (size_t)nrec);
+    double *rd = (double *)malloc(3 * sizeof(double) * (size_t)nrec);
+    int bad = fk_receiver_geometry(true, g->nz, g->nx, g->ny, 0.0, 0.0, 0.0, g->dz, g->dx, g->dy,
+                                   nrec, zrec, xrec, yrec, ri, rd);
+    fk_dfree(g->ri_dev); fk_dfree(g->rd_dev);
+    g->ri_dev = (int *)fk_dalloc(3 * sizeof(int) * (size_t)nrec, who);
+    g->rd_dev = (double *)fk_dalloc(3 * sizeof(double) * (size_t)nrec, who);
+    int e = 1;
+    if (g->ri_dev && g->rd_dev) {
+        e = (int)cudaMemcpy(g->ri_dev, ri, 3 * sizeof(int) * (size_t)nrec, cudaMemcpyHostToDevice);
+        if (!e) e = (int)cudaMemcpy(g->rd_dev, rd, 3 * sizeof(double) * (size_t)nrec, cudaMemcpyHostToDevice);
+        e = fk_check(e, who);
+    }
+    free(ri); free(rd);
+    g->nrec = e ? 0 : nrec;
+    *ierr = (e || bad) ? 1 : 0;
+}
+
+static int cmp_work(const void *a, const void *b)
+{
+    /* largest grids (most CTA steps) first */
+    const int ga = (*(const int *)a) >> 20, gb = (*(const int *)b) >> 20;
+    const long wa = (long)SB.g[ga].nz * SB.g[ga].ny * ((SB.g[ga].nx + 31) / 32);
+    const long wb = (long)SB.g[gb].nz * SB.g[gb].ny * ((SB.g[gb].nx + 31) / 32);
+    if (wa != wb) return wa < wb ? 1 : -1;
+    return (*(const int *)a) - (*(const int *)b);
+}
+
+static int build_work(const char *who)
+{
+    int nwork = 0, max_nx = 0, max_nz = 0;
+    for (int i = 0; i < SB.ngrid; i++) {
+        bgrid_t *g = &SB.g[i];
+        if (!g->have_model) { FK_ERR("%s: grid %d has no velocity model", who, i + 1); return 1; }
+        if (g->nsrc < 1) continue;
+        if (g->nsrc >= (1 << 20)) { FK_ERR("%s: too many sources", who); return 1; }
+        nwork += g->nsrc;
+        if (g->nx > max_nx) max_nx = g->nx;
+        if (g->nz > max_nz) max_nz = g->nz;
+    }
+    if (nwork == 0) { FK_ERR("%s: no sources", who); return 1; }
+    fk_dfree(SB.grids_dev); fk_dfree(SB.work_dev); fk_dfree(SB.res_dev);
+    free(SB.res_host); free(SB.work_order);
+    SB.grids_dev = (fk_grid3d_t *)fk_dalloc(sizeof(fk_grid3d_t) * (size_t)SB.ngrid, who);
+    SB.work_dev = (fk_work3d_t *)fk_dalloc(sizeof(fk_work3d_t) * (size_t)nwork, who);
+    SB.res_dev = (fk_result3d_t *)fk_dalloc(sizeof(fk_result3d_t) * (size_t)nwork, who);
+    SB.res_host = (fk_result3d_t *)calloc((size_t)nwork, sizeof(fk_result3d_t));
+    SB.work_order = (int *)malloc(sizeof(int) * (size_t)nwork);
+    if (!SB.grids_dev || !SB.work_dev || !SB.res_dev) return 1;
+    fk_grid3d_t *gh = (fk_grid3d_t *)malloc(sizeof(fk_grid3d_t) * (size_t)SB.ngrid);
+    fk_work3d_t *wh = (fk_work3d_t *)malloc(sizeof(fk_work3d_t) * (size_t)nwork);
+    int k = 0;
+    for (int i = 0; i < SB.ngrid; i++) {
+        bgrid_t *g = &SB.g[i];
+        gh[i].nz = g->nz; gh[i].nx = g->nx; gh[i].ny = g->ny;
+        gh[i].zp = g->zp; gh[i].zcp = g->zcp;
+        gh[i].dz = g->dz; gh[i].dx = g->dx; gh[i].dy = g->dy;
+        gh[i].slow = g->slow_dev;
+        for (int s = 0; s < g->nsrc; s++) SB.work_order[k++] = (i << 20) | s;
+    }
+    qsort(SB.work_order, (size_t)nwork, sizeof(int), cmp_work);
+    for (int w = 0; w < nwork; w++) {
+        const int i = SB.work_order[w] >> 20, s = SB.work_order[w] & ((1 << 20) - 1);
+        bgrid_t *g = &SB.g[i];
+        const size_t fbytes = (size_t)g->zp * g->nx * g->ny * (size_t)SB.precision;
+        wh[w].grid = i;
+        wh[w].zsi = g->zsi[s]; wh[w].xsi = g->xsi[s]; wh[w].ysi = g->ysi[s];
+        wh[w].zsa = g->zsa[s]; wh[w].xsa = g->xsa[s]; wh[w].ysa = g->ysa[s];
+        wh[w].szero = g->slow[((long)(g->ysi[s] - 1) * (g->nx - 1) + (g->xsi[s] - 1)) * (g->nz - 1) +
+                              (g->zsi[s] - 1)];
+        wh[w].tt = (char *)g->fields + fbytes * (size_t)s;
+    }
+    int e = (int)cudaMemcpy(SB.grids_dev, gh, sizeof(fk_grid3d_t) * (size_t)SB.ngrid, cudaMemcpyHostToDevice);
+    if (!e) e = (int)cudaMemcpy(SB.work_dev, wh, sizeof(fk_work3d_t) * (size_t)nwork, cudaMemcpyHostToDevice);
+    free(gh);
+    free(wh);
+    SB.nwork = nwork;
+    SB.max_nx = max_nx;
+    SB.max_nz = max_nz;
+    return fk_check(e, who);
+}
+
+void fteik_b200_batch3d_solve(int *ierr)
+{
+    const char *who = "fteik_b200_batch3d_solve";
+    *ierr = 1;
+    if (!SB.init) { FK_ERR("%s: batch not initialized", who); return; }
+    cudaStream_t s = fk_stream();
+    if (!SB.graph_ok) {
+        if (build_work(who)) return;
+        /* warm the kernel attributes outside capture, then capture */
+        cudaGraph_t graph;
+        int e = fk3d_prepare(SB.precision, SB.max_nx, SB.max_nz);
+        if (!e) e = (int)cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (!e) {
+            int le = fk3d_solve(SB.precision, SB.grids_dev, SB.work_dev, SB.res_dev, SB.nwork,
+                                SB.max_nx, SB.max_nz, SB.eps, SB.nsweep, SB.conv_tol, SB.max_pass, s);
+            e = (int)cudaStreamEndCapture(s, &graph);
+            if (!e) e = le;
+        }
+        if (!e) e = (int)cudaGraphInstantiate(&SB.graph, graph, 0);
+        if (!e) cudaGraphDestroy(graph);
+        if (fk_check(e, who)) return;
+        SB.graph_ok = true;
+    }
+    int e = (int)cudaGraphLaunch(SB.graph, s);
+    if (!e) e = (int)cudaMemcpyAsync(SB.res_host, SB.res_dev, sizeof(fk_result3d_t) * (size_t)SB.nwork,
+                                    cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    if (fk_check(e, who)) return;
+    for (int w = 0; w < SB.nwork; w++)
+        if (SB.res_host[w].status) { FK_ERR("%s: work item %d failed", who, w); return; }
+    SB.solved = true;
+    *ierr = 0;
+}
+
+/* Launch the solve without waiting (the caller synchronises); used for
+ * timing back-to-back solves. */
+int fteik_b200_batch3d_solveAsync(void)
+{
+    if (!SB.graph_ok) return 1;
+    return (int)cudaGraphLaunch(SB.graph, fk_stream());
+}
+
+static const fk_result3d_t *result_of(int igrid, int isrc, const char *who)
+{
+    bgrid_t *g = grid_of(igrid, who);
+    if (!g) return NULL;
+    if (!SB.solved) { FK_ERR("%s: not solved", who); return NULL; }
+    if (isrc < 1 || isrc > g->nsrc) { FK_ERR("%s: source %d out of range", who, isrc); return NULL; }
+    for (int w = 0; w < SB.nwork; w++)
+        if (SB.work_order[w] == (((igrid - 1) << 20) | (isrc - 1))) return &SB.res_host[w];
+    return NULL;
+}
+
+void fteik_b200_batch3d_getSolveInfo(int igrid, int isrc, double *residual, int *npass, int *ierr)
+{
+    const fk_result3d_t *r = result_of(igrid, isrc, "fteik_b200_batch3d_getSolveInfo");
+    *ierr = r ? 0 : 1;
+    *residual = r ? r->residual : 0.0;
+    *npass = r ? r->npass : 0;
+}
+
+static int ensure_export(size_t n)
+{
+    if (SB.export_buf && SB.export_cap >= n) return 0;
+    fk_dfree(SB.export_buf);
+    SB.export_buf = (double *)fk_dalloc(sizeof(double) * n, "fteik_b200_batch3d");
+    SB.export_cap = SB.export_buf ? n : 0;
+    return SB.export_buf == NULL;
+}
+
+void fteik_b200_batch3d_getTravelTimeField64f(int igrid, int isrc, int ngrd, int order, double tt[],
+                                              int *ierr)
+{
+    const char *who = "fteik_b200_batch3d_getTravelTimeField64f";
+    *ierr = 1;
+    if (!result_of(igrid, isrc, who)) return;
+    bgrid_t *g = &SB.g[igrid - 1];
+    if (ngrd != g->ngrd) { FK_ERR("%s: ngrd=%d, grid has %d", who, ngrd, g->ngrd); return; }
+    if (ensure_export((size_t)ngrd)) return;
+    const size_t fbytes = (size_t)g->zp * g->nx * g->ny * (size_t)SB.precision;
+    cudaStream_t s = fk_stream();
+    int e = fk_field_to_f64(SB.precision, 1, g->nz, g->nx, g->ny, g->zp,
+                            (char *)g->fields + fbytes * (size_t)(isrc - 1), order, SB.export_buf, s);
+    if (!e) e = (int)cudaMemcpyAsync(tt, SB.export_buf, sizeof(double) * (size_t)ngrd, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    *ierr = fk_check(e, who);
+}
+
+void fteik_b200_batch3d_getTravelTimeFields32f(int igrid, long long nval, float tt[], int *ierr)
+{
+    /* Unpadding copy of every source's FP32 field: one 2D memcpy per grid
+     * (rows of nz floats with pitch zp). */
+    const char *who = "fteik_b200_batch3d_getTravelTimeFields32f";
+    *ierr = 1;
+    bgrid_t *g = grid_of(igrid, who);
+    if (!g) return;
+    if (!SB.solved) { FK_ERR("%s: not solved", who); return; }
+    if (SB.precision != 4) { FK_ERR("%s: the batch was solved in FP64", who); return; }
+    if (nval < (long long)g->nsrc * g->ngrd) { FK_ERR("%s: nval too small", who); return; }
+    int e = (int)cudaMemcpy2DAsync(tt, sizeof(float) * (size_t)g->nz, g->fields,
+                                   sizeof(float) * (size_t)g->zp, sizeof(float) * (size_t)g->nz,
+                                   (size_t)g->nx * g->ny * g->nsrc, cudaMemcpyDeviceToHost, fk_stream());
+    if (!e) e = (int)cudaStreamSynchronize(fk_stream());
+    *ierr = fk_check(e, who);
+}
+
+void fteik_b200_batch3d_getTravelTimes64f(int igrid, int nval, double ttr[], int *ierr)
+{
+    const char *who = "fteik_b200_batch3d_getTravelTimes64f";
+    *ierr = 1;
+    bgrid_t *g = grid_of(igrid, who);
+    if (!g) return;
+    if (!SB.solved) { FK_ERR("%s: not solved", who); return; }
+    if (g->nrec < 1) { FK_ERR("%s: no receivers", who); return; }
+    if (nval < g->nsrc * g->nrec) { FK_ERR("%s: nval too small", who); return; }
+    const size_t n = (size_t)g->nsrc * g->nrec;
+    const size_t fbytes = (size_t)g->zp * g->nx * g->ny * (size_t)SB.precision;
+    void **ptrs = (void **)malloc(sizeof(void *) * (size_t)g->nsrc);
+    for (int s2 = 0; s2 < g->nsrc; s2++) ptrs[s2] = (char *)g->fields + fbytes * (size_t)s2;
+    void **ptrs_dev = (void **)fk_dalloc(sizeof(void *) * (size_t)g->nsrc, who);
+    if (!ptrs_dev || ensure_export(n)) { free(ptrs); fk_dfree(ptrs_dev); return; }
+    cudaStream_t s = fk_stream();
+    int e = (int)cudaMemcpyAsync(ptrs_dev, ptrs, sizeof(void *) * (size_t)g->nsrc, cudaMemcpyHostToDevice, s);
+    if (!e) e = fk_receivers_batch(SB.precision, g->nz, g->nx, g->ny, g->zp, g->dz, g->dx, g->dy,
+                                  ptrs_dev, g->nsrc, g->nrec, g->ri_dev, g->rd_dev, SB.export_buf, s);
+    if (!e) e = (int)cudaMemcpyAsync(ttr, SB.export_buf, sizeof(double) * n, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    free(ptrs);
+    fk_dfree(ptrs_dev);
+    *ierr = fk_check(e, who);
+}
+
+float *fk_locate_table_row(int itf, int ngrd);
+
+void fteik_b200_batch3d_exportToLocator(int igrid, int itf0, int *ierr)
+{
+    const char *who = "fteik_b200_batch3d_exportToLocator";
+    *ierr = 1;
+    bgrid_t *g = grid_of(igrid, who);
+    if (!g) return;
+    if (!SB.solved) { FK_ERR("%s: not solved", who); return; }
+    if (SB.precision != 4) { FK_ERR("%s: the batch was solved in FP64", who); return; }
+    float *dst0 = fk_locate_table_row(itf0, g->ngrd);
+    float *dst1 = fk_locate_table_row(itf0 + g->nsrc - 1, g->ngrd);
+    if (!dst0 || !dst1) { FK_ERR("%s: locator tables %d..%d unavailable for ngrd=%d", who, itf0, itf0 + g->nsrc - 1, g->ngrd); return; }
+    const size_t fbytes = (size_t)g->zp * g->nx * g->ny * sizeof(float);
+    int e = 0;
+    for (int s2 = 0; s2 < g->nsrc && !e; s2++) {
+        float *dst = fk_locate_table_row(itf0 + s2, g->ngrd);
+        e = (int)cudaMemcpy2DAsync(dst, sizeof(float) * (size_t)g->nz,
+                                   (char *)g->fields + fbytes * (size_t)s2, sizeof(float) * (size_t)g->zp,
+                                   sizeof(float) * (size_t)g->nz, (size_t)g->nx * g->ny,
+                                   cudaMemcpyDeviceToDevice, fk_stream());
+    }
+    if (!e) e = (int)cudaStreamSynchronize(fk_stream());
+    *ierr = fk_check(e, who);
+}

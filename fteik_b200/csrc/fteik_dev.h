@@ -1,0 +1,135 @@
+/*
+ * fteik_dev.h -- internal C interface between the C host layer and the CUDA
+ * kernels of libfteik_shared.so.  Plain C types and device pointers only.
+ *
+ * Device data layout (all grids column major, z fastest, like the reference):
+ *   travel-time field of one source : [ny][nx][zp]   zp  = pitch >= nz
+ *   cell slowness of one grid       : [ny-1][nx-1][zcp] zcp = pitch >= nz-1
+ * Pitches are multiples of 8 elements so every z column starts on a 32-byte
+ * boundary.
+ */
+#ifndef FTEIK_DEV_H
+#define FTEIK_DEV_H
+
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FK_HUGE 99999.0
+#define FK_PITCH(n) ((((n) + 7) / 8) * 8)
+
+/* One 3D grid of a (possibly batched) solve. */
+typedef struct {
+    int nz, nx, ny;
+    int zp, zcp;          /* field / slowness z pitches (elements) */
+    double dz, dx, dy;
+    const void *slow;     /* device: float (FP32 solve) or double (FP64 solve) */
+} fk_grid3d_t;
+
+/* One (grid, source) work item. */
+typedef struct {
+    int grid;             /* index into the grid table */
+    int zsi, xsi, ysi;    /* 1-based source cell (source.F90 conventions) */
+    double zsa, xsa, ysa; /* 1-based fractional source position */
+    double szero;         /* slowness of the source cell */
+    void *tt;             /* device field, [ny][nx][zp] */
+} fk_work3d_t;
+
+/* Per-work-item outputs of a solve. */
+typedef struct {
+    double residual;      /* FP64 max |dt| of the last pass */
+    int npass;            /* Gauss-Seidel passes run after the init pass */
+    int status;           /* 0 ok */
+} fk_result3d_t;
+
+/* Solve every work item: field initialisation, 8 initialisation sweeps, then
+ * nsweep passes of 8 sweeps (or, when conv_tol >= 0 and max_pass > 0,
+ * passes until a pass changes no node by more than conv_tol).
+ * precision: 4 (FP32 field, FP64 near-source stencil) or 8 (FP64 field).
+ * grids/work/results are device arrays.  Returns a cudaError_t. */
+int fk3d_solve(int precision, const fk_grid3d_t *grids, const fk_work3d_t *work,
+               fk_result3d_t *results, int nwork, int max_nx, int max_nz,
+               double eps, int nsweep, double conv_tol, int max_pass,
+               cudaStream_t stream);
+
+/* Set the kernel attributes a later fk3d_solve needs (call before a CUDA
+ * graph capture of fk3d_solve). */
+int fk3d_prepare(int precision, int max_nx, int max_nz);
+
+/* Dynamic shared memory the solve kernels need for these sizes. */
+size_t fk3d_smem_bytes(int precision, int max_nx, int max_nz);
+
+/* ---- 2D ---------------------------------------------------------------- */
+typedef struct {
+    int nz, nx, zp, zcp;
+    double dz, dx;
+    const double *slow;   /* device, [nx-1][zcp] */
+} fk_grid2d_t;
+
+typedef struct {
+    int grid;
+    int zsi, xsi;
+    double zsa, xsa, szero;
+    double *tt;           /* device, [nx][zp] FP64 */
+} fk_work2d_t;
+
+/* 2D LSM (fsm = 0) or FSM (fsm = 1) solve of every work item in FP64. */
+int fk2d_solve(int fsm, const fk_grid2d_t *grids, const fk_work2d_t *work,
+               fk_result3d_t *results, int nwork, int max_nx, double eps,
+               int nsweep, double conv_tol, int max_pass, cudaStream_t stream);
+
+/* ---- field utilities --------------------------------------------------- */
+/* Fill a padded slowness array (precision 4 or 8) from FP64 cell slowness in
+ * the reference's natural layout. */
+int fk_pack_slowness(int precision, int is3d, int nz, int nx, int ny, int zcp,
+                     const double *slow_nat, void *slow_dev, cudaStream_t s);
+/* Copy a padded field (precision 4 or 8) to FP64 in the requested ordering:
+ * 0 natural (z fastest), 1 XYZ / XZ (x fastest, z slowest), 2 ZYX. */
+int fk_field_to_f64(int precision, int is3d, int nz, int nx, int ny, int zp,
+                    const void *tt, int order, double *out, cudaStream_t s);
+/* Cell-averaged field (getTravelTimeFieldCell64f). */
+int fk_field_cell_to_f64(int precision, int is3d, int nz, int nx, int ny,
+                         int zp, const void *tt, int order, double *out,
+                         cudaStream_t s);
+/* Trilinear (3D) / bilinear (2D) receiver interpolation, receiver.F90. */
+int fk_receivers(int precision, int is3d, int nz, int nx, int ny, int zp,
+                 double dz, double dx, double dy, const void *tt, int nrec,
+                 const int *ri /* 3*nrec: zri,xri,yri 1-based */,
+                 const double *rd /* 3*nrec: zdr,xdr,ydr */, double *ttr,
+                 cudaStream_t s);
+/* Batched receiver extraction for many fields sharing one geometry:
+ * fields[f] -> ttr[f*nrec + r]. */
+int fk_receivers_batch(int precision, int nz, int nx, int ny, int zp,
+                       double dz, double dx, double dy, void *const *fields,
+                       int nfield, int nrec, const int *ri, const double *rd,
+                       double *ttr, cudaStream_t s);
+/* Analytic fields (analytic.F90) in the solver's natural order. */
+int fk_analytic_field(int kind /*0 const, 1 linear*/, int nz, int nx, int ny,
+                      double z0, double x0, double y0, double dz, double dx,
+                      double dy, double v0, double v1, double zs, double xs,
+                      double ys, double *out, cudaStream_t s);
+
+/* Analytic times at arbitrary points for nsrc sources: out[s*ldr + p]. */
+int fk_analytic_points(int kind, int nz, double z0, double dz, double v0, double v1,
+                       int npts, const double *z, const double *x, const double *y,
+                       int nsrc, const double *zs, const double *xs, const double *ys,
+                       int ldr, double *out, cudaStream_t s);
+int fk_f64_to_f32(size_t n, const double *in, float *out, cudaStream_t s);
+
+/* ---- locate ------------------------------------------------------------- */
+/* Exact FP32 L2 grid search (locate.F90:620-744) for nev events:
+ * tables [ntf][ldgrd] FP32; obs/wts [nev][ntf] FP32 (0 weight = skipped);
+ * out_idx 0-based, out_t0 / out_obj FP32 values at the optimum. */
+int fk_locate_l2_exact(int ngrd, int ldgrd, int ntf, const float *tables,
+                       int nev, const float *obs, const float *wts,
+                       int *out_idx, float *out_t0, float *out_obj,
+                       void *scratch, size_t scratch_bytes, cudaStream_t s);
+size_t fk_locate_l2_exact_scratch(int ngrd, int nev);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

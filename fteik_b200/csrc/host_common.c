@@ -1,0 +1,85 @@
+/*
+ * host_common.c -- device context, stream and allocation helpers of the C
+ * host layer.
+ */
+#include "host_common.h"
+
+#include <stdlib.h>
+
+static int g_dev_state = 0; /* 0 unknown, 1 ready, -1 unusable */
+static cudaStream_t g_stream = NULL;
+static int g_device = -1;
+
+int fk_dev_ready(const char *who)
+{
+    if (g_dev_state == 1) return 0;
+    if (g_dev_state == -1) {
+        FK_ERR("%s: no usable CUDA device; this library has no CPU path", who);
+        return 1;
+    }
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n < 1) {
+        g_dev_state = -1;
+        FK_ERR("%s: no usable CUDA device (%s); this library has no CPU path", who,
+               e != cudaSuccess ? cudaGetErrorString(e) : "device count 0");
+        return 1;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    e = cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        g_dev_state = -1;
+        FK_ERR("%s: cannot create a CUDA stream (%s)", who, cudaGetErrorString(e));
+        return 1;
+    }
+    g_device = dev;
+    g_dev_state = 1;
+    return 0;
+}
+
+int fteik_b200_device(void) { return g_dev_state == 1 ? g_device : -1; }
+
+const char *fteik_b200_version(void) { return "fteik-b200 0.1 (sm_100a)"; }
+
+cudaStream_t fk_stream(void) { return g_stream; }
+
+void *fteik_b200_stream(void)
+{
+    if (fk_dev_ready("fteik_b200_stream")) return NULL;
+    return (void *)g_stream;
+}
+
+void *fk_dalloc(size_t bytes, const char *who)
+{
+    if (fk_dev_ready(who)) return NULL;
+    void *p = NULL;
+    cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+    if (e != cudaSuccess) {
+        FK_ERR("%s: cudaMalloc of %zu bytes failed (%s)", who, bytes, cudaGetErrorString(e));
+        return NULL;
+    }
+    return p;
+}
+
+void fk_dfree(void *p)
+{
+    if (p && g_dev_state == 1) cudaFree(p);
+}
+
+int fk_check(int err, const char *who)
+{
+    if (err == 0) return 0;
+    FK_ERR("%s: CUDA error %d (%s)", who, err, cudaGetErrorString((cudaError_t)err));
+    return 1;
+}
+
+int fk_sync(const char *who)
+{
+    cudaError_t e = cudaStreamSynchronize(g_stream);
+    if (e != cudaSuccess) {
+        FK_ERR("%s: CUDA error (%s)", who, cudaGetErrorString(e));
+        return 1;
+    }
+    return 0;
+}

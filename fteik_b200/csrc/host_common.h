@@ -1,0 +1,74 @@
+/*
+ * host_common.h -- process-wide state of the C host layer (the counterpart
+ * of the reference's Fortran SAVE module variables) and small helpers.
+ */
+#ifndef FTEIK_HOST_COMMON_H
+#define FTEIK_HOST_COMMON_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdio.h>
+#include <cuda_runtime.h>
+
+#include "fteik_dev.h"
+
+#define FK_ERR(...) do { fprintf(stderr, __VA_ARGS__); fputc('\n', stderr); } while (0)
+
+/* ---- device, stream, allocation ---- */
+int fk_dev_ready(const char *who);           /* 0 if a CUDA device is usable */
+cudaStream_t fk_stream(void);
+void *fk_dalloc(size_t bytes, const char *who);
+void fk_dfree(void *p);
+int fk_check(int cuda_err, const char *who);  /* 0 on success, prints otherwise */
+int fk_sync(const char *who);
+
+/* ---- model (model.F90) ---- */
+typedef struct {
+    bool lis3d, have_geom, have_model;
+    int nz, nx, ny, ngrd, ncell, verbose;
+    double dz, dx, dy, z0, x0, y0;
+    double *slow;          /* host FP64, natural cell order */
+    void *slow_dev32;      /* device FP32 padded */
+    void *slow_dev64;      /* device FP64 padded */
+    bool dev32_ok, dev64_ok;
+} fk_model_t;
+extern fk_model_t fk_model;
+const void *fk_model_slow_dev(int precision); /* uploads lazily */
+void fk_model_invalidate_dev(void);
+
+/* ---- sources (source.F90) ---- */
+typedef struct {
+    int nsrc, verbose;
+    bool have;
+    int *zsi, *xsi, *ysi;
+    double *zsa, *xsa, *ysa, *zs_true, *xs_true, *ys_true;
+} fk_source_t;
+extern fk_source_t fk_source;
+/* source.F90:82-236 for one source; 0 on success */
+int fk_snap_source(bool is3d, int nz, int nx, int ny, double z0, double x0,
+                   double y0, double dz, double dx, double dy, double zsrc,
+                   double xsrc, double ysrc, int isrc, int *zsi, int *xsi,
+                   int *ysi, double *zsa, double *xsa, double *ysa);
+double fk_source_szero(int isrc); /* slowness of the source cell */
+
+/* ---- receivers (receiver.F90) ---- */
+typedef struct {
+    int nrec, verbose;
+    bool have;
+    int *ri;          /* host 3*nrec: zri, xri, yri */
+    double *rd;       /* host 3*nrec: zdr, xdr, ydr */
+    double *zrec, *xrec, *yrec;
+    int *ri_dev;
+    double *rd_dev;
+} fk_receiver_t;
+extern fk_receiver_t fk_receiver;
+int fk_receiver_setup(int nrec, const double *z, const double *x,
+                      const double *y, int verbose); /* returns ierr */
+int fk_receiver_upload(void);
+/* receiver.F90:62-164 for an arbitrary geometry */
+int fk_receiver_geometry(bool is3d, int nz, int nx, int ny, double z0,
+                         double x0, double y0, double dz, double dx, double dy,
+                         int nrec, const double *z, const double *x,
+                         const double *y, int *ri, double *rd);
+
+#endif

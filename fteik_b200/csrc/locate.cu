@@ -1,0 +1,163 @@
+/*
+ * locate.cu -- grid-search event location (locate.F90:620-744, :112-126).
+ *
+ * fk_locate_l2_exact reproduces the reference's FP32 objective bit for bit:
+ * for every grid point g and event e, in the reference's order,
+ *   t0[g]  += w_i * (xnorm * (o_i - T_i[g]))            over used tables i
+ *   obj[g] += ((sqrt(1/2) * w_i) * (o_i - (T_i[g] + t0[g])))^2
+ * with no fused multiply-add, then MINLOC (first minimum).  A thread keeps
+ * the tables of its grid point in registers and evaluates a block of events
+ * against them, so the tables stream from HBM once per event block rather
+ * than once per event.  The argmin is a 64-bit atomicMin on
+ * (float bits of obj) << 32 | g, which for non-negative objectives orders by
+ * value and then by the smaller index, as MINLOC does.
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "fteik_dev.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kEvBlock = 32;  /* events per CTA */
+constexpr int kMaxTf = 64;    /* tables held in registers */
+
+__device__ __forceinline__ unsigned long long pack_key(float obj, int g)
+{
+    return ((unsigned long long)__float_as_uint(obj) << 32) | (unsigned)g;
+}
+
+template <int NTF>
+__global__ void __launch_bounds__(kThreads)
+l2_exact_kernel(int ngrd, int ldgrd, int ntf, const float *__restrict__ tables, int nev,
+                const float *__restrict__ obs, const float *__restrict__ wts,
+                const float *__restrict__ xnorm, unsigned long long *__restrict__ best)
+{
+    __shared__ float s_obs[kEvBlock][NTF];
+    __shared__ float s_w[kEvBlock][NTF];
+    __shared__ float s_xn[kEvBlock];
+    __shared__ unsigned long long s_best[kThreads / 32];
+    const int g = blockIdx.x * kThreads + threadIdx.x;
+    const int e0 = blockIdx.y * kEvBlock;
+    const int nev_blk = min(kEvBlock, nev - e0);
+    for (int t = threadIdx.x; t < kEvBlock * NTF; t += kThreads) {
+        const int e = t / NTF, i = t % NTF;
+        const bool ok = e < nev_blk && i < ntf;
+        s_obs[e][i] = ok ? obs[(size_t)(e0 + e) * ntf + i] : 0.0f;
+        s_w[e][i] = ok ? wts[(size_t)(e0 + e) * ntf + i] : 0.0f;
+    }
+    if (threadIdx.x < kEvBlock) s_xn[threadIdx.x] = (threadIdx.x < nev_blk) ? xnorm[e0 + threadIdx.x] : 0.0f;
+    float T[NTF];
+#pragma unroll
+    for (int i = 0; i < NTF; ++i)
+        T[i] = (g < ngrd && i < ntf) ? __ldg(tables + (size_t)i * ldgrd + g) : 0.0f;
+    __syncthreads();
+    const float sqrtHalf = 0.70710677f; /* SQRT(0.5) in FP32 (constants.F90) */
+    for (int e = 0; e < nev_blk; ++e) {
+        const float xn = s_xn[e];
+        float t0 = 0.0f;
+#pragma unroll
+        for (int i = 0; i < NTF; ++i) {
+            const float w = s_w[e][i];
+            if (i < ntf && w > 0.0f) {
+                const float res = __fmul_rn(xn, __fsub_rn(s_obs[e][i], __fadd_rn(T[i], 0.0f)));
+                t0 = __fadd_rn(t0, __fmul_rn(w, res));
+            }
+        }
+        float obj = 0.0f;
+#pragma unroll
+        for (int i = 0; i < NTF; ++i) {
+            const float w = s_w[e][i];
+            if (i < ntf && w > 0.0f) {
+                const float wt = __fmul_rn(sqrtHalf, w);
+                const float est = __fadd_rn(__fadd_rn(T[i], t0), 0.0f);
+                const float res = __fmul_rn(wt, __fsub_rn(s_obs[e][i], est));
+                obj = __fadd_rn(obj, __fmul_rn(res, res));
+            }
+        }
+        unsigned long long key = (g < ngrd) ? pack_key(obj, g) : ~0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long k2 = __shfl_xor_sync(0xffffffffu, key, o);
+            key = k2 < key ? k2 : key;
+        }
+        if ((threadIdx.x & 31) == 0) s_best[threadIdx.x >> 5] = key;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long k = s_best[0];
+            for (int w2 = 1; w2 < kThreads / 32; ++w2) k = s_best[w2] < k ? s_best[w2] : k;
+            atomicMin(best + e0 + e, k);
+        }
+        __syncthreads();
+    }
+}
+
+/* t0 and obj at the optimum, same arithmetic. */
+__global__ void l2_at_opt_kernel(int ngrd, int ldgrd, int ntf, const float *__restrict__ tables,
+                                 int nev, const float *__restrict__ obs,
+                                 const float *__restrict__ wts, const float *__restrict__ xnorm,
+                                 const unsigned long long *__restrict__ best, int *out_idx,
+                                 float *out_t0, float *out_obj)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nev) return;
+    const int g = (int)(best[e] & 0xffffffffu);
+    const float xn = xnorm[e];
+    const float *o = obs + (size_t)e * ntf, *w = wts + (size_t)e * ntf;
+    float t0 = 0.0f;
+    for (int i = 0; i < ntf; ++i)
+        if (w[i] > 0.0f)
+            t0 = __fadd_rn(t0, __fmul_rn(w[i], __fmul_rn(xn, __fsub_rn(o[i], tables[(size_t)i * ldgrd + g]))));
+    float obj = 0.0f;
+    for (int i = 0; i < ntf; ++i)
+        if (w[i] > 0.0f) {
+            const float res = __fmul_rn(__fmul_rn(0.70710677f, w[i]),
+                                        __fsub_rn(o[i], __fadd_rn(tables[(size_t)i * ldgrd + g], t0)));
+            obj = __fadd_rn(obj, __fmul_rn(res, res));
+        }
+    out_idx[e] = g;
+    out_t0[e] = t0;
+    out_obj[e] = obj;
+}
+
+__global__ void xnorm_kernel(int nev, int ntf, const float *__restrict__ wts, float *xnorm,
+                             unsigned long long *best)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nev) return;
+    float s = 0.0f; /* SUM over the padded weight row, in order */
+    for (int i = 0; i < ntf; ++i) s = __fadd_rn(s, wts[(size_t)e * ntf + i]);
+    xnorm[e] = __fdiv_rn(1.0f, s);
+    best[e] = ~0ull;
+}
+
+} // namespace
+
+extern "C" size_t fk_locate_l2_exact_scratch(int ngrd, int nev)
+{
+    (void)ngrd;
+    return (size_t)nev * (sizeof(unsigned long long) + sizeof(float)) + 256;
+}
+
+extern "C" int fk_locate_l2_exact(int ngrd, int ldgrd, int ntf, const float *tables, int nev,
+                                  const float *obs, const float *wts, int *out_idx,
+                                  float *out_t0, float *out_obj, void *scratch,
+                                  size_t scratch_bytes, cudaStream_t s)
+{
+    if (nev <= 0) return 0;
+    if (ntf > kMaxTf || ntf < 1) return (int)cudaErrorInvalidValue;
+    if (scratch_bytes < fk_locate_l2_exact_scratch(ngrd, nev)) return (int)cudaErrorInvalidValue;
+    unsigned long long *best = (unsigned long long *)scratch;
+    float *xn = (float *)(best + nev);
+    xnorm_kernel<<<(nev + 127) / 128, 128, 0, s>>>(nev, ntf, wts, xn, best);
+    dim3 grid((ngrd + kThreads - 1) / kThreads, (nev + kEvBlock - 1) / kEvBlock);
+    if (ntf <= 16)
+        l2_exact_kernel<16><<<grid, kThreads, 0, s>>>(ngrd, ldgrd, ntf, tables, nev, obs, wts, xn, best);
+    else if (ntf <= 32)
+        l2_exact_kernel<32><<<grid, kThreads, 0, s>>>(ngrd, ldgrd, ntf, tables, nev, obs, wts, xn, best);
+    else
+        l2_exact_kernel<64><<<grid, kThreads, 0, s>>>(ngrd, ldgrd, ntf, tables, nev, obs, wts, xn, best);
+    l2_at_opt_kernel<<<(nev + 127) / 128, 128, 0, s>>>(ngrd, ldgrd, ntf, tables, nev, obs, wts, xn,
+                                                       best, out_idx, out_t0, out_obj);
+    return (int)cudaGetLastError();
+}

@@ -1,0 +1,38 @@
+/*
+ * sweep3d_f32.cu -- FP32 instantiation of the 3D solve (the product path):
+ * FP32 travel times and plane-wave stencils, FP64 for the analytic source
+ * corners, the near-source spherical stencil and the convergence residual.
+ */
+#include "sweep3d_impl.cuh"
+
+extern "C" int fk3d_solve_f64(const fk_grid3d_t *grids, const fk_work3d_t *work,
+                              fk_result3d_t *results, int nwork, int max_nx, int max_nz,
+                              double eps, int nsweep, double conv_tol, int max_pass,
+                              cudaStream_t stream);
+
+extern "C" int fk3d_solve(int precision, const fk_grid3d_t *grids, const fk_work3d_t *work,
+                          fk_result3d_t *results, int nwork, int max_nx, int max_nz,
+                          double eps, int nsweep, double conv_tol, int max_pass,
+                          cudaStream_t stream)
+{
+    if (precision == 8)
+        return fk3d_solve_f64(grids, work, results, nwork, max_nx, max_nz, eps, nsweep,
+                              conv_tol, max_pass, stream);
+    if (precision != 4) return (int)cudaErrorInvalidValue;
+    return fk3::launch_solve<float>(grids, work, results, nwork, max_nx, max_nz, eps, nsweep,
+                                    conv_tol, max_pass, stream);
+}
+
+extern "C" int fk3d_prepare_f64(int max_nx, int max_nz);
+
+extern "C" int fk3d_prepare(int precision, int max_nx, int max_nz)
+{
+    if (precision == 8) return fk3d_prepare_f64(max_nx, max_nz);
+    return fk3::prepare_solve<float>(max_nx, max_nz);
+}
+
+extern "C" size_t fk3d_smem_bytes(int precision, int max_nx, int max_nz)
+{
+    return precision == 8 ? fk3::smem_bytes<double>(max_nx, max_nz)
+                          : fk3::smem_bytes<float>(max_nx, max_nz);
+}

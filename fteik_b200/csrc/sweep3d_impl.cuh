@@ -1,0 +1,557 @@
+/*
+ * sweep3d_impl.cuh -- level-set-equivalent fast-sweeping eikonal solve in 3D
+ * (the reference's fteik_solver3d_solveSourceLSM, solver3D.F90:1156-1243,
+ * with the sweeps of autoCode.f90 and the node updates of
+ * localSolver.F90:384-959) as sm_100a CUDA kernels.
+ *
+ * Schedule.  A sweep in direction (sz,sx,sy) updates node (i,j,k) from its
+ * seven upwind neighbours only, so any topological order of that dependency
+ * graph gives the level-set result bit for bit.  Here one CTA owns one
+ * (grid, source) work item and runs the whole solve: each lane owns one
+ * logical x column and walks the (z, y) plane in z-fastest order, lane x
+ * running one step behind lane x-1.  At step s lane x updates walk position
+ * p = s - x, so
+ *   tv   (i-1, j,   k  ) = this lane's previous result          (register)
+ *   te   (i,   j-1, k  ) = lane x-1's previous result           (shuffle)
+ *   tev  (i-1, j-1, k  ) = this lane's previous te              (register)
+ *   tn   (i,   j,   k-1) = this lane's result one y-row earlier (smem ring)
+ *   ten  (i,   j-1, k-1) = lane x-1's previous tn               (shuffle)
+ *   tnv, tnve            = this lane's previous tn, ten         (registers)
+ * Lane 0 of warp w takes lane 31 of warp w-1 through a two-slot shared
+ * buffer; one named barrier per step orders that hand-off.  There are no
+ * inter-CTA waits, so nothing can spin.
+ *
+ * Logical coordinates i' = sz > 0 ? i : n-1-i (0-based) turn every sweep into
+ * the (+,+,+) sweep; the update box of the reference (solver3D.F90:493-565)
+ * becomes i' >= lo_z, j' >= lo_x, k' >= lo_y in logical coordinates.
+ */
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "fteik_dev.h"
+
+namespace fk3 {
+
+constexpr int kMaxWarps = 32;
+
+template <typename R>
+struct Mesh {
+    R dz, dx, dy;
+    R dz2i, dx2i, dy2i, dsum_nine, dsumi, dz2dx2, dz2dy2, dx2dy2;
+    R dz2i_dx2i, dz2i_dy2i, dx2i_dy2i;
+    R dz2i_p_dx2i, dz2i_p_dy2i, dx2i_p_dy2i;
+    R dz2i_p_dx2i_inv, dz2i_p_dy2i_inv, dx2i_p_dy2i_inv;
+};
+
+/* localSolver.F90:905-931: the mesh constants, derived in FP64 and rounded
+ * once to the working precision. */
+template <typename R>
+__device__ void make_mesh(Mesh<R> &m, double dz, double dx, double dy)
+{
+    double dz2 = dz * dz, dx2 = dx * dx, dy2 = dy * dy;
+    double dz2i = 1.0 / dz2, dx2i = 1.0 / dx2, dy2i = 1.0 / dy2;
+    double dsum = dz2i + dx2i + dy2i;
+    m.dz = (R)dz; m.dx = (R)dx; m.dy = (R)dy;
+    m.dz2i = (R)dz2i; m.dx2i = (R)dx2i; m.dy2i = (R)dy2i;
+    m.dsum_nine = (R)(dsum * 9.0);
+    m.dsumi = (R)(1.0 / dsum);
+    m.dz2dx2 = (R)(1.0 / (dz2 * dx2));
+    m.dz2dy2 = (R)(1.0 / (dz2 * dy2));
+    m.dx2dy2 = (R)(1.0 / (dx2 * dy2));
+    m.dz2i_dx2i = (R)(dz2i * dx2i);
+    m.dz2i_dy2i = (R)(dz2i * dy2i);
+    m.dx2i_dy2i = (R)(dx2i * dy2i);
+    m.dz2i_p_dx2i = (R)(dz2i + dx2i);
+    m.dz2i_p_dy2i = (R)(dz2i + dy2i);
+    m.dx2i_p_dy2i = (R)(dx2i + dy2i);
+    m.dz2i_p_dx2i_inv = (R)(1.0 / (dz2i + dx2i));
+    m.dz2i_p_dy2i_inv = (R)(1.0 / (dz2i + dy2i));
+    m.dx2i_p_dy2i_inv = (R)(1.0 / (dx2i + dy2i));
+}
+
+__device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); }
+__device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
+template <typename R> __device__ __forceinline__ R rmin(R a, R b) { return (b < a) ? b : a; }
+template <typename R> __device__ __forceinline__ R rmax(R a, R b) { return (b > a) ? b : a; }
+
+/* localSolver.F90:384-534, one node; tupd enters as the node's time. */
+template <typename R>
+__device__ __forceinline__ R noinit(const Mesh<R> &c, R tv, R te, R tn, R tev,
+                                    R ten, R tnv, R tnve, R s1, R s2, R s3,
+                                    R s4, R s5, R s6, R s7, R tupd)
+{
+    const R HUGEV = (R)FK_HUGE;
+    R t12min = tv + c.dz * s1;
+    t12min = rmin(t12min, te + c.dx * s2);
+    t12min = rmin(t12min, tn + c.dy * s3);
+    R temtv = te - tv;
+    if (temtv < c.dz * s4 && -temtv < c.dx * s4) {
+        R ta = tev + temtv, tb = tev - temtv, tab = ta - tb;
+        R t = ((tb * c.dz2i + ta * c.dx2i) +
+               rsqrt_((R)4 * (s4 * s4) * c.dz2i_p_dx2i - c.dz2i_dx2i * (tab * tab))) *
+              c.dz2i_p_dx2i_inv;
+        t12min = rmin(t12min, t);
+    }
+    R tvmtn = tv - tn;
+    if (tvmtn < c.dy * s5 && -tvmtn < c.dz * s5) {
+        R ta = tvmtn + tnv, tb = -tvmtn + tnv, tab = ta - tb;
+        R t = ((ta * c.dz2i + tb * c.dy2i) +
+               rsqrt_((R)4 * (s5 * s5) * c.dz2i_p_dy2i - c.dz2i_dy2i * (tab * tab))) *
+              c.dz2i_p_dy2i_inv;
+        t12min = rmin(t12min, t);
+    }
+    R temtn = te - tn;
+    if (temtn < c.dy * s6 && -temtn < c.dx * s6) {
+        R ta = temtn + ten, tb = -temtn + ten, tab = ta - tb;
+        R t = ((ta * c.dx2i + tb * c.dy2i) +
+               rsqrt_((R)4 * (s6 * s6) * c.dx2i_p_dy2i - c.dx2i_dy2i * (tab * tab))) *
+              c.dx2i_p_dy2i_inv;
+        t12min = rmin(t12min, t);
+    }
+    R t3d = HUGEV;
+    R tmax = rmax(rmax(tv, te), tn);
+    if (t12min > tmax) {
+        R ta = te + (R)0.5 * (-tn + ten - tv + tev) - tnv + tnve;
+        R tb = tv + (R)0.5 * (-tn + tnv - te + tev) - ten + tnve;
+        R tc = tn + (R)0.5 * (-te + ten - tv + tnv) - tev + tnve;
+        R tab = ta - tb, tbc = tb - tc, tac = ta - tc;
+        R t2 = (s7 * s7) * c.dsum_nine;
+        R t3 = c.dz2dx2 * (tab * tab) + c.dz2dy2 * (tbc * tbc) + c.dx2dy2 * (tac * tac);
+        if (t2 >= t3) {
+            R t1 = tb * c.dz2i + ta * c.dx2i + tc * c.dy2i;
+            t3d = (t1 + rsqrt_(t2 - t3)) * c.dsumi;
+        }
+    }
+    t3d = rmin(t3d, t12min);
+    return rmin(tupd, t3d);
+}
+
+/* Source description used by the initialisation stencil. */
+struct Src {
+    int zsi, xsi, ysi;
+    double zsa, xsa, ysa, szero, szero2, eps_t;
+};
+
+/* localSolver.F90:775-792 */
+template <typename R>
+__device__ __forceinline__ R tana(const Src &q, const Mesh<R> &c, int i, int j, int k)
+{
+    R dz_ = ((R)i - (R)q.zsa) * c.dz;
+    R dx_ = ((R)j - (R)q.xsa) * c.dx;
+    R dy_ = ((R)k - (R)q.ysa) * c.dy;
+    return (R)q.szero * rsqrt_(dz_ * dz_ + dx_ * dx_ + dy_ * dy_);
+}
+
+/* localSolver.F90:538-751, one node.  lcart is the Cartesian/spherical
+ * switch (tmin > epsSolver), evaluated by the caller in FP64. */
+template <typename R>
+__device__ R init_node(const Src &q, const Mesh<R> &c, bool lcart, R tv, R te,
+                       R tn, R tev, R ten, R tnv, R tnve, R tt0, R slow1,
+                       R slow2, R slow3, R slow4, R slow5, R slow6, R slow7,
+                       int i, int j, int k, int sz, int sx, int sy)
+{
+    const R HUGEV = (R)FK_HUGE;
+    const R szero2 = (R)q.szero2;
+    R sgnrz_dzi = (R)sz / c.dz, sgnrx_dxi = (R)sx / c.dx, sgnry_dyi = (R)sy / c.dy;
+    R t1d = tv + c.dz * slow1;
+    t1d = rmin(t1d, te + c.dx * slow2);
+    t1d = rmin(t1d, tn + c.dy * slow3);
+    R tmax = rmax(rmax(tv, te), tn);
+    R t0c = 0, tzc = 0, txc = 0, tyc = 0;
+    R tauv = HUGEV, taue = HUGEV, taun = HUGEV, tauev = HUGEV, tauen = HUGEV,
+      taunv = HUGEV, taunve = HUGEV;
+    if (!lcart) {
+        /* localSolver.F90:819-851 (tAnaD) */
+        R dz_ = ((R)i - (R)q.zsa) * c.dz;
+        R dx_ = ((R)j - (R)q.xsa) * c.dx;
+        R dy_ = ((R)k - (R)q.ysa) * c.dy;
+        R d0 = dz_ * dz_ + dx_ * dx_ + dy_ * dy_;
+        R d0i_szero = 0;
+        if (d0 > (R)0) {
+            R sq = rsqrt_(d0);
+            t0c = (R)q.szero * sq;
+            d0i_szero = (R)q.szero / sq;
+        }
+        tzc = d0i_szero * dz_;
+        txc = d0i_szero * dx_;
+        tyc = d0i_szero * dy_;
+        tauv = tv - tana(q, c, i - sz, j, k);
+        taue = te - tana(q, c, i, j - sx, k);
+        taun = tn - tana(q, c, i, j, k - sy);
+        tauev = tev - tana(q, c, i - sz, j - sx, k);
+        tauen = ten - tana(q, c, i, j - sx, k - sy);
+        taunv = tnv - tana(q, c, i - sz, j, k - sy);
+        taunve = tnve - tana(q, c, i - sz, j - sx, k - sy);
+    }
+    bool ldoZX = (tv < te + c.dx * slow4) && (te < tv + c.dz * slow4);
+    bool ldoZY = (tv < tn + c.dy * slow5) && (tn < tv + c.dz * slow5);
+    bool ldoXY = (te < tn + c.dy * slow6) && (tn < te + c.dx * slow6);
+    bool zxc = ldoZX && (lcart || k != q.ysi);
+    bool zyc = ldoZY && (lcart || j != q.xsi);
+    bool xyc = ldoXY && (lcart || i != q.zsi);
+    bool zxs = ldoZX && !zxc, zys = ldoZY && !zyc, xys = ldoXY && !xyc;
+    R t1_2d = HUGEV;
+    if (zxc) {
+        R ta = tev + te - tv, tb = tev - te + tv, tab = ta - tb;
+        t1_2d = ((tb * c.dz2i + ta * c.dx2i) +
+                 rsqrt_((R)4 * (slow4 * slow4) * c.dz2i_p_dx2i - c.dz2i_dx2i * (tab * tab))) *
+                c.dz2i_p_dx2i_inv;
+    }
+    if (zxs) {
+        R sref2 = slow4 * slow4;
+        R ta = tauev + taue - tauv, tb = tauev - taue + tauv;
+        R apoly = c.dz2i_p_dx2i;
+        R bpoly = (R)4 * (sgnrx_dxi * txc + sgnrz_dzi * tzc) - (R)2 * (ta * c.dx2i + tb * c.dz2i);
+        R cpoly = ((ta * ta) * c.dx2i) + ((tb * tb) * c.dz2i) -
+                  (R)4 * (sgnrx_dxi * txc * ta + sgnrz_dzi * tzc * tb) +
+                  (R)4 * (szero2 - sref2 + tyc * tyc);
+        R dpoly = bpoly * bpoly - (R)4 * apoly * cpoly;
+        if (dpoly >= (R)0) t1_2d = (rsqrt_(dpoly) - bpoly) / ((R)2 * apoly) + t0c;
+        if (t1_2d < tv || t1_2d < te) t1_2d = HUGEV;
+    }
+    R tmin12 = rmin(t1d, t1_2d);
+    R t2_2d = HUGEV;
+    if (zyc) {
+        R ta = tv - tn + tnv, tb = tn - tv + tnv, tab = ta - tb;
+        t2_2d = ((ta * c.dz2i + tb * c.dy2i) +
+                 rsqrt_((R)4 * (slow5 * slow5) * c.dz2i_p_dy2i - c.dz2i_dy2i * (tab * tab))) *
+                c.dz2i_p_dy2i_inv;
+    }
+    if (zys) {
+        R sref2 = slow5 * slow5;
+        R ta = tauv - taun + taunv, tb = taun - tauv + taunv;
+        R apoly = c.dz2i_p_dy2i;
+        R bpoly = (R)4 * (sgnry_dyi * tyc + sgnrz_dzi * tzc) - (R)2 * (ta * c.dz2i + tb * c.dy2i);
+        R cpoly = ((ta * ta) * c.dz2i) + ((tb * tb) * c.dy2i) -
+                  (R)4 * (sgnrz_dzi * tzc * ta + sgnry_dyi * tyc * tb) +
+                  (R)4 * (szero2 - sref2 + txc * txc);
+        R dpoly = bpoly * bpoly - (R)4 * apoly * cpoly;
+        if (dpoly >= (R)0) t2_2d = (rsqrt_(dpoly) - bpoly) / ((R)2 * apoly) + t0c;
+        if (t2_2d < tv || t2_2d < tn) t2_2d = HUGEV;
+    }
+    tmin12 = rmin(tmin12, t2_2d);
+    R t3_2d = HUGEV;
+    if (xyc) {
+        R ta = te - tn + ten, tb = tn - te + ten, tab = ta - tb;
+        t3_2d = ((ta * c.dx2i + tb * c.dy2i) +
+                 rsqrt_((R)4 * (slow6 * slow6) * c.dx2i_p_dy2i - c.dx2i_dy2i * (tab * tab))) *
+                c.dx2i_p_dy2i_inv;
+    }
+    if (xys) {
+        R sref2 = slow6 * slow6;
+        R ta = taue - taun + tauen, tb = taun - taue + tauen;
+        R apoly = c.dx2i_p_dy2i;
+        R bpoly = (R)4 * (sgnry_dyi * tyc + sgnrx_dxi * txc) - (R)2 * (ta * c.dx2i + tb * c.dy2i);
+        R cpoly = ((ta * ta) * c.dx2i) + ((tb * tb) * c.dy2i) -
+                  (R)4 * (sgnrx_dxi * txc * ta + sgnry_dyi * tyc * tb) +
+                  (R)4 * (szero2 - sref2 + tzc * tzc);
+        R dpoly = bpoly * bpoly - (R)4 * apoly * cpoly;
+        if (dpoly >= (R)0) t3_2d = (rsqrt_(dpoly) - bpoly) / ((R)2 * apoly) + t0c;
+        if (t3_2d < te || t3_2d < tn) t3_2d = HUGEV;
+    }
+    tmin12 = rmin(tmin12, t3_2d);
+    R t3d = HUGEV;
+    bool ldo3D = tmin12 > tmax;
+    if (ldo3D && lcart) {
+        R ta = te + (R)0.5 * (-tn + ten - tv + tev) - tnv + tnve;
+        R tb = tv + (R)0.5 * (-tn + tnv - te + tev) - ten + tnve;
+        R tc = tn + (R)0.5 * (-te + ten - tv + tnv) - tev + tnve;
+        R tab = ta - tb, tbc = tb - tc, tac = ta - tc;
+        R t2 = (slow7 * slow7) * c.dsum_nine;
+        R t3 = c.dz2dx2 * (tab * tab) + c.dz2dy2 * (tbc * tbc) + c.dx2dy2 * (tac * tac);
+        if (t2 >= t3) {
+            R t1 = tb * c.dz2i + ta * c.dx2i + tc * c.dy2i;
+            t3d = (t1 + rsqrt_(t2 - t3)) * c.dsumi;
+        }
+    }
+    if (ldo3D && !lcart) {
+        R sref2 = slow7 * slow7;
+        R ta = taue + (R)0.5 * (-taun + tauen - tauv + tauev) - taunv + taunve;
+        R tb = tauv + (R)0.5 * (-taun + taunv - taue + tauev) - tauen + taunve;
+        R tc = taun + (R)0.5 * (-taue + tauen - tauv + taunv) - tauev + taunve;
+        R apoly = c.dx2i + c.dz2i + c.dy2i;
+        R bpoly = (R)6 * (sgnrz_dzi * tzc + sgnry_dyi * tyc + sgnrx_dxi * txc) -
+                  (R)2 * (ta * c.dx2i + tb * c.dz2i + tc * c.dy2i);
+        R cpoly = ((ta * ta) * c.dx2i) + ((tb * tb) * c.dz2i) + ((tc * tc) * c.dy2i) -
+                  (R)6 * (sgnrx_dxi * txc * ta + sgnrz_dzi * tzc * tb + sgnry_dyi * tyc * tc) +
+                  (R)9 * (szero2 - sref2);
+        R dpoly = bpoly * bpoly - (R)4 * apoly * cpoly;
+        if (dpoly >= (R)0) t3d = (rsqrt_(dpoly) - bpoly) / ((R)2 * apoly) + t0c;
+        if (t3d < te || t3d < tn || t3d < tv) t3d = HUGEV;
+    }
+    R tupd = rmin(tmin12, t3d);
+    return rmin(tt0, tupd);
+}
+
+/* Shared-memory layout of one CTA. */
+template <typename R>
+struct Smem {
+    Mesh<R> mesh;
+    Mesh<double> mesh64;
+    R xres[2][kMaxWarps];
+    R xtn[2][kMaxWarps];
+    double wmax[kMaxWarps];
+    int flag;
+};
+
+__device__ __forceinline__ void named_barrier(int nthreads)
+{
+    asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+__device__ __forceinline__ int ring_pitch(int nz) { return (nz + 1) & ~1; }
+
+/* One sweep of one work item.  Returns this thread's FP64 max |dt|. */
+template <typename R, bool INIT>
+__device__ double sweep_one(Smem<R> &sm, R *ring, const Src &q,
+                            const fk_grid3d_t &g, R *__restrict__ tt,
+                            const R *__restrict__ slow, int sweep, int nthreads)
+{
+    const int nz = g.nz, nx = g.nx, ny = g.ny, zp = g.zp, zcp = g.zcp;
+    const int s0 = sweep - 1;
+    const int sz = (s0 < 4) ? 1 : -1;
+    const int sx = (s0 % 2 == 0) ? 1 : -1;
+    const int sy = ((s0 / 2) % 2 == 0) ? 1 : -1;
+    /* update box in logical coordinates (solver3D.F90:493-565; flipped
+     * initialisation bound clamped to the grid) */
+    int loz = 1, lox = 1, loy = 1;
+    if (INIT) {
+        loz = (sz > 0) ? max(1, q.zsi - 1) : max(1, nz - q.zsi - 1);
+        lox = (sx > 0) ? max(1, q.xsi - 1) : max(1, nx - q.xsi - 1);
+        loy = (sy > 0) ? max(1, q.ysi - 1) : max(1, ny - q.ysi - 1);
+    }
+    const int ky0 = loy - 1; /* first y-row walked: loaded, not updated */
+    const int rows = ny - ky0;
+    const long P = (long)rows * nz;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int xl = threadIdx.x; /* logical x of this lane */
+    const int rp = ring_pitch(nz);
+    R *myring = ring + (size_t)xl * rp;
+    const long nsteps = P + (long)nthreads - 1;
+    const int ix = (sx > 0) ? xl : nx - 1 - xl; /* physical x */
+    const bool xin = xl < nx;
+    /* slowness x cells: upwind U and downwind D (clamped) */
+    const int cxU = (sx > 0) ? ix - 1 : ix;
+    const int cxD = min(max((sx > 0) ? ix : ix - 1, 0), nx - 2);
+    const R HUGEV = (R)FK_HUGE;
+    const unsigned FULL = 0xffffffffu;
+
+    R r_last = HUGEV, te_last = HUGEV, tn_last = HUGEV, ten_last = HUGEV;
+    int il = 0, kl = ky0; /* logical z, y of the next node of this lane */
+    double dmax = 0.0;
+
+    for (long s = 0; s < nsteps; ++s) {
+        R te = __shfl_up_sync(FULL, r_last, 1);
+        R ten = __shfl_up_sync(FULL, tn_last, 1);
+        if (lane == 0 && warp > 0) {
+            te = sm.xres[(s + 1) & 1][warp - 1];
+            ten = sm.xtn[(s + 1) & 1][warp - 1];
+        }
+        const long p = s - xl;
+        const bool act = xin && p >= 0 && p < P;
+        R result = r_last, tn = tn_last;
+        if (act) {
+            const int iz = (sz > 0) ? il : nz - 1 - il;
+            const int iy = (sy > 0) ? kl : ny - 1 - kl;
+            const size_t idx = ((size_t)iy * nx + ix) * zp + iz;
+            const R told = tt[idx];
+            tn = (kl > ky0) ? myring[il] : HUGEV;
+            result = told;
+            const bool upd = (il >= loz) && (xl >= lox) && (kl >= loy);
+            if (upd) {
+                const R tv = r_last, tev = te_last, tnv = tn_last, tnve = ten_last;
+                /* slowness: 8 cells around the node, U = upwind, D = other */
+                const int czU = (sz > 0) ? iz - 1 : iz;
+                const int czD = min(max((sz > 0) ? iz : iz - 1, 0), nz - 2);
+                const int cyU = (sy > 0) ? iy - 1 : iy;
+                const int cyD = min(max((sy > 0) ? iy : iy - 1, 0), ny - 2);
+                const size_t rowUU = ((size_t)cyU * (nx - 1) + cxU) * zcp;
+                const size_t rowUD = ((size_t)cyD * (nx - 1) + cxU) * zcp; /* x U, y D */
+                const size_t rowDU = ((size_t)cyU * (nx - 1) + cxD) * zcp; /* x D, y U */
+                const size_t rowDD = ((size_t)cyD * (nx - 1) + cxD) * zcp;
+                const R sUUU = __ldg(slow + rowUU + czU), sDUU = __ldg(slow + rowUU + czD);
+                const R sUUD = __ldg(slow + rowUD + czU), sDUD = __ldg(slow + rowUD + czD);
+                const R sUDU = __ldg(slow + rowDU + czU), sDDU = __ldg(slow + rowDU + czD);
+                const R sUDD = __ldg(slow + rowDD + czU), sDDD = __ldg(slow + rowDD + czD);
+                /* naming: s<z><x><y> */
+                const R s1 = rmin(rmin(sUUU, sUUD), rmin(sUDU, sUDD));
+                const R s2 = rmin(rmin(sUUU, sUUD), rmin(sDUU, sDUD));
+                const R s3 = rmin(rmin(sUUU, sUDU), rmin(sDUU, sDDU));
+                const R s4 = rmin(sUUU, sUUD);
+                const R s5 = rmin(sUUU, sUDU);
+                const R s6 = rmin(sUUU, sDUU);
+                const R s7 = sUUU;
+                if (!INIT) {
+                    result = noinit(sm.mesh, tv, te, tn, tev, ten, tnv, tnve, s1, s2,
+                                    s3, s4, s5, s6, s7, told);
+                } else {
+                    const double tmin = (double)rmin(rmin(tv, te), tn);
+                    const bool lcart = tmin > q.eps_t;
+                    if (lcart || sizeof(R) == 8) {
+                        result = init_node<R>(q, sm.mesh, lcart, tv, te, tn, tev, ten,
+                                              tnv, tnve, told, s1, s2, s3, s4, s5, s6,
+                                              s7, iz + 1, ix + 1, iy + 1, sz, sx, sy);
+                    } else {
+                        /* near-source spherical stencil in FP64 */
+                        result = (R)init_node<double>(
+                            q, sm.mesh64, lcart, (double)tv, (double)te, (double)tn,
+                            (double)tev, (double)ten, (double)tnv, (double)tnve,
+                            (double)told, (double)s1, (double)s2, (double)s3,
+                            (double)s4, (double)s5, (double)s6, (double)s7, iz + 1,
+                            ix + 1, iy + 1, sz, sx, sy);
+                    }
+                }
+                if (result != told) {
+                    tt[idx] = result;
+                    const double d = fabs((double)result - (double)told);
+                    dmax = d > dmax ? d : dmax;
+                }
+            }
+            myring[il] = result;
+            if (++il == nz) { il = 0; ++kl; }
+        }
+        te_last = te;
+        ten_last = ten;
+        r_last = result;
+        tn_last = tn;
+        if (lane == 31) {
+            sm.xres[s & 1][warp] = result;
+            sm.xtn[s & 1][warp] = tn;
+        }
+        named_barrier(nthreads);
+    }
+    return dmax;
+}
+
+template <typename R>
+__device__ __forceinline__ double block_max(Smem<R> &sm, double v, int nthreads)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        double w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
+    }
+    const int warp = threadIdx.x >> 5, nw = nthreads >> 5;
+    if ((threadIdx.x & 31) == 0) sm.wmax[warp] = v;
+    named_barrier(nthreads);
+    double m = 0.0;
+    for (int w = 0; w < nw; ++w) m = sm.wmax[w] > m ? sm.wmax[w] : m;
+    named_barrier(nthreads);
+    return m;
+}
+
+template <typename R>
+__device__ __forceinline__ void setup_src(Src &q, const fk_work3d_t &w,
+                                          const fk_grid3d_t &g, double eps)
+{
+    q.zsi = w.zsi; q.xsi = w.xsi; q.ysi = w.ysi;
+    q.zsa = w.zsa; q.xsa = w.xsa; q.ysa = w.ysa;
+    q.szero = w.szero; q.szero2 = w.szero * w.szero;
+    double hmin = g.dz < g.dx ? g.dz : g.dx;
+    hmin = g.dy < hmin ? g.dy : hmin;
+    q.eps_t = eps * hmin * w.szero; /* localSolver.F90:906 */
+}
+
+/* Whole solve of one work item per CTA. */
+template <typename R, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1)
+solve_kernel(const fk_grid3d_t *__restrict__ grids, const fk_work3d_t *__restrict__ work,
+             fk_result3d_t *__restrict__ results, double eps, int nsweep,
+             double conv_tol, int max_pass)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem<R> &sm = *reinterpret_cast<Smem<R> *>(smem_raw);
+    R *ring = reinterpret_cast<R *>(smem_raw + ((sizeof(Smem<R>) + 15) & ~size_t(15)));
+    const fk_work3d_t w = work[blockIdx.x];
+    const fk_grid3d_t g = grids[w.grid];
+    const int nthreads = ((g.nx + 31) / 32) * 32;
+    if ((int)threadIdx.x >= nthreads) return;
+    R *tt = reinterpret_cast<R *>(w.tt);
+    const R *slow = reinterpret_cast<const R *>(g.slow);
+    Src q;
+    setup_src<R>(q, w, g, eps);
+    if (threadIdx.x == 0) {
+        make_mesh<R>(sm.mesh, g.dz, g.dx, g.dy);
+        make_mesh<double>(sm.mesh64, g.dz, g.dx, g.dy);
+    }
+    if (threadIdx.x < 2 * kMaxWarps) {
+        sm.xres[threadIdx.x >> 5][threadIdx.x & 31] = (R)FK_HUGE;
+        sm.xtn[threadIdx.x >> 5][threadIdx.x & 31] = (R)FK_HUGE;
+    }
+    /* solver3D.F90:1201-1202: the field starts at HUGE ... */
+    const size_t nfield = (size_t)g.ny * g.nx * g.zp;
+    for (size_t e = threadIdx.x; e < nfield; e += nthreads) tt[e] = (R)FK_HUGE;
+    named_barrier(nthreads);
+    /* ... with the analytic times on the 8 corners of the source cell
+     * (localSolver.F90:933-956), computed in FP64 */
+    if (threadIdx.x < 8) {
+        const int di = threadIdx.x & 1, dj = (threadIdx.x >> 1) & 1, dk = (threadIdx.x >> 2) & 1;
+        const double t = tana<double>(q, sm.mesh64, q.zsi + di, q.xsi + dj, q.ysi + dk);
+        tt[((size_t)(q.ysi - 1 + dk) * g.nx + (q.xsi - 1 + dj)) * g.zp + (q.zsi - 1 + di)] = (R)t;
+    }
+    __threadfence_block();
+    named_barrier(nthreads);
+    for (int s = 1; s <= 8; ++s)
+        sweep_one<R, true>(sm, ring, q, g, tt, slow, s, nthreads);
+    const bool converge = conv_tol >= 0.0 && max_pass > 0;
+    const int npasses = converge ? max_pass : nsweep;
+    double res = 0.0;
+    int ran = 0;
+    for (int it = 0; it < npasses; ++it) {
+        double d = 0.0;
+        for (int s = 1; s <= 8; ++s) {
+            double ds = sweep_one<R, false>(sm, ring, q, g, tt, slow, s, nthreads);
+            d = ds > d ? ds : d;
+        }
+        res = block_max(sm, d, nthreads);
+        ++ran;
+        if (converge && res <= conv_tol) break;
+    }
+    if (threadIdx.x == 0) {
+        results[blockIdx.x].residual = res;
+        results[blockIdx.x].npass = ran;
+        results[blockIdx.x].status = 0;
+    }
+}
+
+template <typename R>
+inline size_t smem_bytes(int max_nx, int max_nz)
+{
+    const int nthreads = ((max_nx + 31) / 32) * 32;
+    return ((sizeof(Smem<R>) + 15) & ~size_t(15)) +
+           (size_t)nthreads * (size_t)((max_nz + 1) & ~1) * sizeof(R);
+}
+
+template <typename R>
+inline int prepare_solve(int max_nx, int max_nz)
+{
+    const size_t smem = smem_bytes<R>(max_nx, max_nz);
+    const int nthreads = ((max_nx + 31) / 32) * 32;
+    auto kern = (nthreads <= 256) ? solve_kernel<R, 256> : solve_kernel<R, 1024>;
+    return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <typename R>
+inline int launch_solve(const fk_grid3d_t *grids, const fk_work3d_t *work,
+                        fk_result3d_t *results, int nwork, int max_nx, int max_nz,
+                        double eps, int nsweep, double conv_tol, int max_pass,
+                        cudaStream_t stream)
+{
+    if (nwork <= 0) return 0;
+    if (max_nx > kMaxWarps * 32) return (int)cudaErrorInvalidValue;
+    const size_t smem = smem_bytes<R>(max_nx, max_nz);
+    const int nthreads = ((max_nx + 31) / 32) * 32;
+    auto kern = (nthreads <= 256) ? solve_kernel<R, 256> : solve_kernel<R, 1024>;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(stream, &cap);
+    if (e != cudaSuccess) return (int)e;
+    if (cap == cudaStreamCaptureStatusNone) {
+        /* under capture the caller has run prepare_solve already */
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
+    kern<<<nwork, nthreads, smem, stream>>>(grids, work, results, eps, nsweep, conv_tol,
+                                           max_pass);
+    return (int)cudaGetLastError();
+}
+
+} // namespace fk3

@@ -1,0 +1,323 @@
+/*
+ * fteik_b200.h -- C ABI of libfteik_shared.so, the B200 implementation of
+ * fteik's eikonal solver and grid-search locator.
+ *
+ * Part 1 declares the reference's own entry points with the reference's
+ * exact symbol names, argument passing (scalars by value, arrays and outputs
+ * by pointer, bool = C _Bool) and conventions (1-based source, event and
+ * table numbers; ierr = 0 on success; travel times in FP64 with 99999 for
+ * unreached nodes).  Each cites the Fortran BIND(C) routine it replaces
+ * (paths relative to the reference repository).  Where the reference's own
+ * header include/fteik/fteik_fortran.h disagrees with its Fortran, the
+ * Fortran is followed.
+ *
+ * Part 2 declares additions with no reference counterpart (prefix
+ * fteik_b200_): a batched multi-source, multi-grid 3D solve, device-resident
+ * hand-off and batched location.
+ *
+ * The library owns one CUDA stream and uses the current CUDA device (device
+ * 0 unless the caller selected another); callers need no CUDA context.  It
+ * has no CPU fallback: without a usable CUDA device every compute entry
+ * point fails with ierr = 1 and a message on stderr.  Like the reference,
+ * the state is a process-wide singleton and the API is not re-entrant.
+ */
+#ifndef FTEIK_B200_H
+#define FTEIK_B200_H
+
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Orderings, constants.F90:29-39 */
+enum fteikOrder_enum {
+    FTEIK_NATURAL_ORDERING = 0,
+    FTEIK_ZXY_ORDERING = 0,
+    FTEIK_ZX_ORDERING = 0,
+    FTEIK_XYZ_ORDERING = 1,
+    FTEIK_XZ_ORDERING = 1,
+    FTEIK_ZYX_ORDERING = 2
+};
+
+/* =====================  Part 1: reference entry points  ================== */
+
+/* ---- model: model.F90 ---- */
+/* model.F90:88-129 */
+void fteik_model_initializeGeometry(bool lis3d, int nz, int nx, int ny,
+                                    double z0, double x0, double y0,
+                                    double dz, double dx, double dy, int *ierr);
+/* model.F90:181-216 */
+void fteik_model_setGridSize(bool lis3d, int nz, int nx, int ny, int *ierr);
+/* model.F90:134-172 */
+void fteik_model_setGridSpacing(bool lis3d, double dz, double dx, double dy,
+                                int *ierr);
+/* model.F90:225-240 / :245-258 */
+void fteik_model_setOrigin3D(double z0, double x0, double y0);
+void fteik_model_setOrigin2D(double z0, double x0);
+/* model.F90:264-296 */
+void fteik_model_getGridSize(int *nz, int *nx, int *ny, int *ngrd, int *ncell,
+                             int *ierr);
+/* model.F90:719-754 */
+void fteik_model_setVelocityModel64f(int nv, const double vel[], int *ierr);
+/* model.F90:311-449 (order 0 natural, 1 XYZ, 2 ZYX) */
+void fteik_model_setNodalVelocityModel64f(int ng, int order,
+                                          const double vel[], int *ierr);
+/* model.F90:505-607 */
+void fteik_model_setCellVelocityModel64f(int nc, int order,
+                                         const double vel[], int *ierr);
+/* model.F90:760-780 (1-based) and fwrapper.c:8-14 (0-based) */
+int fteik_model_grid2indexF(int i, int j, int k, int nz, int nzx);
+int fteik_model_grid2index(int iz, int ix, int iy, int nz, int nzx);
+/* model.F90:790-810 */
+void fteik_model_index2gridF(int igrd, int *i, int *j, int *k, int *ierr);
+/* model.F90:827-836 */
+int fteik_model_velGrid2indexF(int i, int j, int k, int nzm1, int nzm1_nxm1);
+/* model.F90:612-640 */
+void fteik_model_free(void);
+
+/* ---- source: source.F90 ---- */
+/* source.F90:82-236 */
+void fteik_source_initialize64f(int nsrc, const double zsrc[],
+                                const double xsrc[], const double ysrc[],
+                                int verbose, int *ierr);
+/* source.F90:290-330 */
+void fteik_source_getSolverInfo64fF(int isrc, int *zsi, int *xsi, int *ysi,
+                                    double *zsa, double *xsa, double *ysa,
+                                    double *szero, double *szero2, int *ierr);
+/* source.F90:341-370 / :381-410 / :429-464 */
+void fteik_source_getSourceIndices64fF(int isrc, double *zsa, double *xsa,
+                                       double *ysa, int *ierr);
+void fteik_source_getSourceIndices32iF(int isrc, int *zsi, int *xsi, int *ysi,
+                                       int *ierr);
+void fteik_source_getSzero64fF(int isrc, double *szero, double *szero2,
+                               int *ierr);
+void fteik_source_getNumberOfSources(int *nsrc, int *ierr);
+void fteik_source_free(void);
+
+/* ---- receivers: receiver.F90 ---- */
+/* receiver.F90:62-164 */
+void fteik_receiver_initialize64f(int nrec, const double z[], const double x[],
+                                  const double y[], int verbose, int *ierr);
+/* receiver.F90:217-313: interpolates a caller-supplied FP64 field */
+void fteik_receiver_getTravelTimes64f(int nrec, int ngrd, const double ttimes[],
+                                      double ttr[], int *ierr);
+void fteik_receiver_getNumberOfReceivers(int *nrec, int *ierr);
+void fteik_receiver_free(void);
+
+/* ---- 3D solver: solver3D.F90 ---- */
+/* solver3D.F90:126-184 */
+void fteik_solver3d_initialize(int nz, int nx, int ny, double z0, double x0,
+                               double y0, double dz, double dx, double dy,
+                               int nsweep, double eps, double convTol,
+                               int verbose, int *ierr);
+/* solver3D.F90:575-610 */
+void fteik_solver3d_free(void);
+/* solver3D.F90:191-196 / :206-211 */
+void fteik_solver3d_setVerbosity(int verbose);
+void fteik_solver3d_setConvergenceTolerance(double convTol);
+/* solver3D.F90:683-698 / :640-673 */
+void fteik_solver3d_setNumberOfSweeps(int nsweep, int *ierr);
+void fteik_solver3d_setSphereToCartEpsilon(double eps, int *ierr);
+/* solver3D.F90:1138-1148 / :1115-1125 / :1083-1093 */
+void fteik_solver3d_setVelocityModel64f(int ncell, const double vel[], int *ierr);
+void fteik_solver3d_setCellVelocityModel64f(int nc, int order,
+                                            const double vel[], int *ierr);
+void fteik_solver3d_setNodalVelocityModel64f(int ng, int order,
+                                             const double vel[], int *ierr);
+/* solver3D.F90:717-727 / :737-748 */
+void fteik_solver3d_setSources64f(int nsrc, const double zsrc[],
+                                  const double xsrc[], const double ysrc[],
+                                  int *ierr);
+void fteik_solver3d_getNumberOfSources(int *nsrc, int *ierr);
+/* solver3D.F90:1045-1062 / :1024-1032 */
+void fteik_solver3d_setReceivers64f(int nrec, const double zrec[],
+                                    const double xrec[], const double yrec[],
+                                    int *ierr);
+void fteik_solver3d_getNumberOfReceivers(int *nrec, int *ierr);
+/* solver3D.F90:1156-1243 */
+void fteik_solver3d_solveSourceLSM(int isrc, int *ierr);
+/* solver3D.F90:844-897 */
+void fteik_solver3d_getTravelTimeField64f(int ngrd, int order, double tt[],
+                                          int *ierr);
+/* solver3D.F90:915-980 */
+void fteik_solver3d_getTravelTimeFieldCell64f(int ncell, int order,
+                                              double tt[], int *ierr);
+/* solver3D.F90:990-1016 */
+void fteik_solver3d_getTravelTimes64f(int nrec, double ttr[], int *ierr);
+/* solver3D.F90:757-823: ray tracing is outside this library (ierr = 1) */
+void fteik_solver3d_traceRaysToReceivers(int *ierr);
+void fteik_solver3d_traceRaysToPoints(int np, const double zp[],
+                                      const double xp[], const double yp[],
+                                      int *ierr);
+
+/* ---- 2D solver: solver2D.F90 ---- */
+/* solver2D.F90:124-198 */
+void fteik_solver2d_initialize(int nz, int nx, double z0, double x0, double dz,
+                               double dx, int nsweep, double eps,
+                               double convTol, int verbose, int *ierr);
+void fteik_solver2d_free(void);
+void fteik_solver2d_setVerbosity(int verbose);
+void fteik_solver2d_setConvergenceTolerance(double convTol);
+void fteik_solver2d_setNumberOfSweeps(int nsweep, int *ierr);
+void fteik_solver2d_setSphereToCartEpsilon(double eps, int *ierr);
+void fteik_solver2d_setVelocityModel64f(int ncell, const double vel[], int *ierr);
+void fteik_solver2d_setCellVelocityModel64f(int nc, int order,
+                                            const double vel[], int *ierr);
+void fteik_solver2d_setNodalVelocityModel64f(int ng, int order,
+                                             const double vel[], int *ierr);
+void fteik_solver2d_setSources64f(int nsrc, const double zsrc[],
+                                  const double xsrc[], int *ierr);
+void fteik_solver2d_setReceivers64f(int nrec, const double zrec[],
+                                    const double xrec[], int *ierr);
+void fteik_solver2d_getNumberOfReceivers(int *nrec, int *ierr);
+/* solver2D.F90:782-978 */
+void fteik_solver2d_solveSourceLSM(int isrc, int *ierr);
+/* solver2D.F90:1042-1280 */
+void fteik_solver2d_solveSourceFSM(int isrc, int *ierr);
+/* solver2D.F90:740-773: every source */
+void fteik_solver2d_solveLSM(int *ierr);
+/* solver2D.F90:1295-1340 / :1350-1400 */
+void fteik_solver2d_getTravelTimeField64f(int ngrd, int order, double tt[],
+                                          int *ierr);
+void fteik_solver2d_getTravelTimeFieldCell64f(int ncell, int order,
+                                              double tt[], int *ierr);
+/* solver2D.F90:1410-1447: ttr[ldr*nsrc], receiver times of every source */
+void fteik_solver2d_getTravelTimes64f(int ldr, double ttr[], int *ierr);
+void fteik_solver2d_traceRaysToReceivers(int *ierr);
+void fteik_solver2d_traceRaysToPoints(int np, const double xp[],
+                                      const double zp[], int *ierr);
+
+/* ---- analytic solutions: analytic.F90 ---- */
+void fteik_analytic_initialize64f(int nz, int nx, int ny, double z0, double x0,
+                                  double y0, double dz, double dx, double dy,
+                                  int verbose, int *ierr);
+void fteik_analytic_setSources64f(int nsrc, const double zsrc[],
+                                  const double xsrc[], const double ysrc[],
+                                  int *ierr);
+void fteik_analytic_setReceivers64f(int nrec, const double zrec[],
+                                    const double xrec[], const double yrec[],
+                                    int *ierr);
+void fteik_analytic_setConstantVelocity64f(double vconst, int *ierr);
+void fteik_analytic_setLinearVelocityGradient64f(double v0, double v1,
+                                                 int *ierr);
+void fteik_analytic_solveSourceConstantVelocity64f(int isrc, int *ierr);
+void fteik_analytic_solveSourceLinearVelocityGradient64f(int isrc, int *ierr);
+void fteik_analytic_getTravelTimeField64f(int ngrd, int order, double tt[],
+                                          int *ierr);
+/* analytic.F90:747-842: ttr[ldr*nsrc], exact times at every receiver */
+void fteik_analytic_getTravelTimesConstantVel64f(int ldr, double ttr[],
+                                                 int *ierr);
+void fteik_analytic_getTravelTimesGradientVel64f(int ldr, double ttr[],
+                                                 int *ierr);
+void fteik_analytic_free(void);
+
+/* ---- locator: locate.F90 ---- */
+/* locate.F90:142-223 */
+void locate_initialize(int nEvents, int ntf, int ngrd, int *ierr);
+/* locate.F90:233-270 */
+void locate_finalize(void);
+/* locate.F90:287-343 (itf 1-based) */
+void locate_setTravelTimeField64f(int ngrd, int itf, const double tt[],
+                                  int *ierr);
+/* locate.F90:361-396 (the Fortran takes float[]) */
+void locate_setTravelTimeField32f(int ngrd, int itf, const float tt[],
+                                  int *ierr);
+/* locate.F90:431-497 (evnmbr and obs2tf 1-based) */
+void locate_setObservation64f(int evnmbr, int nttimes, bool lhaveOT,
+                              double t0, const int obs2tf[],
+                              const double pickTimes[], const double wts[],
+                              int *ierr);
+/* fwrapper.c:42-55 (0-based event and table numbers) */
+void locate_setObservation64fC(int evnmbr, int nttimes, bool lhaveOT,
+                               double t0, const int obs2tf[],
+                               const double pickTimes[], const double wts[],
+                               int *ierr);
+/* locate.F90:112-126 (optIndx 1-based grid index) */
+void locate_locateEvent(int evnmbr, int *optIndx, double *t0Opt,
+                        double *objOpt);
+/* locate.F90:511-531 / :541-560 / :573-592 */
+void locate_setNumberOfEvents(int nEvents, int *ierr);
+void locate_setNumberOfTravelTimeFields(int ntf, int *ierr);
+void locate_setNumberOfGridPointsF(int ngrd, int *ierr);
+
+/* ---- HDF5 archive (h5io.F90): not built into this library; each call
+ * returns non-zero so python/fteik3d.py can bind its symbols ---- */
+int fteik_h5io_initializeF(const char *fileName);
+int fteik_h5io_finalizeF(void);
+int fteik_h5io_writeLevelSchedulesF(void);
+int fteik_h5io_writeVelocityModelF(const char *velName);
+int fteik_h5io_writeTravelTimesF(const char *ttName);
+
+/* =====================  Part 2: additions (fteik_b200_)  ================= */
+
+/* Library version string and the CUDA device in use (-1 if none). */
+const char *fteik_b200_version(void);
+int fteik_b200_device(void);
+/* The library's CUDA stream (a cudaStream_t), for callers that time or
+ * order their own work against the library's; NULL without a device. */
+void *fteik_b200_stream(void);
+
+/* Precision of fteik_solver3d_solveSourceLSM: 4 (default; FP32 fields with
+ * FP64 source corners, near-source stencil and residual) or 8 (FP64 fields,
+ * the reference's precision).  Applies from the next solve. */
+void fteik_b200_solver3d_setPrecision(int precision, int *ierr);
+/* FP64 max |dt| of the last Gauss-Seidel pass and passes run, for the last
+ * fteik_solver3d_solveSourceLSM. */
+void fteik_b200_solver3d_getSolveInfo(double *residual, int *npass, int *ierr);
+
+/* Batched 3D solve: ngrid grids of any size, each with its own sources, all
+ * solved by one kernel launch (one CTA per grid x source), replayed from a
+ * CUDA graph.  precision 4 = FP32 fields (near-source stencil, source
+ * corners and residual in FP64), 8 = FP64 fields.  nsweep / convTol /
+ * maxPass as for fteik_solver3d_initialize, except that convTol >= 0 with
+ * maxPass > 0 iterates every source to convergence.  Grid and source
+ * numbers are 1-based. */
+void fteik_b200_batch3d_initialize(int ngrid, const int nz[], const int nx[],
+                                   const int ny[], const double dz[],
+                                   const double dx[], const double dy[],
+                                   int nsweep, double eps, double convTol,
+                                   int maxPass, int precision, int *ierr);
+/* Cell velocities of grid igrid in the natural (z fastest) order. */
+void fteik_b200_batch3d_setVelocityModel64f(int igrid, int ncell,
+                                            const double vel[], int *ierr);
+/* Sources of grid igrid, coordinates relative to the grid origin (0,0,0). */
+void fteik_b200_batch3d_setSources64f(int igrid, int nsrc, const double zsrc[],
+                                      const double xsrc[], const double ysrc[],
+                                      int *ierr);
+void fteik_b200_batch3d_setReceivers64f(int igrid, int nrec,
+                                        const double zrec[], const double xrec[],
+                                        const double yrec[], int *ierr);
+/* Solve every (grid, source) pair. */
+void fteik_b200_batch3d_solve(int *ierr);
+/* Replay the last solve's CUDA graph on the library stream without waiting;
+ * returns a cudaError_t (non-zero also when no solve was captured yet). */
+int fteik_b200_batch3d_solveAsync(void);
+/* Field of one source, FP64 in a reference ordering. */
+void fteik_b200_batch3d_getTravelTimeField64f(int igrid, int isrc, int ngrd,
+                                              int order, double tt[], int *ierr);
+/* Fields of every source of a grid as FP32, natural order, [nsrc][ngrd]. */
+void fteik_b200_batch3d_getTravelTimeFields32f(int igrid, long long nval,
+                                               float tt[], int *ierr);
+/* Receiver times of every source of a grid: ttr[isrc*nrec + irec]. */
+void fteik_b200_batch3d_getTravelTimes64f(int igrid, int nval, double ttr[],
+                                          int *ierr);
+/* Residual (FP64 max |dt| of the last pass) and passes run. */
+void fteik_b200_batch3d_getSolveInfo(int igrid, int isrc, double *residual,
+                                     int *npass, int *ierr);
+/* Copy the FP32 tables of every source of grid igrid into the locator's
+ * device table store (tables itf0 .. itf0+nsrc-1, 1-based) without leaving
+ * the device.  The locator must have been initialised with ngrd equal to
+ * that grid's node count. */
+void fteik_b200_batch3d_exportToLocator(int igrid, int itf0, int *ierr);
+void fteik_b200_batch3d_finalize(void);
+
+/* Locate events ev[0..n-1] (1-based) in one batch with the reference's FP32
+ * objective (bit-identical optimum); outputs as locate_locateEvent. */
+void fteik_b200_locate_locateEvents(int n, const int ev[], int optIndx[],
+                                    double t0Opt[], double objOpt[], int *ierr);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

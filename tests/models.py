@@ -1,0 +1,53 @@
+"""Seeded synthetic velocity models and source sets used by the tests and the
+benchmark (the reference publishes no data sets; shapes follow the
+configurations the benchmark names)."""
+import numpy as np
+
+
+def linear_vz_cells(nz, nx, ny, h, v0=3000.0, grad=0.5):
+    """Cell velocities v(z) = v0 + grad*z_c at the cell centre, natural order
+    (z fastest), shape (ny-1, nx-1, nz-1)."""
+    zc = (np.arange(nz - 1) + 0.5) * h
+    v = v0 + grad * zc
+    return np.broadcast_to(v, (max(ny - 1, 1), nx - 1, nz - 1)).copy()
+
+
+def gaussian_field(shape, corr_cells, seed):
+    """Unit-variance Gaussian random field with a Gaussian correlation of
+    corr_cells cells (FFT-filtered white noise), clipped to +-3 sigma."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal(shape)
+    k = [np.fft.fftfreq(n) for n in shape]
+    kk = np.meshgrid(*k, indexing="ij")
+    k2 = sum(q * q for q in kk)
+    filt = np.exp(-0.5 * k2 * (2.0 * np.pi * corr_cells) ** 2)
+    f = np.real(np.fft.ifftn(np.fft.fftn(w) * filt))
+    f = (f - f.mean()) / f.std()
+    return np.clip(f, -3.0, 3.0)
+
+
+def layered_grf_cells(nz, nx, ny, seed=2, vels=(3000.0, 4000.0, 5000.0, 6000.0),
+                      min_cells=5, amp=0.05, corr=10.0):
+    """4 layers with seeded interface depths (>= min_cells cells each) times
+    (1 + amp * GRF); shape (ny-1, nx-1, nz-1), natural order."""
+    nzc = nz - 1
+    rng = np.random.default_rng(seed)
+    nl = len(vels)
+    while True:
+        cuts = np.sort(rng.integers(min_cells, nzc - min_cells, size=nl - 1))
+        th = np.diff(np.concatenate([[0], cuts, [nzc]]))
+        if th.min() >= min_cells:
+            break
+    vz = np.empty(nzc)
+    edges = np.concatenate([[0], cuts, [nzc]])
+    for i in range(nl):
+        vz[edges[i]:edges[i + 1]] = vels[i]
+    g = gaussian_field((ny - 1, nx - 1, nzc), corr, seed)
+    return vz[None, None, :] * (1.0 + amp * g)
+
+
+def interior_source(n, h, seed):
+    rng = np.random.default_rng(seed)
+    nz, nx, ny = n
+    return (rng.uniform(0.1, 0.9) * (nz - 1) * h[0], rng.uniform(0.1, 0.9) * (nx - 1) * h[1],
+            rng.uniform(0.1, 0.9) * (ny - 1) * h[2])

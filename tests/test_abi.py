@@ -1,0 +1,119 @@
+"""The C ABI library without a GPU: it loads, exports every entry point the
+public header declares, and runs its host-only logic."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import fteik_b200
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "fteik_b200.h")
+
+
+def _declared():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b((?:fteik|locate)_\w+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol(fk):
+    out = subprocess.check_output(["nm", "-D", "--defined-only", fteik_b200.LIB_PATH]).decode()
+    exported = {l.split()[-1] for l in out.splitlines() if l.strip()}
+    missing = [s for s in _declared() if s not in exported]
+    assert not missing, missing
+    # and nothing but the C ABI is exported
+    assert all(s.startswith(("fteik_", "locate_")) for s in exported), exported
+    for s in _declared():
+        getattr(fk.lib(), s)
+
+
+def test_reference_python_wrapper_symbols_present(fk):
+    """python/fteik3d.py, fteik2d.py and fteikAnalytic.py bind these at
+    construction; every one must resolve."""
+    names = ["fteik_solver3d_initialize", "fteik_solver3d_setReceivers64f",
+             "fteik_solver3d_solveSourceLSM", "fteik_solver3d_getTravelTimeField64f",
+             "fteik_solver3d_getTravelTimeFieldCell64f", "fteik_solver3d_setCellVelocityModel64f",
+             "fteik_solver3d_setNodalVelocityModel64f", "fteik_solver3d_setSources64f",
+             "fteik_solver3d_getTravelTimes64f", "fteik_solver3d_getNumberOfReceivers",
+             "fteik_h5io_initializeF", "fteik_h5io_writeLevelSchedulesF",
+             "fteik_h5io_writeTravelTimesF", "fteik_h5io_writeVelocityModelF",
+             "fteik_h5io_finalizeF", "fteik_solver3d_free", "fteik_solver2d_initialize",
+             "fteik_solver2d_setCellVelocityModel64f", "fteik_solver2d_setNodalVelocityModel64f",
+             "fteik_solver2d_setReceivers64f", "fteik_solver2d_solveLSM",
+             "fteik_solver2d_solveSourceLSM", "fteik_solver2d_solveSourceFSM",
+             "fteik_solver2d_getTravelTimeField64f", "fteik_solver2d_getTravelTimeFieldCell64f",
+             "fteik_solver2d_setSources64f", "fteik_solver2d_getTravelTimes64f",
+             "fteik_solver2d_getNumberOfReceivers", "fteik_solver2d_free",
+             "fteik_analytic_initialize64f", "fteik_analytic_setReceivers64f",
+             "fteik_analytic_solveSourceLinearVelocityGradient64f",
+             "fteik_analytic_solveSourceConstantVelocity64f",
+             "fteik_analytic_setLinearVelocityGradient64f", "fteik_analytic_setConstantVelocity64f",
+             "fteik_analytic_getTravelTimeField64f", "fteik_analytic_getTravelTimesConstantVel64f",
+             "fteik_analytic_getTravelTimesGradientVel64f", "fteik_analytic_setSources64f",
+             "fteik_analytic_free"]
+    L = fk.lib()
+    for n in names:
+        getattr(L, n)
+
+
+def test_index_round_trip(fk):
+    """testing/tests.c:262-302 on 34 x 10 x 21."""
+    L = fk.lib()
+    ierr = ctypes.c_int(1)
+    L.fteik_model_setGridSize(True, 34, 10, 21, ctypes.byref(ierr))
+    assert ierr.value == 0
+    i1, j1, k1 = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    for k in range(1, 22):
+        for j in range(1, 11):
+            for i in range(1, 35):
+                g = L.fteik_model_grid2indexF(i, j, k, 34, 340)
+                L.fteik_model_index2gridF(g, ctypes.byref(i1), ctypes.byref(j1), ctypes.byref(k1),
+                                          ctypes.byref(ierr))
+                assert ierr.value == 0 and (i1.value, j1.value, k1.value) == (i, j, k)
+                assert L.fteik_model_grid2index(i - 1, j - 1, k - 1, 34, 340) == g - 1
+    L.fteik_model_free()
+
+
+def test_host_validation(fk):
+    L = fk.lib()
+    ierr = ctypes.c_int(0)
+    L.fteik_model_setGridSize(True, 2, 10, 10, ctypes.byref(ierr))
+    assert ierr.value == 1
+    L.fteik_model_initializeGeometry(True, 10, 11, 12, 0.0, 0.0, 0.0, 10.0, 10.0, 10.0, ctypes.byref(ierr))
+    assert ierr.value == 0
+    v = np.full(9 * 10 * 11, 2000.0)
+    v[5] = -1.0
+    L.fteik_model_setVelocityModel64f(v.size, v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                      ctypes.byref(ierr))
+    assert ierr.value == 1
+    z = np.array([5.0, 95.0])
+    x = np.array([5.0, 100.0])
+    y = np.array([5.0, 110.5])
+    PD = ctypes.POINTER(ctypes.c_double)
+    L.fteik_source_initialize64f(2, z.ctypes.data_as(PD), x.ctypes.data_as(PD),
+                                 y.ctypes.data_as(PD), 0, ctypes.byref(ierr))
+    assert ierr.value == 1          # y = 110.5 lies outside [0, 110]
+    assert L.fteik_h5io_initializeF(b"x.h5") != 0
+    L.fteik_model_free()
+
+
+def _no_gpu():
+    try:
+        import torch
+        return not torch.cuda.is_available()
+    except Exception:
+        return True
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="checks the behaviour without a CUDA device")
+def test_compute_fails_loudly_without_gpu(fk):
+    L = fk.lib()
+    ierr = ctypes.c_int(0)
+    L.fteik_solver3d_initialize(10, 10, 10, 0, 0, 0, 10, 10, 10, 2, 5.0, 0.0, 0, ctypes.byref(ierr))
+    assert ierr.value == 1
+    L.locate_initialize(1, 4, 100, ctypes.byref(ierr))
+    assert ierr.value == 1

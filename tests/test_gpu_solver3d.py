@@ -1,0 +1,191 @@
+"""3D solver on the GPU (through the C ABI) against the FP64 CPU oracle.
+
+* precision 8 (FP64 fields): same schedule-independent arithmetic as the
+  oracle, so the fields agree to a few ulp;
+* precision 4 (FP32 fields, FP64 near-source stencil): the product path,
+  relative error <= 1e-4 against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from models import interior_source, layered_grf_cells, linear_vz_cells
+
+pytestmark = pytest.mark.gpu
+
+TOL32 = 1e-4  # relative travel-time error of the FP32 path vs the FP64 oracle
+
+
+def _case(name):
+    if name == "grf":
+        n, h = (23, 19, 17), (25.0, 20.0, 30.0)
+        vel = layered_grf_cells(*n, seed=5, min_cells=3)
+        src = interior_source(n, h, 7)
+    elif name == "linear":
+        n, h = (30, 21, 18), (50.0, 50.0, 50.0)
+        vel = linear_vz_cells(*n, h[0])
+        src = (0.0, 523.0, 411.0)           # surface source: z = 0 nudge
+    elif name == "lastcell":
+        n, h = (12, 14, 13), (10.0, 10.0, 10.0)
+        vel = layered_grf_cells(*n, seed=9, min_cells=2)
+        src = (109.99, 129.5, 119.2)        # source cell at nz-1, nx-1, ny-1
+    elif name == "node":
+        n, h = (15, 16, 17), (10.0, 10.0, 10.0)
+        vel = np.full((16, 15, 14), 4000.0)
+        src = (70.0, 80.0, 90.0)            # exactly on a node
+    elif name == "wide":
+        n, h = (9, 70, 11), (10.0, 10.0, 10.0)  # several warps across x
+        vel = layered_grf_cells(*n, seed=3, min_cells=2)
+        src = (41.0, 333.0, 52.0)
+    return n, h, vel, src
+
+
+def _gpu(fk, n, h, vel, src, precision, nsweep=2, eps=5.0, rec=None):
+    s = fk.fteik3d()
+    s.initialize(n[1], n[2], n[0], h[1], h[2], h[0], nsweep=nsweep, eps=eps, precision=precision)
+    s.setCellSlownessNatural(vel)
+    s.setSources(src[1], src[2], src[0])
+    if rec is not None:
+        s.setReceivers(rec[1], rec[2], rec[0])
+    s.solveSourceLSM(1)
+    return s
+
+
+def _oracle(n, h, vel, src, nsweep=2, eps=5.0, **kw):
+    si, sa = O.source_snap(True, n, (0, 0, 0), h, src)
+    tt, npass = O.solve3d(n, h, 1.0 / np.ravel(vel), si, sa, eps, nsweep, **kw)
+    return tt
+
+
+@pytest.mark.parametrize("name", ["grf", "linear", "lastcell", "node", "wide"])
+def test_fp64_matches_oracle(fk, name):
+    n, h, vel, src = _case(name)
+    s = _gpu(fk, n, h, vel, src, precision=8)
+    tt = s.getTravelTimeField()
+    ref = _oracle(n, h, vel, src)
+    assert np.max(np.abs(tt - ref)) <= 1e-12 * np.max(ref)
+    s.free()
+
+
+@pytest.mark.parametrize("name", ["grf", "linear", "lastcell", "node", "wide"])
+def test_fp32_within_tolerance(fk, name):
+    n, h, vel, src = _case(name)
+    s = _gpu(fk, n, h, vel, src, precision=4)
+    tt = s.getTravelTimeField()
+    ref = _oracle(n, h, vel, src)
+    rel = np.abs(tt - ref) / np.maximum(ref, 1e-6)
+    assert np.max(rel) <= TOL32, (np.max(rel), np.sqrt(np.mean(rel ** 2)))
+    s.free()
+
+
+@pytest.mark.parametrize("nsweep", [0, 1, 3])
+def test_nsweep_passes(fk, nsweep):
+    n, h, vel, src = _case("grf")
+    s = _gpu(fk, n, h, vel, src, precision=8, nsweep=nsweep)
+    tt = s.getTravelTimeField()
+    ref = _oracle(n, h, vel, src, nsweep=nsweep)
+    assert np.max(np.abs(tt - ref)) <= 1e-12 * np.max(ref)
+    assert s.getSolveInfo()[1] == nsweep
+    s.free()
+
+
+def test_orderings_and_cells(fk):
+    n, h, vel, src = _case("grf")
+    nz, nx, ny = n
+    s = _gpu(fk, n, h, vel, src, precision=8)
+    nat = s.getTravelTimeField().reshape(ny, nx, nz)
+    xyz = s.getTravelTimeField(order=fk.FTEIK_XYZ_ORDERING)
+    zyx = s.getTravelTimeField(order=fk.FTEIK_ZYX_ORDERING)
+    assert np.array_equal(xyz, nat.transpose(2, 0, 1).ravel())   # x fastest, z slowest
+    assert np.array_equal(zyx, nat.transpose(1, 0, 2).ravel())   # z fastest, then y, x
+    cell = s.getTravelTimeField(wantCell=True).reshape(ny - 1, nx - 1, nz - 1)
+    avg = np.zeros_like(cell)
+    for a in (0, 1):
+        for b in (0, 1):
+            for c in (0, 1):
+                avg += nat[a:ny - 1 + a, b:nx - 1 + b, c:nz - 1 + c]
+    assert np.allclose(cell, 0.125 * avg, rtol=1e-14, atol=0)
+    s.free()
+
+
+def test_receivers_match_oracle(fk):
+    n, h, vel, src = _case("grf")
+    rng = np.random.default_rng(4)
+    ext = [(n[i] - 1) * h[i] for i in range(3)]
+    rec = [rng.uniform(0, ext[i], 25) for i in range(3)]
+    rec[0][0], rec[1][1], rec[2][2] = ext[0], 0.0, ext[2]   # on the faces
+    s = _gpu(fk, n, h, vel, src, precision=8, rec=rec)
+    ttr = s.getTravelTimes()
+    ref = _oracle(n, h, vel, src)
+    want, ierr = O.receivers(True, n, (0, 0, 0), h, rec[0], rec[1], rec[2], ref)
+    assert ierr == 0
+    assert np.max(np.abs(ttr - want)) <= 1e-12 * np.max(want)
+    s.free()
+
+
+def test_errors_are_reported(fk):
+    import ctypes
+    L = fk.lib()
+    ierr = ctypes.c_int(0)
+    L.fteik_solver3d_free()
+    L.fteik_solver3d_initialize(10, 10, 10, 0, 0, 0, 10, 10, 10, 2, 5.0, 0.0, 0, ctypes.byref(ierr))
+    assert ierr.value == 0
+    L.fteik_solver3d_solveSourceLSM(1, ctypes.byref(ierr))       # no model yet
+    assert ierr.value == 1
+    vel = np.full(9 ** 3, 3000.0)
+    L.fteik_solver3d_setVelocityModel64f(vel.size, vel.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                         ctypes.byref(ierr))
+    assert ierr.value == 0
+    L.fteik_solver3d_solveSourceLSM(1, ctypes.byref(ierr))       # no sources
+    assert ierr.value == 1
+    z = np.array([200.0])                                        # outside the model
+    p = z.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    L.fteik_solver3d_setSources64f(1, p, p, p, ctypes.byref(ierr))
+    assert ierr.value == 1
+    L.fteik_solver3d_free()
+
+
+def test_batched_multi_grid(fk):
+    grids = [(14, 40, 12, 25.0, 25.0, 25.0), (20, 17, 15, 30.0, 20.0, 25.0)]
+    for prec in (8, 4):
+        b = fk.Batch3D(grids, nsweep=2, eps=5.0, precision=prec)
+        cases = []
+        for ig, (nz, nx, ny, dz, dx, dy) in enumerate(grids, start=1):
+            vel = layered_grf_cells(nz, nx, ny, seed=20 + ig, min_cells=2)
+            b.setVelocityModel(ig, vel)
+            rng = np.random.default_rng(ig)
+            srcs = [(rng.uniform(0, (nz - 1) * dz), rng.uniform(0, (nx - 1) * dx),
+                     rng.uniform(0, (ny - 1) * dy)) for _ in range(3)]
+            srcs[0] = (0.0, srcs[0][1], srcs[0][2])
+            b.setSources(ig, [s[0] for s in srcs], [s[1] for s in srcs], [s[2] for s in srcs])
+            cases.append((ig, (nz, nx, ny), (dz, dx, dy), vel, srcs))
+        b.solve()
+        for ig, n, h, vel, srcs in cases:
+            for k, src in enumerate(srcs, start=1):
+                tt = b.field(ig, k)
+                ref = _oracle(n, h, vel, src)
+                if prec == 8:
+                    assert np.max(np.abs(tt - ref)) <= 1e-12 * np.max(ref)
+                else:
+                    assert np.max(np.abs(tt - ref) / np.maximum(ref, 1e-6)) <= TOL32
+            f32 = b.fields32(ig) if prec == 4 else None
+            if f32 is not None:
+                assert np.array_equal(f32.reshape(len(srcs), -1)[1], b.field(ig, 2).astype(np.float32))
+        b.finalize()
+
+
+def test_batched_converged(fk):
+    grids = [(16, 18, 14, 25.0, 25.0, 25.0)]
+    nz, nx, ny, dz, dx, dy = grids[0]
+    vel = layered_grf_cells(nz, nx, ny, seed=31, min_cells=2)
+    src = (173.0, 211.0, 96.0)
+    b = fk.Batch3D(grids, eps=5.0, convTol=0.0, maxPass=20, precision=8)
+    b.setVelocityModel(1, vel)
+    b.setSources(1, [src[0]], [src[1]], [src[2]])
+    b.solve()
+    tt = b.field(1, 1)
+    res, npass = b.solveInfo(1, 1)
+    ref = _oracle((nz, nx, ny), (dz, dx, dy), vel, src, conv_tol=0.0, max_pass=20)
+    assert res == 0.0 and npass < 20
+    assert np.max(np.abs(tt - ref)) <= 1e-12 * np.max(ref)
+    b.finalize()
