@@ -140,7 +140,7 @@ class Clocks:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons}
 
 
-def cpu_reference(grids, steps, warmup, nthreads, sample_src=1):
+def cpu_reference(grids, steps, warmup, nthreads, sample_src=24):
     """CPU restatement of the reference (oracle/), timed on a bounded sample:
     `sample_src` sources on the largest grid per step."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))

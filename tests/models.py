@@ -33,13 +33,12 @@ def layered_grf_cells(nz, nx, ny, seed=2, vels=(3000.0, 4000.0, 5000.0, 6000.0),
     nzc = nz - 1
     rng = np.random.default_rng(seed)
     nl = len(vels)
-    while True:
-        cuts = np.sort(rng.integers(min_cells, nzc - min_cells, size=nl - 1))
-        th = np.diff(np.concatenate([[0], cuts, [nzc]]))
-        if th.min() >= min_cells:
-            break
+    mc = max(1, min(min_cells, nzc // nl))
+    # each layer gets mc cells plus a seeded share of the rest
+    extra = rng.multinomial(nzc - nl * mc, np.ones(nl) / nl)
+    th = mc + extra
+    edges = np.concatenate([[0], np.cumsum(th)])
     vz = np.empty(nzc)
-    edges = np.concatenate([[0], cuts, [nzc]])
     for i in range(nl):
         vz[edges[i]:edges[i + 1]] = vels[i]
     g = gaussian_field((ny - 1, nx - 1, nzc), corr, seed)
