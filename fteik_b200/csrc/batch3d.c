@@ -42,6 +42,8 @@ static struct {
     fk_result3d_t *res_host;
     int nwork, max_nx, max_nz;
     int *work_order;        /* work item -> (grid, src) packed as grid<<20|src */
+    int *groups_dev;        /* [ngroups][S] work items walked together */
+    int ngroups, S;
     cudaGraphExec_t graph;
     bool graph_ok;
     double *export_buf;
@@ -69,6 +71,7 @@ void fteik_b200_batch3d_finalize(void)
     for (int i = 0; i < SB.ngrid; i++) free_grid(&SB.g[i]);
     free(SB.g);
     fk_dfree(SB.grids_dev); fk_dfree(SB.work_dev); fk_dfree(SB.res_dev); fk_dfree(SB.export_buf);
+    fk_dfree(SB.groups_dev);
     free(SB.res_host); free(SB.work_order);
     memset(&SB, 0, sizeof(SB));
 }
@@ -261,13 +264,33 @@ static int build_work(const char *who)
                               (g->zsi[s] - 1)];
         wh[w].tt = (char *)g->fields + fbytes * (size_t)s;
     }
-    int e = (int)cudaMemcpy(SB.grids_dev, gh, sizeof(fk_grid3d_t) * (size_t)SB.ngrid, cudaMemcpyHostToDevice);
+    /* groups of S consecutive work items of the same grid (work items are
+     * sorted by grid, so a group never spans two grids) */
+    const int S = fk3d_pick_s(SB.precision, max_nx, max_nz, nwork);
+    int *gr = (int *)malloc(sizeof(int) * (size_t)nwork * S);
+    int ng = 0;
+    for (int w = 0; w < nwork;) {
+        const int gi = SB.work_order[w] >> 20;
+        for (int k = 0; k < S; k++) {
+            if (w < nwork && (SB.work_order[w] >> 20) == gi) gr[ng * S + k] = w++;
+            else gr[ng * S + k] = -1;
+        }
+        ng++;
+    }
+    fk_dfree(SB.groups_dev);
+    SB.groups_dev = (int *)fk_dalloc(sizeof(int) * (size_t)ng * S, who);
+    int e = SB.groups_dev ? 0 : 1;
+    if (!e) e = (int)cudaMemcpy(SB.groups_dev, gr, sizeof(int) * (size_t)ng * S, cudaMemcpyHostToDevice);
+    if (!e) e = (int)cudaMemcpy(SB.grids_dev, gh, sizeof(fk_grid3d_t) * (size_t)SB.ngrid, cudaMemcpyHostToDevice);
     if (!e) e = (int)cudaMemcpy(SB.work_dev, wh, sizeof(fk_work3d_t) * (size_t)nwork, cudaMemcpyHostToDevice);
+    free(gr);
     free(gh);
     free(wh);
     SB.nwork = nwork;
     SB.max_nx = max_nx;
     SB.max_nz = max_nz;
+    SB.S = S;
+    SB.ngroups = ng;
     return fk_check(e, who);
 }
 
@@ -281,11 +304,12 @@ void fteik_b200_batch3d_solve(int *ierr)
         if (build_work(who)) return;
         /* warm the kernel attributes outside capture, then capture */
         cudaGraph_t graph;
-        int e = fk3d_prepare(SB.precision, SB.max_nx, SB.max_nz);
+        int e = fk3d_prepare(SB.precision, SB.max_nx, SB.max_nz, SB.S);
         if (!e) e = (int)cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (!e) {
-            int le = fk3d_solve(SB.precision, SB.grids_dev, SB.work_dev, SB.res_dev, SB.nwork,
-                                SB.max_nx, SB.max_nz, SB.eps, SB.nsweep, SB.conv_tol, SB.max_pass, s);
+            int le = fk3d_solve(SB.precision, SB.grids_dev, SB.work_dev, SB.groups_dev, SB.ngroups,
+                                SB.S, SB.res_dev, SB.nwork, SB.max_nx, SB.max_nz, SB.eps, SB.nsweep,
+                                SB.conv_tol, SB.max_pass, s);
             e = (int)cudaStreamEndCapture(s, &graph);
             if (!e) e = le;
         }

@@ -49,17 +49,24 @@ typedef struct {
  * nsweep passes of 8 sweeps (or, when conv_tol >= 0 and max_pass > 0,
  * passes until a pass changes no node by more than conv_tol).
  * precision: 4 (FP32 field, FP64 near-source stencil) or 8 (FP64 field).
- * grids/work/results are device arrays.  Returns a cudaError_t. */
+ * groups: device [ngroups][S] work indices of one grid each (-1 = empty);
+ * the passes run one group per CTA, S (1 or 2, see fk3d_pick_s) sources
+ * walking together.  grids/work/results are device arrays.  Returns a
+ * cudaError_t. */
 int fk3d_solve(int precision, const fk_grid3d_t *grids, const fk_work3d_t *work,
-               fk_result3d_t *results, int nwork, int max_nx, int max_nz,
-               double eps, int nsweep, double conv_tol, int max_pass,
-               cudaStream_t stream);
+               const int *groups, int ngroups, int S, fk_result3d_t *results, int nwork,
+               int max_nx, int max_nz, double eps, int nsweep, double conv_tol,
+               int max_pass, cudaStream_t stream);
+
+/* Sources per CTA for the passes: 2 when the shared memory allows it and
+ * there are at least as many work items as SMs, else 1. */
+int fk3d_pick_s(int precision, int max_nx, int max_nz, int nwork);
 
 /* Set the kernel attributes a later fk3d_solve needs (call before a CUDA
  * graph capture of fk3d_solve). */
-int fk3d_prepare(int precision, int max_nx, int max_nz);
+int fk3d_prepare(int precision, int max_nx, int max_nz, int S);
 
-/* Dynamic shared memory the solve kernels need for these sizes. */
+/* Dynamic shared memory of the initialisation kernel for these sizes. */
 size_t fk3d_smem_bytes(int precision, int max_nx, int max_nz);
 
 /* ---- 2D ---------------------------------------------------------------- */

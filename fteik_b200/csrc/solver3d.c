@@ -17,6 +17,7 @@ static struct {
     fk_grid3d_t *grid_dev;
     fk_work3d_t *work_dev;
     fk_result3d_t *res_dev;
+    int *group_dev;
     fk_result3d_t last;
 } S3 = {.precision = 4};
 
@@ -27,6 +28,7 @@ static void free_buffers(void)
     fk_dfree(S3.grid_dev); S3.grid_dev = NULL;
     fk_dfree(S3.work_dev); S3.work_dev = NULL;
     fk_dfree(S3.res_dev); S3.res_dev = NULL;
+    fk_dfree(S3.group_dev); S3.group_dev = NULL;
 }
 
 void fteik_solver3d_free(void)
@@ -167,7 +169,12 @@ static int ensure_buffers(void)
     if (!S3.grid_dev) S3.grid_dev = (fk_grid3d_t *)fk_dalloc(sizeof(fk_grid3d_t), "fteik_solver3d");
     if (!S3.work_dev) S3.work_dev = (fk_work3d_t *)fk_dalloc(sizeof(fk_work3d_t), "fteik_solver3d");
     if (!S3.res_dev) S3.res_dev = (fk_result3d_t *)fk_dalloc(sizeof(fk_result3d_t), "fteik_solver3d");
-    return !(S3.tt && S3.grid_dev && S3.work_dev && S3.res_dev);
+    if (!S3.group_dev) {
+        S3.group_dev = (int *)fk_dalloc(sizeof(int), "fteik_solver3d");
+        if (S3.group_dev && fk_check((int)cudaMemset(S3.group_dev, 0, sizeof(int)), "fteik_solver3d"))
+            return 1;
+    }
+    return !(S3.tt && S3.grid_dev && S3.work_dev && S3.res_dev && S3.group_dev);
 }
 
 void fteik_solver3d_solveSourceLSM(int isrc, int *ierr)
@@ -208,8 +215,8 @@ void fteik_solver3d_solveSourceLSM(int isrc, int *ierr)
     int e = (int)cudaMemcpyAsync(S3.grid_dev, &g, sizeof(g), cudaMemcpyHostToDevice, s);
     if (!e) e = (int)cudaMemcpyAsync(S3.work_dev, &w, sizeof(w), cudaMemcpyHostToDevice, s);
     /* the reference's 3D solver has no convergence test: nsweep passes */
-    if (!e) e = fk3d_solve(S3.precision, S3.grid_dev, S3.work_dev, S3.res_dev, 1, g.nx, g.nz,
-                          S3.eps, S3.nsweep, -1.0, 0, s);
+    if (!e) e = fk3d_solve(S3.precision, S3.grid_dev, S3.work_dev, S3.group_dev, 1, 1, S3.res_dev,
+                          1, g.nx, g.nz, S3.eps, S3.nsweep, -1.0, 0, s);
     if (!e) e = (int)cudaMemcpyAsync(&S3.last, S3.res_dev, sizeof(S3.last), cudaMemcpyDeviceToHost, s);
     if (!e) e = (int)cudaStreamSynchronize(s);
     if (fk_check(e, "fteik_solver3d_solveSourceLSM") || S3.last.status != 0) {
