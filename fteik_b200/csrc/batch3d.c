@@ -11,6 +11,7 @@
  */
 #include "host_common.h"
 #include "fteik_b200.h"
+#include "tileplan.h"
 
 #include <stdlib.h>
 #include <string.h>
@@ -44,6 +45,8 @@ static struct {
     int *work_order;        /* work item -> (grid, src) packed as grid<<20|src */
     int *groups_dev;        /* [ngroups][S] work items walked together */
     int ngroups, S;
+    fk_tileplan_t plan;     /* tile-wavefront schedule */
+    bool walker;
     cudaGraphExec_t graph;
     bool graph_ok;
     double *export_buf;
@@ -72,6 +75,7 @@ void fteik_b200_batch3d_finalize(void)
     free(SB.g);
     fk_dfree(SB.grids_dev); fk_dfree(SB.work_dev); fk_dfree(SB.res_dev); fk_dfree(SB.export_buf);
     fk_dfree(SB.groups_dev);
+    fk_tileplan_free(&SB.plan);
     free(SB.res_host); free(SB.work_order);
     memset(&SB, 0, sizeof(SB));
 }
@@ -284,6 +288,19 @@ static int build_work(const char *who)
     if (!e) e = (int)cudaMemcpy(SB.grids_dev, gh, sizeof(fk_grid3d_t) * (size_t)SB.ngrid, cudaMemcpyHostToDevice);
     if (!e) e = (int)cudaMemcpy(SB.work_dev, wh, sizeof(fk_work3d_t) * (size_t)nwork, cudaMemcpyHostToDevice);
     free(gr);
+    SB.walker = fk_schedule_walker();
+    if (!e && !SB.walker) {
+        int *wnx = (int *)malloc(sizeof(int) * (size_t)nwork);
+        int *wny = (int *)malloc(sizeof(int) * (size_t)nwork);
+        for (int w = 0; w < nwork; w++) {
+            wnx[w] = gh[wh[w].grid].nx;
+            wny[w] = gh[wh[w].grid].ny;
+        }
+        const int np = (SB.conv_tol >= 0.0 && SB.max_pass > 0) ? SB.max_pass : SB.nsweep;
+        e = fk_tileplan_build(&SB.plan, nwork, wnx, wny, np, who);
+        free(wnx);
+        free(wny);
+    }
     free(gh);
     free(wh);
     SB.nwork = nwork;
@@ -304,12 +321,17 @@ void fteik_b200_batch3d_solve(int *ierr)
         if (build_work(who)) return;
         /* warm the kernel attributes outside capture, then capture */
         cudaGraph_t graph;
-        int e = fk3d_prepare(SB.precision, SB.max_nx, SB.max_nz, SB.S);
+        int e = SB.walker ? fk3d_prepare(SB.precision, SB.max_nx, SB.max_nz, SB.S) : 0;
         if (!e) e = (int)cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (!e) {
-            int le = fk3d_solve(SB.precision, SB.grids_dev, SB.work_dev, SB.groups_dev, SB.ngroups,
+            int le;
+            if (SB.walker)
+                le = fk3d_solve(SB.precision, SB.grids_dev, SB.work_dev, SB.groups_dev, SB.ngroups,
                                 SB.S, SB.res_dev, SB.nwork, SB.max_nx, SB.max_nz, SB.eps, SB.nsweep,
                                 SB.conv_tol, SB.max_pass, s);
+            else
+                le = fk3d_solve_tiles(SB.precision, SB.grids_dev, SB.work_dev, SB.nwork, &SB.plan.dev,
+                                      SB.res_dev, SB.eps, SB.nsweep, SB.conv_tol, SB.max_pass, s);
             e = (int)cudaStreamEndCapture(s, &graph);
             if (!e) e = le;
         }

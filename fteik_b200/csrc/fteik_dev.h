@@ -69,6 +69,31 @@ int fk3d_prepare(int precision, int max_nx, int max_nz, int S);
 /* Dynamic shared memory of the initialisation kernel for these sizes. */
 size_t fk3d_smem_bytes(int precision, int max_nx, int max_nz);
 
+/* Tile-wavefront plan of a 3D solve (device buffers; see tile3d_impl.cuh).
+ * tasks: one sweep's tile tasks as int pairs {work, by' * ntx + bx'}
+ * ordered by tile level bx' + by'; done_base: each work item's first tile in
+ * done[]; the other buffers are scratch sized as noted. */
+typedef struct {
+    const int *tasks;              /* 2 * ntask_sweep ints */
+    const int *done_base;          /* nwork */
+    int ntask_sweep, ntiles_total;
+    int *done;                     /* ntiles_total */
+    unsigned long long *tickets;   /* 2 */
+    int *error;                    /* 1 */
+    unsigned long long *resid;     /* nwork * max(npass, 1) */
+    int *pass_tiles;               /* nwork * max(npass, 1) */
+    int *conv_pass;                /* nwork */
+    long long spin_limit;          /* bounded waits: polls before giving up */
+} fk_tiles3d_t;
+
+#define FK_TILE_X 32
+#define FK_TILE_Y 8
+
+/* Tile-wavefront solve of every work item (same semantics as fk3d_solve). */
+int fk3d_solve_tiles(int precision, const fk_grid3d_t *grids, const fk_work3d_t *work,
+                     int nwork, const fk_tiles3d_t *plan, fk_result3d_t *results, double eps,
+                     int nsweep, double conv_tol, int max_pass, cudaStream_t stream);
+
 /* ---- 2D ---------------------------------------------------------------- */
 typedef struct {
     int nz, nx, zp, zcp;

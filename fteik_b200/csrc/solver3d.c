@@ -4,6 +4,7 @@
  */
 #include "host_common.h"
 #include "fteik_b200.h"
+#include "tileplan.h"
 
 #include <stdlib.h>
 #include <string.h>
@@ -18,6 +19,8 @@ static struct {
     fk_work3d_t *work_dev;
     fk_result3d_t *res_dev;
     int *group_dev;
+    fk_tileplan_t plan;
+    int plan_npass;
     fk_result3d_t last;
 } S3 = {.precision = 4};
 
@@ -29,6 +32,8 @@ static void free_buffers(void)
     fk_dfree(S3.work_dev); S3.work_dev = NULL;
     fk_dfree(S3.res_dev); S3.res_dev = NULL;
     fk_dfree(S3.group_dev); S3.group_dev = NULL;
+    fk_tileplan_free(&S3.plan);
+    S3.plan_npass = 0;
 }
 
 void fteik_solver3d_free(void)
@@ -215,8 +220,20 @@ void fteik_solver3d_solveSourceLSM(int isrc, int *ierr)
     int e = (int)cudaMemcpyAsync(S3.grid_dev, &g, sizeof(g), cudaMemcpyHostToDevice, s);
     if (!e) e = (int)cudaMemcpyAsync(S3.work_dev, &w, sizeof(w), cudaMemcpyHostToDevice, s);
     /* the reference's 3D solver has no convergence test: nsweep passes */
-    if (!e) e = fk3d_solve(S3.precision, S3.grid_dev, S3.work_dev, S3.group_dev, 1, 1, S3.res_dev,
-                          1, g.nx, g.nz, S3.eps, S3.nsweep, -1.0, 0, s);
+    if (!e && fk_schedule_walker()) {
+        e = fk3d_solve(S3.precision, S3.grid_dev, S3.work_dev, S3.group_dev, 1, 1, S3.res_dev, 1,
+                       g.nx, g.nz, S3.eps, S3.nsweep, -1.0, 0, s);
+    } else if (!e) {
+        if (!S3.plan.mem || S3.plan_npass < S3.nsweep) {
+            if (fk_tileplan_build(&S3.plan, 1, &g.nx, &g.ny, S3.nsweep, "fteik_solver3d")) {
+                *ierr = 1;
+                return;
+            }
+            S3.plan_npass = S3.nsweep;
+        }
+        e = fk3d_solve_tiles(S3.precision, S3.grid_dev, S3.work_dev, 1, &S3.plan.dev, S3.res_dev,
+                             S3.eps, S3.nsweep, -1.0, 0, s);
+    }
     if (!e) e = (int)cudaMemcpyAsync(&S3.last, S3.res_dev, sizeof(S3.last), cudaMemcpyDeviceToHost, s);
     if (!e) e = (int)cudaStreamSynchronize(s);
     if (fk_check(e, "fteik_solver3d_solveSourceLSM") || S3.last.status != 0) {

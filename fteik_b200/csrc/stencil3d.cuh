@@ -1,0 +1,264 @@
+/*
+ * stencil3d.cuh -- the 3D node updates of the reference's local solver
+ * (localSolver.F90:384-959) for the CUDA sweep kernels, templated on the
+ * working precision.  Every expression keeps the reference's operand order.
+ */
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "fteik_dev.h"
+
+namespace fk3 {
+
+constexpr int kMaxWarps = 32;
+
+template <typename R>
+struct Mesh {
+    R dz, dx, dy;
+    R dz2i, dx2i, dy2i, dsum_nine, dsumi, dz2dx2, dz2dy2, dx2dy2;
+    R dz2i_dx2i, dz2i_dy2i, dx2i_dy2i;
+    R dz2i_p_dx2i, dz2i_p_dy2i, dx2i_p_dy2i;
+    R dz2i_p_dx2i_inv, dz2i_p_dy2i_inv, dx2i_p_dy2i_inv;
+};
+
+/* localSolver.F90:905-931: the mesh constants, derived in FP64 and rounded
+ * once to the working precision. */
+template <typename R>
+__device__ void make_mesh(Mesh<R> &m, double dz, double dx, double dy)
+{
+    double dz2 = dz * dz, dx2 = dx * dx, dy2 = dy * dy;
+    double dz2i = 1.0 / dz2, dx2i = 1.0 / dx2, dy2i = 1.0 / dy2;
+    double dsum = dz2i + dx2i + dy2i;
+    m.dz = (R)dz; m.dx = (R)dx; m.dy = (R)dy;
+    m.dz2i = (R)dz2i; m.dx2i = (R)dx2i; m.dy2i = (R)dy2i;
+    m.dsum_nine = (R)(dsum * 9.0);
+    m.dsumi = (R)(1.0 / dsum);
+    m.dz2dx2 = (R)(1.0 / (dz2 * dx2));
+    m.dz2dy2 = (R)(1.0 / (dz2 * dy2));
+    m.dx2dy2 = (R)(1.0 / (dx2 * dy2));
+    m.dz2i_dx2i = (R)(dz2i * dx2i);
+    m.dz2i_dy2i = (R)(dz2i * dy2i);
+    m.dx2i_dy2i = (R)(dx2i * dy2i);
+    m.dz2i_p_dx2i = (R)(dz2i + dx2i);
+    m.dz2i_p_dy2i = (R)(dz2i + dy2i);
+    m.dx2i_p_dy2i = (R)(dx2i + dy2i);
+    m.dz2i_p_dx2i_inv = (R)(1.0 / (dz2i + dx2i));
+    m.dz2i_p_dy2i_inv = (R)(1.0 / (dz2i + dy2i));
+    m.dx2i_p_dy2i_inv = (R)(1.0 / (dx2i + dy2i));
+}
+
+__device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); }
+__device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
+template <typename R> __device__ __forceinline__ R rmin(R a, R b) { return (b < a) ? b : a; }
+template <typename R> __device__ __forceinline__ R rmax(R a, R b) { return (b > a) ? b : a; }
+
+/* localSolver.F90:384-534, one node; tupd enters as the node's time. */
+template <typename R>
+__device__ __forceinline__ R noinit(const Mesh<R> &c, R tv, R te, R tn, R tev,
+                                    R ten, R tnv, R tnve, R s1, R s2, R s3,
+                                    R s4, R s5, R s6, R s7, R tupd)
+{
+    const R HUGEV = (R)FK_HUGE;
+    R t12min = tv + c.dz * s1;
+    t12min = rmin(t12min, te + c.dx * s2);
+    t12min = rmin(t12min, tn + c.dy * s3);
+    R temtv = te - tv;
+    if (temtv < c.dz * s4 && -temtv < c.dx * s4) {
+        R ta = tev + temtv, tb = tev - temtv, tab = ta - tb;
+        R t = ((tb * c.dz2i + ta * c.dx2i) +
+               rsqrt_((R)4 * (s4 * s4) * c.dz2i_p_dx2i - c.dz2i_dx2i * (tab * tab))) *
+              c.dz2i_p_dx2i_inv;
+        t12min = rmin(t12min, t);
+    }
+    R tvmtn = tv - tn;
+    if (tvmtn < c.dy * s5 && -tvmtn < c.dz * s5) {
+        R ta = tvmtn + tnv, tb = -tvmtn + tnv, tab = ta - tb;
+        R t = ((ta * c.dz2i + tb * c.dy2i) +
+               rsqrt_((R)4 * (s5 * s5) * c.dz2i_p_dy2i - c.dz2i_dy2i * (tab * tab))) *
+              c.dz2i_p_dy2i_inv;
+        t12min = rmin(t12min, t);
+    }
+    R temtn = te - tn;
+    if (temtn < c.dy * s6 && -temtn < c.dx * s6) {
+        R ta = temtn + ten, tb = -temtn + ten, tab = ta - tb;
+        R t = ((ta * c.dx2i + tb * c.dy2i) +
+               rsqrt_((R)4 * (s6 * s6) * c.dx2i_p_dy2i - c.dx2i_dy2i * (tab * tab))) *
+              c.dx2i_p_dy2i_inv;
+        t12min = rmin(t12min, t);
+    }
+    R t3d = HUGEV;
+    R tmax = rmax(rmax(tv, te), tn);
+    if (t12min > tmax) {
+        R ta = te + (R)0.5 * (-tn + ten - tv + tev) - tnv + tnve;
+        R tb = tv + (R)0.5 * (-tn + tnv - te + tev) - ten + tnve;
+        R tc = tn + (R)0.5 * (-te + ten - tv + tnv) - tev + tnve;
+        R tab = ta - tb, tbc = tb - tc, tac = ta - tc;
+        R t2 = (s7 * s7) * c.dsum_nine;
+        R t3 = c.dz2dx2 * (tab * tab) + c.dz2dy2 * (tbc * tbc) + c.dx2dy2 * (tac * tac);
+        if (t2 >= t3) {
+            R t1 = tb * c.dz2i + ta * c.dx2i + tc * c.dy2i;
+            t3d = (t1 + rsqrt_(t2 - t3)) * c.dsumi;
+        }
+    }
+    t3d = rmin(t3d, t12min);
+    return rmin(tupd, t3d);
+}
+
+/* Source description used by the initialisation stencil. */
+struct Src {
+    int zsi, xsi, ysi;
+    double zsa, xsa, ysa, szero, szero2, eps_t;
+};
+
+/* localSolver.F90:775-792 */
+template <typename R>
+__device__ __forceinline__ R tana(const Src &q, const Mesh<R> &c, int i, int j, int k)
+{
+    R dz_ = ((R)i - (R)q.zsa) * c.dz;
+    R dx_ = ((R)j - (R)q.xsa) * c.dx;
+    R dy_ = ((R)k - (R)q.ysa) * c.dy;
+    return (R)q.szero * rsqrt_(dz_ * dz_ + dx_ * dx_ + dy_ * dy_);
+}
+
+/* localSolver.F90:538-751, one node.  lcart is the Cartesian/spherical
+ * switch (tmin > epsSolver), evaluated by the caller in FP64. */
+template <typename R>
+__device__ R init_node(const Src &q, const Mesh<R> &c, bool lcart, R tv, R te,
+                       R tn, R tev, R ten, R tnv, R tnve, R tt0, R slow1,
+                       R slow2, R slow3, R slow4, R slow5, R slow6, R slow7,
+                       int i, int j, int k, int sz, int sx, int sy)
+{
+    const R HUGEV = (R)FK_HUGE;
+    const R szero2 = (R)q.szero2;
+    R sgnrz_dzi = (R)sz / c.dz, sgnrx_dxi = (R)sx / c.dx, sgnry_dyi = (R)sy / c.dy;
+    R t1d = tv + c.dz * slow1;
+    t1d = rmin(t1d, te + c.dx * slow2);
+    t1d = rmin(t1d, tn + c.dy * slow3);
+    R tmax = rmax(rmax(tv, te), tn);
+    R t0c = 0, tzc = 0, txc = 0, tyc = 0;
+    R tauv = HUGEV, taue = HUGEV, taun = HUGEV, tauev = HUGEV, tauen = HUGEV,
+      taunv = HUGEV, taunve = HUGEV;
+    if (!lcart) {
+        /* localSolver.F90:819-851 (tAnaD) */
+        R dz_ = ((R)i - (R)q.zsa) * c.dz;
+        R dx_ = ((R)j - (R)q.xsa) * c.dx;
+        R dy_ = ((R)k - (R)q.ysa) * c.dy;
+        R d0 = dz_ * dz_ + dx_ * dx_ + dy_ * dy_;
+        R d0i_szero = 0;
+        if (d0 > (R)0) {
+            R sq = rsqrt_(d0);
+            t0c = (R)q.szero * sq;
+            d0i_szero = (R)q.szero / sq;
+        }
+        tzc = d0i_szero * dz_;
+        txc = d0i_szero * dx_;
+        tyc = d0i_szero * dy_;
+        tauv = tv - tana(q, c, i - sz, j, k);
+        taue = te - tana(q, c, i, j - sx, k);
+        taun = tn - tana(q, c, i, j, k - sy);
+        tauev = tev - tana(q, c, i - sz, j - sx, k);
+        tauen = ten - tana(q, c, i, j - sx, k - sy);
+        taunv = tnv - tana(q, c, i - sz, j, k - sy);
+        taunve = tnve - tana(q, c, i - sz, j - sx, k - sy);
+    }
+    bool ldoZX = (tv < te + c.dx * slow4) && (te < tv + c.dz * slow4);
+    bool ldoZY = (tv < tn + c.dy * slow5) && (tn < tv + c.dz * slow5);
+    bool ldoXY = (te < tn + c.dy * slow6) && (tn < te + c.dx * slow6);
+    bool zxc = ldoZX && (lcart || k != q.ysi);
+    bool zyc = ldoZY && (lcart || j != q.xsi);
+    bool xyc = ldoXY && (lcart || i != q.zsi);
+    bool zxs = ldoZX && !zxc, zys = ldoZY && !zyc, xys = ldoXY && !xyc;
+    R t1_2d = HUGEV;
+    if (zxc) {
+        R ta = tev + te - tv, tb = tev - te + tv, tab = ta - tb;
+        t1_2d = ((tb * c.dz2i + ta * c.dx2i) +
+                 rsqrt_((R)4 * (slow4 * slow4) * c.dz2i_p_dx2i - c.dz2i_dx2i * (tab * tab))) *
+                c.dz2i_p_dx2i_inv;
+    }
+    if (zxs) {
+        R sref2 = slow4 * slow4;
+        R ta = tauev + taue - tauv, tb = tauev - taue + tauv;
+        R apoly = c.dz2i_p_dx2i;
+        R bpoly = (R)4 * (sgnrx_dxi * txc + sgnrz_dzi * tzc) - (R)2 * (ta * c.dx2i + tb * c.dz2i);
+        R cpoly = ((ta * ta) * c.dx2i) + ((tb * tb) * c.dz2i) -
+                  (R)4 * (sgnrx_dxi * txc * ta + sgnrz_dzi * tzc * tb) +
+                  (R)4 * (szero2 - sref2 + tyc * tyc);
+        R dpoly = bpoly * bpoly - (R)4 * apoly * cpoly;
+        if (dpoly >= (R)0) t1_2d = (rsqrt_(dpoly) - bpoly) / ((R)2 * apoly) + t0c;
+        if (t1_2d < tv || t1_2d < te) t1_2d = HUGEV;
+    }
+    R tmin12 = rmin(t1d, t1_2d);
+    R t2_2d = HUGEV;
+    if (zyc) {
+        R ta = tv - tn + tnv, tb = tn - tv + tnv, tab = ta - tb;
+        t2_2d = ((ta * c.dz2i + tb * c.dy2i) +
+                 rsqrt_((R)4 * (slow5 * slow5) * c.dz2i_p_dy2i - c.dz2i_dy2i * (tab * tab))) *
+                c.dz2i_p_dy2i_inv;
+    }
+    if (zys) {
+        R sref2 = slow5 * slow5;
+        R ta = tauv - taun + taunv, tb = taun - tauv + taunv;
+        R apoly = c.dz2i_p_dy2i;
+        R bpoly = (R)4 * (sgnry_dyi * tyc + sgnrz_dzi * tzc) - (R)2 * (ta * c.dz2i + tb * c.dy2i);
+        R cpoly = ((ta * ta) * c.dz2i) + ((tb * tb) * c.dy2i) -
+                  (R)4 * (sgnrz_dzi * tzc * ta + sgnry_dyi * tyc * tb) +
+                  (R)4 * (szero2 - sref2 + txc * txc);
+        R dpoly = bpoly * bpoly - (R)4 * apoly * cpoly;
+        if (dpoly >= (R)0) t2_2d = (rsqrt_(dpoly) - bpoly) / ((R)2 * apoly) + t0c;
+        if (t2_2d < tv || t2_2d < tn) t2_2d = HUGEV;
+    }
+    tmin12 = rmin(tmin12, t2_2d);
+    R t3_2d = HUGEV;
+    if (xyc) {
+        R ta = te - tn + ten, tb = tn - te + ten, tab = ta - tb;
+        t3_2d = ((ta * c.dx2i + tb * c.dy2i) +
+                 rsqrt_((R)4 * (slow6 * slow6) * c.dx2i_p_dy2i - c.dx2i_dy2i * (tab * tab))) *
+                c.dx2i_p_dy2i_inv;
+    }
+    if (xys) {
+        R sref2 = slow6 * slow6;
+        R ta = taue - taun + tauen, tb = taun - taue + tauen;
+        R apoly = c.dx2i_p_dy2i;
+        R bpoly = (R)4 * (sgnry_dyi * tyc + sgnrx_dxi * txc) - (R)2 * (ta * c.dx2i + tb * c.dy2i);
+        R cpoly = ((ta * ta) * c.dx2i) + ((tb * tb) * c.dy2i) -
+                  (R)4 * (sgnrx_dxi * txc * ta + sgnry_dyi * tyc * tb) +
+                  (R)4 * (szero2 - sref2 + tzc * tzc);
+        R dpoly = bpoly * bpoly - (R)4 * apoly * cpoly;
+        if (dpoly >= (R)0) t3_2d = (rsqrt_(dpoly) - bpoly) / ((R)2 * apoly) + t0c;
+        if (t3_2d < te || t3_2d < tn) t3_2d = HUGEV;
+    }
+    tmin12 = rmin(tmin12, t3_2d);
+    R t3d = HUGEV;
+    bool ldo3D = tmin12 > tmax;
+    if (ldo3D && lcart) {
+        R ta = te + (R)0.5 * (-tn + ten - tv + tev) - tnv + tnve;
+        R tb = tv + (R)0.5 * (-tn + tnv - te + tev) - ten + tnve;
+        R tc = tn + (R)0.5 * (-te + ten - tv + tnv) - tev + tnve;
+        R tab = ta - tb, tbc = tb - tc, tac = ta - tc;
+        R t2 = (slow7 * slow7) * c.dsum_nine;
+        R t3 = c.dz2dx2 * (tab * tab) + c.dz2dy2 * (tbc * tbc) + c.dx2dy2 * (tac * tac);
+        if (t2 >= t3) {
+            R t1 = tb * c.dz2i + ta * c.dx2i + tc * c.dy2i;
+            t3d = (t1 + rsqrt_(t2 - t3)) * c.dsumi;
+        }
+    }
+    if (ldo3D && !lcart) {
+        R sref2 = slow7 * slow7;
+        R ta = taue + (R)0.5 * (-taun + tauen - tauv + tauev) - taunv + taunve;
+        R tb = tauv + (R)0.5 * (-taun + taunv - taue + tauev) - tauen + taunve;
+        R tc = taun + (R)0.5 * (-taue + tauen - tauv + taunv) - tauev + taunve;
+        R apoly = c.dx2i + c.dz2i + c.dy2i;
+        R bpoly = (R)6 * (sgnrz_dzi * tzc + sgnry_dyi * tyc + sgnrx_dxi * txc) -
+                  (R)2 * (ta * c.dx2i + tb * c.dz2i + tc * c.dy2i);
+        R cpoly = ((ta * ta) * c.dx2i) + ((tb * tb) * c.dz2i) + ((tc * tc) * c.dy2i) -
+                  (R)6 * (sgnrx_dxi * txc * ta + sgnrz_dzi * tzc * tb + sgnry_dyi * tyc * tc) +
+                  (R)9 * (szero2 - sref2);
+        R dpoly = bpoly * bpoly - (R)4 * apoly * cpoly;
+        if (dpoly >= (R)0) t3d = (rsqrt_(dpoly) - bpoly) / ((R)2 * apoly) + t0c;
+        if (t3d < te || t3d < tn || t3d < tv) t3d = HUGEV;
+    }
+    R tupd = rmin(tmin12, t3d);
+    return rmin(tt0, tupd);
+}
+
+} // namespace fk3

@@ -4,6 +4,7 @@
  * corners, the near-source spherical stencil and the convergence residual.
  */
 #include "sweep3d_impl.cuh"
+#include "tile3d_impl.cuh"
 
 extern "C" int fk3d_solve_f64(const fk_grid3d_t *grids, const fk_work3d_t *work,
                               const int *groups, int ngroups, int S, fk_result3d_t *results,
@@ -45,4 +46,21 @@ extern "C" size_t fk3d_smem_bytes(int precision, int max_nx, int max_nz)
 {
     const int nt = ((max_nx + 31) / 32) * 32;
     return precision == 8 ? fk3::smem_need<double, 1>(nt, max_nz) : fk3::smem_need<float, 1>(nt, max_nz);
+}
+
+extern "C" int fk3d_solve_tiles_f64(const fk_grid3d_t *grids, const fk_work3d_t *work, int nwork,
+                                    const fk_tiles3d_t *plan, fk_result3d_t *results, double eps,
+                                    int nsweep, double conv_tol, int max_pass, cudaStream_t stream);
+
+extern "C" int fk3d_solve_tiles(int precision, const fk_grid3d_t *grids, const fk_work3d_t *work,
+                                int nwork, const fk_tiles3d_t *plan, fk_result3d_t *results,
+                                double eps, int nsweep, double conv_tol, int max_pass,
+                                cudaStream_t stream)
+{
+    if (precision == 8)
+        return fk3d_solve_tiles_f64(grids, work, nwork, plan, results, eps, nsweep, conv_tol,
+                                    max_pass, stream);
+    if (precision != 4) return (int)cudaErrorInvalidValue;
+    return fk3tw::launch_tiles<float>(grids, work, nwork, plan, results, eps, nsweep, conv_tol,
+                                      max_pass, stream);
 }

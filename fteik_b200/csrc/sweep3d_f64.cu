@@ -5,6 +5,7 @@
  * and offered as a full-precision mode.
  */
 #include "sweep3d_impl.cuh"
+#include "tile3d_impl.cuh"
 
 extern "C" int fk3d_solve_f64(const fk_grid3d_t *grids, const fk_work3d_t *work,
                               const int *groups, int ngroups, int S, fk_result3d_t *results,
@@ -23,4 +24,12 @@ extern "C" int fk3d_prepare_f64(int max_nx, int max_nz, int S)
 extern "C" int fk3d_pick_s_f64(int max_nx, int max_nz, int nwork, int nsm)
 {
     return fk3::pick_s<double>(max_nx, max_nz, nwork, nsm);
+}
+
+extern "C" int fk3d_solve_tiles_f64(const fk_grid3d_t *grids, const fk_work3d_t *work, int nwork,
+                                    const fk_tiles3d_t *plan, fk_result3d_t *results, double eps,
+                                    int nsweep, double conv_tol, int max_pass, cudaStream_t stream)
+{
+    return fk3tw::launch_tiles<double>(grids, work, nwork, plan, results, eps, nsweep, conv_tol,
+                                       max_pass, stream);
 }
