@@ -47,6 +47,7 @@ static struct {
     int ngroups, S;
     fk_tileplan_t plan;     /* tile-wavefront schedule */
     bool walker;
+    bool work_dirty;        /* source positions changed, shape unchanged */
     cudaGraphExec_t graph;
     bool graph_ok;
     double *export_buf;
@@ -155,6 +156,7 @@ void fteik_b200_batch3d_setVelocityModel64f(int igrid, int ncell, const double v
     if (fk_check(e, who)) return;
     g->have_model = true;
     SB.solved = false;
+    SB.work_dirty = true; /* szero of this grid's sources */
     *ierr = 0;
 }
 
@@ -166,8 +168,9 @@ void fteik_b200_batch3d_setSources64f(int igrid, int nsrc, const double zsrc[],
     bgrid_t *g = grid_of(igrid, who);
     if (!g) return;
     if (nsrc < 1) { FK_ERR("%s: No sources", who); return; }
+    const bool same_shape = g->fields != NULL && nsrc == g->nsrc;
     free(g->zsi); free(g->xsi); free(g->ysi); free(g->zsa); free(g->xsa); free(g->ysa);
-    fk_dfree(g->fields); g->fields = NULL;
+    if (!same_shape) { fk_dfree(g->fields); g->fields = NULL; }
     g->nsrc = 0;
     g->zsi = (int *)malloc(sizeof(int) * (size_t)nsrc);
     g->xsi = (int *)malloc(sizeof(int) * (size_t)nsrc);
@@ -181,10 +184,17 @@ void fteik_b200_batch3d_setSources64f(int igrid, int nsrc, const double zsrc[],
                            &g->xsa[i], &g->ysa[i]))
             return;
     const size_t fbytes = (size_t)g->zp * g->nx * g->ny * (size_t)SB.precision;
-    g->fields = fk_dalloc(fbytes * (size_t)nsrc, who);
+    if (!g->fields) g->fields = fk_dalloc(fbytes * (size_t)nsrc, who);
     if (!g->fields) return;
     g->nsrc = nsrc;
-    invalidate();
+    if (same_shape) {
+        /* same work list: the captured graph stays valid, only the work
+         * descriptors it reads change */
+        SB.work_dirty = true;
+        SB.solved = false;
+    } else {
+        invalidate();
+    }
     *ierr = 0;
 }
 
@@ -224,6 +234,31 @@ static int cmp_work(const void *a, const void *b)
     return (*(const int *)a) - (*(const int *)b);
 }
 
+static void fill_work(fk_work3d_t *wh)
+{
+    for (int w = 0; w < SB.nwork; w++) {
+        const int i = SB.work_order[w] >> 20, s = SB.work_order[w] & ((1 << 20) - 1);
+        bgrid_t *g = &SB.g[i];
+        const size_t fbytes = (size_t)g->zp * g->nx * g->ny * (size_t)SB.precision;
+        wh[w].grid = i;
+        wh[w].zsi = g->zsi[s]; wh[w].xsi = g->xsi[s]; wh[w].ysi = g->ysi[s];
+        wh[w].zsa = g->zsa[s]; wh[w].xsa = g->xsa[s]; wh[w].ysa = g->ysa[s];
+        wh[w].szero = g->slow[((long)(g->ysi[s] - 1) * (g->nx - 1) + (g->xsi[s] - 1)) * (g->nz - 1) +
+                              (g->zsi[s] - 1)];
+        wh[w].tt = (char *)g->fields + fbytes * (size_t)s;
+    }
+}
+
+static int upload_work(const char *who)
+{
+    fk_work3d_t *wh = (fk_work3d_t *)malloc(sizeof(fk_work3d_t) * (size_t)SB.nwork);
+    fill_work(wh);
+    int e = (int)cudaMemcpy(SB.work_dev, wh, sizeof(fk_work3d_t) * (size_t)SB.nwork, cudaMemcpyHostToDevice);
+    free(wh);
+    SB.work_dirty = false;
+    return fk_check(e, who);
+}
+
 static int build_work(const char *who)
 {
     int nwork = 0, max_nx = 0, max_nz = 0;
@@ -257,17 +292,8 @@ static int build_work(const char *who)
         for (int s = 0; s < g->nsrc; s++) SB.work_order[k++] = (i << 20) | s;
     }
     qsort(SB.work_order, (size_t)nwork, sizeof(int), cmp_work);
-    for (int w = 0; w < nwork; w++) {
-        const int i = SB.work_order[w] >> 20, s = SB.work_order[w] & ((1 << 20) - 1);
-        bgrid_t *g = &SB.g[i];
-        const size_t fbytes = (size_t)g->zp * g->nx * g->ny * (size_t)SB.precision;
-        wh[w].grid = i;
-        wh[w].zsi = g->zsi[s]; wh[w].xsi = g->xsi[s]; wh[w].ysi = g->ysi[s];
-        wh[w].zsa = g->zsa[s]; wh[w].xsa = g->xsa[s]; wh[w].ysa = g->ysa[s];
-        wh[w].szero = g->slow[((long)(g->ysi[s] - 1) * (g->nx - 1) + (g->xsi[s] - 1)) * (g->nz - 1) +
-                              (g->zsi[s] - 1)];
-        wh[w].tt = (char *)g->fields + fbytes * (size_t)s;
-    }
+    SB.nwork = nwork;
+    fill_work(wh);
     /* groups of S consecutive work items of the same grid (work items are
      * sorted by grid, so a group never spans two grids) */
     const int S = fk3d_pick_s(SB.precision, max_nx, max_nz, nwork);
@@ -317,8 +343,12 @@ void fteik_b200_batch3d_solve(int *ierr)
     *ierr = 1;
     if (!SB.init) { FK_ERR("%s: batch not initialized", who); return; }
     cudaStream_t s = fk_stream();
+    if (SB.graph_ok && SB.work_dirty) {
+        if (upload_work(who)) return;
+    }
     if (!SB.graph_ok) {
         if (build_work(who)) return;
+        SB.work_dirty = false;
         /* warm the kernel attributes outside capture, then capture */
         cudaGraph_t graph;
         int e = SB.walker ? fk3d_prepare(SB.precision, SB.max_nx, SB.max_nz, SB.S) : 0;

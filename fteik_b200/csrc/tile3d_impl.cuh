@@ -128,6 +128,32 @@ __device__ double tile_sweep(const fk_grid3d_t &g, R *__restrict__ tt, const R *
     const unsigned FULL = 0xffffffffu;
     const int zoff = (sz > 0) ? 0 : zp - nz; /* padded walk: dummy positions */
     const int nsteps = zp + (TX - 1) + (TY - 1);
+    const bool edge_x = ox == 0, edge_y = oy == 0;
+    const bool has_x = xlog >= 1, has_y = ylog >= 1;
+
+    /* Global operands of a walk position, loaded one step ahead. */
+    struct Pre {
+        R told, te, tn, ten;
+        R uuu, duu, uud, dud, udu, ddu, udd; /* slowness s<z><x><y> */
+    };
+    auto fetch = [&](int qpos, Pre &f) {
+        const int iz = (sz > 0) ? qpos : zp - 1 - qpos;
+        if (!(col && qpos >= 0 && qpos < zp && iz < nz)) return;
+        f.told = ldcg(tt + cbase + iz);
+        if (edge_x) f.te = has_x ? ldcg(tt + cbase_x + iz) : HUGEV;
+        if (edge_y) f.tn = has_y ? ldcg(tt + cbase_y + iz) : HUGEV;
+        if (edge_x && edge_y) f.ten = (has_x && has_y) ? ldcg(tt + cbase_xy + iz) : HUGEV;
+        if (colupd && qpos - zoff >= loz) {
+            const int czU = (sz > 0) ? iz - 1 : iz;
+            const int czD = min(max((sz > 0) ? iz : iz - 1, 0), nz - 2);
+            f.uuu = __ldg(slow + sUU + czU); f.duu = __ldg(slow + sUU + czD);
+            f.uud = __ldg(slow + sUD + czU); f.dud = __ldg(slow + sUD + czD);
+            f.udu = __ldg(slow + sDU + czU); f.ddu = __ldg(slow + sDU + czD);
+            f.udd = __ldg(slow + sDD + czU);
+        }
+    };
+    Pre cur, nxt;
+    fetch(0 - ox - oy, nxt);
 
     R r_last = HUGEV, te_last = HUGEV, tn_last = HUGEV, ten_last = HUGEV;
     double dmax = 0.0;
@@ -136,61 +162,51 @@ __device__ double tile_sweep(const fk_grid3d_t &g, R *__restrict__ tt, const R *
         const R sh_r = __shfl_sync(FULL, r_last, srcx & 31);
         const R sh_tn = __shfl_sync(FULL, tn_last, srcx & 31);
         const int qpos = st - ox - oy;
+        cur = nxt;
+        fetch(qpos + 1, nxt);
         R te = HUGEV, tn = HUGEV, ten = HUGEV, result = r_last;
-        if (col && qpos >= 0 && qpos < zp) {
-            const int iz = (sz > 0) ? qpos : zp - 1 - qpos;
+        const int iz = (sz > 0) ? qpos : zp - 1 - qpos;
+        if (col && qpos >= 0 && qpos < zp && iz < nz) {
             const int il = qpos - zoff; /* logical unpadded z */
-            const bool real = iz < nz;
-            if (real) {
-                const R told = ldcg(tt + cbase + iz);
-                result = told;
-                /* every real node gathers its upwind values: downstream lanes
-                 * and warps take them over even where this node is not updated */
-                te = (ox > 0) ? sh_r : (xlog >= 1 ? ldcg(tt + cbase_x + iz) : HUGEV);
-                tn = (oy > 0) ? xr[pp][wy][tx] : (ylog >= 1 ? ldcg(tt + cbase_y + iz) : HUGEV);
-                ten = (oy > 0) ? xte[pp][wy][tx]
-                               : ((ox > 0) ? sh_tn
-                                           : ((xlog >= 1 && ylog >= 1) ? ldcg(tt + cbase_xy + iz) : HUGEV));
-                if (colupd && il >= loz) {
-                    const int czU = (sz > 0) ? iz - 1 : iz;
-                    const int czD = min(max((sz > 0) ? iz : iz - 1, 0), nz - 2);
-                    const R s_UUU = __ldg(slow + sUU + czU), s_DUU = __ldg(slow + sUU + czD);
-                    const R s_UUD = __ldg(slow + sUD + czU), s_DUD = __ldg(slow + sUD + czD);
-                    const R s_UDU = __ldg(slow + sDU + czU), s_DDU = __ldg(slow + sDU + czD);
-                    const R s_UDD = __ldg(slow + sDD + czU);
-                    const R s1 = rmin(rmin(s_UUU, s_UUD), rmin(s_UDU, s_UDD));
-                    const R s2 = rmin(rmin(s_UUU, s_UUD), rmin(s_DUU, s_DUD));
-                    const R s3 = rmin(rmin(s_UUU, s_UDU), rmin(s_DUU, s_DDU));
-                    const R s4 = rmin(s_UUU, s_UUD);
-                    const R s5 = rmin(s_UUU, s_UDU);
-                    const R s6 = rmin(s_UUU, s_DUU);
-                    const R s7 = s_UUU;
-                    const R tv = r_last, tev = te_last, tnv = tn_last, tnve = ten_last;
-                    R r;
-                    if (!INIT) {
-                        r = fk3::noinit(mesh, tv, te, tn, tev, ten, tnv, tnve, s1, s2, s3, s4, s5, s6,
-                                        s7, told);
-                    } else {
-                        const double tmin = (double)rmin(rmin(tv, te), tn);
-                        const bool lcart = tmin > q.eps_t;
-                        if (lcart || sizeof(R) == 8)
-                            r = fk3::init_node<R>(q, mesh, lcart, tv, te, tn, tev, ten, tnv, tnve,
-                                                  told, s1, s2, s3, s4, s5, s6, s7, iz + 1, x + 1,
-                                                  y + 1, sz, sx, sy);
-                        else /* near-source spherical stencil in FP64 */
-                            r = (R)fk3::init_node<double>(
-                                q, mesh64, lcart, (double)tv, (double)te, (double)tn, (double)tev,
-                                (double)ten, (double)tnv, (double)tnve, (double)told, (double)s1,
-                                (double)s2, (double)s3, (double)s4, (double)s5, (double)s6,
-                                (double)s7, iz + 1, x + 1, y + 1, sz, sx, sy);
-                    }
-                    if (r != told) {
-                        tt[cbase + iz] = r;
-                        const double d = fabs((double)r - (double)told);
-                        dmax = d > dmax ? d : dmax;
-                    }
-                    result = r;
+            const R told = cur.told;
+            result = told;
+            /* every real node gathers its upwind values: downstream lanes
+             * and warps take them over even where this node is not updated */
+            te = edge_x ? cur.te : sh_r;
+            tn = edge_y ? cur.tn : xr[pp][wy][tx];
+            ten = !edge_y ? xte[pp][wy][tx] : (!edge_x ? sh_tn : cur.ten);
+            if (colupd && il >= loz) {
+                const R s1 = rmin(rmin(cur.uuu, cur.uud), rmin(cur.udu, cur.udd));
+                const R s2 = rmin(rmin(cur.uuu, cur.uud), rmin(cur.duu, cur.dud));
+                const R s3 = rmin(rmin(cur.uuu, cur.udu), rmin(cur.duu, cur.ddu));
+                const R s4 = rmin(cur.uuu, cur.uud);
+                const R s5 = rmin(cur.uuu, cur.udu);
+                const R s6 = rmin(cur.uuu, cur.duu);
+                const R s7 = cur.uuu;
+                const R tv = r_last, tev = te_last, tnv = tn_last, tnve = ten_last;
+                R r;
+                if (!INIT) {
+                    r = fk3::noinit(mesh, tv, te, tn, tev, ten, tnv, tnve, s1, s2, s3, s4, s5, s6, s7,
+                                    told);
+                } else {
+                    const double tmin = (double)rmin(rmin(tv, te), tn);
+                    const bool lcart = tmin > q.eps_t;
+                    if (lcart || sizeof(R) == 8)
+                        r = fk3::init_node<R>(q, mesh, lcart, tv, te, tn, tev, ten, tnv, tnve, told, s1,
+                                              s2, s3, s4, s5, s6, s7, iz + 1, x + 1, y + 1, sz, sx, sy);
+                    else /* near-source spherical stencil in FP64 */
+                        r = (R)fk3::init_node<double>(
+                            q, mesh64, lcart, (double)tv, (double)te, (double)tn, (double)tev,
+                            (double)ten, (double)tnv, (double)tnve, (double)told, (double)s1,
+                            (double)s2, (double)s3, (double)s4, (double)s5, (double)s6, (double)s7,
+                            iz + 1, x + 1, y + 1, sz, sx, sy);
                 }
+                if (r != told) {
+                    tt[cbase + iz] = r;
+                    const double d = fabs((double)r - (double)told);
+                    dmax = d > dmax ? d : dmax;
+                }
+                result = r;
             }
         }
         xr[cp][ty][tx] = result;
