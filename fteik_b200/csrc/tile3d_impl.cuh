@@ -111,49 +111,53 @@ __device__ double tile_sweep(const fk_grid3d_t &g, R *__restrict__ tt, const R *
     const bool colupd = col && xlog >= lox && ylog >= loy;
     const int srcx = tx - sx;                    /* x-upwind lane */
     const int wy = ty - sy;                      /* y-upwind warp */
-    /* column bases */
-    const size_t nzp = (size_t)zp;
-    const size_t cbase = ((size_t)y * nx + x) * nzp;
-    const size_t cbase_x = ((size_t)y * nx + (x - sx)) * nzp;        /* valid when colupd */
-    const size_t cbase_y = ((size_t)(y - sy) * nx + x) * nzp;
-    const size_t cbase_xy = ((size_t)(y - sy) * nx + (x - sx)) * nzp;
+    /* column offsets (32-bit: a field and a slowness grid hold < 2^31 entries) */
+    const int cbase = (y * nx + x) * zp;
+    const int cbase_x = (y * nx + (x - sx)) * zp;        /* used when the neighbour exists */
+    const int cbase_y = ((y - sy) * nx + x) * zp;
+    const int cbase_xy = ((y - sy) * nx + (x - sx)) * zp;
     /* slowness columns: U upwind cell, D other (clamped) */
     const int cxU = (sx > 0) ? x - 1 : x, cxD = min(max((sx > 0) ? x : x - 1, 0), nx - 2);
     const int cyU = (sy > 0) ? y - 1 : y, cyD = min(max((sy > 0) ? y : y - 1, 0), ny - 2);
-    const size_t sUU = ((size_t)cyU * (nx - 1) + cxU) * zcp; /* x U, y U */
-    const size_t sUD = ((size_t)cyD * (nx - 1) + cxU) * zcp; /* x U, y D */
-    const size_t sDU = ((size_t)cyU * (nx - 1) + cxD) * zcp; /* x D, y U */
-    const size_t sDD = ((size_t)cyD * (nx - 1) + cxD) * zcp; /* x D, y D */
+    const int sUU = (cyU * (nx - 1) + cxU) * zcp; /* x U, y U */
+    const int sUD = (cyD * (nx - 1) + cxU) * zcp; /* x U, y D */
+    const int sDU = (cyU * (nx - 1) + cxD) * zcp; /* x D, y U */
+    const int sDD = (cyD * (nx - 1) + cxD) * zcp; /* x D, y D */
     const R HUGEV = (R)FK_HUGE;
     const unsigned FULL = 0xffffffffu;
     const int zoff = (sz > 0) ? 0 : zp - nz; /* padded walk: dummy positions */
-    const int nsteps = zp + (TX - 1) + (TY - 1);
+    /* walk only positions a node of this sweep can need: from the z-upwind
+     * neighbour of the first updated level to the last real level */
+    const int qs = zoff + loz - 1, qe = zoff + nz - 1;
+    const int nsteps = (qe - qs + 1) + (TX - 1) + (TY - 1);
     const bool edge_x = ox == 0, edge_y = oy == 0;
     const bool has_x = xlog >= 1, has_y = ylog >= 1;
 
-    /* Global operands of a walk position, loaded one step ahead. */
+    /* Global operands of a walk position, loaded one step ahead: the old
+     * time, the tile-face values and the 4 slowness cells of the z-downwind
+     * layer (the z-upwind layer is the previous position's). */
     struct Pre {
         R told, te, tn, ten;
-        R uuu, duu, uud, dud, udu, ddu, udd; /* slowness s<z><x><y> */
+        R duu, dud, ddu, ddd; /* slowness s<z><x><y>, z = D */
     };
     auto fetch = [&](int qpos, Pre &f) {
+        if (!(col && qpos >= qs && qpos <= qe)) return;
         const int iz = (sz > 0) ? qpos : zp - 1 - qpos;
-        if (!(col && qpos >= 0 && qpos < zp && iz < nz)) return;
-        f.told = ldcg(tt + cbase + iz);
-        if (edge_x) f.te = has_x ? ldcg(tt + cbase_x + iz) : HUGEV;
-        if (edge_y) f.tn = has_y ? ldcg(tt + cbase_y + iz) : HUGEV;
-        if (edge_x && edge_y) f.ten = (has_x && has_y) ? ldcg(tt + cbase_xy + iz) : HUGEV;
-        if (colupd && qpos - zoff >= loz) {
-            const int czU = (sz > 0) ? iz - 1 : iz;
+        f.told = ldcg(tt + (cbase + iz));
+        if (edge_x) f.te = has_x ? ldcg(tt + (cbase_x + iz)) : HUGEV;
+        if (edge_y) f.tn = has_y ? ldcg(tt + (cbase_y + iz)) : HUGEV;
+        if (edge_x && edge_y) f.ten = (has_x && has_y) ? ldcg(tt + (cbase_xy + iz)) : HUGEV;
+        if (colupd) {
             const int czD = min(max((sz > 0) ? iz : iz - 1, 0), nz - 2);
-            f.uuu = __ldg(slow + sUU + czU); f.duu = __ldg(slow + sUU + czD);
-            f.uud = __ldg(slow + sUD + czU); f.dud = __ldg(slow + sUD + czD);
-            f.udu = __ldg(slow + sDU + czU); f.ddu = __ldg(slow + sDU + czD);
-            f.udd = __ldg(slow + sDD + czU);
+            f.duu = __ldg(slow + (sUU + czD));
+            f.dud = __ldg(slow + (sUD + czD));
+            f.ddu = __ldg(slow + (sDU + czD));
+            f.ddd = __ldg(slow + (sDD + czD));
         }
     };
     Pre cur, nxt;
-    fetch(0 - ox - oy, nxt);
+    fetch(qs - ox - oy, nxt);
+    R zu_uu = 0, zu_ud = 0, zu_du = 0, zu_dd = 0; /* z-upwind layer (previous position) */
 
     R r_last = HUGEV, te_last = HUGEV, tn_last = HUGEV, ten_last = HUGEV;
     double dmax = 0.0;
@@ -161,12 +165,12 @@ __device__ double tile_sweep(const fk_grid3d_t &g, R *__restrict__ tt, const R *
         const int pp = (st + 1) & 1, cp = st & 1;
         const R sh_r = __shfl_sync(FULL, r_last, srcx & 31);
         const R sh_tn = __shfl_sync(FULL, tn_last, srcx & 31);
-        const int qpos = st - ox - oy;
+        const int qpos = qs + st - ox - oy;
         cur = nxt;
         fetch(qpos + 1, nxt);
         R te = HUGEV, tn = HUGEV, ten = HUGEV, result = r_last;
         const int iz = (sz > 0) ? qpos : zp - 1 - qpos;
-        if (col && qpos >= 0 && qpos < zp && iz < nz) {
+        if (col && qpos >= qs && qpos <= qe) {
             const int il = qpos - zoff; /* logical unpadded z */
             const R told = cur.told;
             result = told;
@@ -176,13 +180,14 @@ __device__ double tile_sweep(const fk_grid3d_t &g, R *__restrict__ tt, const R *
             tn = edge_y ? cur.tn : xr[pp][wy][tx];
             ten = !edge_y ? xte[pp][wy][tx] : (!edge_x ? sh_tn : cur.ten);
             if (colupd && il >= loz) {
-                const R s1 = rmin(rmin(cur.uuu, cur.uud), rmin(cur.udu, cur.udd));
-                const R s2 = rmin(rmin(cur.uuu, cur.uud), rmin(cur.duu, cur.dud));
-                const R s3 = rmin(rmin(cur.uuu, cur.udu), rmin(cur.duu, cur.ddu));
-                const R s4 = rmin(cur.uuu, cur.uud);
-                const R s5 = rmin(cur.uuu, cur.udu);
-                const R s6 = rmin(cur.uuu, cur.duu);
-                const R s7 = cur.uuu;
+                const R uuu = zu_uu, uud = zu_ud, udu = zu_du, udd = zu_dd;
+                const R s1 = rmin(rmin(uuu, uud), rmin(udu, udd));
+                const R s2 = rmin(rmin(uuu, uud), rmin(cur.duu, cur.dud));
+                const R s3 = rmin(rmin(uuu, udu), rmin(cur.duu, cur.ddu));
+                const R s4 = rmin(uuu, uud);
+                const R s5 = rmin(uuu, udu);
+                const R s6 = rmin(uuu, cur.duu);
+                const R s7 = uuu;
                 const R tv = r_last, tev = te_last, tnv = tn_last, tnve = ten_last;
                 R r;
                 if (!INIT) {
@@ -209,6 +214,7 @@ __device__ double tile_sweep(const fk_grid3d_t &g, R *__restrict__ tt, const R *
                 result = r;
             }
         }
+        if (colupd) { zu_uu = cur.duu; zu_ud = cur.dud; zu_du = cur.ddu; zu_dd = cur.ddd; }
         xr[cp][ty][tx] = result;
         xte[cp][ty][tx] = te;
         r_last = result;
@@ -222,7 +228,7 @@ __device__ double tile_sweep(const fk_grid3d_t &g, R *__restrict__ tt, const R *
 
 /* Persistent tile-task kernel over sweeps [s_begin, s_end). */
 template <typename R, bool INIT>
-__global__ void __launch_bounds__(NT) tile_kernel(Params P)
+__global__ void __launch_bounds__(NT, INIT ? 2 : 3) tile_kernel(Params P)
 {
     __shared__ R xr[2][TY][TX];
     __shared__ R xte[2][TY][TX];
