@@ -52,7 +52,18 @@ static struct {
     bool graph_ok;
     double *export_buf;
     size_t export_cap;
+    void *stage;            /* device staging: slowness upload, dense field export */
+    size_t stage_cap;
 } SB;
+
+static void *stage_buf(size_t bytes, const char *who)
+{
+    if (SB.stage && SB.stage_cap >= bytes) return SB.stage;
+    fk_dfree(SB.stage);
+    SB.stage = fk_dalloc(bytes, who);
+    SB.stage_cap = SB.stage ? bytes : 0;
+    return SB.stage;
+}
 
 static void free_grid(bgrid_t *g)
 {
@@ -76,6 +87,7 @@ void fteik_b200_batch3d_finalize(void)
     free(SB.g);
     fk_dfree(SB.grids_dev); fk_dfree(SB.work_dev); fk_dfree(SB.res_dev); fk_dfree(SB.export_buf);
     fk_dfree(SB.groups_dev);
+    fk_dfree(SB.stage);
     fk_tileplan_free(&SB.plan);
     free(SB.res_host); free(SB.work_order);
     memset(&SB, 0, sizeof(SB));
@@ -145,14 +157,13 @@ void fteik_b200_batch3d_setVelocityModel64f(int igrid, int ncell, const double v
     for (int i = 0; i < ncell; i++) g->slow[i] = 1.0 / vel[i];
     const size_t nelem = (size_t)g->zcp * (g->nx - 1) * (g->ny - 1);
     if (!g->slow_dev) g->slow_dev = fk_dalloc(nelem * (size_t)SB.precision, who);
-    double *tmp = (double *)fk_dalloc(sizeof(double) * (size_t)ncell, who);
-    if (!g->slow_dev || !tmp) { fk_dfree(tmp); return; }
+    double *tmp = (double *)stage_buf(sizeof(double) * (size_t)ncell, who);
+    if (!g->slow_dev || !tmp) return;
     cudaStream_t s = fk_stream();
     int e = (int)cudaMemsetAsync(g->slow_dev, 0, nelem * (size_t)SB.precision, s);
     if (!e) e = (int)cudaMemcpyAsync(tmp, g->slow, sizeof(double) * (size_t)ncell, cudaMemcpyHostToDevice, s);
     if (!e) e = fk_pack_slowness(SB.precision, 1, g->nz, g->nx, g->ny, g->zcp, tmp, g->slow_dev, s);
     if (!e) e = (int)cudaStreamSynchronize(s);
-    fk_dfree(tmp);
     if (fk_check(e, who)) return;
     g->have_model = true;
     SB.solved = false;
@@ -446,10 +457,23 @@ void fteik_b200_batch3d_getTravelTimeFields32f(int igrid, long long nval, float 
     if (!SB.solved) { FK_ERR("%s: not solved", who); return; }
     if (SB.precision != 4) { FK_ERR("%s: the batch was solved in FP64", who); return; }
     if (nval < (long long)g->nsrc * g->ngrd) { FK_ERR("%s: nval too small", who); return; }
-    int e = (int)cudaMemcpy2DAsync(tt, sizeof(float) * (size_t)g->nz, g->fields,
-                                   sizeof(float) * (size_t)g->zp, sizeof(float) * (size_t)g->nz,
-                                   (size_t)g->nx * g->ny * g->nsrc, cudaMemcpyDeviceToHost, fk_stream());
-    if (!e) e = (int)cudaStreamSynchronize(fk_stream());
+    /* unpad on the device in chunks of sources, one contiguous copy each */
+    const size_t per_src = (size_t)g->ngrd * sizeof(float);
+    int chunk = (int)((256u << 20) / per_src);
+    if (chunk < 1) chunk = 1;
+    if (chunk > g->nsrc) chunk = g->nsrc;
+    float *st = (float *)stage_buf(per_src * (size_t)chunk, who);
+    if (!st) return;
+    cudaStream_t s = fk_stream();
+    int e = 0;
+    for (int s0 = 0; s0 < g->nsrc && !e; s0 += chunk) {
+        const int ns = (g->nsrc - s0) < chunk ? (g->nsrc - s0) : chunk;
+        const float *src = (const float *)g->fields + (size_t)s0 * g->zp * g->nx * g->ny;
+        e = fk_unpad_f32(src, st, (size_t)ns * g->nx * g->ny, g->nz, g->zp, s);
+        if (!e) e = (int)cudaMemcpyAsync(tt + (size_t)s0 * g->ngrd, st, per_src * (size_t)ns,
+                                        cudaMemcpyDeviceToHost, s);
+    }
+    if (!e) e = (int)cudaStreamSynchronize(s);
     *ierr = fk_check(e, who);
 }
 

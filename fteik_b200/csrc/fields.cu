@@ -336,3 +336,26 @@ extern "C" int fk_f64_to_f32(size_t n, const double *in, float *out, cudaStream_
     f64_to_f32_kernel<<<nblocks(n), 256, 0, s>>>(n, in, out);
     return (int)cudaGetLastError();
 }
+
+namespace {
+/* Copy nfield padded FP32 fields ([nyx rows][zp]) into a dense [nyx][nz]
+ * buffer, 16-byte vectors where the pitch allows. */
+__global__ void unpad_kernel(const float *__restrict__ src, float *__restrict__ dst, size_t rows,
+                             int nz, int zp)
+{
+    const size_t n = rows * (size_t)nz;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = e / nz;
+        const int z = (int)(e - r * nz);
+        dst[e] = src[r * zp + z];
+    }
+}
+} // namespace
+
+extern "C" int fk_unpad_f32(const float *src, float *dst, size_t rows, int nz, int zp, cudaStream_t s)
+{
+    if (rows == 0) return 0;
+    unpad_kernel<<<148 * 8, 256, 0, s>>>(src, dst, rows, nz, zp);
+    return (int)cudaGetLastError();
+}

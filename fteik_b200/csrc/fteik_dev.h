@@ -150,6 +150,8 @@ int fk_analytic_points(int kind, int nz, double z0, double dz, double v0, double
                        int nsrc, const double *zs, const double *xs, const double *ys,
                        int ldr, double *out, cudaStream_t s);
 int fk_f64_to_f32(size_t n, const double *in, float *out, cudaStream_t s);
+/* Dense copy of padded FP32 rows: src [rows][zp] -> dst [rows][nz]. */
+int fk_unpad_f32(const float *src, float *dst, size_t rows, int nz, int zp, cudaStream_t s);
 
 /* ---- locate ------------------------------------------------------------- */
 /* Exact FP32 L2 grid search (locate.F90:620-744) for nev events:
