@@ -134,6 +134,9 @@ _SIGS = {
     "fteik_b200_batch3d_exportToLocator": [c_int, c_int, _PI],
     "fteik_b200_batch3d_finalize": [],
     "fteik_b200_locate_locateEvents": [c_int, _PI, _PI, _PD, _PD, _PI],
+    "fteik_b200_locate_l2_noalloc": [c_int, c_int, c_int, ctypes.c_void_p, c_int, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_void_p, _PI],
     "fteik_h5io_initializeF": [ctypes.c_char_p],
     "fteik_h5io_finalizeF": [],
     "fteik_h5io_writeLevelSchedulesF": [],

@@ -14,6 +14,7 @@
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
 #include "fteik_dev.h"
 
 namespace {
@@ -160,4 +161,71 @@ extern "C" int fk_locate_l2_exact(int ngrd, int ldgrd, int ntf, const float *tab
     l2_at_opt_kernel<<<(nev + 127) / 128, 128, 0, s>>>(ngrd, ldgrd, ntf, tables, nev, obs, wts, xn,
                                                        best, out_idx, out_t0, out_obj);
     return (int)cudaGetLastError();
+}
+
+/* ------------------------------------------------------------------------ */
+/* Allocation-free variant.                                                 */
+/*                                                                          */
+/* Some callers cannot let a library call cudaMalloc: a host that hands out */
+/* all device memory from its own pool (a framework's caching allocator, a  */
+/* real-time service with a fixed memory budget) or that must not trigger   */
+/* the device-wide synchronisation cudaMalloc/cudaFree can cause.  For them */
+/* fteik_b200_locate_l2_noalloc runs the same grid search on buffers the    */
+/* caller owns, keeping its per-event scratch (the best (misfit, index) key */
+/* and the weight normaliser, 12 bytes per event) in the fixed array below. */
+/* ------------------------------------------------------------------------ */
+
+#define FK_NOALLOC_MAX_EVENTS 65536
+/* Lives on every device that loads this library until the process exits. */
+static __device__ __align__(256) unsigned char g_noalloc_scratch[FK_NOALLOC_MAX_EVENTS * 12 + 256];
+
+static void *g_noalloc_ptr[64];  /* device address of the array, per device */
+static int g_noalloc_ready[64];
+
+extern "C" void fteik_b200_locate_l2_noalloc(int ngrd, int ldgrd, int ntf, const float *tables,
+                                             int nev, const float *obs, const float *wts,
+                                             int *opt_index, float *t0, float *obj, void *stream,
+                                             int *ierr)
+{
+    *ierr = 1;
+    if (nev < 1 || nev > FK_NOALLOC_MAX_EVENTS) {
+        fprintf(stderr, "fteik_b200_locate_l2_noalloc: nev=%d must be in [1,%d]\n", nev,
+                FK_NOALLOC_MAX_EVENTS);
+        return;
+    }
+    if (ntf < 1 || ntf > kMaxTf || ngrd < 1 || ldgrd < ngrd) {
+        fprintf(stderr, "fteik_b200_locate_l2_noalloc: need 1 <= ntf <= %d and 1 <= ngrd <= ldgrd\n",
+                kMaxTf);
+        return;
+    }
+    if (!tables || !obs || !wts || !opt_index || !t0 || !obj) {
+        fprintf(stderr, "fteik_b200_locate_l2_noalloc: null buffer\n");
+        return;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64) {
+        fprintf(stderr, "fteik_b200_locate_l2_noalloc: no usable CUDA device\n");
+        return;
+    }
+    if (!g_noalloc_ready[dev]) {
+        /* once per device, with that device current: the host-side name of
+         * the array is not a device address */
+        e = cudaGetSymbolAddress(&g_noalloc_ptr[dev], g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            fprintf(stderr, "fteik_b200_locate_l2_noalloc: cudaGetSymbolAddress failed (%s)\n",
+                    cudaGetErrorString(e));
+            return;
+        }
+        g_noalloc_ready[dev] = 1;
+    }
+    const int rc = fk_locate_l2_exact(ngrd, ldgrd, ntf, tables, nev, obs, wts, opt_index, t0, obj,
+                                      g_noalloc_ptr[dev], sizeof(g_noalloc_scratch),
+                                      (cudaStream_t)stream);
+    if (rc != 0) {
+        fprintf(stderr, "fteik_b200_locate_l2_noalloc: launch failed (%s)\n",
+                cudaGetErrorString((cudaError_t)rc));
+        return;
+    }
+    *ierr = 0;
 }

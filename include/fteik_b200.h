@@ -317,6 +317,28 @@ void fteik_b200_batch3d_finalize(void);
 void fteik_b200_locate_locateEvents(int n, const int ev[], int optIndx[],
                                     double t0Opt[], double objOpt[], int *ierr);
 
+/* Allocation-free grid search (no counterpart in the reference).  For
+ * callers that cannot let a library allocate device memory -- a host that
+ * hands out every device buffer from its own pool, or a service that must
+ * avoid the device-wide synchronisation cudaMalloc/cudaFree can cause.  All
+ * buffers are device pointers the caller owns: tables[ntf][ldgrd] FP32,
+ * obs/wts[nev][ntf] FP32 (picks already reduced by the event's largest pick,
+ * weight 0 = skipped pick), and the outputs opt_index (0-based grid index;
+ * add 1 for locate_locateEvent's optIndx), t0 and obj in FP32 -- the same
+ * objective and optimum as locate_locateEvent.  stream is a cudaStream_t
+ * (NULL: the legacy default stream); the call returns after launching.
+ * Limits: 1 <= nev <= 65536, 1 <= ntf <= 64.  Its scratch (12 bytes per
+ * event) is a fixed array that every device loading the library keeps until
+ * exit; the first call on a device looks up that array's device address, so
+ * make that first call before any stream capture.  Every call reuses the
+ * same array, so calls whose work overlaps on the GPU race: order them on
+ * one stream.  It allocates nothing (no cudaMalloc, cudaFree or stream
+ * creation). */
+void fteik_b200_locate_l2_noalloc(int ngrd, int ldgrd, int ntf, const float *tables,
+                                  int nev, const float *obs, const float *wts,
+                                  int *opt_index, float *t0, float *obj, void *stream,
+                                  int *ierr);
+
 #ifdef __cplusplus
 }
 #endif
