@@ -54,6 +54,8 @@ static struct {
     size_t export_cap;
     void *stage;            /* device staging: slowness upload, dense field export */
     size_t stage_cap;
+    cudaEvent_t ev[3];      /* in the graph: before init, after init, after passes */
+    bool have_ev;
 } SB;
 
 static void *stage_buf(size_t bytes, const char *who)
@@ -89,6 +91,7 @@ void fteik_b200_batch3d_finalize(void)
     fk_dfree(SB.groups_dev);
     fk_dfree(SB.stage);
     fk_tileplan_free(&SB.plan);
+    if (SB.have_ev) for (int i = 0; i < 3; i++) cudaEventDestroy(SB.ev[i]);
     free(SB.res_host); free(SB.work_order);
     memset(&SB, 0, sizeof(SB));
 }
@@ -370,9 +373,16 @@ void fteik_b200_batch3d_solve(int *ierr)
                 le = fk3d_solve(SB.precision, SB.grids_dev, SB.work_dev, SB.groups_dev, SB.ngroups,
                                 SB.S, SB.res_dev, SB.nwork, SB.max_nx, SB.max_nz, SB.eps, SB.nsweep,
                                 SB.conv_tol, SB.max_pass, s);
-            else
+            else {
+                if (!SB.have_ev) {
+                    SB.have_ev = true;
+                    for (int i = 0; i < 3; i++) cudaEventCreate(&SB.ev[i]);
+                }
+                fk3d_tiles_set_events(SB.ev);
                 le = fk3d_solve_tiles(SB.precision, SB.grids_dev, SB.work_dev, SB.nwork, &SB.plan.dev,
                                       SB.res_dev, SB.eps, SB.nsweep, SB.conv_tol, SB.max_pass, s);
+                fk3d_tiles_set_events(NULL);
+            }
             e = (int)cudaStreamEndCapture(s, &graph);
             if (!e) e = le;
         }
@@ -527,4 +537,17 @@ void fteik_b200_batch3d_exportToLocator(int igrid, int itf0, int *ierr)
     }
     if (!e) e = (int)cudaStreamSynchronize(fk_stream());
     *ierr = fk_check(e, who);
+}
+
+/* Device time of the last solve's initialisation kernel and Gauss-Seidel
+ * kernel, from events recorded inside the solve graph. */
+void fteik_b200_batch3d_getKernelTimes(float *init_ms, float *pass_ms, int *ierr)
+{
+    *init_ms = *pass_ms = 0.0f;
+    *ierr = 1;
+    if (!SB.have_ev || !SB.graph_ok) return;
+    int e = (int)cudaEventSynchronize(SB.ev[2]);
+    if (!e) e = (int)cudaEventElapsedTime(init_ms, SB.ev[0], SB.ev[1]);
+    if (!e) e = (int)cudaEventElapsedTime(pass_ms, SB.ev[1], SB.ev[2]);
+    *ierr = fk_check(e, "fteik_b200_batch3d_getKernelTimes");
 }

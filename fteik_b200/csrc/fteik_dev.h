@@ -93,6 +93,10 @@ typedef struct {
 int fk3d_solve_tiles(int precision, const fk_grid3d_t *grids, const fk_work3d_t *work,
                      int nwork, const fk_tiles3d_t *plan, fk_result3d_t *results, double eps,
                      int nsweep, double conv_tol, int max_pass, cudaStream_t stream);
+/* Optional timing: events recorded before the initialisation kernel, after
+ * it and after the Gauss-Seidel kernel of every later fk3d_solve_tiles on
+ * this host thread (NULL to stop). */
+void fk3d_tiles_set_events(cudaEvent_t *ev3);
 
 /* ---- 2D ---------------------------------------------------------------- */
 typedef struct {

@@ -6,6 +6,12 @@
 #include "sweep3d_impl.cuh"
 #include "tile3d_impl.cuh"
 
+namespace fk3tw {
+cudaEvent_t *g_tile_events = nullptr;
+}
+
+extern "C" void fk3d_tiles_set_events(cudaEvent_t *ev3) { fk3tw::g_tile_events = ev3; }
+
 extern "C" int fk3d_solve_f64(const fk_grid3d_t *grids, const fk_work3d_t *work,
                               const int *groups, int ngroups, int S, fk_result3d_t *results,
                               int nwork, int max_nx, int max_nz, double eps, int nsweep,

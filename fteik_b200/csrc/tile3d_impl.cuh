@@ -404,6 +404,8 @@ inline int occupancy_ctas(const void *fn, int threads)
     return nsm * per;
 }
 
+extern cudaEvent_t *g_tile_events; /* sweep3d_f32.cu */
+
 template <typename R>
 inline int launch_tiles(const fk_grid3d_t *grids, const fk_work3d_t *work, int nwork,
                         const fk_tiles3d_t *pl, fk_result3d_t *results, double eps, int nsweep,
@@ -443,7 +445,9 @@ inline int launch_tiles(const fk_grid3d_t *grids, const fk_work3d_t *work, int n
     P.s_end = 8;
     P.ticket = pl->tickets;
     const int gi = occupancy_ctas((const void *)tile_kernel<R, true>, NT);
+    if (g_tile_events) cudaEventRecord(g_tile_events[0], st);
     tile_kernel<R, true><<<gi, NT, 0, st>>>(P);
+    if (g_tile_events) cudaEventRecord(g_tile_events[1], st);
     if (npass > 0) {
         P.s_begin = 8;
         P.s_end = 8 + 8 * npass;
@@ -451,6 +455,7 @@ inline int launch_tiles(const fk_grid3d_t *grids, const fk_work3d_t *work, int n
         const int gp = occupancy_ctas((const void *)tile_kernel<R, false>, NT);
         tile_kernel<R, false><<<gp, NT, 0, st>>>(P);
     }
+    if (g_tile_events) cudaEventRecord(g_tile_events[2], st);
     finalize_kernel<<<(nwork + 127) / 128, 128, 0, st>>>(nwork, npr, converge, npass, pl->resid,
                                                           pl->conv_pass, pl->error, results);
     return (int)cudaGetLastError();

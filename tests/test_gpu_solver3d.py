@@ -197,3 +197,23 @@ def test_batched_converged(fk):
     assert res == 0.0 and npass < 20
     assert np.max(np.abs(tt - ref)) <= 1e-12 * np.max(ref)
     b.finalize()
+
+
+def test_config2_converged_accuracy(fk):
+    """128^3, h = 25 m, 4 layers x (1 + 0.05 GRF), interior off-grid source,
+    solved to convergence: FP32 GPU vs the FP64 oracle, relative error
+    <= 1e-4 at every node."""
+    n, h = (128, 128, 128), (25.0, 25.0, 25.0)
+    vel = layered_grf_cells(*n, seed=2)
+    src = interior_source(n, h, 3)
+    b = fk.Batch3D([(n[0], n[1], n[2], *h)], eps=5.0, convTol=0.0, maxPass=30, precision=4)
+    b.setVelocityModel(1, vel)
+    b.setSources(1, [src[0]], [src[1]], [src[2]])
+    b.solve()
+    tt = b.field(1, 1)
+    res, npass = b.solveInfo(1, 1)
+    b.finalize()
+    ref = _oracle(n, h, vel, src, conv_tol=0.0, max_pass=30, level_set=True)
+    rel = np.abs(tt - ref) / ref.clip(1e-6)
+    assert npass < 30 and res == 0.0
+    assert np.max(rel) <= TOL32, (np.max(rel), np.sqrt(np.mean(rel ** 2)), npass)
