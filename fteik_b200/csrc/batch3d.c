@@ -366,6 +366,11 @@ void fteik_b200_batch3d_solve(int *ierr)
         /* warm the kernel attributes outside capture, then capture */
         cudaGraph_t graph;
         int e = SB.walker ? fk3d_prepare(SB.precision, SB.max_nx, SB.max_nz, SB.S) : 0;
+        if (!e && !SB.have_ev) { /* timing events, created outside the capture */
+            bool ok = true;
+            for (int i = 0; i < 3; i++) ok = ok && cudaEventCreate(&SB.ev[i]) == cudaSuccess;
+            SB.have_ev = ok;
+        }
         if (!e) e = (int)cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (!e) {
             int le;
@@ -374,11 +379,7 @@ void fteik_b200_batch3d_solve(int *ierr)
                                 SB.S, SB.res_dev, SB.nwork, SB.max_nx, SB.max_nz, SB.eps, SB.nsweep,
                                 SB.conv_tol, SB.max_pass, s);
             else {
-                if (!SB.have_ev) {
-                    SB.have_ev = true;
-                    for (int i = 0; i < 3; i++) cudaEventCreate(&SB.ev[i]);
-                }
-                fk3d_tiles_set_events(SB.ev);
+                fk3d_tiles_set_events(SB.have_ev ? SB.ev : NULL);
                 le = fk3d_solve_tiles(SB.precision, SB.grids_dev, SB.work_dev, SB.nwork, &SB.plan.dev,
                                       SB.res_dev, SB.eps, SB.nsweep, SB.conv_tol, SB.max_pass, s);
                 fk3d_tiles_set_events(NULL);
