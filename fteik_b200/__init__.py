@@ -133,7 +133,7 @@ _SIGS = {
     "fteik_b200_batch3d_getSolveInfo": [c_int, c_int, _PD, _PI, _PI],
     "fteik_b200_batch3d_exportToLocator": [c_int, c_int, _PI],
     "fteik_b200_batch3d_finalize": [],
-    "fteik_b200_batch3d_getKernelTimes": [POINTER(c_float), POINTER(c_float), _PI],
+    "fteik_b200_batch3d_timeSolve": [POINTER(c_float), POINTER(c_float), _PI],
     "fteik_b200_locate_locateEvents": [c_int, _PI, _PI, _PD, _PD, _PI],
     "fteik_b200_locate_l2_noalloc": [c_int, c_int, c_int, ctypes.c_void_p, c_int, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -525,8 +525,8 @@ class Batch3D:
 
     def kernelTimes(self):
         a, b, ierr = c_float(), c_float(), c_int(1)
-        self.lib.fteik_b200_batch3d_getKernelTimes(byref(a), byref(b), byref(ierr))
-        _check(ierr, "batch3d_getKernelTimes")
+        self.lib.fteik_b200_batch3d_timeSolve(byref(a), byref(b), byref(ierr))
+        _check(ierr, "batch3d_timeSolve")
         return a.value, b.value
 
     def exportToLocator(self, igrid, itf0=1):

@@ -366,11 +366,6 @@ void fteik_b200_batch3d_solve(int *ierr)
         /* warm the kernel attributes outside capture, then capture */
         cudaGraph_t graph;
         int e = SB.walker ? fk3d_prepare(SB.precision, SB.max_nx, SB.max_nz, SB.S) : 0;
-        if (!e && !SB.have_ev) { /* timing events, created outside the capture */
-            bool ok = true;
-            for (int i = 0; i < 3; i++) ok = ok && cudaEventCreate(&SB.ev[i]) == cudaSuccess;
-            SB.have_ev = ok;
-        }
         if (!e) e = (int)cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (!e) {
             int le;
@@ -378,12 +373,9 @@ void fteik_b200_batch3d_solve(int *ierr)
                 le = fk3d_solve(SB.precision, SB.grids_dev, SB.work_dev, SB.groups_dev, SB.ngroups,
                                 SB.S, SB.res_dev, SB.nwork, SB.max_nx, SB.max_nz, SB.eps, SB.nsweep,
                                 SB.conv_tol, SB.max_pass, s);
-            else {
-                fk3d_tiles_set_events(SB.have_ev ? SB.ev : NULL);
+            else
                 le = fk3d_solve_tiles(SB.precision, SB.grids_dev, SB.work_dev, SB.nwork, &SB.plan.dev,
                                       SB.res_dev, SB.eps, SB.nsweep, SB.conv_tol, SB.max_pass, s);
-                fk3d_tiles_set_events(NULL);
-            }
             e = (int)cudaStreamEndCapture(s, &graph);
             if (!e) e = le;
         }
@@ -540,15 +532,29 @@ void fteik_b200_batch3d_exportToLocator(int igrid, int itf0, int *ierr)
     *ierr = fk_check(e, who);
 }
 
-/* Device time of the last solve's initialisation kernel and Gauss-Seidel
- * kernel, from events recorded inside the solve graph. */
-void fteik_b200_batch3d_getKernelTimes(float *init_ms, float *pass_ms, int *ierr)
+/* Run one solve outside the graph with CUDA events around its
+ * initialisation kernel and its Gauss-Seidel kernel; returns their device
+ * times.  The fields end as after fteik_b200_batch3d_solve. */
+void fteik_b200_batch3d_timeSolve(float *init_ms, float *pass_ms, int *ierr)
 {
+    const char *who = "fteik_b200_batch3d_timeSolve";
     *init_ms = *pass_ms = 0.0f;
     *ierr = 1;
-    if (!SB.have_ev || !SB.graph_ok) return;
-    int e = (int)cudaEventSynchronize(SB.ev[2]);
+    if (!SB.graph_ok || SB.walker) { FK_ERR("%s: solve once first (tile schedule)", who); return; }
+    if (SB.work_dirty && upload_work(who)) return;
+    if (!SB.have_ev) {
+        bool ok = true;
+        for (int i = 0; i < 3; i++) ok = ok && cudaEventCreate(&SB.ev[i]) == cudaSuccess;
+        SB.have_ev = ok;
+        if (!ok) { FK_ERR("%s: cannot create events", who); return; }
+    }
+    cudaStream_t s = fk_stream();
+    fk3d_tiles_set_events(SB.ev);
+    int e = fk3d_solve_tiles(SB.precision, SB.grids_dev, SB.work_dev, SB.nwork, &SB.plan.dev,
+                             SB.res_dev, SB.eps, SB.nsweep, SB.conv_tol, SB.max_pass, s);
+    fk3d_tiles_set_events(NULL);
+    if (!e) e = (int)cudaEventSynchronize(SB.ev[2]);
     if (!e) e = (int)cudaEventElapsedTime(init_ms, SB.ev[0], SB.ev[1]);
     if (!e) e = (int)cudaEventElapsedTime(pass_ms, SB.ev[1], SB.ev[2]);
-    *ierr = fk_check(e, "fteik_b200_batch3d_getKernelTimes");
+    *ierr = fk_check(e, who);
 }

@@ -302,9 +302,10 @@ void fteik_b200_batch3d_getTravelTimeFields32f(int igrid, long long nval,
 /* Receiver times of every source of a grid: ttr[isrc*nrec + irec]. */
 void fteik_b200_batch3d_getTravelTimes64f(int igrid, int nval, double ttr[],
                                           int *ierr);
-/* Device time (ms) of the last solve's initialisation sweeps and of its
- * Gauss-Seidel passes, timed by CUDA events inside the solve graph. */
-void fteik_b200_batch3d_getKernelTimes(float *init_ms, float *pass_ms, int *ierr);
+/* Run one solve outside its CUDA graph with events around the
+ * initialisation kernel and the Gauss-Seidel kernel and return their device
+ * times (ms); the fields end as after fteik_b200_batch3d_solve. */
+void fteik_b200_batch3d_timeSolve(float *init_ms, float *pass_ms, int *ierr);
 /* Residual (FP64 max |dt| of the last pass) and passes run. */
 void fteik_b200_batch3d_getSolveInfo(int igrid, int isrc, double *residual,
                                      int *npass, int *ierr);
