@@ -135,6 +135,9 @@ _SIGS = {
     "fteik_b200_batch3d_finalize": [],
     "fteik_b200_batch3d_timeSolve": [POINTER(c_float), POINTER(c_float), _PI],
     "fteik_b200_locate_locateEvents": [c_int, _PI, _PI, _PD, _PD, _PI],
+    "fteik_b200_locate_setMethod": [c_int, _PI],
+    "fteik_b200_locate_setRescoreCandidates": [c_int, _PI],
+    "fteik_b200_locate_debugAccumulators": [c_int, _PF, _PI],
     "fteik_b200_locate_l2_noalloc": [c_int, c_int, c_int, ctypes.c_void_p, c_int, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, _PI],
@@ -431,6 +434,31 @@ class Locator:
                                                 ob.ctypes.data_as(_PD), byref(ierr))
         _check(ierr, "fteik_b200_locate_locateEvents")
         return oi, t0, ob
+
+    def setMethod(self, method):
+        """0: exact FP32 search (the reference's arithmetic); 1: tensor-core
+        BF16 hi+lo ranking with FP64 re-score of the best candidates."""
+        ierr = c_int(1)
+        self.lib.fteik_b200_locate_setMethod(int(method), byref(ierr))
+        _check(ierr, "fteik_b200_locate_setMethod")
+
+    def setRescoreCandidates(self, ncand):
+        ierr = c_int(1)
+        self.lib.fteik_b200_locate_setRescoreCandidates(int(ncand), byref(ierr))
+        _check(ierr, "fteik_b200_locate_setRescoreCandidates")
+
+    def debugAccumulators(self, enable):
+        """enable=True: record the first accumulator tiles at the next
+        tensor-core search; enable=False: return them as [256, 128]."""
+        ierr = c_int(1)
+        if enable:
+            self.lib.fteik_b200_locate_debugAccumulators(1, None, byref(ierr))
+            _check(ierr, "fteik_b200_locate_debugAccumulators")
+            return None
+        out = np.zeros((256, 128), np.float32)
+        self.lib.fteik_b200_locate_debugAccumulators(0, out.ctypes.data_as(_PF), byref(ierr))
+        _check(ierr, "fteik_b200_locate_debugAccumulators")
+        return out
 
 
 class Batch3D:

@@ -1,0 +1,659 @@
+/*
+ * locate_tc.cu -- the batched L2 grid search (locate.F90:620-744) as a
+ * tensor-core contraction.
+ *
+ * For an event whose picks cover every table with one common weight w, the
+ * reference's misfit at grid point g,
+ *     t0(g)  = sum_i w (o_i - T_i(g)) / sum_i w
+ *     obj(g) = sum_i (sqrt(1/2) w (o_i - T_i(g) - t0(g)))^2,
+ * equals (1/2) w^2 sum_i (o'_i - T'_i(g))^2, where o' is the picks minus their
+ * mean and T'(g) the tables at g minus their mean over tables.  Because
+ * sum_i o'_i = 0 this is
+ *     obj(g) = (1/2) w^2 ( p + q(g) - 2 sum_i o'_i T'_i(g) ),
+ *     p = sum o'^2 (per event),  q(g) = sum T'(g)^2 (per grid point),
+ * so ranking grid points needs one events x stations by stations x points
+ * product.  It runs on tcgen05 in BF16 with FP32 accumulation, each operand
+ * split as x = hi + lo (hi = bf16(x), lo = bf16(x - hi)) and the product
+ * formed as hi*hi + hi*lo + lo*hi (relative error about 2^-16 per term).
+ * Each CTA keeps, per event and per partition of the grid, the four best
+ * approximate scores; a second kernel re-scores the best candidates in FP64
+ * with the reference's formula on the FP32 tables and returns the minimum
+ * (first index among equal misfits).
+ *
+ * Operand layout: both operands are K-major (stations contiguous) in the
+ * tcgen05 128-byte swizzled canonical form, prepacked in global memory so
+ * that one untiled bulk copy moves a whole tile into shared memory:
+ *   tile = 128 rows x 64 stations of bf16 = 16 KB, row r at r * 128 bytes,
+ *   16-byte chunk c of row r stored at chunk position c ^ (r % 8);
+ *   a tile pair is [hi tile][lo tile] = 32 KB.
+ * Grid points of the padded last table tile score +inf and never enter a
+ * candidate list.
+ * Tables: one tile pair per 128 grid points.  Events: one pair per 128 events.
+ *
+ * Kernel roles (320 threads, one CTA per SM):
+ *   warp 0, one lane   bulk copies: the CTA's two event tiles per work item,
+ *                      then a 4-stage ring of table tile pairs
+ *   warp 1, one lane   tcgen05.mma: per table tile, 2 event tiles x 4 k-steps
+ *                      x 3 products into a 128 x 128 FP32 accumulator each;
+ *                      two accumulator sets (512 TMEM columns) alternate
+ *   warps 2-9          tcgen05.ld of the accumulators, score q - 2 C, running
+ *                      top 4 per event row
+ * A work item is (event group of 256, grid partition).  Items are ordered
+ * partition-major so the CTAs running at one time read the same table tiles
+ * (L2 reuse).  Every wait is bounded; on timeout the CTA records an error,
+ * stops issuing, waits (bounded) for its copies and MMAs, frees TMEM and
+ * returns.
+ */
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <stdio.h>
+#include "fteik_dev.h"
+
+namespace fktc {
+
+constexpr int BM = 128;                    /* events per tile (TMEM lanes) */
+constexpr int BN = 128;                    /* grid points per tile */
+constexpr int BK = 64;                     /* stations: one 128-byte row of bf16 */
+constexpr int TILE_BYTES = BM * BK * 2;    /* 16 KB */
+constexpr int PAIR_BYTES = 2 * TILE_BYTES; /* hi + lo */
+constexpr int NSTAGE = 4;
+constexpr int TOPK = FK_TC_TOPK;
+constexpr int NTHREADS = 320;
+constexpr int SMEM_A = 2 * PAIR_BYTES;
+constexpr int SMEM_B = NSTAGE * PAIR_BYTES;
+constexpr int NBAR = 2 * NSTAGE + 7;
+constexpr int SMEM_BYTES = SMEM_A + SMEM_B + NBAR * 8 + 1024;
+constexpr uint32_t TMEM_COLS = 512;
+
+/* instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A BF16 (7-9 = 1),
+ * B BF16 (10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24 */
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+
+/* byte offset of element (row, k) inside one swizzled 16 KB tile */
+__host__ __device__ __forceinline__ uint32_t swz(int row, int k)
+{
+    return (uint32_t)row * 128u + ((uint32_t)(((k >> 3) ^ (row & 7))) << 4) + (uint32_t)(k & 7) * 2u;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+/* shared-memory matrix descriptor: 128-byte swizzle, K-major; leading byte
+ * offset 16 B (unused by this layout), stride 1024 B between 8-row groups,
+ * descriptor version 1 (bit 46) */
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+/* Bounded wait for the phase of the given parity.  False on timeout or when
+ * another role has aborted. */
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort,
+                                          long long limit)
+{
+    for (long long i = 0; i < limit; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(IDESC), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+#define FKTC_R8(i) "=r"(r[i]), "=r"(r[i + 1]), "=r"(r[i + 2]), "=r"(r[i + 3]), "=r"(r[i + 4]), \
+                   "=r"(r[i + 5]), "=r"(r[i + 6]), "=r"(r[i + 7])
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : FKTC_R8(0), FKTC_R8(8), FKTC_R8(16), FKTC_R8(24)
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct Params {
+    const uint8_t *apack;   /* [2 * nmg][hi, lo] event tiles */
+    const uint8_t *bpack;   /* [ntile][hi, lo] table tiles */
+    const float *q;         /* [ntile * BN] sum of centred squares (padding: +inf) */
+    int nev, ntile, nmg, npart, nitems;
+    float *cand_v;          /* [nev][npart][TOPK] */
+    int *cand_i;
+    int *error;
+    float *dbg;             /* optional: item 0's first accumulators, [256][128] */
+    long long spin_limit;
+};
+
+__device__ __forceinline__ void part_range(const Params &P, int p, int &tb, int &te)
+{
+    tb = (int)((long long)p * P.ntile / P.npart);
+    te = (int)((long long)(p + 1) * P.ntile / P.npart);
+}
+
+__device__ __forceinline__ void set_abort(volatile int *abort, int *error, int code)
+{
+    *abort = 1;
+    atomicCAS(error, 0, code);
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1) l2_tc_kernel(Params P)
+{
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_abort;
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t sA = (raw + 1023u) & ~1023u;
+    const uint32_t sB = sA + SMEM_A;
+    const uint32_t bar0 = sB + SMEM_B;
+    /* barriers: full[s], empty[s], a_full, a_empty, tfull[2], tempty[2], drain */
+    auto FULL = [&](int s) { return bar0 + 8u * (uint32_t)s; };
+    auto EMPTY = [&](int s) { return bar0 + 8u * (uint32_t)(NSTAGE + s); };
+    const uint32_t A_FULL = bar0 + 8u * (2 * NSTAGE);
+    const uint32_t A_EMPTY = A_FULL + 8u;
+    auto TFULL = [&](int b) { return A_EMPTY + 8u + 8u * (uint32_t)b; };
+    auto TEMPTY = [&](int b) { return A_EMPTY + 24u + 8u * (uint32_t)b; };
+    const uint32_t DRAIN = A_EMPTY + 40u;
+    volatile int *abort = &s_abort;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NSTAGE; ++s) { mbar_init(FULL(s), 1); mbar_init(EMPTY(s), 1); }
+        mbar_init(A_FULL, 1);
+        mbar_init(A_EMPTY, 1);
+        for (int b = 0; b < 2; ++b) { mbar_init(TFULL(b), 1); mbar_init(TEMPTY(b), 8); }
+        mbar_init(DRAIN, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_abort = 0;
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const long long lim = P.spin_limit;
+
+    if (warp == 0 && lane == 0) {
+        /* ---- producer ---- */
+        int stage = 0;
+        uint32_t ph = 0, a_ph = 0;
+        bool issued[NSTAGE] = {false, false, false, false};
+        uint32_t iss_ph[NSTAGE] = {0, 0, 0, 0};
+        bool a_issued = false;
+        uint32_t a_iss_ph = 0;
+        for (int item = blockIdx.x; item < P.nitems && !*abort; item += gridDim.x) {
+            const int p = item / P.nmg, mg = item % P.nmg;
+            if (!mbar_wait(A_EMPTY, a_ph ^ 1u, abort, lim)) { set_abort(abort, P.error, 1); break; }
+            mbar_expect_tx(A_FULL, (uint32_t)SMEM_A);
+            bulk_g2s(sA, P.apack + (size_t)(2 * mg) * PAIR_BYTES, (uint32_t)PAIR_BYTES, A_FULL);
+            bulk_g2s(sA + PAIR_BYTES, P.apack + (size_t)(2 * mg + 1) * PAIR_BYTES, (uint32_t)PAIR_BYTES,
+                     A_FULL);
+            a_issued = true;
+            a_iss_ph = a_ph;
+            a_ph ^= 1u;
+            int tb, te;
+            part_range(P, p, tb, te);
+            for (int t = tb; t < te; ++t) {
+                if (!mbar_wait(EMPTY(stage), ph ^ 1u, abort, lim)) { set_abort(abort, P.error, 2); break; }
+                mbar_expect_tx(FULL(stage), (uint32_t)PAIR_BYTES);
+                bulk_g2s(sB + (uint32_t)stage * PAIR_BYTES, P.bpack + (size_t)t * PAIR_BYTES,
+                         (uint32_t)PAIR_BYTES, FULL(stage));
+                issued[stage] = true;
+                iss_ph[stage] = ph;
+                if (++stage == NSTAGE) { stage = 0; ph ^= 1u; }
+            }
+        }
+        /* every copy this thread issued has landed before the CTA exits */
+        for (int s = 0; s < NSTAGE; ++s)
+            if (issued[s])
+                for (long long i = 0; i < lim && !mbar_try(FULL(s), iss_ph[s]); ++i) {}
+        if (a_issued)
+            for (long long i = 0; i < lim && !mbar_try(A_FULL, a_iss_ph); ++i) {}
+    } else if (warp == 1 && lane == 0) {
+        /* ---- MMA issuer ---- */
+        int stage = 0, buf = 0;
+        uint32_t ph = 0, a_ph = 0;
+        uint32_t tph[2] = {0, 0};
+        for (int item = blockIdx.x; item < P.nitems && !*abort; item += gridDim.x) {
+            const int p = item / P.nmg;
+            if (!mbar_wait(A_FULL, a_ph, abort, lim)) { set_abort(abort, P.error, 3); break; }
+            a_ph ^= 1u;
+            tc_fence_after();
+            int tb, te;
+            part_range(P, p, tb, te);
+            bool ok = true;
+            for (int t = tb; t < te; ++t) {
+                if (!mbar_wait(TEMPTY(buf), tph[buf] ^ 1u, abort, lim)) { ok = false; set_abort(abort, P.error, 4); break; }
+                if (!mbar_wait(FULL(stage), ph, abort, lim)) { ok = false; set_abort(abort, P.error, 5); break; }
+                tc_fence_after();
+                const uint32_t b_hi = sB + (uint32_t)stage * PAIR_BYTES, b_lo = b_hi + TILE_BYTES;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t d = tmem + (uint32_t)buf * 256u + (uint32_t)h * 128u;
+                    const uint32_t a_hi = sA + (uint32_t)h * PAIR_BYTES, a_lo = a_hi + TILE_BYTES;
+#pragma unroll
+                    for (int k = 0; k < BK / 16; ++k) {
+                        const uint32_t ko = (uint32_t)k * 32u;
+                        mma_bf16(d, sdesc(a_hi + ko), sdesc(b_hi + ko), k > 0 ? 1u : 0u);
+                        mma_bf16(d, sdesc(a_hi + ko), sdesc(b_lo + ko), 1u);
+                        mma_bf16(d, sdesc(a_lo + ko), sdesc(b_hi + ko), 1u);
+                    }
+                }
+                mma_commit(EMPTY(stage));
+                mma_commit(TFULL(buf));
+                if (++stage == NSTAGE) { stage = 0; ph ^= 1u; }
+                tph[buf] ^= 1u;
+                buf ^= 1;
+            }
+            mma_commit(A_EMPTY);
+            if (!ok) break;
+        }
+        /* no MMA of this CTA is in flight when TMEM is freed */
+        mma_commit(DRAIN);
+        for (long long i = 0; i < lim && !mbar_try(DRAIN, 0); ++i) {}
+    } else if (warp >= 2) {
+        /* ---- epilogue: thread = one event row of one event tile ---- */
+        const int quad = warp & 3;            /* TMEM lane quarter this warp may read */
+        const int h = (warp - 2) >> 2;        /* event tile 0 or 1 of the group */
+        const int row = quad * 32 + lane;
+        int buf = 0;
+        uint32_t tph[2] = {0, 0};
+        bool first_tile = true;
+        /* control flow stays warp-uniform: tcgen05.ld is .sync.aligned */
+        for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
+            if (__any_sync(0xffffffffu, *abort != 0)) break;
+            const int p = item / P.nmg, mg = item % P.nmg;
+            float bv[TOPK];
+            int bi[TOPK];
+#pragma unroll
+            for (int k = 0; k < TOPK; ++k) { bv[k] = 3.0e38f; bi[k] = -1; }
+            int tb, te;
+            part_range(P, p, tb, te);
+            bool ok = true;
+            for (int t = tb; t < te; ++t) {
+                const bool got = mbar_wait(TFULL(buf), tph[buf], abort, lim);
+                if (!__all_sync(0xffffffffu, got)) {
+                    ok = false;
+                    if (lane == 0) set_abort(abort, P.error, 6);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)buf * 256u +
+                                       (uint32_t)h * 128u;
+                const float4 *qp = reinterpret_cast<const float4 *>(P.q + (size_t)t * BN);
+#pragma unroll 1
+                for (int c = 0; c < BN / 32; ++c) {
+                    uint32_t r[32];
+                    tmem_ld32(taddr + (uint32_t)c * 32u, r);
+                    if (P.dbg && first_tile && blockIdx.x == 0) {
+                        for (int j = 0; j < 32; ++j)
+                            P.dbg[(size_t)(h * BM + row) * BN + c * 32 + j] = __uint_as_float(r[j]);
+                    }
+#pragma unroll
+                    for (int j4 = 0; j4 < 8; ++j4) {
+                        const float4 qq = __ldg(qp + c * 8 + j4);
+                        const float qv[4] = {qq.x, qq.y, qq.z, qq.w};
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const float v = fmaf(-2.0f, __uint_as_float(r[j4 * 4 + u]), qv[u]);
+                            if (v < bv[TOPK - 1]) {
+                                const int g = t * BN + c * 32 + j4 * 4 + u;
+                                float cv = v;
+                                int ci = g;
+#pragma unroll
+                                for (int k = 0; k < TOPK; ++k) {
+                                    if (cv < bv[k]) {
+                                        const float tv = bv[k];
+                                        const int ti = bi[k];
+                                        bv[k] = cv; bi[k] = ci;
+                                        cv = tv; ci = ti;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+                first_tile = false;
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(TEMPTY(buf));
+                tph[buf] ^= 1u;
+                buf ^= 1;
+            }
+            if (!ok) break;
+            const int e = (2 * mg + h) * BM + row;
+            if (e < P.nev) {
+                const size_t o = ((size_t)e * P.npart + p) * TOPK;
+#pragma unroll
+                for (int k = 0; k < TOPK; ++k) { P.cand_v[o + k] = bv[k]; P.cand_i[o + k] = bi[k]; }
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS)
+                     : "memory");
+    }
+}
+
+/* ---- packing ------------------------------------------------------------ */
+
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 &hi, __nv_bfloat16 &lo)
+{
+    hi = __float2bfloat16_rn((float)x);
+    lo = __float2bfloat16_rn((float)(x - (double)__bfloat162float(hi)));
+}
+
+/* One thread per grid point (rows of the padded last tile included). */
+__global__ void pack_tables_kernel(int ngrd, int ldgrd, int ntf, int ntile,
+                                   const float *__restrict__ tables, uint8_t *__restrict__ bpack,
+                                   float *__restrict__ q)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ntile * BN) return;
+    const int tile = g / BN, r = g % BN;
+    uint8_t *hi = bpack + (size_t)tile * PAIR_BYTES, *lo = hi + TILE_BYTES;
+    const bool real = g < ngrd;
+    double mean = 0.0;
+    if (real) {
+        for (int i = 0; i < ntf; ++i) mean += (double)__ldg(tables + (size_t)i * ldgrd + g);
+        mean /= (double)ntf;
+    }
+    double qq = 0.0;
+    for (int c = 0; c < BK / 8; ++c) {
+        __align__(16) __nv_bfloat16 vh[8], vl[8];
+        for (int j = 0; j < 8; ++j) {
+            const int k = c * 8 + j;
+            double d = 0.0;
+            if (real && k < ntf) {
+                d = (double)__ldg(tables + (size_t)k * ldgrd + g) - mean;
+                qq += d * d;
+            }
+            split_bf16(d, vh[j], vl[j]);
+        }
+        const uint32_t off = swz(r, c * 8);
+        *reinterpret_cast<uint4 *>(hi + off) = *reinterpret_cast<const uint4 *>(vh);
+        *reinterpret_cast<uint4 *>(lo + off) = *reinterpret_cast<const uint4 *>(vl);
+    }
+    q[g] = real ? (float)qq : __int_as_float(0x7f800000); /* +inf: never a candidate */
+}
+
+/* One thread per event row slot.  Rows of ineligible or padding events are
+ * zero (their scores are not used). */
+__global__ void pack_events_kernel(int nev, int nrows, int ntf, const double *__restrict__ obs,
+                                   const unsigned char *__restrict__ elig, uint8_t *__restrict__ apack)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nrows) return;
+    const int tile = e / BM, r = e % BM;
+    uint8_t *hi = apack + (size_t)tile * PAIR_BYTES, *lo = hi + TILE_BYTES;
+    const bool use = e < nev && elig[e];
+    double mean = 0.0;
+    if (use) {
+        for (int i = 0; i < ntf; ++i) mean += obs[(size_t)e * ntf + i];
+        mean /= (double)ntf;
+    }
+    for (int c = 0; c < BK / 8; ++c) {
+        __align__(16) __nv_bfloat16 vh[8], vl[8];
+        for (int j = 0; j < 8; ++j) {
+            const int k = c * 8 + j;
+            const double d = (use && k < ntf) ? obs[(size_t)e * ntf + k] - mean : 0.0;
+            split_bf16(d, vh[j], vl[j]);
+        }
+        const uint32_t off = swz(r, c * 8);
+        *reinterpret_cast<uint4 *>(hi + off) = *reinterpret_cast<const uint4 *>(vh);
+        *reinterpret_cast<uint4 *>(lo + off) = *reinterpret_cast<const uint4 *>(vl);
+    }
+}
+
+/* ---- FP64 re-score -------------------------------------------------------- */
+
+__device__ __forceinline__ bool lex_lt(float v, int i, float w, int j)
+{
+    return v < w || (v == w && i < j);
+}
+
+__device__ __forceinline__ double warp_sum(double x)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+/* One warp per event: take the R best candidates by approximate score (ties
+ * by index), evaluate the reference's misfit in FP64 at each, keep the
+ * minimum (first index among equal misfits). */
+__global__ void rescore_kernel(int nev, int npart, int ngrd, int ntf, int ldgrd, int R,
+                               const float *__restrict__ tables, const double *__restrict__ obs,
+                               const double *__restrict__ wts, const unsigned char *__restrict__ elig,
+                               const float *__restrict__ cand_v, const int *__restrict__ cand_i,
+                               int *__restrict__ out_idx, double *__restrict__ out_t0,
+                               double *__restrict__ out_obj)
+{
+    const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (e >= nev || !elig[e]) return;
+    const int C = npart * TOPK;
+    const float *cv = cand_v + (size_t)e * C;
+    const int *ci = cand_i + (size_t)e * C;
+    const double *o = obs + (size_t)e * ntf, *w = wts + (size_t)e * ntf;
+    float pv = -3.0e38f;
+    int pi = -1;
+    double best_obj = 1.0e300, best_t0 = 0.0;
+    int best_g = 0x7fffffff;
+    for (int r = 0; r < R; ++r) {
+        float mv = 3.0e38f;
+        int mi = 0x7fffffff;
+        for (int c = lane; c < C; c += 32) {
+            const int i = ci[c];
+            const float v = cv[c];
+            if (i >= 0 && i < ngrd && lex_lt(pv, pi, v, i) && lex_lt(v, i, mv, mi)) { mv = v; mi = i; }
+        }
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const float ov = __shfl_xor_sync(0xffffffffu, mv, s);
+            const int oi = __shfl_xor_sync(0xffffffffu, mi, s);
+            if (lex_lt(ov, oi, mv, mi)) { mv = ov; mi = oi; }
+        }
+        if (mi == 0x7fffffff) break;
+        pv = mv;
+        pi = mi;
+        const int g = mi;
+        double a = 0.0, sw = 0.0;
+        for (int i = lane; i < ntf; i += 32)
+            if (w[i] > 0.0) {
+                a += w[i] * (o[i] - (double)__ldg(tables + (size_t)i * ldgrd + g));
+                sw += w[i];
+            }
+        a = warp_sum(a);
+        sw = warp_sum(sw);
+        const double t0 = a / sw;
+        double ob = 0.0;
+        for (int i = lane; i < ntf; i += 32)
+            if (w[i] > 0.0) {
+                const double rr = w[i] * (o[i] - (double)__ldg(tables + (size_t)i * ldgrd + g) - t0);
+                ob += 0.5 * rr * rr;
+            }
+        ob = warp_sum(ob);
+        if (ob < best_obj || (ob == best_obj && g < best_g)) { best_obj = ob; best_g = g; best_t0 = t0; }
+    }
+    if (lane == 0) {
+        out_idx[e] = best_g;
+        out_t0[e] = best_t0;
+        out_obj[e] = best_obj;
+    }
+}
+
+} // namespace fktc
+
+using namespace fktc;
+
+extern "C" size_t fk_locate_tc_table_bytes(int ngrd)
+{
+    const size_t ntile = ((size_t)ngrd + BN - 1) / BN;
+    return ntile * PAIR_BYTES;
+}
+
+extern "C" size_t fk_locate_tc_event_bytes(int nev)
+{
+    const size_t nmg = ((size_t)nev + 2 * BM - 1) / (2 * BM);
+    return nmg * 2 * PAIR_BYTES;
+}
+
+extern "C" int fk_locate_tc_pack_tables(int ngrd, int ldgrd, int ntf, const float *tables,
+                                        void *bpack, float *q, cudaStream_t s)
+{
+    if (ntf < 1 || ntf > BK) return (int)cudaErrorInvalidValue;
+    const int ntile = (ngrd + BN - 1) / BN;
+    const int n = ntile * BN;
+    pack_tables_kernel<<<(n + 255) / 256, 256, 0, s>>>(ngrd, ldgrd, ntf, ntile, tables,
+                                                       (uint8_t *)bpack, q);
+    return (int)cudaGetLastError();
+}
+
+/* Partitions of the grid: enough work items to fill whole waves of CTAs. */
+static int pick_npart(int nmg, int ntile, int nsm)
+{
+    int best = 1;
+    double best_eff = -1.0;
+    for (int waves = 1; waves <= 16; ++waves) {
+        int P = (waves * nsm + nmg - 1) / nmg;
+        if (P > ntile) P = ntile;
+        if (P < 1) P = 1;
+        const long long items = (long long)P * nmg;
+        const long long slots = (items + nsm - 1) / nsm * nsm;
+        const double eff = (double)items / (double)slots;
+        if (eff > best_eff + 1e-9) { best_eff = eff; best = P; }
+        if (eff > 0.97) break;
+    }
+    return best;
+}
+
+extern "C" int fk_locate_tc_npart(int nev, int ngrd)
+{
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int nmg = (nev + 2 * BM - 1) / (2 * BM);
+    const int ntile = (ngrd + BN - 1) / BN;
+    return pick_npart(nmg, ntile, nsm);
+}
+
+extern "C" int fk_locate_tc(int ngrd, int ldgrd, int ntf, const float *tables, const void *bpack,
+                            const float *q, int nev, const double *obs, const double *wts,
+                            const unsigned char *elig, void *apack, int npart, float *cand_v,
+                            int *cand_i, int rescore, int *out_idx, double *out_t0,
+                            double *out_obj, int *error, float *dbg, cudaStream_t s)
+{
+    if (nev <= 0) return 0;
+    if (ntf < 1 || ntf > BK || npart < 1) return (int)cudaErrorInvalidValue;
+    const int nmg = (nev + 2 * BM - 1) / (2 * BM);
+    const int ntile = (ngrd + BN - 1) / BN;
+    if (npart > ntile) return (int)cudaErrorInvalidValue;
+    pack_events_kernel<<<(nmg * 2 * BM + 127) / 128, 128, 0, s>>>(nev, nmg * 2 * BM, ntf, obs, elig,
+                                                                  (uint8_t *)apack);
+    static int attr_done = 0;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cs);
+    if (!attr_done && cs == cudaStreamCaptureStatusNone) {
+        cudaError_t e = cudaFuncSetAttribute(l2_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             SMEM_BYTES);
+        if (e != cudaSuccess) return (int)e;
+        attr_done = 1;
+    }
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    Params P;
+    P.apack = (const uint8_t *)apack;
+    P.bpack = (const uint8_t *)bpack;
+    P.q = q;
+    P.nev = nev;
+    P.ntile = ntile;
+    P.nmg = nmg;
+    P.npart = npart;
+    P.nitems = nmg * npart;
+    P.cand_v = cand_v;
+    P.cand_i = cand_i;
+    P.error = error;
+    P.dbg = dbg;
+    P.spin_limit = 1ll << 22;
+    const int grid = P.nitems < nsm ? P.nitems : nsm;
+    l2_tc_kernel<<<grid, NTHREADS, SMEM_BYTES, s>>>(P);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return (int)e;
+    if (rescore > 0) {
+        rescore_kernel<<<(nev * 32 + 255) / 256, 256, 0, s>>>(nev, npart, ngrd, ntf, ldgrd, rescore, tables,
+                                                              obs, wts, elig, cand_v, cand_i, out_idx,
+                                                              out_t0, out_obj);
+        e = cudaGetLastError();
+    }
+    return (int)e;
+}

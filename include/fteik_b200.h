@@ -321,6 +321,22 @@ void fteik_b200_batch3d_finalize(void);
 void fteik_b200_locate_locateEvents(int n, const int ev[], int optIndx[],
                                     double t0Opt[], double objOpt[], int *ierr);
 
+/* Search method of locate_locateEvent and fteik_b200_locate_locateEvents
+ * (the reference has one method, locate.F90:620-744):
+ *   0  exact FP32 search, the reference's arithmetic and optimum (default);
+ *   1  tensor-core search: the L2 misfit ranked by a BF16 hi+lo contraction
+ *      with FP32 accumulation, the best candidates re-scored with the
+ *      reference's formula in FP64 (t0Opt and objOpt are those FP64 values).
+ *      Events whose picks do not cover every table with one common weight
+ *      fall back to method 0. */
+void fteik_b200_locate_setMethod(int method, int *ierr);
+/* Candidates per event re-scored in FP64 by method 1 (default 8). */
+void fteik_b200_locate_setRescoreCandidates(int ncand, int *ierr);
+/* Diagnostic for method 1: enable = 1 records, at the next search, the first
+ * two accumulator tiles (events 1..256 x grid points 1..128, FP32, row-major
+ * by event); enable = 0 copies them to out (32768 floats, may be NULL). */
+void fteik_b200_locate_debugAccumulators(int enable, float *out, int *ierr);
+
 /* Allocation-free grid search (no counterpart in the reference).  For
  * callers that cannot let a library allocate device memory -- a host that
  * hands out every device buffer from its own pool, or a service that must

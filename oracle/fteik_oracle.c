@@ -1319,3 +1319,48 @@ void orc_locate_l2_points64(int ngrd, int ldgrd, int ntf, const float *tables,
         t0[p] = a;
     }
 }
+
+void orc_locate_l2_best64(int ngrd, int ldgrd, int ntf, const float *tables,
+                          const double *obs, const double *wts, int nthreads,
+                          int *idx, double *t0Opt, double *objOpt)
+{
+    /* locate.F90:675-708 evaluated in FP64 at every grid point; MINLOC
+     * (first minimum) as locate.F90:122 */
+    double sw = 0.0;
+    for (int i = 0; i < ntf; i++) if (wts[i] > 0.0) sw += wts[i];
+    int nth = nthreads > 0 ? nthreads : 1;
+    double *bo = (double *)malloc(sizeof(double) * (size_t)nth);
+    double *bt = (double *)malloc(sizeof(double) * (size_t)nth);
+    int *bg = (int *)malloc(sizeof(int) * (size_t)nth);
+    for (int t = 0; t < nth; t++) { bo[t] = HUGE_VAL; bt[t] = 0.0; bg[t] = -1; }
+#pragma omp parallel num_threads(nth)
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        /* static contiguous chunks: each thread's first minimum is the
+         * first within its chunk, chunks are merged in order below */
+        long long lo = (long long)ngrd * tid / nth, hi = (long long)ngrd * (tid + 1) / nth;
+        for (long long g = lo; g < hi; g++) {
+            double a = 0.0;
+            for (int i = 0; i < ntf; i++)
+                if (wts[i] > 0.0) a += wts[i] * (obs[i] - (double)tables[(size_t)i * ldgrd + g]);
+            a /= sw;
+            double o = 0.0;
+            for (int i = 0; i < ntf; i++)
+                if (wts[i] > 0.0) {
+                    double r = wts[i] * (obs[i] - (double)tables[(size_t)i * ldgrd + g] - a);
+                    o += 0.5 * r * r;
+                }
+            if (o < bo[tid]) { bo[tid] = o; bt[tid] = a; bg[tid] = (int)g; }
+        }
+    }
+    int best = 0;
+    for (int t = 1; t < nth; t++)
+        if (bo[t] < bo[best]) best = t;
+    *idx = bg[best];
+    *t0Opt = bt[best];
+    *objOpt = bo[best];
+    free(bo); free(bt); free(bg);
+}

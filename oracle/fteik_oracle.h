@@ -144,6 +144,13 @@ void orc_locate_l2_points64(int ngrd, int ldgrd, int ntf, const float *tables,
                             const unsigned char *skip, int npts,
                             const int *pts, double *obj, double *t0);
 
+/* Exhaustive FP64 search with the same misfit: picks and weights in FP64
+ * (reduced picks, weight 0 = skipped), tables FP32.  Returns the 0-based
+ * index of the first minimum and the FP64 t0 / misfit there. */
+void orc_locate_l2_best64(int ngrd, int ldgrd, int ntf, const float *tables,
+                          const double *obs, const double *wts, int nthreads,
+                          int *idx, double *t0Opt, double *objOpt);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,3 +50,34 @@ def interior_source(n, h, seed):
     nz, nx, ny = n
     return (rng.uniform(0.1, 0.9) * (nz - 1) * h[0], rng.uniform(0.1, 0.9) * (nx - 1) * h[1],
             rng.uniform(0.1, 0.9) * (ny - 1) * h[2])
+
+
+def station_tables(nz, nx, ny, h, nsta, v=3000.0, seed=11):
+    """Constant-velocity travel-time tables from nsta surface stations to every
+    grid node, FP32, shape (nsta, nz*nx*ny), node index z fastest."""
+    rng = np.random.default_rng(seed)
+    sx = rng.uniform(0, (nx - 1) * h, nsta)
+    sy = rng.uniform(0, (ny - 1) * h, nsta)
+    z = np.arange(nz) * h
+    x = np.arange(nx) * h
+    y = np.arange(ny) * h
+    Y, X, Z = np.meshgrid(y, x, z, indexing="ij")      # [ny][nx][nz] -> z fastest
+    Z, X, Y = Z.ravel(), X.ravel(), Y.ravel()
+    t = np.empty((nsta, Z.size), np.float32)
+    for i in range(nsta):
+        t[i] = (np.sqrt(Z ** 2 + (X - sx[i]) ** 2 + (Y - sy[i]) ** 2) / v).astype(np.float32)
+    return t
+
+
+def synthetic_events(tables, nev, seed=5, noise=0.02, outlier_frac=0.05):
+    """Events at random grid nodes: picks = table times + origin time U[0,60]
+    + N(0, noise), a fraction of picks replaced by exact + U[-1, 1] s.
+    Returns (true node indices, picks [nev][ntf] FP64)."""
+    rng = np.random.default_rng(seed)
+    ntf, ngrd = tables.shape
+    true = rng.integers(0, ngrd, nev)
+    exact = tables[:, true].T.astype(np.float64) + rng.uniform(0, 60, (nev, 1))
+    picks = exact + rng.normal(0, noise, exact.shape)
+    out = rng.random(exact.shape) < outlier_frac
+    picks[out] = exact[out] + rng.uniform(-1, 1, out.sum())
+    return true, picks

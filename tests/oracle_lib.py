@@ -207,3 +207,20 @@ def locate_l2_field(tables, obs, wts, skip, nthreads=0):
                             _ptr(wts, c_float), _ptr(skip, ctypes.c_ubyte), int(nthreads),
                             _ptr(obj, c_float), _ptr(t0, c_float))
     return obj, t0
+
+
+def locate_l2_best64(tables, obs, wts, nthreads=0):
+    """Exhaustive FP64 L2 search for one event: 0-based index of the first
+    minimum, FP64 t0 and misfit.  obs/wts: FP64 per table (weight 0 =
+    skipped), picks already reduced."""
+    lib = load()
+    tables = np.ascontiguousarray(tables, np.float32)
+    ntf, ngrd = tables.shape
+    obs = np.ascontiguousarray(obs, np.float64)
+    wts = np.ascontiguousarray(wts, np.float64)
+    oi, t0, ob = c_int(), c_double(), c_double()
+    nth = int(nthreads) if nthreads else (os.cpu_count() or 1)
+    lib.orc_locate_l2_best64(ngrd, ngrd, ntf, _ptr(tables, c_float), _ptr(obs, c_double),
+                             _ptr(wts, c_double), nth, ctypes.byref(oi), ctypes.byref(t0),
+                             ctypes.byref(ob))
+    return oi.value, t0.value, ob.value

@@ -1,0 +1,130 @@
+"""Tensor-core L2 search (locate method 1) against the CPU oracle.
+
+* The raw accumulators equal an exact emulation of the BF16 hi+lo
+  contraction (checks operand packing, swizzle and MMA descriptors).
+* The located node equals the exhaustive FP64 search of the oracle, and t0 /
+  misfit equal the oracle's FP64 values there.
+* Events outside the tensor-core form (a skipped pick, unequal weights) fall
+  back to the exact FP32 search and match it bit for bit.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from models import station_tables, synthetic_events
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16(x32):
+    """Round float32 to bfloat16 (nearest even), returned as float32."""
+    b = np.ascontiguousarray(x32, np.float32).view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
+    return b.astype(np.uint32).view(np.float32)
+
+
+def _split(d64):
+    hi = _bf16(d64.astype(np.float32))
+    lo = _bf16((d64 - hi.astype(np.float64)).astype(np.float32))
+    return hi.astype(np.float64), lo.astype(np.float64)
+
+
+def _locator(fk, tables, picks, wts=None):
+    ntf, ngrd = tables.shape
+    nev = picks.shape[0]
+    loc = fk.Locator(nev, ntf, ngrd)
+    for k in range(ntf):
+        loc.setTravelTimeField32f(k + 1, tables[k])
+    o2t = np.arange(1, ntf + 1)
+    for e in range(nev):
+        w = np.ones(ntf) if wts is None else wts[e]
+        loc.setObservation(e + 1, o2t, picks[e], w)
+    return loc
+
+
+def _reduced(picks):
+    return picks - picks.max(axis=1, keepdims=True)
+
+
+def test_accumulators_match_bf16_emulation(fk):
+    tables = station_tables(16, 24, 20, 100.0, 64, seed=3)
+    _, picks = synthetic_events(tables, 300, seed=4)
+    loc = _locator(fk, tables, picks)
+    loc.setMethod(1)
+    loc.debugAccumulators(True)
+    loc.locateEvents(np.arange(1, 301))
+    acc = loc.debugAccumulators(False).astype(np.float64)
+    # item 0 of CTA 0: events 0..255 x grid points 0..127
+    T = tables[:, :128].astype(np.float64)
+    Tp = T - T.mean(axis=0, keepdims=True)
+    o = _reduced(picks)[:256]
+    op = o - o.mean(axis=1, keepdims=True)
+    ah, al = _split(op)
+    bh, bl = _split(Tp.T)
+    want = ah @ bh.T + ah @ bl.T + al @ bh.T
+    scale = np.abs(ah) @ np.abs(bh).T + 1e-6
+    err = np.abs(acc - want) / scale
+    assert err.max() < 2e-6, f"max scaled error {err.max():.3g}"
+    loc.finalize()
+
+
+@pytest.mark.parametrize("shape,ntf,nev", [((16, 24, 20), 64, 300), ((13, 17, 11), 20, 37)])
+def test_tc_matches_fp64_exhaustive(fk, shape, ntf, nev):
+    tables = station_tables(*shape, 100.0, ntf, seed=7)
+    _, picks = synthetic_events(tables, nev, seed=8)
+    loc = _locator(fk, tables, picks)
+    loc.setMethod(1)
+    oi, t0, ob = loc.locateEvents(np.arange(1, nev + 1))
+    red = _reduced(picks)
+    tep = picks.max(axis=1)
+    w = np.ones(ntf)
+    miss = 0
+    for e in range(nev):
+        gi, gt0, gob = O.locate_l2_best64(tables, red[e], w)
+        if oi[e] - 1 != gi:
+            # only an exact FP64 tie may pick a different node
+            _, _, ob_here = O.locate_l2_best64(tables[:, [oi[e] - 1]], red[e], w)
+            assert abs(ob_here - gob) <= 1e-12 * max(gob, 1e-30), (e, oi[e] - 1, gi)
+            miss += 1
+            continue
+        assert abs(t0[e] - (gt0 + tep[e])) <= 1e-9 * max(1.0, abs(gt0 + tep[e]))
+        assert abs(ob[e] - gob) <= 1e-10 * max(gob, 1e-12)
+    assert miss <= nev // 100
+    loc.finalize()
+
+
+def test_ineligible_events_use_exact_search(fk):
+    tables = station_tables(12, 16, 14, 100.0, 32, seed=9)
+    _, picks = synthetic_events(tables, 20, seed=10)
+    wts = np.ones_like(picks)
+    wts[3, 5] = 0.0          # a skipped pick
+    wts[7, :] = 2.0          # uniform but not 1: still eligible
+    wts[9, 2] = 0.5          # unequal weights
+    loc = _locator(fk, tables, picks, wts)
+    ev = np.arange(1, 21)
+    oi0, t00, ob0 = loc.locateEvents(ev)
+    loc.setMethod(1)
+    oi1, t01, ob1 = loc.locateEvents(ev)
+    for e in (3, 9):
+        assert oi1[e] == oi0[e] and t01[e] == t00[e] and ob1[e] == ob0[e]
+    red = _reduced(picks)
+    gi, _, gob = O.locate_l2_best64(tables, red[7], wts[7])
+    assert oi1[7] - 1 == gi and abs(ob1[7] - gob) <= 1e-10 * gob
+    loc.finalize()
+
+
+def test_tc_single_event_and_rescore_count(fk):
+    tables = station_tables(10, 12, 9, 100.0, 16, seed=12)
+    _, picks = synthetic_events(tables, 3, seed=13)
+    loc = _locator(fk, tables, picks)
+    loc.setMethod(1)
+    loc.setRescoreCandidates(1)
+    a = loc.locateEvent(2)
+    loc.setRescoreCandidates(32)
+    b = loc.locateEvent(2)
+    gi, gt0, gob = O.locate_l2_best64(tables, _reduced(picks)[1], np.ones(16))
+    assert b[0] - 1 == gi
+    assert a[2] >= b[2]
+    with pytest.raises(RuntimeError):
+        loc.setMethod(5)
+    loc.finalize()
