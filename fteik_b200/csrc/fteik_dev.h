@@ -168,27 +168,26 @@ int fk_locate_l2_exact(int ngrd, int ldgrd, int ntf, const float *tables,
 size_t fk_locate_l2_exact_scratch(int ngrd, int nev);
 
 /* Tensor-core L2 search (locate_tc.cu).  Events with every table picked at
- * one common weight (elig[e] = 1) are ranked by a BF16 hi+lo contraction and
- * their best candidates re-scored in FP64.
- *   pack_tables: tables [ntf][ldgrd] -> bpack (fk_locate_tc_table_bytes) and
- *                q [ntiles * 128] floats (ntiles = ceil(ngrd / 128)).
+ * one common weight (elig[e] = 1) are ranked by a BF16 hi+lo contraction in
+ * runs of 32 grid points; the best runs are re-scored point by point in FP64.
+ *   pack_tables: tables [ntf][ldgrd] -> bpack (fk_locate_tc_table_bytes).
  *   fk_locate_tc: obs / wts [nev][ntf] FP64 picks (reduced) and weights;
  *                apack scratch (fk_locate_tc_event_bytes); cand_v / cand_i
- *                [nev][npart][FK_TC_TOPK]; rescore = candidates re-scored per
- *                event (0: ranking only); out_idx 0-based, out_t0 / out_obj
- *                FP64; error: device int, 0 on success; dbg optional
- *                [256][128] floats of the first accumulators. */
+ *                [nev][npart][FK_TC_TOPK] (run minima / run numbers);
+ *                rescore = runs re-scored per event (0: ranking only);
+ *                out_idx 0-based, out_t0 / out_obj FP64; error: device int,
+ *                0 on success; dbg optional [256][128] floats of the first
+ *                accumulators. */
 #define FK_TC_TOPK 4
 size_t fk_locate_tc_table_bytes(int ngrd);
 size_t fk_locate_tc_event_bytes(int nev);
 int fk_locate_tc_npart(int nev, int ngrd);
 int fk_locate_tc_pack_tables(int ngrd, int ldgrd, int ntf, const float *tables, void *bpack,
-                             float *q, cudaStream_t s);
+                             cudaStream_t s);
 int fk_locate_tc(int ngrd, int ldgrd, int ntf, const float *tables, const void *bpack,
-                 const float *q, int nev, const double *obs, const double *wts,
-                 const unsigned char *elig, void *apack, int npart, float *cand_v, int *cand_i,
-                 int rescore, int *out_idx, double *out_t0, double *out_obj, int *error,
-                 float *dbg, cudaStream_t s);
+                 int nev, const double *obs, const double *wts, const unsigned char *elig,
+                 void *apack, int npart, float *cand_v, int *cand_i, int rescore, int *out_idx,
+                 double *out_t0, double *out_obj, int *error, float *dbg, cudaStream_t s);
 
 #ifdef __cplusplus
 }

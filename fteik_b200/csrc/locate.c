@@ -32,7 +32,6 @@ static struct {
     double *obs64_dev, *w64_dev;
     unsigned char *elig_dev;
     void *bpack;
-    float *q;
     void *apack;
     size_t apack_bytes;
     float *cand_v;
@@ -52,7 +51,7 @@ void locate_finalize(void)
     fk_dfree(SL.idx_dev); fk_dfree(SL.t0_dev); fk_dfree(SL.obj_dev); fk_dfree(SL.scratch);
     free(SL.obs64); free(SL.w64); free(SL.elig);
     fk_dfree(SL.obs64_dev); fk_dfree(SL.w64_dev); fk_dfree(SL.elig_dev); fk_dfree(SL.bpack);
-    fk_dfree(SL.q); fk_dfree(SL.apack); fk_dfree(SL.cand_v); fk_dfree(SL.cand_i);
+    fk_dfree(SL.apack); fk_dfree(SL.cand_v); fk_dfree(SL.cand_i);
     fk_dfree(SL.tc_idx); fk_dfree(SL.tc_t0); fk_dfree(SL.tc_obj); fk_dfree(SL.err_dev);
     fk_dfree(SL.dbg_dev);
     memset(&SL, 0, sizeof(SL));
@@ -296,13 +295,11 @@ static int pack_tables(void)
 {
     if (!SL.tables_dirty && SL.bpack) return 0;
     if (!SL.bpack) {
-        const size_t ntile = ((size_t)SL.ngrd + 127) / 128;
         SL.bpack = fk_dalloc(fk_locate_tc_table_bytes(SL.ngrd), "locate: table pack");
-        SL.q = (float *)fk_dalloc(sizeof(float) * ntile * 128, "locate: table pack");
         SL.err_dev = (int *)fk_dalloc(sizeof(int), "locate: table pack");
-        if (!SL.bpack || !SL.q || !SL.err_dev) return 1;
+        if (!SL.bpack || !SL.err_dev) return 1;
     }
-    int e = fk_locate_tc_pack_tables(SL.ngrd, SL.ldgrd, SL.ntf, SL.tables, SL.bpack, SL.q, fk_stream());
+    int e = fk_locate_tc_pack_tables(SL.ngrd, SL.ldgrd, SL.ntf, SL.tables, SL.bpack, fk_stream());
     if (fk_check(e, "locate: table pack")) return 1;
     SL.tables_dirty = false;
     return 0;
@@ -345,7 +342,7 @@ static int locate_range_tc(int e0, int n, int *idx, double *t0, double *obj)
     cudaStream_t s = fk_stream();
     int e = (int)cudaMemsetAsync(SL.err_dev, 0, sizeof(int), s);
     if (!e)
-        e = fk_locate_tc(SL.ngrd, SL.ldgrd, SL.ntf, SL.tables, SL.bpack, SL.q, n,
+        e = fk_locate_tc(SL.ngrd, SL.ldgrd, SL.ntf, SL.tables, SL.bpack, n,
                          SL.obs64_dev + (size_t)e0 * SL.ntf, SL.w64_dev + (size_t)e0 * SL.ntf,
                          SL.elig_dev + e0, SL.apack, npart, SL.cand_v, SL.cand_i, SL.rescore,
                          SL.tc_idx, SL.tc_t0, SL.tc_obj, SL.err_dev, SL.dbg_dev, s);
@@ -387,7 +384,7 @@ void fteik_b200_locate_setRescoreCandidates(int ncand, int *ierr)
 {
     *ierr = 0;
     if (ncand < 1 || ncand > 256) {
-        FK_ERR("fteik_b200_locate_setRescoreCandidates: ncand=%d must be in [1,256]", ncand);
+        FK_ERR("fteik_b200_locate_setRescoreCandidates: ncand=%d must be in [1,256] (runs of 32 grid points)", ncand);
         *ierr = 1;
         return;
     }

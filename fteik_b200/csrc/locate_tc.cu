@@ -9,35 +9,44 @@
  * equals (1/2) w^2 sum_i (o'_i - T'_i(g))^2, where o' is the picks minus their
  * mean and T'(g) the tables at g minus their mean over tables.  Because
  * sum_i o'_i = 0 this is
- *     obj(g) = (1/2) w^2 ( p + q(g) - 2 sum_i o'_i T'_i(g) ),
+ *     obj(g) = (1/2) w^2 ( p + s(g) ),   s(g) = q(g) - 2 sum_i o'_i T'_i(g),
  *     p = sum o'^2 (per event),  q(g) = sum T'(g)^2 (per grid point),
- * so ranking grid points needs one events x stations by stations x points
- * product.  It runs on tcgen05 in BF16 with FP32 accumulation, each operand
- * split as x = hi + lo (hi = bf16(x), lo = bf16(x - hi)) and the product
- * formed as hi*hi + hi*lo + lo*hi (relative error about 2^-16 per term).
- * Each CTA keeps, per event and per partition of the grid, the four best
- * approximate scores; a second kernel re-scores the best candidates in FP64
- * with the reference's formula on the FP32 tables and returns the minimum
- * (first index among equal misfits).
+ * so ranking grid points by s needs one events x stations by stations x points
+ * product.  It runs on tcgen05 in BF16 with FP32 accumulation:
+ *   - each operand is split as x = hi + lo (hi = bf16(x), lo = bf16(x - hi));
+ *     the product is hi*hi + hi*lo + lo*hi (relative error about 2^-16);
+ *   - the event operand carries -2 o' (an exact scaling of the split);
+ *   - q(g) enters as one more K step: the event side holds 1, 1, 1 and the
+ *     table side q's three-way bf16 split (about 2^-24 relative), so the
+ *     accumulator is s(g) itself.
+ * Every thread of the epilogue owns one event row; it reduces each run of 32
+ * grid points to its minimum and keeps the four best runs of its partition.
+ * A second kernel takes each event's best runs over all partitions and
+ * evaluates every point of them with the reference's formula in FP64 on the
+ * FP32 tables (one lane per point, coalesced), returning the minimum (first
+ * index among equal misfits).
  *
- * Operand layout: both operands are K-major (stations contiguous) in the
- * tcgen05 128-byte swizzled canonical form, prepacked in global memory so
- * that one untiled bulk copy moves a whole tile into shared memory:
- *   tile = 128 rows x 64 stations of bf16 = 16 KB, row r at r * 128 bytes,
- *   16-byte chunk c of row r stored at chunk position c ^ (r % 8);
- *   a tile pair is [hi tile][lo tile] = 32 KB.
- * Grid points of the padded last table tile score +inf and never enter a
- * candidate list.
- * Tables: one tile pair per 128 grid points.  Events: one pair per 128 events.
+ * Operand layout (all K-major, prepacked in global memory so that one untiled
+ * bulk copy moves a tile into shared memory):
+ *   main tile: 128 rows x 64 stations of bf16 = 16 KB in the 128-byte
+ *     swizzled canonical form: row r at r * 128 bytes, 16-byte chunk c of row
+ *     r at chunk position c ^ (r % 8);
+ *   extra tile (the q step): 128 rows x 16 k of bf16 = 4 KB, no swizzle:
+ *     8-row groups 256 bytes apart, k 0-7 and 8-15 in two 128-byte halves,
+ *     row r of a group at 16 r;
+ *   table tile = [hi][lo][extra] = 36 KB per 128 grid points;
+ *   event tile = [hi][lo] = 32 KB per 128 events; the event side of the extra
+ *     step is the same for all rows and is built once in shared memory.
+ * Grid points of the padded last table tile get q = 1e30 and T' = 0.
  *
  * Kernel roles (320 threads, one CTA per SM):
- *   warp 0, one lane   bulk copies: the CTA's two event tiles per work item,
- *                      then a 4-stage ring of table tile pairs
- *   warp 1, one lane   tcgen05.mma: per table tile, 2 event tiles x 4 k-steps
- *                      x 3 products into a 128 x 128 FP32 accumulator each;
- *                      two accumulator sets (512 TMEM columns) alternate
- *   warps 2-9          tcgen05.ld of the accumulators, score q - 2 C, running
- *                      top 4 per event row
+ *   warp 0, one lane   bulk copies: two event tiles per work item, then a
+ *                      4-stage ring of table tiles
+ *   warp 1, one lane   tcgen05.mma: per table tile, 2 event tiles x (4 k-steps
+ *                      x 3 products + the q step) into a 128 x 128 FP32
+ *                      accumulator each; two accumulator sets (512 TMEM
+ *                      columns) alternate
+ *   warps 2-9          tcgen05.ld of the accumulators, run minima, top 4 runs
  * A work item is (event group of 256, grid partition).  Items are ordered
  * partition-major so the CTAs running at one time read the same table tiles
  * (L2 reuse).  Every wait is bounded; on timeout the CTA records an error,
@@ -55,26 +64,38 @@ namespace fktc {
 constexpr int BM = 128;                    /* events per tile (TMEM lanes) */
 constexpr int BN = 128;                    /* grid points per tile */
 constexpr int BK = 64;                     /* stations: one 128-byte row of bf16 */
+constexpr int RUN = 32;                    /* grid points per candidate run */
 constexpr int TILE_BYTES = BM * BK * 2;    /* 16 KB */
 constexpr int PAIR_BYTES = 2 * TILE_BYTES; /* hi + lo */
+constexpr int XTRA_BYTES = BN * 16 * 2;    /* 4 KB: the q step */
+constexpr int BTILE_BYTES = PAIR_BYTES + XTRA_BYTES;
 constexpr int NSTAGE = 4;
 constexpr int TOPK = FK_TC_TOPK;
 constexpr int NTHREADS = 320;
 constexpr int SMEM_A = 2 * PAIR_BYTES;
-constexpr int SMEM_B = NSTAGE * PAIR_BYTES;
+constexpr int SMEM_AX = XTRA_BYTES;
+constexpr int SMEM_B = NSTAGE * BTILE_BYTES;
 constexpr int NBAR = 2 * NSTAGE + 7;
-constexpr int SMEM_BYTES = SMEM_A + SMEM_B + NBAR * 8 + 1024;
+constexpr int SMEM_BYTES = SMEM_A + SMEM_AX + SMEM_B + NBAR * 8 + 1024;
 constexpr uint32_t TMEM_COLS = 512;
+constexpr float PAD_Q = 1.0e30f;
 
 /* instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A BF16 (7-9 = 1),
  * B BF16 (10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24 */
 constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                            ((uint32_t)(BM >> 4) << 24);
 
-/* byte offset of element (row, k) inside one swizzled 16 KB tile */
+/* byte offset of element (row, k) inside one swizzled 16 KB main tile */
 __host__ __device__ __forceinline__ uint32_t swz(int row, int k)
 {
     return (uint32_t)row * 128u + ((uint32_t)(((k >> 3) ^ (row & 7))) << 4) + (uint32_t)(k & 7) * 2u;
+}
+
+/* byte offset of element (row, k), k < 16, inside one 4 KB extra tile */
+__host__ __device__ __forceinline__ uint32_t xoff(int row, int k)
+{
+    return (uint32_t)(row >> 3) * 256u + (uint32_t)(k >> 3) * 128u + (uint32_t)(row & 7) * 16u +
+           (uint32_t)(k & 7) * 2u;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -82,13 +103,20 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p)
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-/* shared-memory matrix descriptor: 128-byte swizzle, K-major; leading byte
- * offset 16 B (unused by this layout), stride 1024 B between 8-row groups,
- * descriptor version 1 (bit 46) */
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr)
+/* shared-memory matrix descriptors (descriptor version 1 at bit 46):
+ * 128-byte swizzle, K-major: leading offset 16 B (unused), 8-row groups
+ * 1024 B apart; no swizzle, K-major: k halves 128 B apart (leading offset),
+ * 8-row groups 256 B apart (stride offset) */
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr)
 {
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
            ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ uint64_t sdesc_plain(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
+           ((uint64_t)(256 >> 4) << 32) | ((uint64_t)1 << 46);
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
@@ -162,26 +190,28 @@ __device__ __forceinline__ void mma_commit(uint32_t bar)
 #define FKTC_R8(i) "=r"(r[i]), "=r"(r[i + 1]), "=r"(r[i + 2]), "=r"(r[i + 3]), "=r"(r[i + 4]), \
                    "=r"(r[i + 5]), "=r"(r[i + 6]), "=r"(r[i + 7])
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+/* 32 consecutive columns of this warp's 32 TMEM lanes; no wait */
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *r)
 {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
         "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
         "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
         : FKTC_R8(0), FKTC_R8(8), FKTC_R8(16), FKTC_R8(24)
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        : "r"(taddr)
+        : "memory");
 }
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 struct Params {
     const uint8_t *apack;   /* [2 * nmg][hi, lo] event tiles */
-    const uint8_t *bpack;   /* [ntile][hi, lo] table tiles */
-    const float *q;         /* [ntile * BN] sum of centred squares (padding: +inf) */
+    const uint8_t *bpack;   /* [ntile][hi, lo, extra] table tiles */
     int nev, ntile, nmg, npart, nitems;
-    float *cand_v;          /* [nev][npart][TOPK] */
-    int *cand_i;
+    float *cand_v;          /* [nev][npart][TOPK]: run minima */
+    int *cand_i;            /*                     run numbers (first point / RUN) */
     int *error;
-    float *dbg;             /* optional: item 0's first accumulators, [256][128] */
+    float *dbg;             /* optional: CTA 0's first accumulators, [256][128] */
     long long spin_limit;
 };
 
@@ -204,7 +234,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) l2_tc_kernel(Params P)
     __shared__ int s_abort;
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t sA = (raw + 1023u) & ~1023u;
-    const uint32_t sB = sA + SMEM_A;
+    const uint32_t sAX = sA + SMEM_A;
+    const uint32_t sB = sAX + SMEM_AX;
     const uint32_t bar0 = sB + SMEM_B;
     /* barriers: full[s], empty[s], a_full, a_empty, tfull[2], tempty[2], drain */
     auto FULL = [&](int s) { return bar0 + 8u * (uint32_t)s; };
@@ -217,6 +248,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) l2_tc_kernel(Params P)
     volatile int *abort = &s_abort;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    /* event side of the q step: k = 0, 1, 2 hold 1.0, the rest 0 */
+    {
+        uint8_t *ax = smem_raw + (sAX - raw);
+        for (int i = threadIdx.x; i < XTRA_BYTES / 16; i += NTHREADS) {
+            const int row = i >> 1, khalf = i & 1;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (khalf == 0) { v.x = 0x3F803F80u; v.y = 0x00003F80u; }
+            *reinterpret_cast<uint4 *>(ax + xoff(row, khalf * 8)) = v;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
     if (threadIdx.x == 0) {
         for (int s = 0; s < NSTAGE; ++s) { mbar_init(FULL(s), 1); mbar_init(EMPTY(s), 1); }
         mbar_init(A_FULL, 1);
@@ -260,9 +302,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) l2_tc_kernel(Params P)
             part_range(P, p, tb, te);
             for (int t = tb; t < te; ++t) {
                 if (!mbar_wait(EMPTY(stage), ph ^ 1u, abort, lim)) { set_abort(abort, P.error, 2); break; }
-                mbar_expect_tx(FULL(stage), (uint32_t)PAIR_BYTES);
-                bulk_g2s(sB + (uint32_t)stage * PAIR_BYTES, P.bpack + (size_t)t * PAIR_BYTES,
-                         (uint32_t)PAIR_BYTES, FULL(stage));
+                mbar_expect_tx(FULL(stage), (uint32_t)BTILE_BYTES);
+                bulk_g2s(sB + (uint32_t)stage * BTILE_BYTES, P.bpack + (size_t)t * BTILE_BYTES,
+                         (uint32_t)BTILE_BYTES, FULL(stage));
                 issued[stage] = true;
                 iss_ph[stage] = ph;
                 if (++stage == NSTAGE) { stage = 0; ph ^= 1u; }
@@ -279,6 +321,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) l2_tc_kernel(Params P)
         int stage = 0, buf = 0;
         uint32_t ph = 0, a_ph = 0;
         uint32_t tph[2] = {0, 0};
+        const uint64_t ax_desc = sdesc_plain(sAX);
         for (int item = blockIdx.x; item < P.nitems && !*abort; item += gridDim.x) {
             const int p = item / P.nmg;
             if (!mbar_wait(A_FULL, a_ph, abort, lim)) { set_abort(abort, P.error, 3); break; }
@@ -291,17 +334,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) l2_tc_kernel(Params P)
                 if (!mbar_wait(TEMPTY(buf), tph[buf] ^ 1u, abort, lim)) { ok = false; set_abort(abort, P.error, 4); break; }
                 if (!mbar_wait(FULL(stage), ph, abort, lim)) { ok = false; set_abort(abort, P.error, 5); break; }
                 tc_fence_after();
-                const uint32_t b_hi = sB + (uint32_t)stage * PAIR_BYTES, b_lo = b_hi + TILE_BYTES;
+                const uint32_t b_hi = sB + (uint32_t)stage * BTILE_BYTES, b_lo = b_hi + TILE_BYTES;
+                const uint64_t bx_desc = sdesc_plain(b_hi + PAIR_BYTES);
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const uint32_t d = tmem + (uint32_t)buf * 256u + (uint32_t)h * 128u;
                     const uint32_t a_hi = sA + (uint32_t)h * PAIR_BYTES, a_lo = a_hi + TILE_BYTES;
+                    mma_bf16(d, ax_desc, bx_desc, 0u);      /* q(g) */
 #pragma unroll
                     for (int k = 0; k < BK / 16; ++k) {
                         const uint32_t ko = (uint32_t)k * 32u;
-                        mma_bf16(d, sdesc(a_hi + ko), sdesc(b_hi + ko), k > 0 ? 1u : 0u);
-                        mma_bf16(d, sdesc(a_hi + ko), sdesc(b_lo + ko), 1u);
-                        mma_bf16(d, sdesc(a_lo + ko), sdesc(b_hi + ko), 1u);
+                        mma_bf16(d, sdesc_sw128(a_hi + ko), sdesc_sw128(b_hi + ko), 1u);
+                        mma_bf16(d, sdesc_sw128(a_hi + ko), sdesc_sw128(b_lo + ko), 1u);
+                        mma_bf16(d, sdesc_sw128(a_lo + ko), sdesc_sw128(b_hi + ko), 1u);
                     }
                 }
                 mma_commit(EMPTY(stage));
@@ -331,7 +376,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) l2_tc_kernel(Params P)
             float bv[TOPK];
             int bi[TOPK];
 #pragma unroll
-            for (int k = 0; k < TOPK; ++k) { bv[k] = 3.0e38f; bi[k] = -1; }
+            for (int k = 0; k < TOPK; ++k) { bv[k] = __int_as_float(0x7f800000); bi[k] = -1; }
             int tb, te;
             part_range(P, p, tb, te);
             bool ok = true;
@@ -345,44 +390,42 @@ __global__ void __launch_bounds__(NTHREADS, 1) l2_tc_kernel(Params P)
                 tc_fence_after();
                 const uint32_t taddr = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)buf * 256u +
                                        (uint32_t)h * 128u;
-                const float4 *qp = reinterpret_cast<const float4 *>(P.q + (size_t)t * BN);
-#pragma unroll 1
-                for (int c = 0; c < BN / 32; ++c) {
-                    uint32_t r[32];
-                    tmem_ld32(taddr + (uint32_t)c * 32u, r);
-                    if (P.dbg && first_tile && blockIdx.x == 0) {
-                        for (int j = 0; j < 32; ++j)
-                            P.dbg[(size_t)(h * BM + row) * BN + c * 32 + j] = __uint_as_float(r[j]);
-                    }
+                uint32_t r[BN];
 #pragma unroll
-                    for (int j4 = 0; j4 < 8; ++j4) {
-                        const float4 qq = __ldg(qp + c * 8 + j4);
-                        const float qv[4] = {qq.x, qq.y, qq.z, qq.w};
+                for (int c = 0; c < BN / 32; ++c) tmem_ld32(taddr + (uint32_t)c * 32u, r + c * 32);
+                tmem_wait_ld();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(TEMPTY(buf));   /* accumulators are in registers */
+                if (P.dbg && first_tile && blockIdx.x == 0) {
+                    for (int j = 0; j < BN; ++j)
+                        P.dbg[(size_t)(h * BM + row) * BN + j] = __uint_as_float(r[j]);
+                }
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const float v = fmaf(-2.0f, __uint_as_float(r[j4 * 4 + u]), qv[u]);
-                            if (v < bv[TOPK - 1]) {
-                                const int g = t * BN + c * 32 + j4 * 4 + u;
-                                float cv = v;
-                                int ci = g;
+                for (int c = 0; c < BN / RUN; ++c) {
+                    float m[16];
 #pragma unroll
-                                for (int k = 0; k < TOPK; ++k) {
-                                    if (cv < bv[k]) {
-                                        const float tv = bv[k];
-                                        const int ti = bi[k];
-                                        bv[k] = cv; bi[k] = ci;
-                                        cv = tv; ci = ti;
-                                    }
-                                }
+                    for (int j = 0; j < 16; ++j)
+                        m[j] = fminf(__uint_as_float(r[c * 32 + j]), __uint_as_float(r[c * 32 + 16 + j]));
+#pragma unroll
+                    for (int w = 8; w > 0; w >>= 1)
+#pragma unroll
+                        for (int j = 0; j < w; ++j) m[j] = fminf(m[j], m[j + w]);
+                    float cv = m[0];
+                    if (cv < bv[TOPK - 1]) {
+                        int ci = (t * BN) / RUN + c;
+#pragma unroll
+                        for (int k = 0; k < TOPK; ++k) {
+                            if (cv < bv[k]) {
+                                const float tv = bv[k];
+                                const int ti = bi[k];
+                                bv[k] = cv; bi[k] = ci;
+                                cv = tv; ci = ti;
                             }
                         }
                     }
-                    __syncwarp();
                 }
                 first_tile = false;
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(TEMPTY(buf));
                 tph[buf] ^= 1u;
                 buf ^= 1;
             }
@@ -413,20 +456,19 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16 &hi, __nv_bfl
 
 /* One thread per grid point (rows of the padded last tile included). */
 __global__ void pack_tables_kernel(int ngrd, int ldgrd, int ntf, int ntile,
-                                   const float *__restrict__ tables, uint8_t *__restrict__ bpack,
-                                   float *__restrict__ q)
+                                   const float *__restrict__ tables, uint8_t *__restrict__ bpack)
 {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= ntile * BN) return;
     const int tile = g / BN, r = g % BN;
-    uint8_t *hi = bpack + (size_t)tile * PAIR_BYTES, *lo = hi + TILE_BYTES;
+    uint8_t *hi = bpack + (size_t)tile * BTILE_BYTES, *lo = hi + TILE_BYTES, *xt = hi + PAIR_BYTES;
     const bool real = g < ngrd;
     double mean = 0.0;
     if (real) {
         for (int i = 0; i < ntf; ++i) mean += (double)__ldg(tables + (size_t)i * ldgrd + g);
         mean /= (double)ntf;
     }
-    double qq = 0.0;
+    double q = 0.0;
     for (int c = 0; c < BK / 8; ++c) {
         __align__(16) __nv_bfloat16 vh[8], vl[8];
         for (int j = 0; j < 8; ++j) {
@@ -434,7 +476,7 @@ __global__ void pack_tables_kernel(int ngrd, int ldgrd, int ntf, int ntile,
             double d = 0.0;
             if (real && k < ntf) {
                 d = (double)__ldg(tables + (size_t)k * ldgrd + g) - mean;
-                qq += d * d;
+                q += d * d;
             }
             split_bf16(d, vh[j], vl[j]);
         }
@@ -442,11 +484,21 @@ __global__ void pack_tables_kernel(int ngrd, int ldgrd, int ntf, int ntile,
         *reinterpret_cast<uint4 *>(hi + off) = *reinterpret_cast<const uint4 *>(vh);
         *reinterpret_cast<uint4 *>(lo + off) = *reinterpret_cast<const uint4 *>(vl);
     }
-    q[g] = real ? (float)qq : __int_as_float(0x7f800000); /* +inf: never a candidate */
+    if (!real) q = (double)PAD_Q;
+    /* q = q1 + q2 + q3, three bf16 terms */
+    __align__(16) __nv_bfloat16 vx[8];
+    const __nv_bfloat16 z = __float2bfloat16_rn(0.0f);
+    for (int j = 0; j < 8; ++j) vx[j] = z;
+    vx[0] = __float2bfloat16_rn((float)q);
+    const double r1 = q - (double)__bfloat162float(vx[0]);
+    vx[1] = __float2bfloat16_rn((float)r1);
+    vx[2] = __float2bfloat16_rn((float)(r1 - (double)__bfloat162float(vx[1])));
+    *reinterpret_cast<uint4 *>(xt + xoff(r, 0)) = *reinterpret_cast<const uint4 *>(vx);
+    *reinterpret_cast<uint4 *>(xt + xoff(r, 8)) = make_uint4(0u, 0u, 0u, 0u);
 }
 
-/* One thread per event row slot.  Rows of ineligible or padding events are
- * zero (their scores are not used). */
+/* One thread per event row slot: -2 (o - mean o), split.  Rows of
+ * ineligible or padding events are zero (their scores are not used). */
 __global__ void pack_events_kernel(int nev, int nrows, int ntf, const double *__restrict__ obs,
                                    const unsigned char *__restrict__ elig, uint8_t *__restrict__ apack)
 {
@@ -464,7 +516,7 @@ __global__ void pack_events_kernel(int nev, int nrows, int ntf, const double *__
         __align__(16) __nv_bfloat16 vh[8], vl[8];
         for (int j = 0; j < 8; ++j) {
             const int k = c * 8 + j;
-            const double d = (use && k < ntf) ? obs[(size_t)e * ntf + k] - mean : 0.0;
+            const double d = (use && k < ntf) ? -2.0 * (obs[(size_t)e * ntf + k] - mean) : 0.0;
             split_bf16(d, vh[j], vl[j]);
         }
         const uint32_t off = swz(r, c * 8);
@@ -480,16 +532,14 @@ __device__ __forceinline__ bool lex_lt(float v, int i, float w, int j)
     return v < w || (v == w && i < j);
 }
 
-__device__ __forceinline__ double warp_sum(double x)
+__device__ __forceinline__ bool lex_lt_d(double v, int i, double w, int j)
 {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    return x;
+    return v < w || (v == w && i < j);
 }
 
-/* One warp per event: take the R best candidates by approximate score (ties
- * by index), evaluate the reference's misfit in FP64 at each, keep the
- * minimum (first index among equal misfits). */
+/* One warp per event: take the R best runs by approximate score (ties by run
+ * number), evaluate the reference's misfit in FP64 at every point of each run
+ * (lane = point), keep the minimum (first index among equal misfits). */
 __global__ void rescore_kernel(int nev, int npart, int ngrd, int ntf, int ldgrd, int R,
                                const float *__restrict__ tables, const double *__restrict__ obs,
                                const double *__restrict__ wts, const unsigned char *__restrict__ elig,
@@ -504,6 +554,8 @@ __global__ void rescore_kernel(int nev, int npart, int ngrd, int ntf, int ldgrd,
     const float *cv = cand_v + (size_t)e * C;
     const int *ci = cand_i + (size_t)e * C;
     const double *o = obs + (size_t)e * ntf, *w = wts + (size_t)e * ntf;
+    double sw = 0.0;
+    for (int i = 0; i < ntf; ++i) sw += w[i];
     float pv = -3.0e38f;
     int pi = -1;
     double best_obj = 1.0e300, best_t0 = 0.0;
@@ -514,7 +566,10 @@ __global__ void rescore_kernel(int nev, int npart, int ngrd, int ntf, int ldgrd,
         for (int c = lane; c < C; c += 32) {
             const int i = ci[c];
             const float v = cv[c];
-            if (i >= 0 && i < ngrd && lex_lt(pv, pi, v, i) && lex_lt(v, i, mv, mi)) { mv = v; mi = i; }
+            if (i >= 0 && (long long)i * RUN < ngrd && lex_lt(pv, pi, v, i) && lex_lt(v, i, mv, mi)) {
+                mv = v;
+                mi = i;
+            }
         }
 #pragma unroll
         for (int s = 16; s > 0; s >>= 1) {
@@ -525,24 +580,29 @@ __global__ void rescore_kernel(int nev, int npart, int ngrd, int ntf, int ldgrd,
         if (mi == 0x7fffffff) break;
         pv = mv;
         pi = mi;
-        const int g = mi;
-        double a = 0.0, sw = 0.0;
-        for (int i = lane; i < ntf; i += 32)
-            if (w[i] > 0.0) {
-                a += w[i] * (o[i] - (double)__ldg(tables + (size_t)i * ldgrd + g));
-                sw += w[i];
-            }
-        a = warp_sum(a);
-        sw = warp_sum(sw);
-        const double t0 = a / sw;
-        double ob = 0.0;
-        for (int i = lane; i < ntf; i += 32)
-            if (w[i] > 0.0) {
-                const double rr = w[i] * (o[i] - (double)__ldg(tables + (size_t)i * ldgrd + g) - t0);
-                ob += 0.5 * rr * rr;
-            }
-        ob = warp_sum(ob);
-        if (ob < best_obj || (ob == best_obj && g < best_g)) { best_obj = ob; best_g = g; best_t0 = t0; }
+        const int g = mi * RUN + lane;
+        double ob = 1.0e300, t0 = 0.0;
+        if (g < ngrd) {
+            double a = 0.0;
+            for (int i = 0; i < ntf; ++i)
+                if (w[i] > 0.0) a += w[i] * (o[i] - (double)__ldg(tables + (size_t)i * ldgrd + g));
+            t0 = a / sw;
+            ob = 0.0;
+            for (int i = 0; i < ntf; ++i)
+                if (w[i] > 0.0) {
+                    const double rr = w[i] * (o[i] - (double)__ldg(tables + (size_t)i * ldgrd + g) - t0);
+                    ob += 0.5 * rr * rr;
+                }
+        }
+        int gg = g < ngrd ? g : 0x7fffffff;
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const double oo = __shfl_xor_sync(0xffffffffu, ob, s);
+            const int og = __shfl_xor_sync(0xffffffffu, gg, s);
+            const double ot = __shfl_xor_sync(0xffffffffu, t0, s);
+            if (lex_lt_d(oo, og, ob, gg)) { ob = oo; gg = og; t0 = ot; }
+        }
+        if (lex_lt_d(ob, gg, best_obj, best_g)) { best_obj = ob; best_g = gg; best_t0 = t0; }
     }
     if (lane == 0) {
         out_idx[e] = best_g;
@@ -558,7 +618,7 @@ using namespace fktc;
 extern "C" size_t fk_locate_tc_table_bytes(int ngrd)
 {
     const size_t ntile = ((size_t)ngrd + BN - 1) / BN;
-    return ntile * PAIR_BYTES;
+    return ntile * BTILE_BYTES;
 }
 
 extern "C" size_t fk_locate_tc_event_bytes(int nev)
@@ -568,13 +628,13 @@ extern "C" size_t fk_locate_tc_event_bytes(int nev)
 }
 
 extern "C" int fk_locate_tc_pack_tables(int ngrd, int ldgrd, int ntf, const float *tables,
-                                        void *bpack, float *q, cudaStream_t s)
+                                        void *bpack, cudaStream_t s)
 {
     if (ntf < 1 || ntf > BK) return (int)cudaErrorInvalidValue;
     const int ntile = (ngrd + BN - 1) / BN;
     const int n = ntile * BN;
     pack_tables_kernel<<<(n + 255) / 256, 256, 0, s>>>(ngrd, ldgrd, ntf, ntile, tables,
-                                                       (uint8_t *)bpack, q);
+                                                       (uint8_t *)bpack);
     return (int)cudaGetLastError();
 }
 
@@ -607,7 +667,7 @@ extern "C" int fk_locate_tc_npart(int nev, int ngrd)
 }
 
 extern "C" int fk_locate_tc(int ngrd, int ldgrd, int ntf, const float *tables, const void *bpack,
-                            const float *q, int nev, const double *obs, const double *wts,
+                            int nev, const double *obs, const double *wts,
                             const unsigned char *elig, void *apack, int npart, float *cand_v,
                             int *cand_i, int rescore, int *out_idx, double *out_t0,
                             double *out_obj, int *error, float *dbg, cudaStream_t s)
@@ -634,7 +694,6 @@ extern "C" int fk_locate_tc(int ngrd, int ldgrd, int ntf, const float *tables, c
     Params P;
     P.apack = (const uint8_t *)apack;
     P.bpack = (const uint8_t *)bpack;
-    P.q = q;
     P.nev = nev;
     P.ntile = ntile;
     P.nmg = nmg;
@@ -650,9 +709,9 @@ extern "C" int fk_locate_tc(int ngrd, int ldgrd, int ntf, const float *tables, c
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return (int)e;
     if (rescore > 0) {
-        rescore_kernel<<<(nev * 32 + 255) / 256, 256, 0, s>>>(nev, npart, ngrd, ntf, ldgrd, rescore, tables,
-                                                              obs, wts, elig, cand_v, cand_i, out_idx,
-                                                              out_t0, out_obj);
+        rescore_kernel<<<(nev * 32 + 255) / 256, 256, 0, s>>>(nev, npart, ngrd, ntf, ldgrd, rescore,
+                                                              tables, obs, wts, elig, cand_v, cand_i,
+                                                              out_idx, out_t0, out_obj);
         e = cudaGetLastError();
     }
     return (int)e;

@@ -47,6 +47,8 @@ def _reduced(picks):
 
 
 def test_accumulators_match_bf16_emulation(fk):
+    """The accumulator of event e at grid point g is the ranking score
+    q(g) - 2 sum_i o'_i T'_i(g), formed from the bf16 splits."""
     tables = station_tables(16, 24, 20, 100.0, 64, seed=3)
     _, picks = synthetic_events(tables, 300, seed=4)
     loc = _locator(fk, tables, picks)
@@ -54,17 +56,28 @@ def test_accumulators_match_bf16_emulation(fk):
     loc.debugAccumulators(True)
     loc.locateEvents(np.arange(1, 301))
     acc = loc.debugAccumulators(False).astype(np.float64)
-    # item 0 of CTA 0: events 0..255 x grid points 0..127
+    # CTA 0's first tile: events 0..255 x grid points 0..127
     T = tables[:, :128].astype(np.float64)
     Tp = T - T.mean(axis=0, keepdims=True)
+    q = (Tp ** 2).sum(axis=0)
+    q1 = _bf16(q.astype(np.float32)).astype(np.float64)
+    q2 = _bf16((q - q1).astype(np.float32)).astype(np.float64)
+    q3 = _bf16((q - q1 - q2).astype(np.float32)).astype(np.float64)
     o = _reduced(picks)[:256]
-    op = o - o.mean(axis=1, keepdims=True)
+    op = -2.0 * (o - o.mean(axis=1, keepdims=True))
     ah, al = _split(op)
     bh, bl = _split(Tp.T)
-    want = ah @ bh.T + ah @ bl.T + al @ bh.T
-    scale = np.abs(ah) @ np.abs(bh).T + 1e-6
+    want = ah @ bh.T + ah @ bl.T + al @ bh.T + (q1 + q2 + q3)[None, :]
+    scale = np.abs(ah) @ np.abs(bh).T + q[None, :] + 1e-6
     err = np.abs(acc - want) / scale
     assert err.max() < 2e-6, f"max scaled error {err.max():.3g}"
+    # the score ranks like the FP64 misfit: p + s = 2 obj (unit weights)
+    p = (o - o.mean(axis=1, keepdims=True)) ** 2
+    obj2 = p.sum(axis=1)[:, None] + acc
+    res = o[:, :, None] - T[None, :, :]
+    t0 = res.mean(axis=1, keepdims=True)
+    want_obj2 = ((res - t0) ** 2).sum(axis=1)
+    assert (np.abs(obj2 - want_obj2) / scale).max() < 4e-5
     loc.finalize()
 
 
