@@ -198,6 +198,9 @@ def run_reference(args, rank, world):
 LOC_GRID = 3        # 1-based: the 160x160x96 grid, 64 station tables
 LOC_NEV = 10000
 LOC_EXACT_SAMPLE = 512
+SUR_WIDTH, SUR_DEPTH = 256, 5          # surrogate: 6 -> 5 x 256 SiLU -> tau
+SUR_SAMPLES, SUR_STEPS, SUR_BATCH = 2_000_000, 3000, 4096
+SUR_BLOCK = (4, 4, 4)                  # fine nodes per coarse block (z, x, y)
 
 
 def locate_workload(b, g, nev, igrid=LOC_GRID):
@@ -220,7 +223,7 @@ def locate_workload(b, g, nev, igrid=LOC_GRID):
     return picks
 
 
-def bench_locate(fk, b, grids, stream, steps, nev=LOC_NEV, igrid=LOC_GRID):
+def bench_locate(fk, b, grids, stream, steps, nev=LOC_NEV, igrid=LOC_GRID, sur_steps=SUR_STEPS):
     import torch
     g = grids[LOC_GRID - 1]
     ngrd = g["nz"] * g["nx"] * g["ny"]
@@ -247,6 +250,29 @@ def bench_locate(fk, b, grids, stream, steps, nev=LOC_NEV, igrid=LOC_GRID):
 
     loc.setMethod(1)
     tc_ms, (tc_idx, _, _) = timed(ev, max(1, steps))
+
+    # learned pruning: surrogate trained on these tables, block centres
+    # ranked on the tensor cores, 8 blocks x 64 = 512 fine cells re-scored
+    # exactly
+    loc.setGeometry(g["nz"], g["nx"], g["ny"], H, H, H, g["zs"], g["xs"], g["ys"])
+    fk.MLP(SUR_WIDTH, SUR_DEPTH, seed=7)
+    torch.cuda.synchronize()
+    t_tr = time.perf_counter()
+    sur_loss = loc.trainSurrogate(nsamples=SUR_SAMPLES, steps=sur_steps, batch=SUR_BATCH, lr=2e-3,
+                                  vref=3000.0, seed=7)
+    t_tr = time.perf_counter() - t_tr
+    t_bd = time.perf_counter()
+    loc.buildSurrogate(SUR_BLOCK)
+    t_bd = time.perf_counter() - t_bd
+    loc.setPruning(4, 8)
+    loc.setMethod(2)
+    pr_ms, (pr_idx, _, _) = timed(ev, max(1, steps))
+    nfb, ncoarse, nblk = loc.pruneInfo()
+    loc.stageTimes(True)
+    loc.locateEvents(ev)
+    stage = loc.stageTimes()
+    loc.stageTimes(False)
+    flops_row = 2 * (6 * SUR_WIDTH + (SUR_DEPTH - 1) * SUR_WIDTH * SUR_WIDTH + SUR_WIDTH)
     loc.setMethod(0)
     sample = ev[:LOC_EXACT_SAMPLE]
     ex_ms, (ex_idx, _, _) = timed(sample, 1)
@@ -270,6 +296,20 @@ def bench_locate(fk, b, grids, stream, steps, nev=LOC_NEV, igrid=LOC_GRID):
                                          "algorithmic_flops": flops,
                                          "note": "2*stations*gridpoints per event, one contracted "
                                                  "term; the 3 hi/lo products are not counted"}},
+            "surrogate_pruned": {
+                "events_per_s": nev / (pr_ms * 1e-3), "ms": pr_ms,
+                "speedup_vs_tensor_core": tc_ms / pr_ms,
+                "hypocentre_agreement_vs_tensor_core": float(np.mean(pr_idx == tc_idx)),
+                "fallback_events": nfb, "coarse_nodes": ncoarse,
+                "fine_blocks_examined_per_event": nblk / max(1, nev - nfb),
+                "stage_ms": {"coarse_ranking": stage[0], "pruned_rescore": stage[1],
+                             "results_to_host": stage[2]},
+                "network": "6 -> %d x %d SiLU -> tau, FP32 CUDA-core kernels" % (SUR_DEPTH, SUR_WIDTH),
+                "training": {"samples": SUR_SAMPLES, "steps": sur_steps, "batch": SUR_BATCH,
+                             "seconds": t_tr, "final_mse_tau": sur_loss,
+                             "tflops": 3.0 * flops_row * sur_steps * SUR_BATCH / t_tr / 1e12},
+                "coarse_build": {"block_zxy": list(SUR_BLOCK), "seconds": t_bd,
+                                 "tflops": flops_row * ncoarse * NSRC / t_bd / 1e12}},
             "exact_fp32": {"events_per_s": len(sample) / (ex_ms * 1e-3), "ms": ex_ms,
                            "sample_events": len(sample)},
             "hypocentre_agreement_tc_vs_exact": agree}
@@ -287,6 +327,7 @@ def main():
     ap.add_argument("--locate-only", action="store_true",
                     help="solve only the 160x160x96 grid once and run the grid-search section")
     ap.add_argument("--locate-events", type=int, default=LOC_NEV)
+    ap.add_argument("--surrogate-steps", type=int, default=SUR_STEPS)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -316,7 +357,8 @@ def main():
         b.setSources(1, g["zs"], g["xs"], g["ys"])
         b.solve()
         stream = torch.cuda.ExternalStream(fk.lib().fteik_b200_stream())
-        res = bench_locate(fk, b, grids, stream, args.steps, nev=args.locate_events, igrid=1)
+        res = bench_locate(fk, b, grids, stream, args.steps, nev=args.locate_events, igrid=1,
+                           sur_steps=args.surrogate_steps)
         print(json.dumps({"locate": res}), flush=True)
         b.finalize()
         return
@@ -421,7 +463,8 @@ def main():
 
     locate = None
     if not args.no_locate:
-        locate = bench_locate(fk, b, grids, stream, args.steps, nev=args.locate_events)
+        locate = bench_locate(fk, b, grids, stream, args.steps, nev=args.locate_events,
+                              sur_steps=args.surrogate_steps)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -138,6 +138,24 @@ _SIGS = {
     "fteik_b200_locate_setMethod": [c_int, _PI],
     "fteik_b200_locate_setRescoreCandidates": [c_int, _PI],
     "fteik_b200_locate_debugAccumulators": [c_int, _PF, _PI],
+    "fteik_b200_locate_setGeometry": [c_int, c_int, c_int, c_double, c_double, c_double, c_int, _PD, _PD,
+                                      _PD, _PI],
+    "fteik_b200_locate_trainSurrogate": [c_longlong, c_int, c_int, c_double, c_double,
+                                         ctypes.c_ulonglong, _PD, _PI],
+    "fteik_b200_locate_buildSurrogate": [c_int, c_int, c_int, _PI],
+    "fteik_b200_locate_setPruning": [c_int, c_int, _PI],
+    "fteik_b200_locate_getPruneInfo": [_PI, _PI, POINTER(c_longlong), _PI, _PI],
+    "fteik_b200_locate_getSurrogateTable": [c_int, c_int, _PF, _PI],
+    "fteik_b200_locate_setStageTiming": [c_int, _PI],
+    "fteik_b200_locate_getStageTimes": [POINTER(c_float), POINTER(c_float), POINTER(c_float), _PI],
+    "fteik_b200_mlp_initialize": [c_int, c_int, ctypes.c_ulonglong, _PI],
+    "fteik_b200_mlp_finalize": [],
+    "fteik_b200_mlp_getNumberOfWeights": [_PI, _PI],
+    "fteik_b200_mlp_getWeights": [c_int, _PF, _PI],
+    "fteik_b200_mlp_setWeights": [c_int, _PF, _PI],
+    "fteik_b200_mlp_forward": [c_int, _PF, _PF, _PI],
+    "fteik_b200_mlp_gradient": [c_int, _PF, _PF, _PD, _PF, _PI],
+    "fteik_b200_mlp_train": [c_int, _PF, _PF, c_int, c_int, c_double, _PD, _PI],
     "fteik_b200_locate_l2_noalloc": [c_int, c_int, c_int, ctypes.c_void_p, c_int, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, _PI],
@@ -447,6 +465,61 @@ class Locator:
         self.lib.fteik_b200_locate_setRescoreCandidates(int(ncand), byref(ierr))
         _check(ierr, "fteik_b200_locate_setRescoreCandidates")
 
+    def setGeometry(self, nz, nx, ny, dz, dx, dy, zsta, xsta, ysta):
+        z, pz = _d(zsta)
+        x, px = _d(xsta)
+        y, py = _d(ysta)
+        ierr = c_int(1)
+        self.lib.fteik_b200_locate_setGeometry(nz, nx, ny, float(dz), float(dx), float(dy), z.size, pz, px, py,
+                                               byref(ierr))
+        _check(ierr, "fteik_b200_locate_setGeometry")
+
+    def trainSurrogate(self, nsamples=2_000_000, steps=3000, batch=4096, lr=2e-3, vref=3000.0, seed=7):
+        loss, ierr = c_double(), c_int(1)
+        self.lib.fteik_b200_locate_trainSurrogate(int(nsamples), int(steps), int(batch), float(lr), float(vref),
+                                                  int(seed), byref(loss), byref(ierr))
+        _check(ierr, "fteik_b200_locate_trainSurrogate")
+        return loss.value
+
+    def buildSurrogate(self, block=(4, 4, 4)):
+        """Network travel times at the centres of blocks of bz x bx x by
+        fine nodes (z, x, y)."""
+        ierr = c_int(1)
+        bz, bx, by = block
+        self.lib.fteik_b200_locate_buildSurrogate(int(bz), int(bx), int(by), byref(ierr))
+        _check(ierr, "fteik_b200_locate_buildSurrogate")
+
+    def setPruning(self, runs=4, nodes=8):
+        ierr = c_int(1)
+        self.lib.fteik_b200_locate_setPruning(int(runs), int(nodes), byref(ierr))
+        _check(ierr, "fteik_b200_locate_setPruning")
+
+    def pruneInfo(self):
+        """(events searched exhaustively, coarse nodes, blocks examined) of
+        the last surrogate-pruned call."""
+        nf, nc, nb, mb, ierr = c_int(), c_int(), c_longlong(), c_int(), c_int(1)
+        self.lib.fteik_b200_locate_getPruneInfo(byref(nf), byref(nc), byref(nb), byref(mb), byref(ierr))
+        self.max_blocks = mb.value
+        return nf.value, nc.value, nb.value
+
+    def stageTimes(self, enable=None):
+        """With enable=True/False switch stage timing; otherwise return the
+        last method-2 call's (coarse ranking, pruned re-score, copy) ms."""
+        ierr = c_int(1)
+        if enable is not None:
+            self.lib.fteik_b200_locate_setStageTiming(int(bool(enable)), byref(ierr))
+            return None
+        a, b, c = c_float(), c_float(), c_float()
+        self.lib.fteik_b200_locate_getStageTimes(byref(a), byref(b), byref(c), byref(ierr))
+        return a.value, b.value, c.value
+
+    def surrogateTable(self, itf, ncoarse):
+        out = np.zeros(ncoarse, np.float32)
+        ierr = c_int(1)
+        self.lib.fteik_b200_locate_getSurrogateTable(int(itf), ncoarse, out.ctypes.data_as(_PF), byref(ierr))
+        _check(ierr, "fteik_b200_locate_getSurrogateTable")
+        return out
+
     def debugAccumulators(self, enable):
         """enable=True: record the first accumulator tiles at the next
         tensor-core search; enable=False: return them as [256, 128]."""
@@ -459,6 +532,67 @@ class Locator:
         self.lib.fteik_b200_locate_debugAccumulators(0, out.ctypes.data_as(_PF), byref(ierr))
         _check(ierr, "fteik_b200_locate_debugAccumulators")
         return out
+
+
+class MLP:
+    """The surrogate network (fteik_b200_mlp_*): 6 normalised inputs ->
+    depth x width SiLU -> tau."""
+
+    def __init__(self, width=256, depth=5, seed=7):
+        self.lib = lib()
+        ierr = c_int(1)
+        self.lib.fteik_b200_mlp_initialize(int(width), int(depth), int(seed), byref(ierr))
+        _check(ierr, "fteik_b200_mlp_initialize")
+        self.width, self.depth = width, depth
+
+    def nweights(self):
+        n, ierr = c_int(), c_int(1)
+        self.lib.fteik_b200_mlp_getNumberOfWeights(byref(n), byref(ierr))
+        _check(ierr, "fteik_b200_mlp_getNumberOfWeights")
+        return n.value
+
+    def weights(self):
+        w = np.zeros(self.nweights(), np.float32)
+        ierr = c_int(1)
+        self.lib.fteik_b200_mlp_getWeights(w.size, w.ctypes.data_as(_PF), byref(ierr))
+        _check(ierr, "fteik_b200_mlp_getWeights")
+        return w
+
+    def setWeights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        ierr = c_int(1)
+        self.lib.fteik_b200_mlp_setWeights(w.size, w.ctypes.data_as(_PF), byref(ierr))
+        _check(ierr, "fteik_b200_mlp_setWeights")
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, 6)
+        out = np.zeros(x.shape[0], np.float32)
+        ierr = c_int(1)
+        self.lib.fteik_b200_mlp_forward(x.shape[0], x.ctypes.data_as(_PF), out.ctypes.data_as(_PF), byref(ierr))
+        _check(ierr, "fteik_b200_mlp_forward")
+        return out
+
+    def gradient(self, x, y):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, 6)
+        y = np.ascontiguousarray(y, np.float32)
+        g = np.zeros(self.nweights(), np.float32)
+        loss, ierr = c_double(), c_int(1)
+        self.lib.fteik_b200_mlp_gradient(x.shape[0], x.ctypes.data_as(_PF), y.ctypes.data_as(_PF), byref(loss),
+                                         g.ctypes.data_as(_PF), byref(ierr))
+        _check(ierr, "fteik_b200_mlp_gradient")
+        return loss.value, g
+
+    def train(self, x, y, steps, batch, lr):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, 6)
+        y = np.ascontiguousarray(y, np.float32)
+        loss, ierr = c_double(), c_int(1)
+        self.lib.fteik_b200_mlp_train(x.shape[0], x.ctypes.data_as(_PF), y.ctypes.data_as(_PF), int(steps),
+                                      int(batch), float(lr), byref(loss), byref(ierr))
+        _check(ierr, "fteik_b200_mlp_train")
+        return loss.value
+
+    def finalize(self):
+        self.lib.fteik_b200_mlp_finalize()
 
 
 class Batch3D:

@@ -189,6 +189,45 @@ int fk_locate_tc(int ngrd, int ldgrd, int ntf, const float *tables, const void *
                  void *apack, int npart, float *cand_v, int *cand_i, int rescore, int *out_idx,
                  double *out_t0, double *out_obj, int *error, float *dbg, cudaStream_t s);
 
+/* Pruned search: coarse runs (cand_* from fk_locate_tc on the coarse
+ * surrogate tables [ntf][ldc], coarse node c = cz + ncz (cx + ncx cy) owning
+ * the fine block [bz cz, bz cz + bz) x [bx cx, ..) x [by cy, ..)) -> the k best
+ * coarse nodes (rc runs examined, rc <= 4, k <= 32) -> FP64 misfit on the
+ * exact tables (block-major copy, fk_locate_block_tables) at every fine
+ * node of their blocks, then a
+ * descent over neighbouring blocks.  flag[e]: 0xFF when the event needs the
+ * exhaustive search, else the number of blocks examined. */
+int fk_locate_prune(int nev, int npart, int rc, int k, int nz, int nx, int ny, int bz, int bx, int by,
+                    int ldgrd, int ldc, int ntf, const float *coarse, const float *fine,
+                    const double *obs, const double *wts, const unsigned char *elig,
+                    const float *cand_v, const int *cand_i, int *out_idx, double *out_t0,
+                    double *out_obj, unsigned char *flag, cudaStream_t s);
+/* Block-major copy of tables [ntf][ldgrd] for fk_locate_prune's fine
+ * stage: out [nblocks][ntf][bz bx by] (ncz ncx ncy blocks, z fastest). */
+int fk_locate_block_tables(int nz, int nx, int ny, int bz, int bx, int by, int ntf, int ldgrd,
+                           const float *tables, float *out, cudaStream_t s);
+
+/* ---- surrogate network (mlp.c / mlp.cu) ----------------------------------- */
+typedef int (*fk_batch_fn)(void *ctx, long long step, int B, float *x, float *y, cudaStream_t s);
+int fk_mlp_ready(void);
+size_t fk_mlp_flops_per_row(void);
+int fk_mlp_train_device(fk_batch_fn next_batch, void *ctx, long long steps, int B, double lr,
+                        double *last_loss);
+int fk_mlp_forward_device(long long n, const float *x, float *tau, cudaStream_t s);
+/* Training batch from tables [ntf][ldgrd] on a z-fastest grid and station
+ * positions sta [ntf][3] (z, x, y): inputs x [B][6], targets tau [B]. */
+int fk_mlp_sample(int nz, int nx, int ny, double dz, double dx, double dy, int ntf, int ldgrd,
+                  double vref, const float *tables, const float *sta, unsigned long long seed,
+                  long long nsamp, long long step, int B, float *x, float *y, cudaStream_t s);
+/* Rows r0 .. r0+nrow-1 of the coarse lattice (row = table * ncoarse + node,
+ * node = the centre of its fine block bz x bx x by, clipped to the grid):
+ * network inputs and distance / v_ref. */
+int fk_mlp_coarse_inputs(int nz, int nx, int ny, double dz, double dx, double dy, int ntf,
+                         double vref, const float *sta, int bz, int bx, int by, int ncz, int ncx,
+                         int ncy, long long r0, long long nrow, float *x, float *dist, cudaStream_t s);
+int fk_mlp_coarse_store(long long r0, long long nrow, long long nc, int ldc, const float *tau,
+                        const float *dist, float *out, cudaStream_t s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,6 +27,7 @@ static struct {
     int method;              /* 0: exact FP32 (reference arithmetic), 1: tensor core */
     int rescore;             /* candidates re-scored in FP64 per event */
     bool dirty64, tables_dirty;
+    long long table_gen;     /* counts table writes */
     double *obs64, *w64;     /* host [nev][ntf], reduced picks and weights */
     unsigned char *elig;     /* host [nev]: every table picked at one weight */
     double *obs64_dev, *w64_dev;
@@ -44,8 +45,45 @@ static struct {
     float *dbg_dev;
 } SL;
 
+/* Surrogate-pruned search state: grid geometry of the tables, station
+ * positions, the coarse lattice and its surrogate tables. */
+static struct {
+    bool have_geom, ready;
+    int nz, nx, ny;
+    double dz, dx, dy, vref;
+    float *sta_dev;          /* [ntf][3] z, x, y */
+    int bz, bx, by, ncz, ncx, ncy, ngrd_c, ldc;
+    float *coarse;           /* device [ntf][ldc] surrogate travel times */
+    float *fine_blk;         /* device block-major copy of the exact tables */
+    long long blk_gen;       /* table generation fine_blk was built from */
+    void *bpack_c;
+    int rc, k;
+    unsigned char *flag_dev;
+    int flag_cap;
+    int last_fallback;
+    long long last_blocks;   /* blocks of fine nodes examined in the last call */
+    int last_max_blocks;
+    bool timing;             /* record stage events in method-2 calls */
+    cudaEvent_t ev[4];
+    float stage_ms[3];       /* coarse ranking, pruned re-score, results to host */
+    double *sub_obs, *sub_w;
+    unsigned char *sub_elig;
+    int sub_cap;
+} SP;
+
+static void surrogate_free(void)
+{
+    for (int k = 0; k < 4; k++)
+        if (SP.ev[k]) cudaEventDestroy(SP.ev[k]);
+    fk_dfree(SP.sta_dev); fk_dfree(SP.coarse); fk_dfree(SP.bpack_c); fk_dfree(SP.flag_dev);
+    fk_dfree(SP.fine_blk);
+    fk_dfree(SP.sub_obs); fk_dfree(SP.sub_w); fk_dfree(SP.sub_elig);
+    memset(&SP, 0, sizeof(SP));
+}
+
 void locate_finalize(void)
 {
+    surrogate_free();
     free(SL.tepoch); free(SL.origin); free(SL.have_ot); free(SL.obs); free(SL.wts);
     fk_dfree(SL.tables); fk_dfree(SL.obs_dev); fk_dfree(SL.wts_dev);
     fk_dfree(SL.idx_dev); fk_dfree(SL.t0_dev); fk_dfree(SL.obj_dev); fk_dfree(SL.scratch);
@@ -116,6 +154,7 @@ void locate_initialize(int nEvents, int ntf, int ngrd, int *ierr)
     SL.dirty = true;
     SL.dirty64 = true;
     SL.tables_dirty = true;
+    SL.table_gen++;
     SL.rescore = 8;
 }
 
@@ -142,6 +181,7 @@ void locate_setTravelTimeField64f(int ngrd, int itf, const double tt[], int *ier
     if (!e) e = (int)cudaStreamSynchronize(s);
     fk_dfree(d);
     SL.tables_dirty = true;
+    SL.table_gen++;
     *ierr = fk_check(e, "locate_setTravelTimeField64f");
 }
 
@@ -154,6 +194,7 @@ void locate_setTravelTimeField32f(int ngrd, int itf, const float tt[], int *ierr
                                  sizeof(float) * (size_t)ngrd, cudaMemcpyHostToDevice, fk_stream());
     if (!e) e = (int)cudaStreamSynchronize(fk_stream());
     SL.tables_dirty = true;
+    SL.table_gen++;
     *ierr = fk_check(e, "locate_setTravelTimeField32f");
 }
 
@@ -161,7 +202,8 @@ void locate_setTravelTimeField32f(int ngrd, int itf, const float tt[], int *ierr
 float *fk_locate_table_row(int itf, int ngrd)
 {
     if (!SL.init || itf < 1 || itf > SL.ntf || ngrd != SL.ngrd) return NULL;
-    SL.tables_dirty = true; /* the caller writes the row */
+    SL.tables_dirty = true;
+    SL.table_gen++; /* the caller writes the row */
     return SL.tables + (size_t)(itf - 1) * SL.ldgrd;
 }
 
@@ -296,8 +338,7 @@ static int pack_tables(void)
     if (!SL.tables_dirty && SL.bpack) return 0;
     if (!SL.bpack) {
         SL.bpack = fk_dalloc(fk_locate_tc_table_bytes(SL.ngrd), "locate: table pack");
-        SL.err_dev = (int *)fk_dalloc(sizeof(int), "locate: table pack");
-        if (!SL.bpack || !SL.err_dev) return 1;
+        if (!SL.bpack) return 1;
     }
     int e = fk_locate_tc_pack_tables(SL.ngrd, SL.ldgrd, SL.ntf, SL.tables, SL.bpack, fk_stream());
     if (fk_check(e, "locate: table pack")) return 1;
@@ -307,6 +348,10 @@ static int pack_tables(void)
 
 static int ensure_tc(int n, int npart)
 {
+    if (!SL.err_dev) {
+        SL.err_dev = (int *)fk_dalloc(sizeof(int), "locate");
+        if (!SL.err_dev) return 1;
+    }
     const size_t ab = fk_locate_tc_event_bytes(n);
     if (ab > SL.apack_bytes) {
         fk_dfree(SL.apack);
@@ -372,8 +417,8 @@ static int locate_range_tc(int e0, int n, int *idx, double *t0, double *obj)
 void fteik_b200_locate_setMethod(int method, int *ierr)
 {
     *ierr = 0;
-    if (method != 0 && method != 1) {
-        FK_ERR("fteik_b200_locate_setMethod: method=%d must be 0 (exact FP32) or 1 (tensor core)", method);
+    if (method < 0 || method > 2) {
+        FK_ERR("fteik_b200_locate_setMethod: method=%d must be 0 (exact FP32), 1 (tensor core) or 2 (surrogate-pruned)", method);
         *ierr = 1;
         return;
     }
@@ -413,9 +458,12 @@ void fteik_b200_locate_debugAccumulators(int enable, float *out, int *ierr)
 }
 
 /* Events [e0, e0+n) with the selected method; t0 excludes tepoch. */
+static int locate_range_pruned(int e0, int n, int *idx, double *t0, double *obj);
+
 static int locate_any(int e0, int n, int *idx, double *t0, double *obj)
 {
     if (SL.method == 1) return locate_range_tc(e0, n, idx, t0, obj);
+    if (SL.method == 2) return locate_range_pruned(e0, n, idx, t0, obj);
     float *ft0 = (float *)malloc(sizeof(float) * (size_t)n);
     float *fobj = (float *)malloc(sizeof(float) * (size_t)n);
     int rc = locate_range(e0, n, idx, ft0, fobj);
@@ -466,4 +514,310 @@ void fteik_b200_locate_locateEvents(int n, const int ev[], int optIndx[], double
             t0Opt[k] += SL.tepoch[ev[k] - 1];
         }
     free(idx);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Surrogate-pruned search (method 2).                                      */
+/* ------------------------------------------------------------------------ */
+
+void fteik_b200_locate_setGeometry(int nz, int nx, int ny, double dz, double dx, double dy, int ntf,
+                                   const double zsta[], const double xsta[], const double ysta[],
+                                   int *ierr)
+{
+    const char *who = "fteik_b200_locate_setGeometry";
+    *ierr = 1;
+    if (!SL.init) { FK_ERR("%s: Locator not initialized", who); return; }
+    if (nz < 2 || nx < 2 || ny < 2 || (long long)nz * nx * ny != SL.ngrd) {
+        FK_ERR("%s: nz*nx*ny must equal ngrd=%d", who, SL.ngrd);
+        return;
+    }
+    if (ntf != SL.ntf || dz <= 0.0 || dx <= 0.0 || dy <= 0.0) { FK_ERR("%s: need ntf=%d and positive spacing", who, SL.ntf); return; }
+    float *h = (float *)malloc(sizeof(float) * 3 * (size_t)ntf);
+    for (int i = 0; i < ntf; i++) {
+        h[3 * i] = (float)zsta[i];
+        h[3 * i + 1] = (float)xsta[i];
+        h[3 * i + 2] = (float)ysta[i];
+    }
+    fk_dfree(SP.sta_dev);
+    SP.sta_dev = (float *)fk_dalloc(sizeof(float) * 3 * (size_t)ntf, who);
+    int e = SP.sta_dev ? (int)cudaMemcpy(SP.sta_dev, h, sizeof(float) * 3 * (size_t)ntf, cudaMemcpyHostToDevice) : 1;
+    free(h);
+    if (fk_check(e, who)) return;
+    SP.nz = nz; SP.nx = nx; SP.ny = ny;
+    SP.dz = dz; SP.dx = dx; SP.dy = dy;
+    SP.have_geom = true;
+    SP.ready = false;
+    if (SP.rc == 0) { SP.rc = 4; SP.k = 8; }
+    *ierr = 0;
+}
+
+typedef struct {
+    unsigned long long seed;
+    long long nsamp;
+} table_batch_t;
+
+static int table_batch(void *ctx, long long step, int B, float *x, float *y, cudaStream_t s)
+{
+    table_batch_t *c = (table_batch_t *)ctx;
+    return fk_mlp_sample(SP.nz, SP.nx, SP.ny, SP.dz, SP.dx, SP.dy, SL.ntf, SL.ldgrd, SP.vref, SL.tables,
+                         SP.sta_dev, c->seed, c->nsamp, step, B, x, y, s);
+}
+
+void fteik_b200_locate_trainSurrogate(long long nsamples, int steps, int batch, double lr, double vref,
+                                      unsigned long long seed, double *loss, int *ierr)
+{
+    /* Trains the surrogate network (fteik_b200_mlp_*; initialised here with
+     * 5 x 256 units when absent) on nsamples (table, grid node) pairs of the
+     * locator's tables, target tau = T v_ref / distance. */
+    const char *who = "fteik_b200_locate_trainSurrogate";
+    *ierr = 1;
+    *loss = 0.0;
+    if (!SL.init || !SP.have_geom) { FK_ERR("%s: set the locator geometry first", who); return; }
+    if (nsamples < 1 || steps < 1 || batch < 1 || lr <= 0.0 || vref <= 0.0) { FK_ERR("%s: bad arguments", who); return; }
+    if (!fk_mlp_ready()) {
+        int e2;
+        fteik_b200_mlp_initialize(256, 5, seed, &e2);
+        if (e2) return;
+    }
+    SP.vref = vref;
+    table_batch_t c;
+    c.seed = seed;
+    c.nsamp = nsamples;
+    if (fk_mlp_train_device(table_batch, &c, steps, batch, lr, loss)) return;
+    SP.ready = false;
+    *ierr = 0;
+}
+
+void fteik_b200_locate_buildSurrogate(int bz, int bx, int by, int *ierr)
+{
+    /* Surrogate travel times at the centres of the coarse blocks (bz x bx x
+     * by fine nodes each), ranked by the tensor-core search in method 2. */
+    const char *who = "fteik_b200_locate_buildSurrogate";
+    *ierr = 1;
+    if (!SL.init || !SP.have_geom || !fk_mlp_ready() || SP.vref <= 0.0) {
+        FK_ERR("%s: needs the locator geometry and a trained surrogate", who);
+        return;
+    }
+    if (bz < 1 || bx < 1 || by < 1 || bz > 32 || bx > 32 || by > 32 || bz * bx * by > 1024 ||
+        bz * bx * by < 2) {
+        FK_ERR("%s: block %dx%dx%d: each side in [1,32], 2 to 1024 nodes", who, bz, bx, by);
+        return;
+    }
+    SP.bz = bz;
+    SP.bx = bx;
+    SP.by = by;
+    SP.ncz = (SP.nz + bz - 1) / bz;
+    SP.ncx = (SP.nx + bx - 1) / bx;
+    SP.ncy = (SP.ny + by - 1) / by;
+    SP.ngrd_c = SP.ncz * SP.ncx * SP.ncy;
+    SP.ldc = (SP.ngrd_c + 15) / 16 * 16;
+    fk_dfree(SP.coarse);
+    fk_dfree(SP.bpack_c);
+    SP.coarse = (float *)fk_dalloc(sizeof(float) * (size_t)SL.ntf * SP.ldc, who);
+    SP.bpack_c = fk_dalloc(fk_locate_tc_table_bytes(SP.ngrd_c), who);
+    const long long nrow = (long long)SL.ntf * SP.ngrd_c;
+    const long long chunk = 1 << 18;
+    float *x = (float *)fk_dalloc(sizeof(float) * 6 * (size_t)chunk, who);
+    float *dist = (float *)fk_dalloc(sizeof(float) * (size_t)chunk, who);
+    float *tau = (float *)fk_dalloc(sizeof(float) * (size_t)chunk, who);
+    int e = (SP.coarse && SP.bpack_c && x && dist && tau) ? 0 : 1;
+    cudaStream_t s = fk_stream();
+    if (!e) e = (int)cudaMemsetAsync(SP.coarse, 0, sizeof(float) * (size_t)SL.ntf * SP.ldc, s);
+    for (long long r0 = 0; r0 < nrow && !e; r0 += chunk) {
+        const long long m = nrow - r0 < chunk ? nrow - r0 : chunk;
+        e = fk_mlp_coarse_inputs(SP.nz, SP.nx, SP.ny, SP.dz, SP.dx, SP.dy, SL.ntf, SP.vref, SP.sta_dev, bz, bx,
+                                 by, SP.ncz, SP.ncx, SP.ncy, r0, m, x, dist, s);
+        if (!e) e = fk_mlp_forward_device(m, x, tau, s);
+        if (!e) e = fk_mlp_coarse_store(r0, m, SP.ngrd_c, SP.ldc, tau, dist, SP.coarse, s);
+    }
+    if (!e) e = fk_locate_tc_pack_tables(SP.ngrd_c, SP.ldc, SL.ntf, SP.coarse, SP.bpack_c, s);
+    fk_dfree(SP.fine_blk);
+    SP.fine_blk = (float *)fk_dalloc(sizeof(float) * (size_t)SP.ngrd_c * SL.ntf * (size_t)(bz * bx * by), who);
+    if (!SP.fine_blk) e = 1;
+    if (!e) e = fk_locate_block_tables(SP.nz, SP.nx, SP.ny, bz, bx, by, SL.ntf, SL.ldgrd, SL.tables, SP.fine_blk, s);
+    SP.blk_gen = SL.table_gen;
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    fk_dfree(x); fk_dfree(dist); fk_dfree(tau);
+    if (fk_check(e, who)) return;
+    SP.ready = true;
+    *ierr = 0;
+}
+
+void fteik_b200_locate_setPruning(int ncoarse_runs, int ncoarse_nodes, int *ierr)
+{
+    *ierr = 1;
+    if (ncoarse_runs < 1 || ncoarse_runs > 4 || ncoarse_nodes < 1 || ncoarse_nodes > 32) {
+        FK_ERR("fteik_b200_locate_setPruning: need 1 <= runs <= 4 and 1 <= nodes <= 32");
+        return;
+    }
+    SP.rc = ncoarse_runs;
+    SP.k = ncoarse_nodes;
+    *ierr = 0;
+}
+
+void fteik_b200_locate_getPruneInfo(int *nfallback, int *ncoarse, long long *nblocks, int *maxblocks, int *ierr)
+{
+    *maxblocks = SP.last_max_blocks;
+    *nfallback = SP.last_fallback;
+    *ncoarse = SP.ready ? SP.ngrd_c : 0;
+    *nblocks = SP.last_blocks;
+    *ierr = 0;
+}
+
+void fteik_b200_locate_getSurrogateTable(int itf, int n, float out[], int *ierr)
+{
+    /* coarse surrogate travel times of table itf (coarse nodes z fastest) */
+    *ierr = 1;
+    if (!SP.ready || itf < 1 || itf > SL.ntf || n < SP.ngrd_c) { FK_ERR("fteik_b200_locate_getSurrogateTable: not built or bad arguments"); return; }
+    *ierr = fk_check((int)cudaMemcpy(out, SP.coarse + (size_t)(itf - 1) * SP.ldc, sizeof(float) * (size_t)SP.ngrd_c,
+                                     cudaMemcpyDeviceToHost), "fteik_b200_locate_getSurrogateTable");
+}
+
+/* Exhaustive tensor-core search of the events evs[0..m-1] (0-based). */
+static int locate_tc_subset(const int *evs, int m, int *idx, double *t0, double *obj)
+{
+    if (m > SP.sub_cap) {
+        fk_dfree(SP.sub_obs); fk_dfree(SP.sub_w); fk_dfree(SP.sub_elig);
+        SP.sub_obs = (double *)fk_dalloc(sizeof(double) * (size_t)m * SL.ntf, "locate");
+        SP.sub_w = (double *)fk_dalloc(sizeof(double) * (size_t)m * SL.ntf, "locate");
+        SP.sub_elig = (unsigned char *)fk_dalloc((size_t)m, "locate");
+        SP.sub_cap = (SP.sub_obs && SP.sub_w && SP.sub_elig) ? m : 0;
+        if (!SP.sub_cap) return 1;
+    }
+    const size_t nt = (size_t)SL.ntf;
+    double *ho = (double *)malloc(sizeof(double) * (size_t)m * nt);
+    double *hw = (double *)malloc(sizeof(double) * (size_t)m * nt);
+    unsigned char *he = (unsigned char *)malloc((size_t)m);
+    for (int i = 0; i < m; i++) {
+        memcpy(ho + i * nt, SL.obs64 + (size_t)evs[i] * nt, sizeof(double) * nt);
+        memcpy(hw + i * nt, SL.w64 + (size_t)evs[i] * nt, sizeof(double) * nt);
+        he[i] = 1;
+    }
+    const int npart = fk_locate_tc_npart(m, SL.ngrd);
+    int e = pack_tables() || ensure_tc(m, npart);
+    cudaStream_t s = fk_stream();
+    int kerr = 0;
+    if (!e) e = (int)cudaMemcpyAsync(SP.sub_obs, ho, sizeof(double) * (size_t)m * nt, cudaMemcpyHostToDevice, s);
+    if (!e) e = (int)cudaMemcpyAsync(SP.sub_w, hw, sizeof(double) * (size_t)m * nt, cudaMemcpyHostToDevice, s);
+    if (!e) e = (int)cudaMemcpyAsync(SP.sub_elig, he, (size_t)m, cudaMemcpyHostToDevice, s);
+    if (!e) e = (int)cudaMemsetAsync(SL.err_dev, 0, sizeof(int), s);
+    if (!e)
+        e = fk_locate_tc(SL.ngrd, SL.ldgrd, SL.ntf, SL.tables, SL.bpack, m, SP.sub_obs, SP.sub_w, SP.sub_elig,
+                         SL.apack, npart, SL.cand_v, SL.cand_i, SL.rescore, SL.tc_idx, SL.tc_t0, SL.tc_obj,
+                         SL.err_dev, NULL, s);
+    if (!e) e = (int)cudaMemcpyAsync(idx, SL.tc_idx, sizeof(int) * (size_t)m, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaMemcpyAsync(t0, SL.tc_t0, sizeof(double) * (size_t)m, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaMemcpyAsync(obj, SL.tc_obj, sizeof(double) * (size_t)m, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaMemcpyAsync(&kerr, SL.err_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    free(ho); free(hw); free(he);
+    if (fk_check(e, "locate (fallback search)")) return 1;
+    if (kerr) { FK_ERR("locate (fallback search): pipeline wait timed out (code %d)", kerr); return 1; }
+    return 0;
+}
+
+static int locate_range_pruned(int e0, int n, int *idx, double *t0, double *obj)
+{
+    if (!SP.ready) { FK_ERR("locate (surrogate-pruned): build the surrogate first"); return 1; }
+    if (SP.blk_gen != SL.table_gen) {
+        /* the exact tables changed since the block-major copy was made */
+        int eb = fk_locate_block_tables(SP.nz, SP.nx, SP.ny, SP.bz, SP.bx, SP.by, SL.ntf, SL.ldgrd, SL.tables,
+                                        SP.fine_blk, fk_stream());
+        if (fk_check(eb, "locate (surrogate-pruned): block copy")) return 1;
+        SP.blk_gen = SL.table_gen;
+    }
+    const int npart = fk_locate_tc_npart(n, SP.ngrd_c);
+    if (upload_obs64() || ensure_tc(n, npart)) return 1;
+    if (n > SP.flag_cap) {
+        fk_dfree(SP.flag_dev);
+        SP.flag_dev = (unsigned char *)fk_dalloc((size_t)n, "locate");
+        SP.flag_cap = SP.flag_dev ? n : 0;
+        if (!SP.flag_dev) return 1;
+    }
+    cudaStream_t s = fk_stream();
+    unsigned char *flag = (unsigned char *)malloc((size_t)n);
+    int kerr = 0;
+    if (SP.timing && !SP.ev[0])
+        for (int k = 0; k < 4; k++) cudaEventCreate(&SP.ev[k]);
+    int e = (int)cudaMemsetAsync(SL.err_dev, 0, sizeof(int), s);
+    if (!e && SP.timing) e = (int)cudaEventRecord(SP.ev[0], s);
+    if (!e)
+        e = fk_locate_tc(SP.ngrd_c, SP.ldc, SL.ntf, SP.coarse, SP.bpack_c, n, SL.obs64_dev + (size_t)e0 * SL.ntf,
+                         SL.w64_dev + (size_t)e0 * SL.ntf, SL.elig_dev + e0, SL.apack, npart, SL.cand_v,
+                         SL.cand_i, 0, NULL, NULL, NULL, SL.err_dev, NULL, s);
+    if (!e && SP.timing) e = (int)cudaEventRecord(SP.ev[1], s);
+    if (!e)
+        e = fk_locate_prune(n, npart, SP.rc, SP.k, SP.nz, SP.nx, SP.ny, SP.bz, SP.bx, SP.by, SL.ldgrd, SP.ldc, SL.ntf,
+                            SP.coarse, SP.fine_blk, SL.obs64_dev + (size_t)e0 * SL.ntf,
+                            SL.w64_dev + (size_t)e0 * SL.ntf, SL.elig_dev + e0, SL.cand_v, SL.cand_i,
+                            SL.tc_idx, SL.tc_t0, SL.tc_obj, SP.flag_dev, s);
+    if (!e && SP.timing) e = (int)cudaEventRecord(SP.ev[2], s);
+    if (!e) e = (int)cudaMemcpyAsync(idx, SL.tc_idx, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaMemcpyAsync(t0, SL.tc_t0, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaMemcpyAsync(obj, SL.tc_obj, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaMemcpyAsync(flag, SP.flag_dev, (size_t)n, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaMemcpyAsync(&kerr, SL.err_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (!e && SP.timing) e = (int)cudaEventRecord(SP.ev[3], s);
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    if (!e && SP.timing)
+        for (int k = 0; k < 3; k++) cudaEventElapsedTime(&SP.stage_ms[k], SP.ev[k], SP.ev[k + 1]);
+    if (fk_check(e, "locate (surrogate-pruned)") || kerr) {
+        if (kerr) FK_ERR("locate (surrogate-pruned): pipeline wait timed out (code %d)", kerr);
+        free(flag);
+        return 1;
+    }
+    /* events whose pruned optimum lies on an unexamined block face: the
+     * exhaustive tensor-core search decides them */
+    int *fb = (int *)malloc(sizeof(int) * (size_t)n);
+    int m = 0;
+    SP.last_blocks = 0;
+    SP.last_max_blocks = 0;
+    for (int i = 0; i < n; i++) {
+        if (!SL.elig[e0 + i]) continue;
+        if (flag[i] == 0xFF) fb[m++] = e0 + i;
+        else {
+            SP.last_blocks += flag[i];
+            if (flag[i] > SP.last_max_blocks) SP.last_max_blocks = flag[i];
+        }
+    }
+    int rc = 0;
+    SP.last_fallback = m;
+    if (m > 0) {
+        int *fi = (int *)malloc(sizeof(int) * (size_t)m);
+        double *ft = (double *)malloc(sizeof(double) * (size_t)m);
+        double *fo = (double *)malloc(sizeof(double) * (size_t)m);
+        rc = locate_tc_subset(fb, m, fi, ft, fo);
+        for (int j = 0; j < m && !rc; j++) {
+            idx[fb[j] - e0] = fi[j];
+            t0[fb[j] - e0] = ft[j];
+            obj[fb[j] - e0] = fo[j];
+        }
+        free(fi); free(ft); free(fo);
+    }
+    free(fb);
+    free(flag);
+    for (int i = 0; i < n && !rc; i++) {
+        if (SL.elig[e0 + i]) continue;
+        int ix;
+        float ft0, fobj;
+        if (locate_range(e0 + i, 1, &ix, &ft0, &fobj)) return 1;
+        idx[i] = ix;
+        t0[i] = (double)ft0;
+        obj[i] = (double)fobj;
+    }
+    return rc;
+}
+
+void fteik_b200_locate_setStageTiming(int enable, int *ierr)
+{
+    SP.timing = enable != 0;
+    *ierr = 0;
+}
+
+void fteik_b200_locate_getStageTimes(float *coarse_ms, float *prune_ms, float *copy_ms, int *ierr)
+{
+    *coarse_ms = SP.stage_ms[0];
+    *prune_ms = SP.stage_ms[1];
+    *copy_ms = SP.stage_ms[2];
+    *ierr = SP.timing ? 0 : 1;
 }

@@ -22,7 +22,7 @@
  * Every thread of the epilogue owns one event row; it reduces each run of 32
  * grid points to its minimum and keeps the four best runs of its partition.
  * A second kernel takes each event's best runs over all partitions and
- * evaluates every point of them with the reference's formula in FP64 on the
+ * evaluates every point of them with the reference's misfit in FP64 on the
  * FP32 tables (one lane per point, coalesced), returning the minimum (first
  * index among equal misfits).
  *
@@ -537,6 +537,60 @@ __device__ __forceinline__ bool lex_lt_d(double v, int i, double w, int j)
     return v < w || (v == w && i < j);
 }
 
+/* FP64 misfit of one grid point, locate.F90:675-708 evaluated in one pass:
+ * with d_i = o_i - T_i(g) and t0 = sum w d / sum w,
+ *   obj = 1/2 sum (w (d - t0))^2 = 1/2 (sum w^2 d^2 - 2 t0 sum w^2 d + t0^2 sum w^2).
+ * Reduced picks keep |d| within tens of seconds, so the cancellation costs
+ * about 1e-12 absolute in FP64.  Picks and weights come from shared memory. */
+__device__ __forceinline__ double misfit64(const float *__restrict__ tab, size_t ld, long long g, int ntf,
+                                           const double *o, const double *w, double sw, double sw2,
+                                           double &t0)
+{
+    double a = 0.0, b = 0.0, c = 0.0;
+#pragma unroll 16
+    for (int i = 0; i < ntf; ++i) {
+        const double wi = w[i];
+        const double d = o[i] - (double)__ldg(tab + (size_t)i * ld + g);
+        const double w2d = wi * wi * d;
+        a += wi * d;
+        b += w2d;
+        c += w2d * d;
+    }
+    t0 = a / sw;
+    return 0.5 * (c - 2.0 * t0 * b + t0 * t0 * sw2);
+}
+
+/* misfit64 for NP grid points at once (independent loads in flight);
+ * g[j] < 0 skips point j (result 1e300). */
+template <int NP>
+__device__ __forceinline__ void misfit64_n(const float *__restrict__ tab, size_t ld, const long long (&g)[NP],
+                                           int ntf, const double *o, const double *w, double sw, double sw2,
+                                           double (&ob)[NP], double (&t0)[NP])
+{
+    double a[NP], b[NP], c[NP];
+    long long gg[NP];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) { a[j] = b[j] = c[j] = 0.0; gg[j] = g[j] < 0 ? 0 : g[j]; }
+#pragma unroll 8
+    for (int i = 0; i < ntf; ++i) {
+        const double wi = w[i], oi = o[i];
+        const float *row = tab + (size_t)i * ld;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+            const double d = oi - (double)__ldg(row + gg[j]);
+            const double w2d = wi * wi * d;
+            a[j] += wi * d;
+            b[j] += w2d;
+            c[j] += w2d * d;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+        t0[j] = a[j] / sw;
+        ob[j] = g[j] < 0 ? 1.0e300 : 0.5 * (c[j] - 2.0 * t0[j] * b[j] + t0[j] * t0[j] * sw2);
+    }
+}
+
 /* One warp per event: take the R best runs by approximate score (ties by run
  * number), evaluate the reference's misfit in FP64 at every point of each run
  * (lane = point), keep the minimum (first index among equal misfits). */
@@ -547,15 +601,22 @@ __global__ void rescore_kernel(int nev, int npart, int ngrd, int ntf, int ldgrd,
                                int *__restrict__ out_idx, double *__restrict__ out_t0,
                                double *__restrict__ out_obj)
 {
+    __shared__ double s_o[8][BK], s_w[8][BK];
+    const int wib = threadIdx.x >> 5;
     const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (e >= nev || !elig[e]) return;
     const int C = npart * TOPK;
     const float *cv = cand_v + (size_t)e * C;
     const int *ci = cand_i + (size_t)e * C;
-    const double *o = obs + (size_t)e * ntf, *w = wts + (size_t)e * ntf;
-    double sw = 0.0;
-    for (int i = 0; i < ntf; ++i) sw += w[i];
+    for (int i = lane; i < BK; i += 32) {
+        s_o[wib][i] = i < ntf ? obs[(size_t)e * ntf + i] : 0.0;
+        s_w[wib][i] = i < ntf ? wts[(size_t)e * ntf + i] : 0.0;
+    }
+    __syncwarp();
+    const double *o = s_o[wib], *w = s_w[wib];
+    double sw = 0.0, sw2 = 0.0;
+    for (int i = 0; i < ntf; ++i) { sw += w[i]; sw2 += w[i] * w[i]; }
     float pv = -3.0e38f;
     int pi = -1;
     double best_obj = 1.0e300, best_t0 = 0.0;
@@ -582,18 +643,7 @@ __global__ void rescore_kernel(int nev, int npart, int ngrd, int ntf, int ldgrd,
         pi = mi;
         const int g = mi * RUN + lane;
         double ob = 1.0e300, t0 = 0.0;
-        if (g < ngrd) {
-            double a = 0.0;
-            for (int i = 0; i < ntf; ++i)
-                if (w[i] > 0.0) a += w[i] * (o[i] - (double)__ldg(tables + (size_t)i * ldgrd + g));
-            t0 = a / sw;
-            ob = 0.0;
-            for (int i = 0; i < ntf; ++i)
-                if (w[i] > 0.0) {
-                    const double rr = w[i] * (o[i] - (double)__ldg(tables + (size_t)i * ldgrd + g) - t0);
-                    ob += 0.5 * rr * rr;
-                }
-        }
+        if (g < ngrd) ob = misfit64(tables, (size_t)ldgrd, g, ntf, o, w, sw, sw2, t0);
         int gg = g < ngrd ? g : 0x7fffffff;
 #pragma unroll
         for (int s = 16; s > 0; s >>= 1) {
@@ -611,6 +661,214 @@ __global__ void rescore_kernel(int nev, int npart, int ngrd, int ntf, int ldgrd,
     }
 }
 
+
+/* ---- pruned search (surrogate coarse lattice) ---------------------------- */
+
+struct PruneGeom {
+    int nz, nx, ny;           /* fine grid */
+    int bz, bx, by;           /* block of fine nodes per coarse node */
+    int ncz, ncx, ncy;
+    int ldgrd, ldc, ntf;
+};
+
+/* One warp per event.
+ *  1. the RC best coarse runs of the tensor-core ranking on the coarse
+ *     (surrogate) tables; every coarse node of them scored in FP64 on those
+ *     tables; the K best coarse nodes kept;
+ *  2. every fine node of the K coarse nodes' blocks (coarse node c owns the
+ *     fine nodes f with floor(f / b) = c on every axis: bz bx by per block,
+ *     bz bx by K in all) scored in FP64 on the exact tables, read from their
+ *     block-major copy (one contiguous run per table and block); the minimum
+ *     returned (first index among equal misfits);
+ *  3. while a node next to that minimum (26-neighbourhood) lies in a block
+ *     not yet examined, that block is examined too (a descent over blocks on
+ *     the exact misfit, 32 blocks at most); flag[e] = 1 when the limit stops
+ *     it, and the caller searches the event exhaustively.
+ * flag[e]: 0xFF for a fall-back event, else the number of blocks examined. */
+__global__ void __launch_bounds__(256, 3) prune_kernel(int nev, int npart, int RC, int K, PruneGeom G,
+                             const float *__restrict__ coarse, const float *__restrict__ fine,
+                             const double *__restrict__ obs, const double *__restrict__ wts,
+                             const unsigned char *__restrict__ elig, const float *__restrict__ cand_v,
+                             const int *__restrict__ cand_i, int *__restrict__ out_idx,
+                             double *__restrict__ out_t0, double *__restrict__ out_obj,
+                             unsigned char *__restrict__ flag)
+{
+    __shared__ int s_sel[8][32];   /* examined coarse nodes per warp */
+    __shared__ double s_o[8][BK], s_w[8][BK];
+    const int wib = threadIdx.x >> 5;
+    const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (e >= nev || !elig[e]) return;
+    const long long ncoarse = (long long)G.ncz * G.ncx * G.ncy;
+    const int C = npart * TOPK;
+    const float *cv = cand_v + (size_t)e * C;
+    const int *ci = cand_i + (size_t)e * C;
+    for (int i = lane; i < BK; i += 32) {
+        s_o[wib][i] = i < G.ntf ? obs[(size_t)e * G.ntf + i] : 0.0;
+        s_w[wib][i] = i < G.ntf ? wts[(size_t)e * G.ntf + i] : 0.0;
+    }
+    __syncwarp();
+    const double *o = s_o[wib], *w = s_w[wib];
+    double sw = 0.0, sw2 = 0.0;
+    for (int i = 0; i < G.ntf; ++i) { sw += w[i]; sw2 += w[i] * w[i]; }
+    /* 1a. best coarse runs; each lane scores its point of every run */
+    double cval[4];
+    int cidx[4];
+    long long cg[4];
+    float pv = -3.0e38f;
+    int pi = -1;
+    for (int r = 0; r < 4; ++r) {
+        cg[r] = -1;
+        cidx[r] = 0x7fffffff;
+        if (r >= RC) continue;
+        float mv = 3.0e38f;
+        int mi = 0x7fffffff;
+        for (int c = lane; c < C; c += 32) {
+            const int i = ci[c];
+            const float v = cv[c];
+            if (i >= 0 && (long long)i * RUN < ncoarse && lex_lt(pv, pi, v, i) && lex_lt(v, i, mv, mi)) {
+                mv = v;
+                mi = i;
+            }
+        }
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const float ov = __shfl_xor_sync(0xffffffffu, mv, s);
+            const int oi = __shfl_xor_sync(0xffffffffu, mi, s);
+            if (lex_lt(ov, oi, mv, mi)) { mv = ov; mi = oi; }
+        }
+        if (mi == 0x7fffffff) continue;
+        pv = mv;
+        pi = mi;
+        const long long c = (long long)mi * RUN + lane;
+        if (c < ncoarse) { cg[r] = c; cidx[r] = (int)c; }
+    }
+    {
+        double ct0[4];
+        misfit64_n<4>(coarse, (size_t)G.ldc, cg, G.ntf, o, w, sw, sw2, cval, ct0);
+    }
+    /* 1b. the K best coarse nodes */
+    double pvd = -1.0e300;
+    int pid = -1;
+    int nsel = 0;
+    for (int k = 0; k < K; ++k) {
+        double mv = 1.0e300;
+        int mi = 0x7fffffff;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+            if (lex_lt_d(pvd, pid, cval[r], cidx[r]) && lex_lt_d(cval[r], cidx[r], mv, mi)) {
+                mv = cval[r];
+                mi = cidx[r];
+            }
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, mv, s);
+            const int oi = __shfl_xor_sync(0xffffffffu, mi, s);
+            if (lex_lt_d(ov, oi, mv, mi)) { mv = ov; mi = oi; }
+        }
+        if (mi == 0x7fffffff) break;
+        pvd = mv;
+        pid = mi;
+        if (lane == 0) s_sel[wib][k] = mi;
+        nsel = k + 1;
+    }
+    __syncwarp();
+    /* 2. fine nodes of the selected blocks */
+    const int nb = G.bz * G.bx * G.by;
+    double best = 1.0e300, bt0 = 0.0;
+    int bg = 0x7fffffff, bk = -1;
+    auto scan_block = [&](int k) {
+        const int c = s_sel[wib][k];
+        const int cz = c % G.ncz, cx = (c / G.ncz) % G.ncx, cy = c / (G.ncz * G.ncx);
+        for (int p0 = lane; p0 < nb; p0 += 64) {
+            long long g2[2];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int p = p0 + 32 * j;
+                const int fz = G.bz * cz + p % G.bz, fx = G.bx * cx + (p / G.bz) % G.bx,
+                          fy = G.by * cy + p / (G.bz * G.bx);
+                g2[j] = (p < nb && fz < G.nz && fx < G.nx && fy < G.ny)
+                            ? fz + (long long)G.nz * (fx + (long long)G.nx * fy) : -1;
+            }
+            /* the block's nodes are contiguous per table in the block-major copy */
+            long long q2[2];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) q2[j] = g2[j] >= 0 ? p0 + 32 * j : -1;
+            double ob[2], t0[2];
+            misfit64_n<2>(fine + (size_t)c * G.ntf * nb, (size_t)nb, q2, G.ntf, o, w, sw, sw2, ob, t0);
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+                if (g2[j] >= 0 && lex_lt_d(ob[j], (int)g2[j], best, bg)) {
+                    best = ob[j]; bg = (int)g2[j]; bt0 = t0[j]; bk = k;
+                }
+        }
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, s);
+            const int og = __shfl_xor_sync(0xffffffffu, bg, s);
+            const double ot = __shfl_xor_sync(0xffffffffu, bt0, s);
+            const int ok = __shfl_xor_sync(0xffffffffu, bk, s);
+            if (lex_lt_d(ob, og, best, bg)) { best = ob; bg = og; bt0 = ot; bk = ok; }
+        }
+    };
+    for (int k = 0; k < nsel; ++k) scan_block(k);
+    /* 3. while a neighbour of the minimum lies in a block not yet examined,
+     * examine that block (a descent over blocks on the exact misfit); give
+     * up after MAXB blocks in all */
+    constexpr int MAXB = 32;
+    unsigned char fb = 0;
+    for (;;) {
+        /* every node of the 26-neighbourhood of the best node must lie in
+         * an examined block: a minimum over face neighbours alone can sit
+         * next to a lower diagonal node in an oblique valley (lane q checks
+         * neighbour q; the first missing block in lane order is added) */
+        int add = -1;
+        if (bk >= 0 && lane < 27 && lane != 13) {
+            const int f0 = bg % G.nz, f1 = (bg / G.nz) % G.nx, f2 = bg / (G.nz * G.nx);
+            const int gz = f0 + lane % 3 - 1, gx = f1 + (lane / 3) % 3 - 1, gy = f2 + lane / 9 - 1;
+            if (gz >= 0 && gx >= 0 && gy >= 0 && gz < G.nz && gx < G.nx && gy < G.ny) {
+                const int cn = gz / G.bz + G.ncz * (gx / G.bx + G.ncx * (gy / G.by));
+                bool have = false;
+                for (int k = 0; k < nsel; ++k) have |= s_sel[wib][k] == cn;
+                if (!have) add = cn;
+            }
+        }
+        const unsigned miss = __ballot_sync(0xffffffffu, add >= 0);
+        add = miss ? __shfl_sync(0xffffffffu, add, __ffs(miss) - 1) : -1;
+        if (add < 0) break;
+        if (nsel >= MAXB) { fb = 1; break; }
+        if (lane == 0) s_sel[wib][nsel] = add;
+        __syncwarp();
+        scan_block(nsel);
+        ++nsel;
+    }
+    if (bk < 0) fb = 1;
+    if (lane != 0) return;
+    out_idx[e] = bg;
+    out_t0[e] = bt0;
+    out_obj[e] = best;
+    flag[e] = fb ? (unsigned char)0xFF : (unsigned char)nsel;
+}
+
+/* Block-major copy of the exact tables for the pruned search:
+ * out[((c * ntf) + i) * nb + p] = T_i(node p of block c), p = pz + bz (px + bx py);
+ * nodes outside the grid hold 0 (never read). */
+__global__ void block_tables_kernel(int nz, int nx, int ny, int bz, int bx, int by, int ncz, int ncx, int ntf,
+                                    int ldgrd, long long nblk, const float *__restrict__ tables,
+                                    float *__restrict__ out)
+{
+    const int nb = bz * bx * by;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= nblk * nb) return;
+    const long long c = t / nb;
+    const int p = (int)(t % nb);
+    const int cz = (int)(c % ncz), cx = (int)((c / ncz) % ncx), cy = (int)(c / ((long long)ncz * ncx));
+    const int fz = bz * cz + p % bz, fx = bx * cx + (p / bz) % bx, fy = by * cy + p / (bz * bx);
+    const bool in = fz < nz && fx < nx && fy < ny;
+    const long long g = in ? fz + (long long)nz * (fx + (long long)nx * fy) : 0;
+    float *dst = out + (size_t)c * ntf * nb + p;
+    for (int i = 0; i < ntf; ++i) dst[(size_t)i * nb] = in ? __ldg(tables + (size_t)i * ldgrd + g) : 0.0f;
+}
 } // namespace fktc
 
 using namespace fktc;
@@ -715,4 +973,35 @@ extern "C" int fk_locate_tc(int ngrd, int ldgrd, int ntf, const float *tables, c
         e = cudaGetLastError();
     }
     return (int)e;
+}
+
+extern "C" int fk_locate_prune(int nev, int npart, int rc, int k, int nz, int nx, int ny, int bz, int bx,
+                               int by, int ldgrd, int ldc, int ntf, const float *coarse, const float *fine,
+                               const double *obs, const double *wts, const unsigned char *elig,
+                               const float *cand_v, const int *cand_i, int *out_idx, double *out_t0,
+                               double *out_obj, unsigned char *flag, cudaStream_t s)
+{
+    if (nev <= 0) return 0;
+    if (rc < 1 || rc > 4 || k < 1 || k > 32 || bz < 1 || bx < 1 || by < 1) return (int)cudaErrorInvalidValue;
+    PruneGeom G;
+    G.nz = nz; G.nx = nx; G.ny = ny;
+    G.bz = bz; G.bx = bx; G.by = by;
+    G.ncz = (nz + bz - 1) / bz;
+    G.ncx = (nx + bx - 1) / bx;
+    G.ncy = (ny + by - 1) / by;
+    G.ldgrd = ldgrd; G.ldc = ldc; G.ntf = ntf;
+    prune_kernel<<<(nev * 32 + 255) / 256, 256, 0, s>>>(nev, npart, rc, k, G, coarse, fine, obs, wts, elig,
+                                                        cand_v, cand_i, out_idx, out_t0, out_obj, flag);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_locate_block_tables(int nz, int nx, int ny, int bz, int bx, int by, int ntf, int ldgrd,
+                                      const float *tables, float *out, cudaStream_t s)
+{
+    const int ncz = (nz + bz - 1) / bz, ncx = (nx + bx - 1) / bx, ncy = (ny + by - 1) / by;
+    const long long nblk = (long long)ncz * ncx * ncy;
+    const long long n = nblk * bz * bx * by;
+    block_tables_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(nz, nx, ny, bz, bx, by, ncz, ncx, ntf, ldgrd,
+                                                                    nblk, tables, out);
+    return (int)cudaGetLastError();
 }

@@ -1,0 +1,337 @@
+/*
+ * mlp.cu -- kernels of the travel-time surrogate: a fully connected network
+ * 6 -> W -> ... -> W -> 1 with SiLU activations, trained and evaluated on
+ * the GPU by these kernels (no library GEMM).
+ *
+ * The network has no counterpart in the reference; it ranks grid points for
+ * the pruned grid search and is judged by the exhaustive search.
+ *
+ * GEMM: C[M][N] = sum_k A(m,k) B(k,n) (+ bias[n]) in FP32 on the CUDA cores,
+ * 128 x 64 output tiles, K in steps of 16 through shared memory, 8 x 4
+ * outputs per thread.  A(m,k) = A[m*lda + k] (ta = 0) or A[k*lda + m]
+ * (ta = 1); B(k,n) = B[k*ldb + n] (tb = 0) or B[n*ldb + k] (tb = 1).
+ * Forward Z = X W^T + b is (ta, tb) = (0, 1); dX = dZ W is (0, 0);
+ * dW = dZ^T X is (1, 0).
+ */
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "fteik_dev.h"
+
+namespace fkmlp {
+
+constexpr int TM = 128, TN = 64, TK = 16;
+constexpr int NT = 256;  /* 16 x 16 threads, 8 x 4 outputs each */
+
+__global__ void __launch_bounds__(NT) gemm_kernel(int M, int N, int K, const float *__restrict__ A,
+                                                  int lda, int ta, const float *__restrict__ B,
+                                                  int ldb, int tb, float *__restrict__ C, int ldc,
+                                                  const float *__restrict__ bias, int accumulate)
+{
+    __shared__ float As[TK][TM + 4];
+    __shared__ float Bs[TK][TN + 4];
+    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+    /* split-K: slice blockIdx.z of gridDim.z; partial sums added atomically */
+    const int kchunk = ((K + gridDim.z * TK - 1) / (gridDim.z * TK)) * TK;
+    const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    float acc[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+    for (int k0 = kb; k0 < ke; k0 += TK) {
+        /* A tile: TM x TK = 2048 values, 8 per thread */
+        for (int t = threadIdx.x; t < TM * TK; t += NT) {
+            int mm, kk;
+            if (ta) { kk = t / TM; mm = t % TM; }     /* consecutive m: contiguous */
+            else { mm = t / TK; kk = t % TK; }        /* consecutive k: contiguous */
+            const int m = m0 + mm, k = k0 + kk;
+            float v = 0.0f;
+            if (m < M && k < ke) v = ta ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k];
+            As[kk][mm] = v;
+        }
+        for (int t = threadIdx.x; t < TN * TK; t += NT) {
+            int nn, kk;
+            if (tb) { nn = t / TK; kk = t % TK; }
+            else { kk = t / TN; nn = t % TN; }
+            const int n = n0 + nn, k = k0 + kk;
+            float v = 0.0f;
+            if (n < N && k < ke) v = tb ? B[(size_t)n * ldb + k] : B[(size_t)k * ldb + n];
+            Bs[kk][nn] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < TK; ++kk) {
+            float a[8], b[4];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = As[kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int m = m0 + ty + 16 * i;
+        if (m >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int n = n0 + tx + 16 * j;
+            if (n >= N) continue;
+            float *c = C + (size_t)m * ldc + n;
+            if (gridDim.z > 1) {
+                atomicAdd(c, acc[i][j] + ((bias && blockIdx.z == 0) ? bias[n] : 0.0f));
+            } else {
+                const float v = acc[i][j] + (bias ? bias[n] : 0.0f);
+                *c = accumulate ? *c + v : v;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ float sigmoid(float z) { return 1.0f / (1.0f + __expf(-z)); }
+
+__global__ void silu_kernel(size_t n, const float *__restrict__ z, float *__restrict__ a)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float v = z[i];
+        a[i] = v * sigmoid(v);
+    }
+}
+
+/* dz = da * d/dz silu(z) = da * s (1 + z (1 - s)), s = sigmoid(z) */
+__global__ void silu_bwd_kernel(size_t n, const float *__restrict__ z, const float *__restrict__ da,
+                                float *__restrict__ dz)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float v = z[i], s = sigmoid(v);
+        dz[i] = da[i] * s * (1.0f + v * (1.0f - s));
+    }
+}
+
+/* db[n] = sum_m dz[m][n] (one thread per column, rows in order) */
+__global__ void colsum_kernel(int M, int N, const float *__restrict__ dz, float *__restrict__ db)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    float s = 0.0f;
+    for (int m = 0; m < M; ++m) s += dz[(size_t)m * N + n];
+    db[n] = s;
+}
+
+/* mean squared error over n outputs: dpred = 2 (pred - y) / n; loss sums
+ * into a double by blocks */
+__global__ void mse_kernel(int n, const float *__restrict__ pred, const float *__restrict__ y,
+                           float *__restrict__ dpred, double *__restrict__ loss)
+{
+    __shared__ double red[256];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double l = 0.0;
+    if (i < n) {
+        const float d = pred[i] - y[i];
+        dpred[i] = 2.0f * d / (float)n;
+        l = (double)d * (double)d / (double)n;
+    }
+    red[threadIdx.x] = l;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(loss, red[0]);
+}
+
+__global__ void adam_kernel(size_t n, float *__restrict__ w, const float *__restrict__ g,
+                            float *__restrict__ m, float *__restrict__ v, float lr, float b1,
+                            float b2, float eps, float c1, float c2)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+/* counter-based hash (splitmix64 finaliser) */
+__device__ __forceinline__ uint64_t mix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+struct Geom {
+    int nz, nx, ny, ntf, ldgrd;
+    float dz, dx, dy;
+    float vref;
+};
+
+__device__ __forceinline__ void norm_inputs(const Geom &G, float zg, float xg, float yg, float zs,
+                                            float xs, float ys, float *x)
+{
+    const float ez = fmaxf((G.nz - 1) * G.dz, 1e-30f), ex = fmaxf((G.nx - 1) * G.dx, 1e-30f),
+                ey = fmaxf((G.ny - 1) * G.dy, 1e-30f);
+    x[0] = 2.0f * zg / ez - 1.0f;
+    x[1] = 2.0f * xg / ex - 1.0f;
+    x[2] = 2.0f * yg / ey - 1.0f;
+    x[3] = 2.0f * zs / ez - 1.0f;
+    x[4] = 2.0f * xs / ex - 1.0f;
+    x[5] = 2.0f * ys / ey - 1.0f;
+}
+
+/* One training batch from the tables: sample b of step t draws sample id
+ * j in [0, nsamp) and from it a table i and a grid node g; input = the
+ * normalised node and station positions, target tau = T v_ref / distance
+ * (distance floored at half a cell). */
+__global__ void sample_kernel(Geom G, const float *__restrict__ tables, const float *__restrict__ sta,
+                              uint64_t seed, long long nsamp, long long t, int B, float *__restrict__ x,
+                              float *__restrict__ y)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= B) return;
+    const long long ngrd = (long long)G.nz * G.nx * G.ny;
+    const uint64_t j = mix64(seed ^ mix64((uint64_t)t * 0x100000001B3ull + (uint64_t)b)) % (uint64_t)nsamp;
+    const uint64_t h = mix64(seed * 0x2545F4914F6CDD1Dull + j);
+    const int i = (int)(h % (uint64_t)G.ntf);
+    const long long g = (long long)(mix64(h) % (uint64_t)ngrd);
+    const int iz = (int)(g % G.nz), ix = (int)((g / G.nz) % G.nx), iy = (int)(g / ((long long)G.nz * G.nx));
+    const float zg = iz * G.dz, xg = ix * G.dx, yg = iy * G.dy;
+    const float zs = sta[3 * i], xs = sta[3 * i + 1], ys = sta[3 * i + 2];
+    norm_inputs(G, zg, xg, yg, zs, xs, ys, x + (size_t)b * 6);
+    const float hmin = fminf(G.dz, fminf(G.dx, G.dy));
+    const float d = fmaxf(sqrtf((zg - zs) * (zg - zs) + (xg - xs) * (xg - xs) + (yg - ys) * (yg - ys)), 0.5f * hmin);
+    y[b] = tables[(size_t)i * G.ldgrd + g] * G.vref / d;
+}
+
+/* Inputs of the coarse lattice: row r = table i, coarse node c (z fastest);
+ * the node sits at the centre of its fine block (bz x bx x by nodes, the
+ * part inside the grid), in general between grid nodes. */
+__device__ __forceinline__ float block_centre(int c, int b, int n, float h)
+{
+    const int lo = b * c, hi = min(b * c + b, n) - 1;
+    return 0.5f * (float)(lo + hi) * h;
+}
+
+__global__ void coarse_inputs_kernel(Geom G, const float *__restrict__ sta, int bz, int bx, int by, int ncz,
+                                     int ncx, int ncy, long long r0, long long nrow, float *__restrict__ x,
+                                     float *__restrict__ dist)
+{
+    const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (r >= nrow) return;
+    const long long row = r0 + r;
+    const long long nc = (long long)ncz * ncx * ncy;
+    const int i = (int)(row / nc);
+    const long long c = row % nc;
+    const int cz = (int)(c % ncz), cx = (int)((c / ncz) % ncx), cy = (int)(c / ((long long)ncz * ncx));
+    const float zg = block_centre(cz, bz, G.nz, G.dz), xg = block_centre(cx, bx, G.nx, G.dx),
+                yg = block_centre(cy, by, G.ny, G.dy);
+    const float zs = sta[3 * i], xs = sta[3 * i + 1], ys = sta[3 * i + 2];
+    norm_inputs(G, zg, xg, yg, zs, xs, ys, x + (size_t)r * 6);
+    dist[r] = sqrtf((zg - zs) * (zg - zs) + (xg - xs) * (xg - xs) + (yg - ys) * (yg - ys)) / G.vref;
+}
+
+/* T = tau * distance / v_ref into the coarse table layout [ntf][ldc] */
+__global__ void coarse_store_kernel(long long r0, long long nrow, long long nc, int ldc,
+                                    const float *__restrict__ tau, const float *__restrict__ dist,
+                                    float *__restrict__ out)
+{
+    const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (r >= nrow) return;
+    const long long row = r0 + r;
+    out[(row / nc) * ldc + row % nc] = tau[r] * dist[r];
+}
+
+} // namespace fkmlp
+
+using namespace fkmlp;
+
+static int grid1d(size_t n) { size_t b = (n + 255) / 256; return (int)(b < 4096 ? (b ? b : 1) : 4096); }
+
+extern "C" int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta, const float *B, int ldb,
+                           int tb, float *C, int ldc, const float *bias, int accumulate, cudaStream_t s)
+{
+    if (M <= 0 || N <= 0) return 0;
+    const int tiles = ((N + TN - 1) / TN) * ((M + TM - 1) / TM);
+    /* long K with few output tiles (weight gradients): split K over CTAs */
+    int split = 1;
+    while (tiles * split < 128 && K / (split * 2) >= 256) split *= 2;
+    if (split > 1 && !accumulate) {
+        /* the slices add into C: start from zero */
+        if (ldc == N) {
+            const cudaError_t e = cudaMemsetAsync(C, 0, sizeof(float) * (size_t)M * N, s);
+            if (e != cudaSuccess) return (int)e;
+        } else {
+            const cudaError_t e = cudaMemset2DAsync(C, sizeof(float) * (size_t)ldc, 0, sizeof(float) * (size_t)N,
+                                                    (size_t)M, s);
+            if (e != cudaSuccess) return (int)e;
+        }
+    }
+    dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM, split);
+    gemm_kernel<<<grid, NT, 0, s>>>(M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_mlp_silu(size_t n, const float *z, float *a, cudaStream_t s)
+{
+    silu_kernel<<<grid1d(n), 256, 0, s>>>(n, z, a);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_mlp_silu_bwd(size_t n, const float *z, const float *da, float *dz, cudaStream_t s)
+{
+    silu_bwd_kernel<<<grid1d(n), 256, 0, s>>>(n, z, da, dz);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_mlp_colsum(int M, int N, const float *dz, float *db, cudaStream_t s)
+{
+    colsum_kernel<<<(N + 127) / 128, 128, 0, s>>>(M, N, dz, db);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_mlp_mse(int n, const float *pred, const float *y, float *dpred, double *loss, cudaStream_t s)
+{
+    mse_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, pred, y, dpred, loss);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_mlp_adam(size_t n, float *w, const float *g, float *m, float *v, float lr, float b1,
+                           float b2, float eps, float c1, float c2, cudaStream_t s)
+{
+    adam_kernel<<<grid1d(n), 256, 0, s>>>(n, w, g, m, v, lr, b1, b2, eps, c1, c2);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_mlp_sample(int nz, int nx, int ny, double dz, double dx, double dy, int ntf, int ldgrd,
+                             double vref, const float *tables, const float *sta, unsigned long long seed,
+                             long long nsamp, long long step, int B, float *x, float *y, cudaStream_t s)
+{
+    Geom G{nz, nx, ny, ntf, ldgrd, (float)dz, (float)dx, (float)dy, (float)vref};
+    sample_kernel<<<(B + 255) / 256, 256, 0, s>>>(G, tables, sta, (uint64_t)seed, nsamp, step, B, x, y);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_mlp_coarse_inputs(int nz, int nx, int ny, double dz, double dx, double dy, int ntf,
+                                    double vref, const float *sta, int bz, int bx, int by, int ncz, int ncx,
+                                    int ncy, long long r0, long long nrow, float *x, float *dist, cudaStream_t s)
+{
+    Geom G{nz, nx, ny, ntf, 0, (float)dz, (float)dx, (float)dy, (float)vref};
+    coarse_inputs_kernel<<<(unsigned)((nrow + 255) / 256), 256, 0, s>>>(G, sta, bz, bx, by, ncz, ncx, ncy, r0,
+                                                                      nrow, x, dist);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_mlp_coarse_store(long long r0, long long nrow, long long nc, int ldc, const float *tau,
+                                   const float *dist, float *out, cudaStream_t s)
+{
+    coarse_store_kernel<<<(unsigned)((nrow + 255) / 256), 256, 0, s>>>(r0, nrow, nc, ldc, tau, dist, out);
+    return (int)cudaGetLastError();
+}

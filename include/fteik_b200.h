@@ -337,6 +337,55 @@ void fteik_b200_locate_setRescoreCandidates(int ncand, int *ierr);
  * by event); enable = 0 copies them to out (32768 floats, may be NULL). */
 void fteik_b200_locate_debugAccumulators(int enable, float *out, int *ierr);
 
+/* ---- surrogate-pruned search (method 2; no counterpart in the reference) --
+ * A small network (fteik_b200_mlp_*) learns tau = T v_ref / distance from
+ * the locator's own tables.  The grid is cut into blocks of bz x bx x by
+ * fine nodes (aligned to the grid: block c holds the nodes f with
+ * floor(f / b) = c on each axis); the network's travel times at the block
+ * centres are ranked by the tensor-core search, the best blocks are
+ * re-scored node by node on the exact tables in FP64, and while the best
+ * node lies on a face of the examined set the neighbouring block is examined
+ * too; events that exceed 32 blocks are searched exhaustively (method 1).
+ * Grid geometry: the tables' nodes are (iz, ix, iy) on a z-fastest grid with
+ * origin 0; station positions in the same frame, one per table. */
+void fteik_b200_locate_setGeometry(int nz, int nx, int ny, double dz, double dx, double dy,
+                                   int ntf, const double zsta[], const double xsta[],
+                                   const double ysta[], int *ierr);
+void fteik_b200_locate_trainSurrogate(long long nsamples, int steps, int batch, double lr,
+                                      double vref, unsigned long long seed, double *loss,
+                                      int *ierr);
+void fteik_b200_locate_buildSurrogate(int bz, int bx, int by, int *ierr);
+/* coarse runs of 32 examined (1-4, default 4) and blocks kept (1-32,
+ * default 8: 8 x 64 = 512 fine nodes with 4 x 4 x 4 blocks) */
+void fteik_b200_locate_setPruning(int ncoarse_runs, int ncoarse_nodes, int *ierr);
+/* last method-2 call: events searched exhaustively, coarse nodes, blocks of
+ * fine nodes examined over the other events, and the most for one event */
+void fteik_b200_locate_getPruneInfo(int *nfallback, int *ncoarse, long long *nblocks, int *maxblocks,
+                                    int *ierr);
+void fteik_b200_locate_getSurrogateTable(int itf, int n, float out[], int *ierr);
+/* Device time of the stages of the last method-2 call (CUDA events on the
+ * library stream, recorded while enabled): coarse ranking, pruned re-score,
+ * results to the host. */
+void fteik_b200_locate_setStageTiming(int enable, int *ierr);
+void fteik_b200_locate_getStageTimes(float *coarse_ms, float *prune_ms, float *copy_ms, int *ierr);
+
+/* ---- surrogate network (no counterpart in the reference) ----------------
+ * 6 normalised inputs (grid node z, x, y and station z, x, y, each mapped to
+ * [-1, 1] over the grid) -> depth hidden layers of width SiLU units -> tau.
+ * FP32 on the GPU, trained by Adam on mean squared error. */
+void fteik_b200_mlp_initialize(int width, int depth, unsigned long long seed, int *ierr);
+void fteik_b200_mlp_finalize(void);
+void fteik_b200_mlp_getNumberOfWeights(int *n, int *ierr);
+/* weights: per linear layer W [out][in] then b [out] */
+void fteik_b200_mlp_getWeights(int n, float w[], int *ierr);
+void fteik_b200_mlp_setWeights(int n, const float w[], int *ierr);
+void fteik_b200_mlp_forward(int n, const float x[], float tau[], int *ierr);
+/* mean squared error of n rows (x [n][6], y [n]) and its gradient (n weights) */
+void fteik_b200_mlp_gradient(int n, const float x[], const float y[], double *loss, float grad[],
+                             int *ierr);
+void fteik_b200_mlp_train(int n, const float x[], const float y[], int steps, int batch, double lr,
+                          double *loss, int *ierr);
+
 /* Allocation-free grid search (no counterpart in the reference).  For
  * callers that cannot let a library allocate device memory -- a host that
  * hands out every device buffer from its own pool, or a service that must

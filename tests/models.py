@@ -81,3 +81,25 @@ def synthetic_events(tables, nev, seed=5, noise=0.02, outlier_frac=0.05):
     out = rng.random(exact.shape) < outlier_frac
     picks[out] = exact[out] + rng.uniform(-1, 1, out.sum())
     return true, picks
+
+
+def linear_gradient_tables(nz, nx, ny, h, nsta, v0=3000.0, grad=0.5, seed=11):
+    """Analytic travel times in v(z) = v0 + grad z (analytic.F90:853-890 form,
+    T = acosh(1 + grad^2 r^2 / (2 v(zs) v(z))) / grad) from nsta surface
+    stations to every node; FP32 tables (nsta, nz*nx*ny), z fastest, and the
+    station positions (z, x, y)."""
+    rng = np.random.default_rng(seed)
+    sx = rng.uniform(0, (nx - 1) * h, nsta)
+    sy = rng.uniform(0, (ny - 1) * h, nsta)
+    sz = np.zeros(nsta)
+    z = np.arange(nz) * h
+    x = np.arange(nx) * h
+    y = np.arange(ny) * h
+    Y, X, Z = np.meshgrid(y, x, z, indexing="ij")
+    Z, X, Y = Z.ravel(), X.ravel(), Y.ravel()
+    t = np.empty((nsta, Z.size), np.float32)
+    for i in range(nsta):
+        r2 = (Z - sz[i]) ** 2 + (X - sx[i]) ** 2 + (Y - sy[i]) ** 2
+        t[i] = (np.arccosh(1.0 + grad ** 2 * r2 / (2.0 * (v0 + grad * sz[i]) * (v0 + grad * Z))) / grad
+                ).astype(np.float32)
+    return t, (sz, sx, sy)

@@ -1,0 +1,116 @@
+"""Surrogate network on the GPU against the FP64 CPU oracle
+(oracle/mlp_oracle.py), and the surrogate-pruned grid search (locate
+method 2) against the exhaustive tensor-core search (method 1), its judge."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from models import linear_gradient_tables, synthetic_events
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
+import mlp_oracle as M  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("width,depth,n", [(32, 3, 64), (256, 5, 300)])
+def test_gradient_matches_oracle(fk, width, depth, n):
+    net = fk.MLP(width, depth, seed=3)
+    rng = np.random.default_rng(1)
+    w = net.weights()
+    x = rng.uniform(-1, 1, (n, 6)).astype(np.float32)
+    y = rng.uniform(0.6, 1.1, n).astype(np.float32)
+    loss, g = net.gradient(x, y)
+    wl, gw = M.loss_and_grad(w.astype(np.float64), width, depth, x, y)
+    assert abs(loss - wl) <= 1e-5 * wl + 1e-9
+    off = 0
+    for o, i in M.layer_shapes(width, depth):
+        for size in (o * i, o):
+            a, b = g[off:off + size].astype(np.float64), gw[off:off + size]
+            assert np.linalg.norm(a - b) <= 2e-4 * np.linalg.norm(b) + 1e-9
+            off += size
+    tau = net.forward(x)
+    want = M.forward(w.astype(np.float64), width, depth, x)[0]
+    assert np.max(np.abs(tau - want)) <= 1e-5 * (1 + np.max(np.abs(want)))
+    net.finalize()
+
+
+def test_training_reduces_loss(fk):
+    net = fk.MLP(64, 3, seed=5)
+    rng = np.random.default_rng(2)
+    x = rng.uniform(-1, 1, (20000, 6)).astype(np.float32)
+    y = (0.8 + 0.1 * np.sin(2 * x[:, 0]) * x[:, 3] + 0.05 * x[:, 1] ** 2).astype(np.float32)
+    l0, _ = net.gradient(x[:4096], y[:4096])
+    net.train(x, y, steps=1500, batch=1024, lr=3e-3)
+    l1, _ = net.gradient(x[:4096], y[:4096])
+    assert l1 < l0 / 50
+    net.finalize()
+
+
+def _prune_problem(fk, nev, seed_ev=21, grad=0.5):
+    nz, nx, ny, h = 24, 40, 36, 100.0
+    tables, (sz, sx, sy) = linear_gradient_tables(nz, nx, ny, h, 64, grad=grad, seed=20)
+    _, picks = synthetic_events(tables, nev, seed=seed_ev)
+    loc = fk.Locator(nev, 64, tables.shape[1])
+    for k in range(64):
+        loc.setTravelTimeField32f(k + 1, tables[k])
+    o2t = np.arange(1, 65)
+    for e in range(nev):
+        loc.setObservation(e + 1, o2t, picks[e], np.ones(64))
+    loc.setGeometry(nz, nx, ny, h, h, h, sz, sx, sy)
+    return loc
+
+
+def test_pruned_search_matches_exhaustive(fk):
+    nev = 600
+    loc = _prune_problem(fk, nev)
+    ev = np.arange(1, nev + 1)
+    loc.setMethod(1)
+    ref = loc.locateEvents(ev)
+    fk.MLP(256, 5, seed=7)                     # fresh network
+    loss = loc.trainSurrogate(nsamples=400_000, steps=1500, batch=4096, lr=2e-3, vref=3000.0, seed=7)
+    assert loss < 1e-4                          # tau ~ 0.9: about 1 % rms
+    loc.buildSurrogate((4, 4, 4))
+    loc.setMethod(2)
+    got = loc.locateEvents(ev)
+    nfb, ncoarse, nblk = loc.pruneInfo()
+    agree = np.mean(got[0] == ref[0])
+    assert agree >= 0.995, (agree, nfb)
+    same = got[0] == ref[0]
+    assert np.all(np.abs(got[2][same] - ref[2][same]) <= 1e-9 * np.abs(ref[2][same]) + 1e-12)
+    assert nfb <= nev // 100
+    assert nblk / (nev - nfb) <= 16       # about 1k of the 34,560 fine nodes per event
+    loc.finalize()
+
+
+def test_training_is_what_makes_pruning_work(fk):
+    """Same pipeline with an untrained network (tau = 1 + noise: straight rays
+    at v_ref) in a strong gradient (v = 3000 + 2 z m/s, up to ~7600 m/s): its
+    coarse ranking is biased in depth, so the descent over blocks has much
+    more to do than with the trained network; both end at the exhaustive
+    search's answer."""
+    nev = 300
+    loc = _prune_problem(fk, nev, seed_ev=22, grad=2.0)
+    ev = np.arange(1, nev + 1)
+    loc.setMethod(1)
+    ref = loc.locateEvents(ev)
+    loc.setPruning(4, 8)
+
+    def run(steps):
+        fk.MLP(256, 5, seed=7)
+        loc.trainSurrogate(nsamples=400_000, steps=steps, batch=4096, lr=2e-3 if steps > 1 else 1e-12,
+                           vref=3000.0, seed=7)
+        loc.buildSurrogate((4, 4, 4))
+        loc.setMethod(2)
+        got = loc.locateEvents(ev)
+        nfb, _, nblk = loc.pruneInfo()
+        extra = nblk - 8 * (nev - nfb) + 540 * nfb   # an exhaustive search ~ 540 blocks
+        return got, extra
+
+    got_u, extra_u = run(1)
+    got_t, extra_t = run(1500)
+    assert np.mean(got_t[0] == ref[0]) >= 0.99
+    assert extra_u >= 3 * max(extra_t, 10), (extra_u, extra_t)
+    loc.finalize()

@@ -125,3 +125,25 @@ def test_oracle_source_snap_rules():
     assert za == pytest.approx(1.0001) and xa == pytest.approx(12.0 - 0.0001)
     with pytest.raises(ValueError):
         O.source_snap(True, n, (0, 0, 0), h, (-1.0, 5.0, 5.0))
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The FP64 network oracle (the judge of the GPU gradients) is pinned by
+    central differences of its own loss."""
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
+    import mlp_oracle as M
+    rng = np.random.default_rng(0)
+    width, depth = 7, 3
+    n = sum(o * i + o for o, i in M.layer_shapes(width, depth))
+    w = rng.normal(0, 0.5, n)
+    x = rng.uniform(-1, 1, (11, 6))
+    y = rng.uniform(0.5, 1.5, 11)
+    _, g = M.loss_and_grad(w, width, depth, x, y)
+    h = 1e-6
+    for k in rng.choice(n, 25, replace=False):
+        wp, wm = w.copy(), w.copy()
+        wp[k] += h
+        wm[k] -= h
+        fd = (M.loss_and_grad(wp, width, depth, x, y)[0] - M.loss_and_grad(wm, width, depth, x, y)[0]) / (2 * h)
+        assert abs(fd - g[k]) <= 1e-7 + 1e-5 * abs(g[k])
