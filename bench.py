@@ -328,6 +328,8 @@ def main():
                     help="solve only the 160x160x96 grid once and run the grid-search section")
     ap.add_argument("--locate-events", type=int, default=LOC_NEV)
     ap.add_argument("--surrogate-steps", type=int, default=SUR_STEPS)
+    ap.add_argument("--grids", default="1,2,3,4",
+                    help="subset of the 4 batched grids (1-based, comma separated) for profiling")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -362,6 +364,10 @@ def main():
         print(json.dumps({"locate": res}), flush=True)
         b.finalize()
         return
+    sel = [int(v) for v in args.grids.split(",")]
+    if sel != [1, 2, 3, 4]:
+        args.no_locate = True   # the grid-search section needs the 160x160x96 grid at index 3
+    grids = [grids[i - 1] for i in sel]
     upd_total = sum(node_updates(g) for g in grids)
     init_bytes, pass_bytes = algorithmic_bytes(grids)
 
@@ -479,7 +485,7 @@ def main():
                 "data": "synthetic",
                 "config": {"workload": "batched tables: 64 surface sources x 4 grids "
                            "(96x96x64, 128x128x80, 160x160x96, 200x120x100), h=50 m, v(z)=3000+0.5z",
-                           "nsweep": NSWEEP, "eps": EPS, "work_items": NSRC * len(GRIDS),
+                           "nsweep": NSWEEP, "eps": EPS, "work_items": NSRC * len(grids),
                            "node_updates_per_step": upd_total,
                            "l2": "fields 1.73 GB > L2 (inputs larger than L2)",
                            "parallelism": "replicas (one batch per GPU)" if world > 1 else "1 GPU"},

@@ -332,14 +332,20 @@ static int build_work(const char *who)
     if (!e && !SB.walker) {
         int *wnx = (int *)malloc(sizeof(int) * (size_t)nwork);
         int *wny = (int *)malloc(sizeof(int) * (size_t)nwork);
+        int *wnz = (int *)malloc(sizeof(int) * (size_t)nwork);
+        int *wg = (int *)malloc(sizeof(int) * (size_t)nwork);
         for (int w = 0; w < nwork; w++) {
             wnx[w] = gh[wh[w].grid].nx;
             wny[w] = gh[wh[w].grid].ny;
+            wnz[w] = gh[wh[w].grid].nz;
+            wg[w] = wh[w].grid;
         }
         const int np = (SB.conv_tol >= 0.0 && SB.max_pass > 0) ? SB.max_pass : SB.nsweep;
-        e = fk_tileplan_build(&SB.plan, nwork, wnx, wny, np, who);
+        e = fk_tileplan_build(&SB.plan, nwork, wnx, wny, wnz, wg, np, who);
         free(wnx);
         free(wny);
+        free(wnz);
+        free(wg);
     }
     free(gh);
     free(wh);

@@ -69,10 +69,12 @@ int fk3d_prepare(int precision, int max_nx, int max_nz, int S);
 /* Dynamic shared memory of the initialisation kernel for these sizes. */
 size_t fk3d_smem_bytes(int precision, int max_nx, int max_nz);
 
-/* Tile-wavefront plan of a 3D solve (device buffers; see tile3d_impl.cuh).
- * tasks: one sweep's tile tasks as int pairs {work, by' * ntx + bx'}
- * ordered by tile level bx' + by'; done_base: each work item's first tile in
- * done[]; the other buffers are scratch sized as noted. */
+/* Plan of a tiled or row-pipelined 3D solve (device buffers; see
+ * tile3d_impl.cuh and row3d_impl.cuh).  Tiles: tasks are one sweep's tile
+ * tasks as int pairs {work, by' * ntx + bx'} ordered by tile level bx' + by',
+ * done[] one counter per tile.  Rows: tasks are slabs of FK_SLAB_Y rows,
+ * {work, j'} ordered by the logical slab j', done[] one counter per slab.  done_base: each work item's first counter;
+ * the other buffers are scratch sized as noted. */
 typedef struct {
     const int *tasks;              /* 2 * ntask_sweep ints */
     const int *done_base;          /* nwork */
@@ -84,12 +86,25 @@ typedef struct {
     int *pass_tiles;               /* nwork * max(npass, 1) */
     int *conv_pass;                /* nwork */
     long long spin_limit;          /* bounded waits: polls before giving up */
+    int kind;                      /* FK_PLAN_TILES or FK_PLAN_ROWS */
+    int max_nx, max_ny, max_nz;    /* largest grid of the plan */
+    /* FK_PLAN_ROWS: the Gauss-Seidel passes run sources of one grid in pairs
+     * (NULL: one source per task); pairs[2 p + i] work items (-1: none),
+     * tasks2 {pair, j'} ordered by j' */
+    const int *pairs;
+    const int *tasks2;
+    int ntask2_sweep;
 } fk_tiles3d_t;
+
+#define FK_PLAN_TILES 0            /* 32 x 8 column tiles, one block per task */
+#define FK_PLAN_ROWS 1             /* FK_SLAB_Y y-rows over the whole x extent per task */
+#define FK_SLAB_Y 4
 
 #define FK_TILE_X 32
 #define FK_TILE_Y 8
 
-/* Tile-wavefront solve of every work item (same semantics as fk3d_solve). */
+/* Tiled or row-pipelined solve of every work item (per plan->kind; same
+ * semantics as fk3d_solve). */
 int fk3d_solve_tiles(int precision, const fk_grid3d_t *grids, const fk_work3d_t *work,
                      int nwork, const fk_tiles3d_t *plan, fk_result3d_t *results, double eps,
                      int nsweep, double conv_tol, int max_pass, cudaStream_t stream);

@@ -1,0 +1,486 @@
+/*
+ * row3d_impl.cuh -- slab-pipelined schedule of the 3D sweeps (the product
+ * path for batched and single-source solves).
+ *
+ * A task is one sweep over one slab of TY = FK_SLAB_Y (4) physical y-rows of
+ * one (grid, source) work item, over the whole x extent, run by one block of
+ * TY warps: warp ty owns row TY P + ty; lane l walks the columns x' = 32 k + l
+ * (k = 0, 1, ... in the sweep's logical x order) one after the other, each
+ * over its z positions.  At block step t the thread works on item
+ * j = t - l - oy (column block k = j / Zp, z position j % Zp), oy being its
+ * row's offset from the slab's upwind edge, so its seven upwind values come
+ * from:
+ *   tv, tev, tnv, tnve   its own previous step                    (registers)
+ *   te                   lane l-1's previous step                 (shuffle)
+ *                        or, for lane 0, lane 31 of block k-1 through a
+ *                        per-warp ring in shared memory (Zp - 31 >= 1 steps old)
+ * (the initialisation sweeps start at the block holding x' = lox - 1)
+ *   tn, ten              the y-upwind warp's previous step         (shared memory)
+ *                        or, for the slab's first row, the upwind slab's
+ *                        last row, final for this sweep            (global, L2)
+ * The skew ramp (31 + TY - 1 steps) is paid once per slab.
+ *
+ * Slabs publish their progress as (sweep << 20) | steps done every 32 steps
+ * and (sweep + 1) << 20 when done (one thread, release store after a block
+ * barrier).  A slab waits (one thread, acquire loads, bounded) for the
+ * upwind slab to be ahead of what it prefetches, and before it starts, for
+ * slabs P-1, P, P+1 to be done with the previous sweep (they read this
+ * slab's old values).  Tasks are claimed through one atomic ticket,
+ * sweep-major and in the sweep's y order, so a slab only waits on slabs with
+ * smaller tickets: the waits cannot cycle.  As in the level-set sweep
+ * (autoCode.f90), each node reads only upwind nodes, so the result equals
+ * the reference's sweep bit for bit in FP64.
+ */
+#pragma once
+#include "tile3d_impl.cuh"
+
+namespace fk3rw {
+using fk3::Mesh;
+using fk3::Src;
+using fk3::rmin;
+using fk3::rmax;
+
+constexpr int TY = FK_SLAB_Y;        /* rows (warps) per slab */
+constexpr int NT = TY * 32;
+constexpr int CH = 32;               /* progress granularity, steps */
+constexpr int SHIFT = 20;            /* counter = (sweep << SHIFT) | steps */
+
+template <typename R, int S>
+struct Pre {
+    R told[S], tn[S];                /* per source */
+    R duu, dud, ddu, ddd;            /* z-downwind slowness layer, s<z><x><y> with z = D */
+    int addr;                        /* node offset in the fields */
+};
+
+/* Bounded acquire wait by one thread until *p >= need; false on timeout. */
+__device__ __forceinline__ bool wait_ge1(const int *p, int need, long long limit, int *error, int code)
+{
+    long long it = 0;
+    while (fk3tw::ld_acquire(p) < need) {
+        if (++it > limit) {
+            atomicCAS(error, 0, code);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    return true;
+}
+
+/* One sweep over physical slab P.  Returns false on a wait timeout (the
+ * whole block returns false). */
+template <typename R, bool INIT, bool RESID, int S>
+__device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_grid3d_t &g, R *const (&ttp)[S],
+                                           const R *__restrict__ slow, const Src &q, int s, int sweep_no,
+                                           int P, int nslab, int *const (&prog)[S], R (*xr)[S][TY][32],
+                                           R (*xte)[S][TY][32], R *ring, int zring, int *s_flag,
+                                           double (&dmax)[S])
+{
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const unsigned FULL = 0xffffffffu;
+    const int nz = g.nz, nx = g.nx, ny = g.ny, zp = g.zp, zcp = g.zcp;
+    const int s0 = sweep_no - 1;
+    const int sz = (s0 < 4) ? 1 : -1;
+    const int sx = (s0 % 2 == 0) ? 1 : -1;
+    const int sy = ((s0 / 2) % 2 == 0) ? 1 : -1;
+    int loz = 1, lox = 1, loy = 1;
+    if (INIT) { /* solver3D.F90:493-565, flipped bound clamped to the grid */
+        loz = (sz > 0) ? max(1, q.zsi - 1) : max(1, nz - q.zsi - 1);
+        lox = (sx > 0) ? max(1, q.xsi - 1) : max(1, nx - q.xsi - 1);
+        loy = (sy > 0) ? max(1, q.ysi - 1) : max(1, ny - q.ysi - 1);
+    }
+    Mesh<R> mesh;
+    fk3::make_mesh<R>(mesh, g.dz, g.dx, g.dy);
+    Mesh<double> mesh64;
+    if (INIT) fk3::make_mesh<double>(mesh64, g.dz, g.dx, g.dy);
+    const R HUGEV = (R)FK_HUGE;
+    const int th = min(TY, ny - TY * P);             /* rows in this slab */
+    const bool row = ty < th;
+    const int y = TY * P + ty;
+    const int oy = (sy > 0) ? ty : th - 1 - ty;      /* offset from the upwind edge */
+    const int yl = (sy > 0) ? y : ny - 1 - y;        /* logical row */
+    const bool rowupd = row && yl >= loy;
+    const int wy = ty - sy;                          /* y-upwind warp (oy >= 1) */
+    const int Z = nz - loz + 1;                      /* walk positions: il = loz-1 .. nz-1 */
+    const int Zp = Z > 32 ? Z : 32;
+    const int K = (nx + 31) / 32;
+    /* column blocks wholly before x' = lox - 1 are neither updated nor read */
+    const int k0 = (lox - 1) / 32;
+    const int T = (K - k0) * Zp + 31 + (TY - 1);
+    const int Pu = P - sy;                           /* upwind slab */
+    const bool has_up = Pu >= 0 && Pu < nslab;
+    /* the upwind slab changes in this sweep when its last logical row does */
+    const int ylast_up = has_up ? ((sy > 0) ? TY * Pu + min(TY, ny - TY * Pu) - 1 : TY * Pu) : 0;
+    const bool wait_up = has_up && (((sy > 0) ? ylast_up : ny - 1 - ylast_up) >= loy);
+    const int yu = y - sy;
+    const bool has_yu = row && yu >= 0 && yu < ny;
+    const int cyU = (sy > 0) ? y - 1 : y;
+    const int cyD = min(max((sy > 0) ? y : y - 1, 0), ny - 2);
+    const int rowU = cyU * (nx - 1), rowD = cyD * (nx - 1);
+    const int ybase = y * nx, yubase = yu * nx;
+
+    auto fetch = [&](int kk, int zz, Pre<R, S> &f) {
+        const int xl = 32 * kk + tx;
+        if (!(row && zz >= 0 && zz < Z && kk < K && xl < nx)) return;
+        const int x = (sx > 0) ? xl : nx - 1 - xl;
+        const int il = loz - 1 + zz;
+        const int iz = (sz > 0) ? il : nz - 1 - il;
+        f.addr = (ybase + x) * zp + iz;
+        const int au = (yubase + x) * zp + iz;
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            if (ttp[i]) {
+                f.told[i] = fk3tw::ldcg(ttp[i] + f.addr);
+                if (oy == 0) f.tn[i] = has_yu ? fk3tw::ldcg(ttp[i] + au) : HUGEV;
+            }
+        }
+        if (rowupd && xl >= lox) {
+            const int cxU = (sx > 0) ? x - 1 : x;
+            const int cxD = min(max((sx > 0) ? x : x - 1, 0), nx - 2);
+            const int czD = min(max((sz > 0) ? iz : iz - 1, 0), nz - 2);
+            f.duu = __ldg(slow + ((rowU + cxU) * zcp + czD));
+            f.dud = __ldg(slow + ((rowD + cxU) * zcp + czD));
+            f.ddu = __ldg(slow + ((rowU + cxD) * zcp + czD));
+            f.ddd = __ldg(slow + ((rowD + cxD) * zcp + czD));
+        }
+    };
+
+    /* the first row's prefetches reach item t + 1 at step t; the upwind
+     * slab's last row works on that item at its step t + 1 + tx + th_up - 1 */
+    const int *prog_up = prog[0] + (has_up ? Pu : P);
+    if (threadIdx.x == 0) {
+        s_flag[0] = 1;
+        if (wait_up && !wait_ge1(prog_up, (s << SHIFT) | min(T, CH + TY + 1), P_.spin_limit, P_.error, 3000))
+            s_flag[0] = 0;
+    }
+    __syncthreads();
+    if (!s_flag[0]) return false;
+
+    int kn = k0, zqn = -tx - oy;         /* item of the next step */
+    Pre<R, S> cur, nxt;
+#pragma unroll
+    for (int i = 0; i < S; ++i) nxt.told[i] = nxt.tn[i] = HUGEV;
+    nxt.duu = nxt.dud = nxt.ddu = nxt.ddd = (R)0;
+    nxt.addr = 0;
+    fetch(kn, zqn, nxt);
+    R zu_uu = 0, zu_ud = 0, zu_du = 0, zu_dd = 0;   /* z-upwind layer (previous step) */
+    R r_last[S], te_last[S], tn_last[S], ten_last[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) r_last[i] = te_last[i] = tn_last[i] = ten_last[i] = HUGEV;
+    R *ring_r = ring, *ring_tn = ring + S * zring;   /* [S][zring] each */
+    for (int t = 0; t < T; ++t) {
+        if (wait_up && t > 0 && t % CH == 0) {
+            if (threadIdx.x == 0 &&
+                !wait_ge1(prog_up, (s << SHIFT) | min(T, t + CH + TY + 1), P_.spin_limit, P_.error, 3001))
+                s_flag[0] = 0;
+            __syncthreads();
+            if (!s_flag[0]) return false;
+        }
+        const int pp = (t + 1) & 1, cp = t & 1;
+        R sh_r[S], sh_tn[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            sh_r[i] = __shfl_up_sync(FULL, r_last[i], 1);
+            sh_tn[i] = __shfl_up_sync(FULL, tn_last[i], 1);
+        }
+        const int k = kn, zq = zqn;
+        cur = nxt;
+        if (++zqn == Zp) { zqn = 0; ++kn; }
+        fetch(kn, zqn, nxt);
+        const int xl = 32 * k + tx;
+        const bool valid = row && zq >= 0 && zq < Z && k < K && xl < nx;
+        const bool from_ring = k > k0 && zq >= 0 && zq < Zp;
+        const bool upd = valid && rowupd && xl >= lox && zq >= 1; /* il = loz - 1 + zq >= loz */
+        R s1, s2, s3, s4, s5, s6, s7;
+        {
+            const R uuu = zu_uu, uud = zu_ud, udu = zu_du, udd = zu_dd;
+            s1 = rmin(rmin(uuu, uud), rmin(udu, udd));
+            s2 = rmin(rmin(uuu, uud), rmin(cur.duu, cur.dud));
+            s3 = rmin(rmin(uuu, udu), rmin(cur.duu, cur.ddu));
+            s4 = rmin(uuu, uud);
+            s5 = rmin(uuu, udu);
+            s6 = rmin(uuu, cur.duu);
+            s7 = uuu;
+        }
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            const R te = (tx == 0) ? (from_ring ? ring_r[i * zring + zq] : HUGEV) : sh_r[i];
+            R tn = HUGEV, ten = HUGEV, result = HUGEV;
+            if (valid) {
+                if (oy == 0) {
+                    tn = cur.tn[i];
+                    ten = (tx == 0) ? (from_ring ? ring_tn[i * zring + zq] : HUGEV) : sh_tn[i];
+                } else {
+                    tn = xr[pp][i][wy][tx];
+                    ten = xte[pp][i][wy][tx];
+                }
+                const R told = cur.told[i];
+                result = told;
+                if (upd && ttp[i]) {
+                    const R tv = r_last[i], tev = te_last[i], tnv = tn_last[i], tnve = ten_last[i];
+                    R r;
+                    if (!INIT) {
+                        r = fk3::noinit(mesh, tv, te, tn, tev, ten, tnv, tnve, s1, s2, s3, s4, s5, s6, s7, told);
+                    } else {
+                        const int x = (sx > 0) ? xl : nx - 1 - xl;
+                        const int il = loz - 1 + zq;
+                        const int iz = (sz > 0) ? il : nz - 1 - il;
+                        const double tmin = (double)rmin(rmin(tv, te), tn);
+                        const bool lcart = tmin > q.eps_t;
+                        if (lcart || sizeof(R) == 8)
+                            r = fk3::init_node<R>(q, mesh, lcart, tv, te, tn, tev, ten, tnv, tnve, told, s1, s2,
+                                                  s3, s4, s5, s6, s7, iz + 1, x + 1, y + 1, sz, sx, sy);
+                        else /* near-source spherical stencil in FP64 */
+                            r = (R)fk3::init_node<double>(
+                                q, mesh64, lcart, (double)tv, (double)te, (double)tn, (double)tev, (double)ten,
+                                (double)tnv, (double)tnve, (double)told, (double)s1, (double)s2, (double)s3,
+                                (double)s4, (double)s5, (double)s6, (double)s7, iz + 1, x + 1, y + 1, sz, sx,
+                                sy);
+                    }
+                    if (r != told) {
+                        ttp[i][cur.addr] = r;
+                        if (RESID) {
+                            const double d = fabs((double)r - (double)told);
+                            dmax[i] = d > dmax[i] ? d : dmax[i];
+                        }
+                    }
+                    result = r;
+                }
+            }
+            if (tx == 31 && zq >= 0 && zq < Zp) {
+                ring_r[i * zring + zq] = result;
+                ring_tn[i * zring + zq] = tn;
+            }
+            xr[cp][i][ty][tx] = result;
+            xte[cp][i][ty][tx] = te;
+            r_last[i] = result;
+            te_last[i] = te;
+            tn_last[i] = tn;
+            ten_last[i] = ten;
+        }
+        if (valid && rowupd && xl >= lox) { zu_uu = cur.duu; zu_ud = cur.dud; zu_du = cur.ddu; zu_dd = cur.ddd; }
+        __syncthreads();
+        if (threadIdx.x == 0 && (t + 1) % CH == 0 && t + 1 < T) {
+            __threadfence();
+#pragma unroll
+            for (int i = 0; i < S; ++i)
+                if (prog[i]) fk3tw::st_release(prog[i] + P, (s << SHIFT) | (t + 1));
+        }
+    }
+    return true;
+}
+
+/* Persistent slab-task kernel over sweeps [s_begin, s_end).  S = 2 runs
+ * two sources of one grid in the same threads (the Gauss-Seidel passes,
+ * whose walk does not depend on the source): the slowness, the indices and
+ * the barriers are shared and the two stencils give each thread two
+ * independent dependency chains.  tasks = {pair, j'} with pairs[2 pair + i]
+ * the work items (-1: none) when S = 2, {work, j'} when S = 1. */
+template <typename R, bool INIT, bool RESID, int S>
+__global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(fk3tw::Params P, const int *pairs,
+                                                                             int zring)
+{
+    __shared__ R xr[2][S][TY][32];
+    __shared__ R xte[2][S][TY][32];
+    __shared__ long long s_task;
+    __shared__ int s_flag[2];
+    __shared__ double s_max[S][TY];
+    extern __shared__ __align__(16) unsigned char slab_smem[];
+    R *ring = reinterpret_cast<R *>(slab_smem) + (size_t)(threadIdx.x >> 5) * 2 * S * zring;
+    const int tid = threadIdx.x;
+    const long long total = (long long)(P.s_end - P.s_begin) * P.ntask_sweep;
+    for (;;) {
+        if (tid == 0) {
+            long long t = (long long)atomicAdd(P.ticket, 1ull);
+            if (t >= total || *((volatile int *)P.error) != 0) t = -1;
+            s_task = t;
+            s_flag[1] = 1;
+        }
+        __syncthreads();
+        const long long t = s_task;
+        if (t < 0) break;
+        const int s = P.s_begin + (int)(t / P.ntask_sweep);
+        const int2 tk = P.tasks[t % P.ntask_sweep];
+        int wi[S];
+        if (S == 1) wi[0] = tk.x;
+        else {
+#pragma unroll
+            for (int i = 0; i < S; ++i) wi[i] = pairs[S * tk.x + i];
+        }
+        const fk_work3d_t w0 = P.work[wi[0]];
+        const fk_grid3d_t g = P.grids[w0.grid];
+        const int nslab = (g.ny + TY - 1) / TY;
+        const int sweep_no = s % 8 + 1;
+        const int s0 = sweep_no - 1;
+        const int sy = ((s0 / 2) % 2 == 0) ? 1 : -1;
+        const int Pp = (sy > 0) ? tk.y : nslab - 1 - tk.y;   /* physical slab */
+        int *prog[S];
+        R *ttp[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            prog[i] = wi[i] >= 0 ? P.done + P.done_base[wi[i]] : nullptr;
+            ttp[i] = wi[i] >= 0 ? reinterpret_cast<R *>(i == 0 ? w0.tt : P.work[wi[i]].tt) : nullptr;
+        }
+        /* slabs P-1, P, P+1 of every source done with the previous sweep */
+        if (tid < 3 * S) {
+            const int i = tid / 3, pq = Pp + tid % 3 - 1;
+            if (prog[i] && pq >= 0 && pq < nslab) {
+                long long it = 0;
+                while (fk3tw::ld_acquire(prog[i] + pq) < (s << SHIFT)) {
+                    if (++it > P.spin_limit) {
+                        atomicCAS(P.error, 0, 2000 + tid);
+                        s_flag[1] = 0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+        __syncthreads();
+        if (!s_flag[1]) break;
+        __threadfence();
+        const int pass = INIT ? -1 : (s - 8) / 8;
+        bool skip = false;
+        if (!INIT && P.converge) {
+            skip = true;
+#pragma unroll
+            for (int i = 0; i < S; ++i)
+                if (wi[i] >= 0) skip = skip && *((volatile int *)(P.conv_pass + wi[i])) < pass;
+        }
+        Src q;
+        fk3tw::tw_setup_src(q, w0, g, P.eps);
+        if (INIT) {
+            /* slabs wholly before this sweep's source-limited rows keep their values */
+            const int loy = (sy > 0) ? max(1, q.ysi - 1) : max(1, g.ny - q.ysi - 1);
+            const int ylast = (sy > 0) ? min(g.ny, TY * (Pp + 1)) - 1 : TY * Pp;
+            const int yl_max = (sy > 0) ? ylast : g.ny - 1 - ylast;
+            skip = yl_max < loy;
+        }
+        double dmax[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) dmax[i] = 0.0;
+        if (!skip) {
+            if (!slab_sweep<R, INIT, RESID, S>(P, g, ttp, reinterpret_cast<const R *>(g.slow), q, s, sweep_no, Pp,
+                                               nslab, prog, xr, xte, ring, zring, s_flag, dmax))
+                break;
+        }
+        __syncthreads();
+        if (RESID && !INIT) {
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                double d = dmax[i];
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double v = __shfl_xor_sync(0xffffffffu, d, o);
+                    d = v > d ? v : d;
+                }
+                if ((tid & 31) == 0) s_max[i][tid >> 5] = d;
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            __threadfence();
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                if (wi[i] < 0) continue;
+                if (RESID && !INIT && pass < P.npass) {
+                    double m = 0.0;
+                    for (int k = 0; k < TY; ++k) m = s_max[i][k] > m ? s_max[i][k] : m;
+                    unsigned long long *rp = P.resid + (size_t)wi[i] * P.npass + pass;
+                    atomicMax(rp, (unsigned long long)__double_as_longlong(m));
+                    if (sweep_no == 8) {
+                        __threadfence();
+                        const int c = atomicAdd(P.pass_tiles + (size_t)wi[i] * P.npass + pass, 1);
+                        if (c == nslab - 1) {
+                            const double r = __longlong_as_double((long long)atomicAdd(rp, 0ull));
+                            if (P.converge && r <= P.conv_tol) atomicMin(P.conv_pass + wi[i], pass);
+                        }
+                    }
+                }
+                fk3tw::st_release(prog[i] + Pp, (s + 1) << SHIFT);
+            }
+        }
+    }
+}
+
+template <typename R, bool INIT, bool RESID, int S>
+inline int launch_slab_kernel(const fk3tw::Params &P, const int *pairs, int zring, cudaStream_t st)
+{
+    const size_t smem = (size_t)TY * 2 * S * zring * sizeof(R);
+    int dev = 0, nsm = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, slab_kernel<R, INIT, RESID, S>, NT, smem);
+    if (per < 1) per = 1;
+    slab_kernel<R, INIT, RESID, S><<<nsm * per, NT, smem, st>>>(P, pairs, zring);
+    return (int)cudaGetLastError();
+}
+
+template <typename R>
+inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nwork, const fk_tiles3d_t *pl,
+                       fk_result3d_t *results, double eps, int nsweep, double conv_tol, int max_pass,
+                       cudaStream_t st)
+{
+    if (nwork <= 0) return 0;
+    const int converge = conv_tol >= 0.0 && max_pass > 0;
+    const int npass = converge ? max_pass : nsweep;
+    const int npr = npass > 0 ? npass : 1;
+    const int zring = pl->max_nz > 32 ? pl->max_nz : 32;
+    /* counters hold (sweep << SHIFT) | steps: steps of a slab and sweep numbers must fit */
+    const long long steps = (long long)((pl->max_nx + 31) / 32) * zring + 31 + TY;
+    if (steps >= (1LL << SHIFT) || 8 + 8 * (long long)npr + 1 >= (1LL << (31 - SHIFT)))
+        return (int)cudaErrorInvalidValue;
+    if ((size_t)TY * 4 * zring * sizeof(R) > 48 * 1024) return (int)cudaErrorInvalidValue;
+    cudaError_t e = cudaSuccess;
+    e = cudaMemsetAsync(pl->done, 0, sizeof(int) * (size_t)pl->ntiles_total, st);
+    if (!e) e = cudaMemsetAsync(pl->tickets, 0, 2 * sizeof(unsigned long long), st);
+    if (!e) e = cudaMemsetAsync(pl->error, 0, sizeof(int), st);
+    if (!e) e = cudaMemsetAsync(pl->resid, 0, sizeof(unsigned long long) * (size_t)nwork * npr, st);
+    if (!e) e = cudaMemsetAsync(pl->pass_tiles, 0, sizeof(int) * (size_t)nwork * npr, st);
+    if (!e) e = cudaMemsetAsync(pl->conv_pass, 0x3f, sizeof(int) * (size_t)nwork, st);
+    if (e) return (int)e;
+    fk3tw::field_init_kernel<R><<<dim3(64, nwork), 256, 0, st>>>(grids, work, eps);
+    fk3tw::corners_kernel<R><<<(nwork * 8 + 127) / 128, 128, 0, st>>>(grids, work, nwork, eps);
+    fk3tw::Params P;
+    P.grids = grids;
+    P.work = work;
+    P.tasks = reinterpret_cast<const int2 *>(pl->tasks);
+    P.done_base = pl->done_base;
+    P.ntask_sweep = pl->ntask_sweep;
+    P.done = pl->done;
+    P.error = pl->error;
+    P.resid = pl->resid;
+    P.pass_tiles = pl->pass_tiles;
+    P.conv_pass = pl->conv_pass;
+    P.npass = npr;
+    P.converge = converge;
+    P.eps = eps;
+    P.conv_tol = conv_tol;
+    P.spin_limit = pl->spin_limit;
+    P.s_begin = 0;
+    P.s_end = 8;
+    P.ticket = pl->tickets;
+    if (fk3tw::g_tile_events) cudaEventRecord(fk3tw::g_tile_events[0], st);
+    int rc = launch_slab_kernel<R, true, false, 1>(P, nullptr, zring, st);
+    if (rc) return rc;
+    if (fk3tw::g_tile_events) cudaEventRecord(fk3tw::g_tile_events[1], st);
+    if (npass > 0) {
+        P.s_begin = 8;
+        P.s_end = 8 + 8 * npass;
+        P.ticket = pl->tickets + 1;
+        if (pl->pairs) { /* two sources per thread */
+            P.tasks = reinterpret_cast<const int2 *>(pl->tasks2);
+            P.ntask_sweep = pl->ntask2_sweep;
+            rc = converge ? launch_slab_kernel<R, false, true, 2>(P, pl->pairs, zring, st)
+                          : launch_slab_kernel<R, false, false, 2>(P, pl->pairs, zring, st);
+        } else {
+            rc = converge ? launch_slab_kernel<R, false, true, 1>(P, nullptr, zring, st)
+                          : launch_slab_kernel<R, false, false, 1>(P, nullptr, zring, st);
+        }
+        if (rc) return rc;
+    }
+    if (fk3tw::g_tile_events) cudaEventRecord(fk3tw::g_tile_events[2], st);
+    fk3tw::finalize_kernel<<<(nwork + 127) / 128, 128, 0, st>>>(nwork, npr, converge, npass, pl->resid,
+                                                                 pl->conv_pass, pl->error, results);
+    return (int)cudaGetLastError();
+}
+
+} // namespace fk3rw

@@ -225,7 +225,8 @@ void fteik_solver3d_solveSourceLSM(int isrc, int *ierr)
                        g.nx, g.nz, S3.eps, S3.nsweep, -1.0, 0, s);
     } else if (!e) {
         if (!S3.plan.mem || S3.plan_npass < S3.nsweep) {
-            if (fk_tileplan_build(&S3.plan, 1, &g.nx, &g.ny, S3.nsweep, "fteik_solver3d")) {
+            const int gid0 = 0;
+            if (fk_tileplan_build(&S3.plan, 1, &g.nx, &g.ny, &g.nz, &gid0, S3.nsweep, "fteik_solver3d")) {
                 *ierr = 1;
                 return;
             }

@@ -5,6 +5,7 @@
  */
 #include "sweep3d_impl.cuh"
 #include "tile3d_impl.cuh"
+#include "row3d_impl.cuh"
 
 namespace fk3tw {
 cudaEvent_t *g_tile_events = nullptr;
@@ -67,6 +68,9 @@ extern "C" int fk3d_solve_tiles(int precision, const fk_grid3d_t *grids, const f
         return fk3d_solve_tiles_f64(grids, work, nwork, plan, results, eps, nsweep, conv_tol,
                                     max_pass, stream);
     if (precision != 4) return (int)cudaErrorInvalidValue;
+    if (plan->kind == FK_PLAN_ROWS)
+        return fk3rw::launch_rows<float>(grids, work, nwork, plan, results, eps, nsweep, conv_tol,
+                                         max_pass, stream);
     return fk3tw::launch_tiles<float>(grids, work, nwork, plan, results, eps, nsweep, conv_tol,
                                       max_pass, stream);
 }

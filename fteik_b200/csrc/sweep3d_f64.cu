@@ -6,6 +6,7 @@
  */
 #include "sweep3d_impl.cuh"
 #include "tile3d_impl.cuh"
+#include "row3d_impl.cuh"
 
 extern "C" int fk3d_solve_f64(const fk_grid3d_t *grids, const fk_work3d_t *work,
                               const int *groups, int ngroups, int S, fk_result3d_t *results,
@@ -30,6 +31,9 @@ extern "C" int fk3d_solve_tiles_f64(const fk_grid3d_t *grids, const fk_work3d_t 
                                     const fk_tiles3d_t *plan, fk_result3d_t *results, double eps,
                                     int nsweep, double conv_tol, int max_pass, cudaStream_t stream)
 {
+    if (plan->kind == FK_PLAN_ROWS)
+        return fk3rw::launch_rows<double>(grids, work, nwork, plan, results, eps, nsweep, conv_tol,
+                                          max_pass, stream);
     return fk3tw::launch_tiles<double>(grids, work, nwork, plan, results, eps, nsweep, conv_tol,
                                        max_pass, stream);
 }
