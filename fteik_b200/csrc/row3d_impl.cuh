@@ -7,18 +7,21 @@
  * TY warps: warp ty owns row TY P + ty; lane l walks the columns x' = 32 k + l
  * (k = 0, 1, ... in the sweep's logical x order) one after the other, each
  * over its z positions.  At block step t the thread works on item
- * j = t - l - oy (column block k = j / Zp, z position j % Zp), oy being its
- * row's offset from the slab's upwind edge, so its seven upwind values come
- * from:
+ * j = t - l - DL oy (column block k = j / Zp, z position j % Zp), oy being
+ * its row's offset from the slab's upwind edge, so its seven upwind values
+ * come from:
  *   tv, tev, tnv, tnve   its own previous step                    (registers)
  *   te                   lane l-1's previous step                 (shuffle)
  *                        or, for lane 0, lane 31 of block k-1 through a
  *                        per-warp ring in shared memory (Zp - 31 >= 1 steps old)
  * (the initialisation sweeps start at the block holding x' = lox - 1)
- *   tn, ten              the y-upwind warp's previous step         (shared memory)
+ *   tn, ten              the y-upwind warp's step t - DL           (shared memory)
  *                        or, for the slab's first row, the upwind slab's
  *                        last row, final for this sweep            (global, L2)
- * The skew ramp (31 + TY - 1 steps) is paid once per slab.
+ * Rows lag DL = 4 steps behind their upwind row, so the block synchronises
+ * once per DL steps (the upwind row's values of the previous window are then
+ * visible) instead of every step.  The skew ramp (31 + DL (TY - 1) steps) is
+ * paid once per slab.
  *
  * Slabs publish their progress as (sweep << 20) | steps done every 32 steps
  * and (sweep + 1) << 20 when done (one thread, release store after a block
@@ -43,6 +46,8 @@ using fk3::rmax;
 constexpr int TY = FK_SLAB_Y;        /* rows (warps) per slab */
 constexpr int NT = TY * 32;
 constexpr int CH = 32;               /* progress granularity, steps */
+constexpr int DL = 4;                /* row-to-row lag inside a slab = block barrier interval */
+constexpr int NB = 2 * DL;           /* row exchange buffer depth */
 constexpr int SHIFT = 20;            /* counter = (sweep << SHIFT) | steps */
 
 template <typename R, int S>
@@ -105,7 +110,7 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
     const int K = (nx + 31) / 32;
     /* column blocks wholly before x' = lox - 1 are neither updated nor read */
     const int k0 = (lox - 1) / 32;
-    const int T = (K - k0) * Zp + 31 + (TY - 1);
+    const int T = (K - k0) * Zp + 31 + DL * (TY - 1);
     const int Pu = P - sy;                           /* upwind slab */
     const bool has_up = Pu >= 0 && Pu < nslab;
     /* the upwind slab changes in this sweep when its last logical row does */
@@ -144,18 +149,19 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
         }
     };
 
-    /* the first row's prefetches reach item t + 1 at step t; the upwind
-     * slab's last row works on that item at its step t + 1 + tx + th_up - 1 */
+    /* the first row's prefetches reach item t + 1 - tx at step t; the upwind
+     * slab's last row works on that item at its step t + 1 + DL (th_up - 1) */
     const int *prog_up = prog[0] + (has_up ? Pu : P);
     if (threadIdx.x == 0) {
         s_flag[0] = 1;
-        if (wait_up && !wait_ge1(prog_up, (s << SHIFT) | min(T, CH + TY + 1), P_.spin_limit, P_.error, 3000))
+        if (wait_up && !wait_ge1(prog_up, (s << SHIFT) | min(T, CH + DL * (TY - 1) + 2), P_.spin_limit, P_.error,
+                                 3000))
             s_flag[0] = 0;
     }
     __syncthreads();
     if (!s_flag[0]) return false;
 
-    int kn = k0, zqn = -tx - oy;         /* item of the next step */
+    int kn = k0, zqn = -tx - DL * oy;    /* item of the next step */
     Pre<R, S> cur, nxt;
 #pragma unroll
     for (int i = 0; i < S; ++i) nxt.told[i] = nxt.tn[i] = HUGEV;
@@ -170,12 +176,13 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
     for (int t = 0; t < T; ++t) {
         if (wait_up && t > 0 && t % CH == 0) {
             if (threadIdx.x == 0 &&
-                !wait_ge1(prog_up, (s << SHIFT) | min(T, t + CH + TY + 1), P_.spin_limit, P_.error, 3001))
+                !wait_ge1(prog_up, (s << SHIFT) | min(T, t + CH + DL * (TY - 1) + 2), P_.spin_limit, P_.error,
+                          3001))
                 s_flag[0] = 0;
             __syncthreads();
             if (!s_flag[0]) return false;
         }
-        const int pp = (t + 1) & 1, cp = t & 1;
+        const int pp = (t + NB - DL) % NB, cp = t % NB;   /* read the upwind row's step t - DL */
         R sh_r[S], sh_tn[S];
 #pragma unroll
         for (int i = 0; i < S; ++i) {
@@ -258,7 +265,8 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
             ten_last[i] = ten;
         }
         if (valid && rowupd && xl >= lox) { zu_uu = cur.duu; zu_ud = cur.dud; zu_du = cur.ddu; zu_dd = cur.ddd; }
-        __syncthreads();
+        if ((t + 1) % DL == 0) __syncthreads();   /* the window's row values become visible */
+        else __syncwarp();                        /* lane 31 -> lane 0 ring */
         if (threadIdx.x == 0 && (t + 1) % CH == 0 && t + 1 < T) {
             __threadfence();
 #pragma unroll
@@ -279,8 +287,8 @@ template <typename R, bool INIT, bool RESID, int S>
 __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(fk3tw::Params P, const int *pairs,
                                                                              int zring)
 {
-    __shared__ R xr[2][S][TY][32];
-    __shared__ R xte[2][S][TY][32];
+    __shared__ R xr[NB][S][TY][32];
+    __shared__ R xte[NB][S][TY][32];
     __shared__ long long s_task;
     __shared__ int s_flag[2];
     __shared__ double s_max[S][TY];

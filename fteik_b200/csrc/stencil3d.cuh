@@ -59,56 +59,103 @@ __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
 template <typename R> __device__ __forceinline__ R rmin(R a, R b) { return (b < a) ? b : a; }
 template <typename R> __device__ __forceinline__ R rmax(R a, R b) { return (b > a) ? b : a; }
 
-/* localSolver.F90:384-534, one node; tupd enters as the node's time. */
+/* localSolver.F90:384-534, one node; tupd enters as the node's time.
+ * Evaluated without branches: every candidate is computed and the ones the
+ * reference's conditions admit are selected, so the result is the
+ * reference's (a candidate whose condition fails may be NaN from the root
+ * of a negative number; the selects never take it). */
+template <typename R>
+__device__ __forceinline__ R noinit(const Mesh<R> &c, R tv, R te, R tn, R tev,
+                                    R ten, R tnv, R tnve, R s1, R s2, R s3,
+                                    R s4, R s5, R s6, R s7, R tupd);
+
+/* FP32: the same operators in fewer operations (the FP32 path is held to
+ * the FP64 result within 1e-4, not bit for bit).  With d = te - tv etc. the
+ * plane operator is  t = tev + d (dx2i - dz2i)/B + (2/B) sqrt(s^2 B - C d^2),
+ * B = dz2i + dx2i, C = dz2i dx2i, and the 3D operator's differences are
+ * ta - tb = 1.5 (te - tv + ten - tnv), tb - tc = 1.5 (tv - tn + tev - ten),
+ * t1 / dsum = tb + ((ta - tb) dx2i - (tb - tc) dy2i) / dsum. */
+__device__ __forceinline__ float noinit_f32(const Mesh<float> &c, float tv, float te, float tn, float tev,
+                                            float ten, float tnv, float tnve, float s1, float s2, float s3,
+                                            float s4, float s5, float s6, float s7, float tupd)
+{
+    const float HUGEV = (float)FK_HUGE;
+    float t12min = fminf(fminf(fmaf(c.dz, s1, tv), fmaf(c.dx, s2, te)), fmaf(c.dy, s3, tn));
+    const float temtv = te - tv, tvmtn = tv - tn, temtn = te - tn;
+    /* zx plane: ta - tb = 2 temtv, tb dz2i + ta dx2i = tev B + temtv (dx2i - dz2i) */
+    const float q_zx = fmaf(s4 * s4, c.dz2i_p_dx2i, -c.dz2i_dx2i * (temtv * temtv));
+    const float t_zx = fmaf(2.0f * c.dz2i_p_dx2i_inv, rsqrt_(q_zx),
+                            fmaf(temtv, (c.dx2i - c.dz2i) * c.dz2i_p_dx2i_inv, tev));
+    /* zy plane: ta = tvmtn + tnv, tb = -tvmtn + tnv; ta dz2i + tb dy2i */
+    const float q_zy = fmaf(s5 * s5, c.dz2i_p_dy2i, -c.dz2i_dy2i * (tvmtn * tvmtn));
+    const float t_zy = fmaf(2.0f * c.dz2i_p_dy2i_inv, rsqrt_(q_zy),
+                            fmaf(tvmtn, (c.dz2i - c.dy2i) * c.dz2i_p_dy2i_inv, tnv));
+    /* xy plane: ta = temtn + ten, tb = -temtn + ten; ta dx2i + tb dy2i */
+    const float q_xy = fmaf(s6 * s6, c.dx2i_p_dy2i, -c.dx2i_dy2i * (temtn * temtn));
+    const float t_xy = fmaf(2.0f * c.dx2i_p_dy2i_inv, rsqrt_(q_xy),
+                            fmaf(temtn, (c.dx2i - c.dy2i) * c.dx2i_p_dy2i_inv, ten));
+    if (temtv < c.dz * s4 && -temtv < c.dx * s4) t12min = fminf(t12min, t_zx);
+    if (tvmtn < c.dy * s5 && -tvmtn < c.dz * s5) t12min = fminf(t12min, t_zy);
+    if (temtn < c.dy * s6 && -temtn < c.dx * s6) t12min = fminf(t12min, t_xy);
+    const float tmax = fmaxf(fmaxf(tv, te), tn);
+    const float tab = 1.5f * (temtv + (ten - tnv));
+    const float tbc = 1.5f * (tvmtn + (tev - ten));
+    const float tac = tab + tbc;
+    const float tb = tv + 0.5f * ((tnv - tn) + (tev - te)) - ten + tnve;
+    const float t2 = (s7 * s7) * c.dsum_nine;
+    const float t3 = fmaf(c.dz2dx2, tab * tab, fmaf(c.dz2dy2, tbc * tbc, c.dx2dy2 * (tac * tac)));
+    const float t3c = fmaf(c.dsumi, rsqrt_(t2 - t3), fmaf(c.dsumi, fmaf(tab, c.dx2i, -tbc * c.dy2i), tb));
+    const float t3d = (t12min > tmax && t2 >= t3) ? t3c : HUGEV;
+    return fminf(tupd, fminf(t3d, t12min));
+}
+
 template <typename R>
 __device__ __forceinline__ R noinit(const Mesh<R> &c, R tv, R te, R tn, R tev,
                                     R ten, R tnv, R tnve, R s1, R s2, R s3,
                                     R s4, R s5, R s6, R s7, R tupd)
 {
+    if constexpr (sizeof(R) == 4)
+        return noinit_f32(c, tv, te, tn, tev, ten, tnv, tnve, s1, s2, s3, s4, s5, s6, s7, tupd);
     const R HUGEV = (R)FK_HUGE;
     R t12min = tv + c.dz * s1;
     t12min = rmin(t12min, te + c.dx * s2);
     t12min = rmin(t12min, tn + c.dy * s3);
-    R temtv = te - tv;
-    if (temtv < c.dz * s4 && -temtv < c.dx * s4) {
+    const R temtv = te - tv;
+    const R tvmtn = tv - tn;
+    const R temtn = te - tn;
+    R t_zx, t_zy, t_xy;
+    {
         R ta = tev + temtv, tb = tev - temtv, tab = ta - tb;
-        R t = ((tb * c.dz2i + ta * c.dx2i) +
-               rsqrt_((R)4 * (s4 * s4) * c.dz2i_p_dx2i - c.dz2i_dx2i * (tab * tab))) *
-              c.dz2i_p_dx2i_inv;
-        t12min = rmin(t12min, t);
+        t_zx = ((tb * c.dz2i + ta * c.dx2i) +
+                rsqrt_((R)4 * (s4 * s4) * c.dz2i_p_dx2i - c.dz2i_dx2i * (tab * tab))) *
+               c.dz2i_p_dx2i_inv;
     }
-    R tvmtn = tv - tn;
-    if (tvmtn < c.dy * s5 && -tvmtn < c.dz * s5) {
+    {
         R ta = tvmtn + tnv, tb = -tvmtn + tnv, tab = ta - tb;
-        R t = ((ta * c.dz2i + tb * c.dy2i) +
-               rsqrt_((R)4 * (s5 * s5) * c.dz2i_p_dy2i - c.dz2i_dy2i * (tab * tab))) *
-              c.dz2i_p_dy2i_inv;
-        t12min = rmin(t12min, t);
+        t_zy = ((ta * c.dz2i + tb * c.dy2i) +
+                rsqrt_((R)4 * (s5 * s5) * c.dz2i_p_dy2i - c.dz2i_dy2i * (tab * tab))) *
+               c.dz2i_p_dy2i_inv;
     }
-    R temtn = te - tn;
-    if (temtn < c.dy * s6 && -temtn < c.dx * s6) {
+    {
         R ta = temtn + ten, tb = -temtn + ten, tab = ta - tb;
-        R t = ((ta * c.dx2i + tb * c.dy2i) +
-               rsqrt_((R)4 * (s6 * s6) * c.dx2i_p_dy2i - c.dx2i_dy2i * (tab * tab))) *
-              c.dx2i_p_dy2i_inv;
-        t12min = rmin(t12min, t);
+        t_xy = ((ta * c.dx2i + tb * c.dy2i) +
+                rsqrt_((R)4 * (s6 * s6) * c.dx2i_p_dy2i - c.dx2i_dy2i * (tab * tab))) *
+               c.dx2i_p_dy2i_inv;
     }
-    R t3d = HUGEV;
-    R tmax = rmax(rmax(tv, te), tn);
-    if (t12min > tmax) {
-        R ta = te + (R)0.5 * (-tn + ten - tv + tev) - tnv + tnve;
-        R tb = tv + (R)0.5 * (-tn + tnv - te + tev) - ten + tnve;
-        R tc = tn + (R)0.5 * (-te + ten - tv + tnv) - tev + tnve;
-        R tab = ta - tb, tbc = tb - tc, tac = ta - tc;
-        R t2 = (s7 * s7) * c.dsum_nine;
-        R t3 = c.dz2dx2 * (tab * tab) + c.dz2dy2 * (tbc * tbc) + c.dx2dy2 * (tac * tac);
-        if (t2 >= t3) {
-            R t1 = tb * c.dz2i + ta * c.dx2i + tc * c.dy2i;
-            t3d = (t1 + rsqrt_(t2 - t3)) * c.dsumi;
-        }
-    }
-    t3d = rmin(t3d, t12min);
-    return rmin(tupd, t3d);
+    if (temtv < c.dz * s4 && -temtv < c.dx * s4) t12min = rmin(t12min, t_zx);
+    if (tvmtn < c.dy * s5 && -tvmtn < c.dz * s5) t12min = rmin(t12min, t_zy);
+    if (temtn < c.dy * s6 && -temtn < c.dx * s6) t12min = rmin(t12min, t_xy);
+    const R tmax = rmax(rmax(tv, te), tn);
+    const R ta = te + (R)0.5 * (-tn + ten - tv + tev) - tnv + tnve;
+    const R tb = tv + (R)0.5 * (-tn + tnv - te + tev) - ten + tnve;
+    const R tc = tn + (R)0.5 * (-te + ten - tv + tnv) - tev + tnve;
+    const R tab = ta - tb, tbc = tb - tc, tac = ta - tc;
+    const R t2 = (s7 * s7) * c.dsum_nine;
+    const R t3 = c.dz2dx2 * (tab * tab) + c.dz2dy2 * (tbc * tbc) + c.dx2dy2 * (tac * tac);
+    const R t1 = tb * c.dz2i + ta * c.dx2i + tc * c.dy2i;
+    const R t3c = (t1 + rsqrt_(t2 - t3)) * c.dsumi;
+    const R t3d = (t12min > tmax && t2 >= t3) ? t3c : HUGEV;
+    return rmin(tupd, rmin(t3d, t12min));
 }
 
 /* Source description used by the initialisation stencil. */
