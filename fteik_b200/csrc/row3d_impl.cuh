@@ -233,7 +233,12 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
                         const int iz = (sz > 0) ? il : nz - 1 - il;
                         const double tmin = (double)rmin(rmin(tv, te), tn);
                         const bool lcart = tmin > q.eps_t;
-                        if (lcart || sizeof(R) == 8)
+                        if (lcart && sizeof(R) == 4)
+                            /* away from the source the initialisation stencil is the
+                             * plane-wave one (localSolver.F90:715-732) */
+                            r = fk3::noinit(mesh, tv, te, tn, tev, ten, tnv, tnve, s1, s2, s3, s4, s5, s6, s7,
+                                            told);
+                        else if (lcart || sizeof(R) == 8)
                             r = fk3::init_node<R>(q, mesh, lcart, tv, te, tn, tev, ten, tnv, tnve, told, s1, s2,
                                                   s3, s4, s5, s6, s7, iz + 1, x + 1, y + 1, sz, sx, sy);
                         else /* near-source spherical stencil in FP64 */
