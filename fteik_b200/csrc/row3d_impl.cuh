@@ -23,8 +23,9 @@
  * visible) instead of every step.  The skew ramp (31 + DL (TY - 1) steps) is
  * paid once per slab.
  *
- * Slabs publish their progress as (sweep << 20) | steps done every 32 steps
- * and (sweep + 1) << 20 when done (one thread, release store after a block
+ * Slabs publish their progress as (sweep << 20) | steps done every CH steps
+ * (8 in the initialisation sweeps, 32 in the passes) and (sweep + 1) << 20
+ * when done (one thread, release store after a block
  * barrier).  A slab waits (one thread, acquire loads, bounded) for the
  * upwind slab to be ahead of what it prefetches, and before it starts, for
  * slabs P-1, P, P+1 to be done with the previous sweep (they read this
@@ -45,7 +46,8 @@ using fk3::rmax;
 
 constexpr int TY = FK_SLAB_Y;        /* rows (warps) per slab */
 constexpr int NT = TY * 32;
-constexpr int CH = 32;               /* progress granularity, steps */
+constexpr int CH_INIT = 8, CH_PASS = 32; /* progress granularity, steps: short initialisation
+                                           * tasks want a short lag, long passes few polls */
 constexpr int DL = 4;                /* row-to-row lag inside a slab = block barrier interval */
 constexpr int NB = 2 * DL;           /* row exchange buffer depth */
 constexpr int SHIFT = 20;            /* counter = (sweep << SHIFT) | steps */
@@ -80,6 +82,7 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
                                            R (*xte)[S][TY][32], R *ring, int zring, int *s_flag,
                                            double (&dmax)[S])
 {
+    constexpr int CH = INIT ? CH_INIT : CH_PASS;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
     const int nz = g.nz, nx = g.nx, ny = g.ny, zp = g.zp, zcp = g.zcp;
