@@ -457,10 +457,10 @@ def main():
         peak_src = "measured"
     achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "tile_pass_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "slab_pass_traffic.json")
     if os.path.exists(tp):
         traffic = json.load(open(tp)).get("dram_bytes_per_launch")
-    roofline = {"bound": "hbm", "kernel": "fk3tw::tile_kernel<float, false> (Gauss-Seidel passes)",
+    roofline = {"bound": "hbm", "kernel": "fk3rw::slab_kernel<float, passes, 2 sources per thread>",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": peak_src, "traffic": traffic,
                 "algorithmic_bytes_per_launch": pass_bytes, "launch_ms": pass_ms,
