@@ -136,6 +136,7 @@ _SIGS = {
     "fteik_b200_batch3d_timeSolve": [POINTER(c_float), POINTER(c_float), _PI],
     "fteik_b200_locate_locateEvents": [c_int, _PI, _PI, _PD, _PD, _PI],
     "fteik_b200_locate_setMethod": [c_int, _PI],
+    "fteik_b200_locate_setNorm": [c_int, _PI],
     "fteik_b200_locate_setRescoreCandidates": [c_int, _PI],
     "fteik_b200_locate_debugAccumulators": [c_int, _PF, _PI],
     "fteik_b200_locate_setGeometry": [c_int, c_int, c_int, c_double, c_double, c_double, c_int, _PD, _PD,
@@ -459,6 +460,12 @@ class Locator:
         ierr = c_int(1)
         self.lib.fteik_b200_locate_setMethod(int(method), byref(ierr))
         _check(ierr, "fteik_b200_locate_setMethod")
+
+    def setNorm(self, norm):
+        """2: the reference's L2 misfit; 1: L1 with median origin time."""
+        ierr = c_int(1)
+        self.lib.fteik_b200_locate_setNorm(int(norm), byref(ierr))
+        _check(ierr, "fteik_b200_locate_setNorm")
 
     def setRescoreCandidates(self, ncand):
         ierr = c_int(1)

@@ -181,6 +181,12 @@ int fk_locate_l2_exact(int ngrd, int ldgrd, int ntf, const float *tables,
                        int *out_idx, float *out_t0, float *out_obj,
                        void *scratch, size_t scratch_bytes, cudaStream_t s);
 size_t fk_locate_l2_exact_scratch(int ngrd, int nev);
+/* Exhaustive L1 search: picks of one common weight per event (0 = skipped);
+ * FP32 obs / wts rank, FP64 obs64 / wts64 give out_t0 (median residual) and
+ * out_obj at the optimum; out_idx 0-based; scratch holds nev 64-bit keys. */
+int fk_locate_l1_exact(int ngrd, int ldgrd, int ntf, const float *tables, int nev, const float *obs,
+                       const float *wts, const double *obs64, const double *wts64, int *out_idx,
+                       double *out_t0, double *out_obj, unsigned long long *scratch, cudaStream_t s);
 
 /* Tensor-core L2 search (locate_tc.cu).  Events with every table picked at
  * one common weight (elig[e] = 1) are ranked by a BF16 hi+lo contraction in

@@ -25,6 +25,12 @@ static struct {
     int cap_ev;
     /* tensor-core search (locate_tc.cu) */
     int method;              /* 0: exact FP32 (reference arithmetic), 1: tensor core */
+    int norm;                /* 2 (the reference's misfit) or 1 */
+    unsigned char *l1ok;     /* host [nev]: positive weights all equal */
+    int *l1_idx;             /* device outputs of the L1 search */
+    double *l1_t0, *l1_obj;
+    unsigned long long *l1_best;
+    int l1_cap;
     int rescore;             /* candidates re-scored in FP64 per event */
     bool dirty64, tables_dirty;
     long long table_gen;     /* counts table writes */
@@ -87,7 +93,8 @@ void locate_finalize(void)
     free(SL.tepoch); free(SL.origin); free(SL.have_ot); free(SL.obs); free(SL.wts);
     fk_dfree(SL.tables); fk_dfree(SL.obs_dev); fk_dfree(SL.wts_dev);
     fk_dfree(SL.idx_dev); fk_dfree(SL.t0_dev); fk_dfree(SL.obj_dev); fk_dfree(SL.scratch);
-    free(SL.obs64); free(SL.w64); free(SL.elig);
+    free(SL.obs64); free(SL.w64); free(SL.elig); free(SL.l1ok);
+    fk_dfree(SL.l1_idx); fk_dfree(SL.l1_t0); fk_dfree(SL.l1_obj); fk_dfree(SL.l1_best);
     fk_dfree(SL.obs64_dev); fk_dfree(SL.w64_dev); fk_dfree(SL.elig_dev); fk_dfree(SL.bpack);
     fk_dfree(SL.apack); fk_dfree(SL.cand_v); fk_dfree(SL.cand_i);
     fk_dfree(SL.tc_idx); fk_dfree(SL.tc_t0); fk_dfree(SL.tc_obj); fk_dfree(SL.err_dev);
@@ -147,6 +154,8 @@ void locate_initialize(int nEvents, int ntf, int ngrd, int *ierr)
     SL.obs64 = (double *)calloc((size_t)nEvents * ntf, sizeof(double));
     SL.w64 = (double *)calloc((size_t)nEvents * ntf, sizeof(double));
     SL.elig = (unsigned char *)calloc((size_t)nEvents, 1);
+    SL.l1ok = (unsigned char *)calloc((size_t)nEvents, 1);
+    SL.norm = 2;
     if (!SL.tables || !SL.obs_dev || !SL.wts_dev) { *ierr = 1; return; }
     if (fk_check((int)cudaMemset(SL.tables, 0, sizeof(float) * (size_t)ntf * SL.ldgrd),
                  "locate_initialize")) { *ierr = 1; return; }
@@ -259,6 +268,15 @@ void locate_setObservation64f(int evnmbr, int nttimes, bool lhaveOT, double t0,
     bool el = true;
     for (int k = 0; k < SL.ntf && el; k++) el = w64[k] > 0.0 && w64[k] == w64[0];
     SL.elig[evnmbr - 1] = el ? 1 : 0;
+    /* the L1 misfit takes picks of one common weight */
+    double wref = 0.0;
+    bool l1 = true;
+    for (int k = 0; k < SL.ntf && l1; k++)
+        if (w64[k] > 0.0) {
+            if (wref == 0.0) wref = w64[k];
+            l1 = w64[k] == wref;
+        }
+    SL.l1ok[evnmbr - 1] = (l1 && wref > 0.0) ? 1 : 0;
     SL.dirty = true;
     SL.dirty64 = true;
 }
@@ -460,8 +478,49 @@ void fteik_b200_locate_debugAccumulators(int enable, float *out, int *ierr)
 /* Events [e0, e0+n) with the selected method; t0 excludes tepoch. */
 static int locate_range_pruned(int e0, int n, int *idx, double *t0, double *obj);
 
+/* L1 search of events [e0, e0+n); t0 excludes tepoch. */
+static int locate_range_l1(int e0, int n, int *idx, double *t0, double *obj)
+{
+    for (int i = 0; i < n; i++)
+        if (!SL.l1ok[e0 + i]) {
+            FK_ERR("locate (L1): event %d has picks of different weights", e0 + i + 1);
+            return 1;
+        }
+    if (upload_obs() || upload_obs64()) return 1;
+    if (n > SL.l1_cap) {
+        fk_dfree(SL.l1_idx); fk_dfree(SL.l1_t0); fk_dfree(SL.l1_obj); fk_dfree(SL.l1_best);
+        SL.l1_idx = (int *)fk_dalloc(sizeof(int) * (size_t)n, "locate");
+        SL.l1_t0 = (double *)fk_dalloc(sizeof(double) * (size_t)n, "locate");
+        SL.l1_obj = (double *)fk_dalloc(sizeof(double) * (size_t)n, "locate");
+        SL.l1_best = (unsigned long long *)fk_dalloc(sizeof(unsigned long long) * (size_t)n, "locate");
+        SL.l1_cap = (SL.l1_idx && SL.l1_t0 && SL.l1_obj && SL.l1_best) ? n : 0;
+        if (!SL.l1_cap) return 1;
+    }
+    cudaStream_t s = fk_stream();
+    int e = fk_locate_l1_exact(SL.ngrd, SL.ldgrd, SL.ntf, SL.tables, n, SL.obs_dev + (size_t)e0 * SL.ntf,
+                               SL.wts_dev + (size_t)e0 * SL.ntf, SL.obs64_dev + (size_t)e0 * SL.ntf,
+                               SL.w64_dev + (size_t)e0 * SL.ntf, SL.l1_idx, SL.l1_t0, SL.l1_obj, SL.l1_best, s);
+    if (!e) e = (int)cudaMemcpyAsync(idx, SL.l1_idx, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaMemcpyAsync(t0, SL.l1_t0, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaMemcpyAsync(obj, SL.l1_obj, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    return fk_check(e, "locate (L1)");
+}
+
+void fteik_b200_locate_setNorm(int norm, int *ierr)
+{
+    *ierr = 0;
+    if (norm != 1 && norm != 2) {
+        FK_ERR("fteik_b200_locate_setNorm: norm=%d must be 1 or 2", norm);
+        *ierr = 1;
+        return;
+    }
+    SL.norm = norm;
+}
+
 static int locate_any(int e0, int n, int *idx, double *t0, double *obj)
 {
+    if (SL.norm == 1) return locate_range_l1(e0, n, idx, t0, obj);
     if (SL.method == 1) return locate_range_tc(e0, n, idx, t0, obj);
     if (SL.method == 2) return locate_range_pruned(e0, n, idx, t0, obj);
     float *ft0 = (float *)malloc(sizeof(float) * (size_t)n);

@@ -229,3 +229,166 @@ extern "C" void fteik_b200_locate_l2_noalloc(int ngrd, int ldgrd, int ntf, const
     }
     *ierr = 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* L1 grid search (no counterpart in the reference, which has L2 only).     */
+/*                                                                          */
+/* For the picks of an event (positive weights, all equal to w) and a grid  */
+/* point g the residuals r_i = o_i - T_i(g) give                            */
+/*   t0(g)  = median of r  (any point between the two middle values when   */
+/*            the count is even; the midpoint is reported)                  */
+/*   obj(g) = w sum_i |r_i - t0| = w (sum of the upper half - sum of the    */
+/*            lower half of the sorted residuals).                          */
+/* A thread holds the 64 residuals of one grid point in registers and sorts */
+/* them with a fully unrolled bitonic network (skipped picks sort last as   */
+/* +inf); the half sums use compile-time indices.  The argmin is the        */
+/* first-index minimum (64-bit atomicMin on (bits << 32) | g); t0 and obj   */
+/* at the optimum are recomputed in FP64.                                   */
+/* ------------------------------------------------------------------------ */
+
+namespace {
+
+template <int N>
+__device__ __forceinline__ void bitonic_sort(float (&v)[N])
+{
+#pragma unroll
+    for (int k = 2; k <= N; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const float a = v[i], b = v[l];
+                    const bool up = (i & k) == 0;
+                    v[i] = up ? fminf(a, b) : fmaxf(a, b);
+                    v[l] = up ? fmaxf(a, b) : fminf(a, b);
+                }
+            }
+}
+
+template <int N>
+__global__ void __launch_bounds__(128) l1_exact_kernel(int ngrd, int ldgrd, int ntf, const float *__restrict__ tables,
+                                                       int nev, const float *__restrict__ obs,
+                                                       const float *__restrict__ wts, unsigned long long *__restrict__ best)
+{
+    constexpr int EVB = 16;
+    __shared__ float s_obs[EVB][N];
+    __shared__ float s_w[EVB][N];
+    __shared__ int s_n[EVB];
+    __shared__ float s_wv[EVB];
+    __shared__ unsigned long long s_best[EVB][4];
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    const int e0 = blockIdx.y * EVB;
+    const int nb = min(EVB, nev - e0);
+    for (int t = threadIdx.x; t < EVB * N; t += blockDim.x) {
+        const int e = t / N, i = t % N;
+        const bool ok = e < nb && i < ntf;
+        s_obs[e][i] = ok ? obs[(size_t)(e0 + e) * ntf + i] : 0.0f;
+        s_w[e][i] = ok ? wts[(size_t)(e0 + e) * ntf + i] : 0.0f;
+    }
+    __syncthreads();
+    if (threadIdx.x < EVB) {
+        int n = 0;
+        float wv = 0.0f;
+        for (int i = 0; i < N; ++i)
+            if (s_w[threadIdx.x][i] > 0.0f) { ++n; wv = s_w[threadIdx.x][i]; }
+        s_n[threadIdx.x] = n;
+        s_wv[threadIdx.x] = wv;
+    }
+    float T[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) T[i] = (g < ngrd && i < ntf) ? __ldg(tables + (size_t)i * ldgrd + g) : 0.0f;
+    __syncthreads();
+    const float INF = __int_as_float(0x7f800000);
+    for (int e = 0; e < nb; ++e) {
+        float r[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i) r[i] = s_w[e][i] > 0.0f ? s_obs[e][i] - T[i] : INF;
+        bitonic_sort<N>(r);
+        const int n = s_n[e], h = n / 2;
+        float obj = 0.0f;
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            /* lower half: i < h; upper half: n - h <= i < n (the middle one of
+             * an odd count drops out) */
+            const float c = i < h ? -1.0f : ((i >= n - h && i < n) ? 1.0f : 0.0f);
+            obj = fmaf(c, (i < n) ? r[i] : 0.0f, obj);
+        }
+        obj *= s_wv[e];
+        unsigned long long key = (g < ngrd && n > 0) ? pack_key(obj, g) : ~0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long k2 = __shfl_xor_sync(0xffffffffu, key, o);
+            key = k2 < key ? k2 : key;
+        }
+        if ((threadIdx.x & 31) == 0) s_best[e][threadIdx.x >> 5] = key;
+    }
+    __syncthreads();
+    if (threadIdx.x < nb) {
+        unsigned long long k = s_best[threadIdx.x][0];
+        for (int w2 = 1; w2 < 4; ++w2) k = s_best[threadIdx.x][w2] < k ? s_best[threadIdx.x][w2] : k;
+        atomicMin(best + e0 + threadIdx.x, k);
+    }
+}
+
+/* FP64 median and misfit at the chosen point from the FP64 picks
+ * (insertion sort, one thread per event). */
+__global__ void l1_at_opt_kernel(int ldgrd, int ntf, const float *__restrict__ tables, int nev,
+                                 const double *__restrict__ obs, const double *__restrict__ wts,
+                                 const unsigned long long *__restrict__ best, int *out_idx, double *out_t0,
+                                 double *out_obj)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nev) return;
+    const int g = (int)(best[e] & 0xffffffffu);
+    double r[64];
+    int n = 0;
+    double wv = 0.0;
+    for (int i = 0; i < ntf; ++i) {
+        const double w = wts[(size_t)e * ntf + i];
+        if (w > 0.0) {
+            const double v = obs[(size_t)e * ntf + i] - (double)tables[(size_t)i * ldgrd + g];
+            int j = n++;
+            while (j > 0 && r[j - 1] > v) { r[j] = r[j - 1]; --j; }
+            r[j] = v;
+            wv = w;
+        }
+    }
+    double t0 = 0.0, obj = 0.0;
+    if (n > 0) {
+        t0 = (n % 2) ? r[n / 2] : 0.5 * (r[n / 2 - 1] + r[n / 2]);
+        for (int i = 0; i < n; ++i) obj += fabs(r[i] - t0);
+        obj *= wv;
+    }
+    out_idx[e] = g;
+    out_t0[e] = t0;
+    out_obj[e] = obj;
+}
+
+__global__ void l1_init_kernel(int nev, unsigned long long *best)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < nev) best[e] = ~0ull;
+}
+
+} // namespace
+
+extern "C" int fk_locate_l1_exact(int ngrd, int ldgrd, int ntf, const float *tables, int nev, const float *obs,
+                                  const float *wts, const double *obs64, const double *wts64, int *out_idx,
+                                  double *out_t0, double *out_obj, unsigned long long *scratch, cudaStream_t s)
+{
+    if (nev <= 0) return 0;
+    if (ntf < 1 || ntf > kMaxTf) return (int)cudaErrorInvalidValue;
+    l1_init_kernel<<<(nev + 255) / 256, 256, 0, s>>>(nev, scratch);
+    dim3 grid((ngrd + 127) / 128, (nev + 15) / 16);
+    if (ntf <= 16)
+        l1_exact_kernel<16><<<grid, 128, 0, s>>>(ngrd, ldgrd, ntf, tables, nev, obs, wts, scratch);
+    else if (ntf <= 32)
+        l1_exact_kernel<32><<<grid, 128, 0, s>>>(ngrd, ldgrd, ntf, tables, nev, obs, wts, scratch);
+    else
+        l1_exact_kernel<64><<<grid, 128, 0, s>>>(ngrd, ldgrd, ntf, tables, nev, obs, wts, scratch);
+    l1_at_opt_kernel<<<(nev + 127) / 128, 128, 0, s>>>(ldgrd, ntf, tables, nev, obs64, wts64, scratch, out_idx,
+                                                       out_t0, out_obj);
+    return (int)cudaGetLastError();
+}

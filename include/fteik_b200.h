@@ -330,6 +330,13 @@ void fteik_b200_locate_locateEvents(int n, const int ev[], int optIndx[],
  *      Events whose picks do not cover every table with one common weight
  *      fall back to method 0. */
 void fteik_b200_locate_setMethod(int method, int *ierr);
+/* Misfit norm of every method (no counterpart in the reference, which has
+ * L2 only): 2 (default) = locate.F90:620-744; 1 = L1 with origin-time
+ * removal, obj(g) = w sum_i |o_i - T_i(g) - t0(g)|, t0(g) = the median of the
+ * residuals (midpoint of the two middle values for an even count), for
+ * events whose positive pick weights are all equal to w; searched
+ * exhaustively on the GPU, the optimum's t0 and misfit in FP64. */
+void fteik_b200_locate_setNorm(int norm, int *ierr);
 /* Candidates per event re-scored in FP64 by method 1 (default 8). */
 void fteik_b200_locate_setRescoreCandidates(int ncand, int *ierr);
 /* Diagnostic for method 1: enable = 1 records, at the next search, the first

@@ -1364,3 +1364,50 @@ void orc_locate_l2_best64(int ngrd, int ldgrd, int ntf, const float *tables,
     *objOpt = bo[best];
     free(bo); free(bt); free(bg);
 }
+
+static int cmp_dbl(const void *a, const void *b)
+{
+    double x = *(const double *)a, y = *(const double *)b;
+    return (x > y) - (x < y);
+}
+
+void orc_locate_l1_best64(int ngrd, int ldgrd, int ntf, const float *tables,
+                          const double *obs, const double *wts, int nthreads,
+                          int *idx, double *t0Opt, double *objOpt)
+{
+    double wv = 0.0;
+    for (int i = 0; i < ntf; i++) if (wts[i] > 0.0) wv = wts[i];
+    int nth = nthreads > 0 ? nthreads : 1;
+    double *bo = (double *)malloc(sizeof(double) * (size_t)nth);
+    double *bt = (double *)malloc(sizeof(double) * (size_t)nth);
+    int *bg = (int *)malloc(sizeof(int) * (size_t)nth);
+    for (int t = 0; t < nth; t++) { bo[t] = HUGE_VAL; bt[t] = 0.0; bg[t] = -1; }
+#pragma omp parallel num_threads(nth)
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        double r[256];
+        long long lo = (long long)ngrd * tid / nth, hi = (long long)ngrd * (tid + 1) / nth;
+        for (long long g = lo; g < hi; g++) {
+            int n = 0;
+            for (int i = 0; i < ntf; i++)
+                if (wts[i] > 0.0) r[n++] = obs[i] - (double)tables[(size_t)i * ldgrd + g];
+            if (n == 0) continue;
+            qsort(r, (size_t)n, sizeof(double), cmp_dbl);
+            double t0 = (n % 2) ? r[n / 2] : 0.5 * (r[n / 2 - 1] + r[n / 2]);
+            double o = 0.0;
+            for (int i = 0; i < n; i++) o += fabs(r[i] - t0);
+            o *= wv;
+            if (o < bo[tid]) { bo[tid] = o; bt[tid] = t0; bg[tid] = (int)g; }
+        }
+    }
+    int best = 0;
+    for (int t = 1; t < nth; t++)
+        if (bo[t] < bo[best]) best = t;
+    *idx = bg[best];
+    *t0Opt = bt[best];
+    *objOpt = bo[best];
+    free(bo); free(bt); free(bg);
+}

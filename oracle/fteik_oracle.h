@@ -151,6 +151,13 @@ void orc_locate_l2_best64(int ngrd, int ldgrd, int ntf, const float *tables,
                           const double *obs, const double *wts, int nthreads,
                           int *idx, double *t0Opt, double *objOpt);
 
+/* Exhaustive FP64 L1 search (no reference counterpart): t0 = median of the
+ * residuals of the picks with positive weight (midpoint for an even count),
+ * obj = w sum |r - t0| with w the common weight; first minimum. */
+void orc_locate_l1_best64(int ngrd, int ldgrd, int ntf, const float *tables,
+                          const double *obs, const double *wts, int nthreads,
+                          int *idx, double *t0Opt, double *objOpt);
+
 #ifdef __cplusplus
 }
 #endif

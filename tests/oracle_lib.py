@@ -224,3 +224,18 @@ def locate_l2_best64(tables, obs, wts, nthreads=0):
                              _ptr(wts, c_double), nth, ctypes.byref(oi), ctypes.byref(t0),
                              ctypes.byref(ob))
     return oi.value, t0.value, ob.value
+
+
+def locate_l1_best64(tables, obs, wts, nthreads=0):
+    """Exhaustive FP64 L1 search for one event (median origin time)."""
+    lib = load()
+    tables = np.ascontiguousarray(tables, np.float32)
+    ntf, ngrd = tables.shape
+    obs = np.ascontiguousarray(obs, np.float64)
+    wts = np.ascontiguousarray(wts, np.float64)
+    oi, t0, ob = c_int(), c_double(), c_double()
+    nth = int(nthreads) if nthreads else (os.cpu_count() or 1)
+    lib.orc_locate_l1_best64(ngrd, ngrd, ntf, _ptr(tables, c_float), _ptr(obs, c_double),
+                             _ptr(wts, c_double), nth, ctypes.byref(oi), ctypes.byref(t0),
+                             ctypes.byref(ob))
+    return oi.value, t0.value, ob.value

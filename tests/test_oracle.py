@@ -147,3 +147,22 @@ def test_mlp_oracle_gradient_matches_finite_differences():
         wm[k] -= h
         fd = (M.loss_and_grad(wp, width, depth, x, y)[0] - M.loss_and_grad(wm, width, depth, x, y)[0]) / (2 * h)
         assert abs(fd - g[k]) <= 1e-7 + 1e-5 * abs(g[k])
+
+
+def test_l1_oracle_matches_numpy():
+    """The FP64 L1 search of the oracle (judge of the GPU L1 search) against a
+    direct numpy evaluation on a small grid, with a skipped pick."""
+    rng = np.random.default_rng(3)
+    ntf, ngrd = 9, 500
+    tables = rng.uniform(0.5, 6.0, (ntf, ngrd)).astype(np.float32)
+    obs = tables[:, 123].astype(np.float64) + 7.0 + rng.normal(0, 0.05, ntf)
+    obs -= obs.max()
+    w = np.ones(ntf) * 1.5
+    w[4] = 0.0
+    gi, t0, ob = O.locate_l1_best64(tables, obs, w)
+    used = w > 0
+    r = obs[used][:, None] - tables[used].astype(np.float64)
+    med = np.median(r, axis=0)
+    objs = 1.5 * np.abs(r - med).sum(axis=0)
+    assert gi == int(np.argmin(objs))
+    assert abs(ob - objs[gi]) <= 1e-12 * objs[gi] and abs(t0 - med[gi]) <= 1e-12
