@@ -176,6 +176,163 @@ def cpu_reference(grids, steps, warmup, nthreads, sample_src=24):
         sample_src, g["nx"], g["ny"], g["nz"], steps)
 
 
+def init_updates3d(n, si):
+    """Node updates of the 8 masked initialisation sweeps for a source in
+    cell si (solver3D.F90:493-565 boxes, flipped axes clamped to n-1)."""
+    total = 0
+    for s in range(8):
+        signs = (1 if s < 4 else -1, 1 if s % 2 == 0 else -1, 1 if (s // 2) % 2 == 0 else -1)
+        cnt = 1
+        for sgn, nn, i in zip(signs, n, si):
+            lo, hi = (max(2, i), nn) if sgn > 0 else (1, min(i + 1, nn - 1))
+            cnt *= max(0, hi - lo + 1)
+        total += cnt
+    return total
+
+
+def field_errors(got, ref):
+    """Max / RMS absolute and relative travel-time error against the FP64
+    field (relative to the reference time, nodes within 1 ms of the source
+    excluded from the relative figures)."""
+    got = np.asarray(got, np.float64)
+    d = np.abs(got - ref)
+    m = ref > 1e-3
+    rel = d[m] / ref[m]
+    return {"max_abs_s": float(d.max()), "rms_abs_s": float(np.sqrt(np.mean(d * d))),
+            "max_rel": float(rel.max()), "rms_rel": float(np.sqrt(np.mean(rel * rel)))}
+
+
+def bench_single_2d(fk, reps=20):
+    """2D plain single source: nz x nx = 201 x 201, h = 10 m, FP64, cell
+    velocity v(z) = 3000 + 0.5 z at the cell centre, source at a seeded
+    uniform off-grid point (seed 1), eps = 5.  The reference's 2D
+    convergence test never fires (solver2D.F90:935-945), so 'converged'
+    means: the smallest nsweep whose field no longer changes with one more
+    pass.  Error against the analytic linear-gradient time
+    (analytic.F90:853-890, velocity measured from z = 0)."""
+    nz = nx = 201
+    h = 10.0
+    zc = (np.arange(nz - 1) + 0.5) * h
+    vel = np.ascontiguousarray(np.broadcast_to(3000.0 + 0.5 * zc, (nx - 1, nz - 1))).ravel()
+    rng = np.random.default_rng(1)
+    zs, xs = rng.uniform(0.05, 0.95) * (nz - 1) * h, rng.uniform(0.05, 0.95) * (nx - 1) * h
+    s = fk.fteik2d()
+
+    def solve(nsweep):
+        s.initialize(nx, nz, h, h, nsweep=nsweep, eps=EPS)
+        s.setCellVelocityNatural(vel)
+        s.setSources(xs, zs)
+        s.solveSourceLSM(1)
+        return s.getTravelTimeField()
+
+    prev, nsweep = solve(1), 1
+    while nsweep < 10:
+        cur = solve(nsweep + 1)
+        if np.array_equal(cur, prev):
+            break
+        prev, nsweep = cur, nsweep + 1
+    tt = solve(nsweep)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        s.solveSourceLSM(1)
+        tt = s.getTravelTimeField()
+    dt = (time.perf_counter() - t0) / reps
+    s.free()
+    z = np.arange(nz) * h
+    x = np.arange(nx) * h
+    Z, X = np.meshgrid(z, x)                       # (nx, nz): z fastest when raveled
+    g = 0.5
+    r2 = (Z - zs) ** 2 + (X - xs) ** 2
+    ana = np.arccosh(1.0 + 0.5 * g * g * r2 / ((3000.0 + g * Z) * (3000.0 + g * zs))) / g
+    zsi, xsi = snap1(nz, h, zs), snap1(nx, h, xs)
+    init = sum(len(range(*zr)) * len(range(*xr)) for zr, xr in (
+        ((max(2, zsi), nz + 1), (max(2, xsi), nx + 1)), ((max(2, zsi), nz + 1), (1, min(xsi + 1, nx - 1) + 1)),
+        ((1, min(zsi + 1, nz - 1) + 1), (max(2, xsi), nx + 1)),
+        ((1, min(zsi + 1, nz - 1) + 1), (1, min(xsi + 1, nx - 1) + 1))))
+    upd = init + nsweep * 4 * (nz - 1) * (nx - 1)
+    return {"workload": "2D single source, 201 x 201 nodes, h = 10 m, v(z) = 3000 + 0.5 z, FP64",
+            "source_zx_m": [zs, xs], "nsweep_converged": nsweep,
+            "gpu_ms_per_solve_e2e": dt * 1e3, "node_updates_per_solve": upd,
+            "node_updates_per_s_e2e": upd / dt,
+            "error_vs_analytic": field_errors(tt, ana.ravel()),
+            "_field": tt, "_src": (zs, xs), "_vel": vel, "_n": (nz, nx), "_h": h}
+
+
+def bench_single_3d(fk, torch, steps):
+    """3D plain single source: 128^3 nodes, h = 25 m, four layers (3000 /
+    4000 / 5000 / 6000 m/s, seeded interfaces, >= 5 cells each) times
+    (1 + 0.05 GRF with a 10-cell correlation length, seed 2), source at a
+    seeded interior off-grid point (seed 3), FP32 on the GPU, iterated to
+    convergence (passes until no FP32 node changes, cap 30)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from models import interior_source, layered_grf_cells
+    n, h = (128, 128, 128), 25.0
+    vel = layered_grf_cells(*n, seed=2)
+    src = interior_source(n, (h, h, h), 3)
+    b = fk.Batch3D([(n[0], n[1], n[2], h, h, h)], eps=EPS, convTol=0.0, maxPass=30, precision=4)
+    b.setVelocityModel(1, vel)
+    b.setSources(1, [src[0]], [src[1]], [src[2]])
+    b.solve()
+    stream = torch.cuda.ExternalStream(fk.lib().fteik_b200_stream())
+    for _ in range(3):
+        b.solveAsync()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        b.solveAsync()
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    init_ms, pass_ms = b.kernelTimes()
+    out = np.empty(n[0] * n[1] * n[2], np.float32)
+    t0 = time.perf_counter()
+    b.setVelocityModel(1, vel)
+    b.setSources(1, [src[0]], [src[1]], [src[2]])
+    b.solve()
+    b.fields32(1, out)
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    res, npass = b.solveInfo(1, 1)
+    b.finalize()
+    si = (snap1(n[0], h, src[0]), snap1(n[1], h, src[1]), snap1(n[2], h, src[2]))
+    upd = init_updates3d(n, si) + npass * 8 * (n[0] - 1) * (n[1] - 1) * (n[2] - 1)
+    return {"workload": "3D single source, 128^3 nodes, h = 25 m, layered + 5 % GRF, FP32, "
+                        "converged", "source_zxy_m": list(src), "passes_to_converge": npass,
+            "gpu_ms": ms, "init_kernel_ms": init_ms, "pass_kernel_ms": pass_ms,
+            "gpu_ms_e2e": e2e_ms, "node_updates": upd, "node_updates_per_s": upd / (ms * 1e-3),
+            "_field": out, "_vel": vel, "_src": src, "_n": n, "_h": h}
+
+
+def single_cpu_baselines(c1, c2, nthreads):
+    """The oracle (FP64 restatement of the reference's solvers) on the two
+    single-source workloads, timed on the host cores: its fields are also
+    the FP64 references for the GPU fields' error."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    nz, nx = c1["_n"]
+    h = c1["_h"]
+    si, sa = O.source_snap(False, (nz, nx, 1), (0, 0, 0), (h, h, 1.0), (c1["_src"][0], c1["_src"][1], 0.0))
+    t0 = time.perf_counter()
+    tt2, _ = O.solve2d((nz, nx), (h, h), 1.0 / c1["_vel"], si[:2], sa[:2], EPS, c1["nsweep_converged"])
+    dt2 = time.perf_counter() - t0
+    c1["cpu_baseline"] = {"value": c1["node_updates_per_solve"] / dt2, "unit": "node-updates/s",
+                          "ms_per_solve": dt2 * 1e3, "cores": 1, "kind": "port",
+                          "sample": "the whole 2D solve"}
+    c1["max_abs_diff_vs_fp64_oracle_s"] = float(np.max(np.abs(c1["_field"] - tt2)))
+    n, h = c2["_n"], c2["_h"]
+    si, sa = O.source_snap(True, n, (0, 0, 0), (h, h, h), c2["_src"])
+    t0 = time.perf_counter()
+    tt3, np64 = O.solve3d(n, (h, h, h), (1.0 / c2["_vel"]).ravel(), si, sa, EPS, 1, conv_tol=0.0,
+                          max_pass=30, level_set=True, nthreads=nthreads)
+    dt3 = time.perf_counter() - t0
+    upd64 = init_updates3d(n, si) + np64 * 8 * (n[0] - 1) * (n[1] - 1) * (n[2] - 1)
+    c2["cpu_baseline"] = {"value": upd64 / dt3, "unit": "node-updates/s", "ms_per_solve": dt3 * 1e3,
+                          "passes_to_converge": np64, "cores": nthreads, "kind": "port",
+                          "sample": "the whole FP64 solve to convergence (max |dt| = 0)"}
+    c2["error_vs_fp64_oracle"] = field_errors(c2["_field"], tt3)
+
+
 def run_reference(args, rank, world):
     grids = workload()
     nth = os.cpu_count() or 1
@@ -333,6 +490,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-locate", action="store_true")
+    ap.add_argument("--no-single", action="store_true",
+                    help="skip the single-source 2D (201x201) and 3D (128^3, converged) sections")
     ap.add_argument("--locate-only", action="store_true",
                     help="solve only the 160x160x96 grid once and run the grid-search section")
     ap.add_argument("--locate-events", type=int, default=LOC_NEV)
@@ -487,6 +646,16 @@ def main():
         cpu = {"value": v, "unit": "node-updates/s", "cores": os.cpu_count(), "kind": "port",
                "sample": sample}
 
+    b.finalize()            # the library holds one batch; the single-source section makes its own
+    single = None
+    if rank == 0 and world == 1 and not args.no_single:
+        c1 = bench_single_2d(fk)
+        c2 = bench_single_3d(fk, torch, args.steps)
+        if not args.no_cpu_baseline:
+            single_cpu_baselines(c1, c2, os.cpu_count() or 1)
+        single = {"plain_2d": {k: v for k, v in c1.items() if not k.startswith("_")},
+                  "plain_3d_128": {k: v for k, v in c2.items() if not k.startswith("_")}}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "node-updates/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -499,9 +668,9 @@ def main():
                            "l2": "fields 1.73 GB > L2 (inputs larger than L2)",
                            "parallelism": "replicas (one batch per GPU)" if world > 1 else "1 GPU"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": 5 * args.steps, "clocks": clk.summary(), "locate": locate}
+                "gpu_launches": 5 * args.steps, "clocks": clk.summary(), "locate": locate,
+                "single_source": single}
         print(json.dumps(line), flush=True)
-    b.finalize()
     if dist is not None:
         dist.destroy_process_group()
 
