@@ -24,7 +24,9 @@
  * paid once per slab.
  *
  * Slabs publish their progress as (sweep << 20) | steps done every CH steps
- * (8 in the initialisation sweeps, 32 in the passes) and (sweep + 1) << 20
+ * (8 in the initialisation sweeps; in the passes 8 when a sweep has few
+ * slab tasks for the resident blocks, whose chains of upwind slabs are then
+ * the critical path, else 32, fewer polls) and (sweep + 1) << 20
  * when done (one thread, release store after a block
  * barrier).  A slab waits (one thread, acquire loads, bounded) for the
  * upwind slab to be ahead of what it prefetches, and before it starts, for
@@ -46,8 +48,8 @@ using fk3::rmax;
 
 constexpr int TY = FK_SLAB_Y;        /* rows (warps) per slab */
 constexpr int NT = TY * 32;
-constexpr int CH_INIT = 8, CH_PASS = 32; /* progress granularity, steps: short initialisation
-                                           * tasks want a short lag, long passes few polls */
+constexpr int CH_INIT = 8;           /* progress granularity of the initialisation sweeps, steps */
+constexpr int CH_FEW = 8, CH_MANY = 32; /* passes: few tasks per sweep want a short lag, many few polls */
 constexpr int DL = 4;                /* row-to-row lag inside a slab = block barrier interval */
 constexpr int NB = 2 * DL;           /* row exchange buffer depth */
 constexpr int SHIFT = 20;            /* counter = (sweep << SHIFT) | steps */
@@ -75,14 +77,14 @@ __device__ __forceinline__ bool wait_ge1(const int *p, int need, long long limit
 
 /* One sweep over physical slab P.  Returns false on a wait timeout (the
  * whole block returns false). */
-template <typename R, bool INIT, bool RESID, int S>
+template <typename R, bool INIT, bool RESID, int S, int CHP>
 __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_grid3d_t &g, R *const (&ttp)[S],
                                            const R *__restrict__ slow, const Src &q, int s, int sweep_no,
                                            int P, int nslab, int *const (&prog)[S], R (*xr)[S][TY][32],
                                            R (*xte)[S][TY][32], R *ring, int zring, int *s_flag,
                                            double (&dmax)[S])
 {
-    constexpr int CH = INIT ? CH_INIT : CH_PASS;
+    constexpr int CH = INIT ? CH_INIT : CHP;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
     const int nz = g.nz, nx = g.nx, ny = g.ny, zp = g.zp, zcp = g.zcp;
@@ -291,7 +293,7 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
  * the barriers are shared and the two stencils give each thread two
  * independent dependency chains.  tasks = {pair, j'} with pairs[2 pair + i]
  * the work items (-1: none) when S = 2, {work, j'} when S = 1. */
-template <typename R, bool INIT, bool RESID, int S>
+template <typename R, bool INIT, bool RESID, int S, int CHP>
 __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(fk3tw::Params P, const int *pairs,
                                                                              int zring)
 {
@@ -375,7 +377,7 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
 #pragma unroll
         for (int i = 0; i < S; ++i) dmax[i] = 0.0;
         if (!skip) {
-            if (!slab_sweep<R, INIT, RESID, S>(P, g, ttp, reinterpret_cast<const R *>(g.slow), q, s, sweep_no, Pp,
+            if (!slab_sweep<R, INIT, RESID, S, CHP>(P, g, ttp, reinterpret_cast<const R *>(g.slow), q, s, sweep_no, Pp,
                                                nslab, prog, xr, xte, ring, zring, s_flag, dmax))
                 break;
         }
@@ -424,9 +426,13 @@ inline int launch_slab_kernel(const fk3tw::Params &P, const int *pairs, int zrin
     int dev = 0, nsm = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, slab_kernel<R, INIT, RESID, S>, NT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, slab_kernel<R, INIT, RESID, S, CH_MANY>, NT, smem);
     if (per < 1) per = 1;
-    slab_kernel<R, INIT, RESID, S><<<nsm * per, NT, smem, st>>>(P, pairs, zring);
+    /* fewer than 4 slab tasks per resident block and sweep: the upwind chains bound the time */
+    if (!INIT && P.ntask_sweep < 4 * nsm * per)
+        slab_kernel<R, INIT, RESID, S, CH_FEW><<<nsm * per, NT, smem, st>>>(P, pairs, zring);
+    else
+        slab_kernel<R, INIT, RESID, S, CH_MANY><<<nsm * per, NT, smem, st>>>(P, pairs, zring);
     return (int)cudaGetLastError();
 }
 
