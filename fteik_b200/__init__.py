@@ -324,6 +324,25 @@ class fteik3d:
         _check(ierr, "getTravelTimes64f")
         return out[: self.nrec]
 
+    def getTravelTimeGradient(self):
+        """(ngrd, 3) array of dT/dx, dT/dy, dT/dz of the current field
+        (solver3D.F90:1249-1321), natural node order."""
+        n = self.nx * self.ny * self.nz
+        out = np.zeros(3 * n)
+        ierr = c_int(1)
+        self.lib.fteik_b200_solver3d_getTravelTimeGradient64f(n, out.ctypes.data_as(_PD), byref(ierr))
+        _check(ierr, "getTravelTimeGradient64f")
+        return out.reshape(n, 3)
+
+    def traceRaysToPoints(self, xp, yp, zp):
+        """solver3D.F90:784-823 semantics: returns ierr."""
+        x, px = _d(np.atleast_1d(xp))
+        y, py = _d(np.atleast_1d(yp))
+        z, pz = _d(np.atleast_1d(zp))
+        ierr = c_int(1)
+        self.lib.fteik_solver3d_traceRaysToPoints(x.size, pz, px, py, byref(ierr))
+        return ierr.value
+
     def getSolveInfo(self):
         r, n, ierr = c_double(), c_int(), c_int(1)
         self.lib.fteik_b200_solver3d_getSolveInfo(byref(r), byref(n), byref(ierr))
@@ -394,6 +413,24 @@ class fteik2d:
         self.lib.fteik_solver2d_getTravelTimeField64f(n, order, out.ctypes.data_as(_PD), byref(ierr))
         _check(ierr, "getTravelTimeField64f")
         return out
+
+    def getTravelTimeGradient(self):
+        """(gradx, gradz) of the current field (solver2D.F90:984-1032)."""
+        n = self.nx * self.nz
+        gx, gz = np.zeros(n), np.zeros(n)
+        ierr = c_int(1)
+        self.lib.fteik_b200_solver2d_getTravelTimeGradient64f(n, gx.ctypes.data_as(_PD), gz.ctypes.data_as(_PD),
+                                                              byref(ierr))
+        _check(ierr, "getTravelTimeGradient64f")
+        return gx, gz
+
+    def traceRaysToPoints(self, xp, zp):
+        """solver2D.F90:310-350 semantics: returns ierr."""
+        x, px = _d(np.atleast_1d(xp))
+        z, pz = _d(np.atleast_1d(zp))
+        ierr = c_int(1)
+        self.lib.fteik_solver2d_traceRaysToPoints(x.size, px, pz, byref(ierr))
+        return ierr.value
 
     def getTravelTimes(self):
         out = np.zeros(max(self.nrec * self.nsrc, 1))

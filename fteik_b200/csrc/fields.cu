@@ -131,7 +131,7 @@ __global__ void receivers_kernel(int is3d, int nx, int zp, double dz, double dx,
 }
 
 template <typename R>
-__global__ void receivers_batch_kernel(int nx, int zp, double dz, double dx, double dy,
+__global__ void receivers_batch_kernel(int is3d, int nx, int zp, double dz, double dx, double dy,
                                        void *const *__restrict__ fields, int nfield, int nrec,
                                        const int *__restrict__ ri, const double *__restrict__ rd,
                                        double *__restrict__ ttr)
@@ -141,8 +141,53 @@ __global__ void receivers_batch_kernel(int nx, int zp, double dz, double dx, dou
          e += (size_t)gridDim.x * blockDim.x) {
         const int f = (int)(e / nrec), r = (int)(e % nrec);
         const R *tt = reinterpret_cast<const R *>(fields[f]);
-        ttr[e] = interp_one<R>(1, nx, zp, dz, dx, dy, tt, ri[r], ri[nrec + r], ri[2 * nrec + r],
+        ttr[e] = interp_one<R>(is3d, nx, zp, dz, dx, dy, tt, ri[r], ri[nrec + r], ri[2 * nrec + r],
                                rd[r], rd[nrec + r], rd[2 * nrec + r]);
+    }
+}
+
+/* solver3D.F90:1249-1321: forward differences along each axis, backward on
+ * the axis' last node; g[3 m + 0, 1, 2] = dT/dx, dT/dy, dT/dz at node m
+ * (natural order, z fastest), computed in FP64 from the field's values. */
+template <typename R>
+__global__ void gradient3d_kernel(int nz, int nx, int ny, int zp, double dz, double dx, double dy,
+                                  const R *__restrict__ tt, double *__restrict__ g)
+{
+    const size_t n = (size_t)nz * nx * ny;
+    const size_t sx = zp, sy = (size_t)nx * zp;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int iz = (int)(e % nz);
+        const size_t r = e / nz;
+        const int ix = (int)(r % nx), iy = (int)(r / nx);
+        const size_t b = (size_t)iy * sy + (size_t)ix * sx + iz;
+        const double t = (double)tt[b];
+        double gx = 0.0, gy = 0.0, gz = 0.0;
+        if (nx > 1) gx = (ix < nx - 1) ? ((double)tt[b + sx] - t) / dx : (t - (double)tt[b - sx]) / dx;
+        if (ny > 1) gy = (iy < ny - 1) ? ((double)tt[b + sy] - t) / dy : (t - (double)tt[b - sy]) / dy;
+        if (nz > 1) gz = (iz < nz - 1) ? ((double)tt[b + 1] - t) / dz : (t - (double)tt[b - 1]) / dz;
+        g[3 * e] = gx;
+        g[3 * e + 1] = gy;
+        g[3 * e + 2] = gz;
+    }
+}
+
+/* solver2D.F90:984-1032: backward differences, forward on the axis' first
+ * node; gx, gz at node m = ix nz + iz. */
+__global__ void gradient2d_kernel(int nz, int nx, int zp, double dz, double dx, const double *__restrict__ tt,
+                                  double *__restrict__ gx, double *__restrict__ gz)
+{
+    const size_t n = (size_t)nz * nx;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int iz = (int)(e % nz), ix = (int)(e / nz);
+        const size_t b = (size_t)ix * zp + iz;
+        const double t = tt[b];
+        double vz = 0.0, vx = 0.0;
+        if (nz > 1) vz = (iz == 0) ? (tt[b + 1] - t) / dz : (t - tt[b - 1]) / dz;
+        if (nx > 1) vx = (ix == 0) ? (tt[b + zp] - t) / dx : (t - tt[b - zp]) / dx;
+        gz[e] = vz;
+        gx[e] = vx;
     }
 }
 
@@ -290,21 +335,34 @@ extern "C" int fk_receivers(int precision, int is3d, int nz, int nx, int ny, int
     return (int)cudaGetLastError();
 }
 
+static int receivers_batch(int precision, int is3d, int nx, int zp, double dz, double dx, double dy,
+                           void *const *fields, int nfield, int nrec, const int *ri, const double *rd,
+                           double *ttr, cudaStream_t s)
+{
+    const size_t n = (size_t)nfield * nrec;
+    if (n == 0) return 0;
+    if (precision == 8)
+        receivers_batch_kernel<double><<<nblocks(n), 256, 0, s>>>(is3d, nx, zp, dz, dx, dy, fields,
+                                                                  nfield, nrec, ri, rd, ttr);
+    else
+        receivers_batch_kernel<float><<<nblocks(n), 256, 0, s>>>(is3d, nx, zp, dz, dx, dy, fields,
+                                                                 nfield, nrec, ri, rd, ttr);
+    return (int)cudaGetLastError();
+}
+
 extern "C" int fk_receivers_batch(int precision, int nz, int nx, int ny, int zp, double dz,
                                   double dx, double dy, void *const *fields, int nfield,
                                   int nrec, const int *ri, const double *rd, double *ttr,
                                   cudaStream_t s)
 {
     (void)nz; (void)ny;
-    const size_t n = (size_t)nfield * nrec;
-    if (n == 0) return 0;
-    if (precision == 8)
-        receivers_batch_kernel<double><<<nblocks(n), 256, 0, s>>>(nx, zp, dz, dx, dy, fields,
-                                                                  nfield, nrec, ri, rd, ttr);
-    else
-        receivers_batch_kernel<float><<<nblocks(n), 256, 0, s>>>(nx, zp, dz, dx, dy, fields,
-                                                                 nfield, nrec, ri, rd, ttr);
-    return (int)cudaGetLastError();
+    return receivers_batch(precision, 1, nx, zp, dz, dx, dy, fields, nfield, nrec, ri, rd, ttr, s);
+}
+
+extern "C" int fk_receivers_batch2d(int nx, int zp, double dz, double dx, void *const *fields, int nfield,
+                                    int nrec, const int *ri, const double *rd, double *ttr, cudaStream_t s)
+{
+    return receivers_batch(8, 0, nx, zp, dz, dx, 1.0, fields, nfield, nrec, ri, rd, ttr, s);
 }
 
 extern "C" int fk_analytic_field(int kind, int nz, int nx, int ny, double z0, double x0,
@@ -357,5 +415,28 @@ extern "C" int fk_unpad_f32(const float *src, float *dst, size_t rows, int nz, i
 {
     if (rows == 0) return 0;
     unpad_kernel<<<148 * 8, 256, 0, s>>>(src, dst, rows, nz, zp);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_gradient3d(int precision, int nz, int nx, int ny, int zp, double dz, double dx, double dy,
+                             const void *tt, double *g, cudaStream_t s)
+{
+    const size_t n = (size_t)nz * nx * ny;
+    if (n == 0) return 0;
+    if (precision == 8)
+        gradient3d_kernel<double><<<nblocks(n), 256, 0, s>>>(nz, nx, ny, zp, dz, dx, dy,
+                                                             (const double *)tt, g);
+    else
+        gradient3d_kernel<float><<<nblocks(n), 256, 0, s>>>(nz, nx, ny, zp, dz, dx, dy,
+                                                            (const float *)tt, g);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_gradient2d(int nz, int nx, int zp, double dz, double dx, const double *tt, double *gx,
+                             double *gz, cudaStream_t s)
+{
+    const size_t n = (size_t)nz * nx;
+    if (n == 0) return 0;
+    gradient2d_kernel<<<nblocks(n), 256, 0, s>>>(nz, nx, zp, dz, dx, tt, gx, gz);
     return (int)cudaGetLastError();
 }

@@ -157,6 +157,15 @@ int fk_receivers_batch(int precision, int nz, int nx, int ny, int zp,
                        double dz, double dx, double dy, void *const *fields,
                        int nfield, int nrec, const int *ri, const double *rd,
                        double *ttr, cudaStream_t s);
+/* The same for FP64 2D fields (bilinear, receiver.F90:246-285 in 2D). */
+int fk_receivers_batch2d(int nx, int zp, double dz, double dx, void *const *fields, int nfield,
+                         int nrec, const int *ri, const double *rd, double *ttr, cudaStream_t s);
+/* Finite-difference travel-time gradients (solver3D.F90:1249-1321,
+ * solver2D.F90:984-1032), FP64 out: 3D g[3 m + {x, y, z}], 2D gx[m], gz[m]. */
+int fk_gradient3d(int precision, int nz, int nx, int ny, int zp, double dz, double dx, double dy,
+                  const void *tt, double *g, cudaStream_t s);
+int fk_gradient2d(int nz, int nx, int zp, double dz, double dx, const double *tt, double *gx,
+                  double *gz, cudaStream_t s);
 /* Analytic fields (analytic.F90) in the solver's natural order. */
 int fk_analytic_field(int kind /*0 const, 1 linear*/, int nz, int nx, int ny,
                       double z0, double x0, double y0, double dz, double dx,

@@ -83,3 +83,30 @@ int fk_sync(const char *who)
     }
     return 0;
 }
+
+int fk_check_ray_points(bool is3d, int np, const double *z, const double *x, const double *y)
+{
+    if (np < 1) {
+        FK_ERR("fteik_rays_setRayDestinations: No origins!");
+        return 1;
+    }
+    const double zmax = fk_model.z0 + (double)(fk_model.nz - 1) * fk_model.dz;
+    const double xmax = fk_model.x0 + (double)(fk_model.nx - 1) * fk_model.dx;
+    const double ymax = is3d ? fk_model.y0 + (double)(fk_model.ny - 1) * fk_model.dy : fk_model.y0;
+    int ierr = 0;
+    for (int i = 0; i < np; i++) {
+        if (z[i] < fk_model.z0 || z[i] > zmax) {
+            FK_ERR("fteik_rays_setRayDestinations: zr(%d)=%g must be in range [%g, %g]", i + 1, z[i], fk_model.z0, zmax);
+            ierr = 1;
+        }
+        if (x[i] < fk_model.x0 || x[i] > xmax) {
+            FK_ERR("fteik_rays_setRayDestinations: xr(%d)=%g must be in range [%g, %g]", i + 1, x[i], fk_model.x0, xmax);
+            ierr = 1;
+        }
+        if (is3d && (y[i] < fk_model.y0 || y[i] > ymax)) {
+            FK_ERR("fteik_rays_setRayDestinations: yr(%d)=%g must be in range [%g, %g]", i + 1, y[i], fk_model.y0, ymax);
+            ierr = 1;
+        }
+    }
+    return ierr;
+}

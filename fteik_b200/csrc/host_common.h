@@ -62,6 +62,9 @@ typedef struct {
     double *rd_dev;
 } fk_receiver_t;
 extern fk_receiver_t fk_receiver;
+/* rays.F90:271-347 (setRayDestinations): at least one point, every point
+ * inside the model; messages as the reference's.  Returns ierr. */
+int fk_check_ray_points(bool is3d, int np, const double *z, const double *x, const double *y);
 int fk_receiver_setup(int nrec, const double *z, const double *x,
                       const double *y, int verbose); /* returns ierr */
 int fk_receiver_upload(void);

@@ -19,12 +19,24 @@ static struct {
     fk_grid2d_t *grid_dev;
     fk_work2d_t *work_dev;
     fk_result3d_t *res_dev;
+    /* solveLSM: all sources of a chunk in one launch */
+    int cap;              /* sources per chunk the buffers hold */
+    double *tt_all;       /* device [cap][nx][zp] */
+    fk_work2d_t *work_all;
+    fk_result3d_t *res_all;
+    void **fptr_dev;      /* device [cap] field pointers (receiver gather) */
+    double *rec_all;      /* device [cap][nrec] */
+    int rec_cap;
+    double *gx, *gz;      /* device [ngrd] gradient of the current field */
+    bool have_grad;
 } S2;
 
 void fteik_solver2d_free(void)
 {
     fk_dfree(S2.tt); fk_dfree(S2.export_buf);
     fk_dfree(S2.grid_dev); fk_dfree(S2.work_dev); fk_dfree(S2.res_dev);
+    fk_dfree(S2.tt_all); fk_dfree(S2.work_all); fk_dfree(S2.res_all); fk_dfree(S2.fptr_dev);
+    fk_dfree(S2.rec_all); fk_dfree(S2.gx); fk_dfree(S2.gz);
     free(S2.tt_rec);
     memset(&S2, 0, sizeof(S2));
     S2.src = -1;
@@ -140,6 +152,15 @@ void fteik_solver2d_getNumberOfReceivers(int *nrec, int *ierr)
     fteik_receiver_getNumberOfReceivers(nrec, ierr);
 }
 
+static void set_work(fk_work2d_t *w, int isrc, double *tt)
+{
+    w->grid = 0;
+    w->zsi = fk_source.zsi[isrc - 1]; w->xsi = fk_source.xsi[isrc - 1];
+    w->zsa = fk_source.zsa[isrc - 1]; w->xsa = fk_source.xsa[isrc - 1];
+    w->szero = fk_source_szero(isrc);
+    w->tt = tt;
+}
+
 static int solve_one(int isrc, int fsm, const char *who)
 {
     S2.have_times = false;
@@ -160,11 +181,7 @@ static int solve_one(int isrc, int fsm, const char *who)
     if (!S2.tt || !S2.grid_dev || !S2.work_dev || !S2.res_dev || !slow) return 1;
     fk_grid2d_t g = {nz, nx, zp, FK_PITCH(nz - 1), fk_model.dz, fk_model.dx, slow};
     fk_work2d_t w;
-    w.grid = 0;
-    w.zsi = fk_source.zsi[isrc - 1]; w.xsi = fk_source.xsi[isrc - 1];
-    w.zsa = fk_source.zsa[isrc - 1]; w.xsa = fk_source.xsa[isrc - 1];
-    w.szero = fk_source_szero(isrc);
-    w.tt = S2.tt;
+    set_work(&w, isrc, S2.tt);
     cudaStream_t s = fk_stream();
     fk_result3d_t res;
     int e = (int)cudaMemcpyAsync(S2.grid_dev, &g, sizeof(g), cudaMemcpyHostToDevice, s);
@@ -176,6 +193,7 @@ static int solve_one(int isrc, int fsm, const char *who)
     if (!e) e = (int)cudaStreamSynchronize(s);
     if (fk_check(e, who) || res.status) return 1;
     S2.have_times = true;
+    S2.have_grad = false;
     return 0;
 }
 
@@ -219,20 +237,98 @@ void fteik_solver2d_solveSourceFSM(int isrc, int *ierr)
     *ierr = solve_one(isrc, 1, "fteik_solver2d_solveSourceFSM");
 }
 
+/* All sources of a chunk solved by one launch (one CTA per source, each
+ * with its own field), then the receiver times of the chunk gathered by one
+ * launch.  Each CTA runs the single-source solve, so the fields equal
+ * solveSourceLSM's bit for bit. */
+static int solve_chunks(const char *who)
+{
+    const int nz = fk_model.nz, nx = fk_model.nx, zp = FK_PITCH(nz), nsrc = fk_source.nsrc;
+    const size_t fsz = (size_t)zp * nx;
+    /* chunk: up to 4096 sources and 1 GiB of fields */
+    int cap = nsrc < 4096 ? nsrc : 4096;
+    while (cap > 1 && (size_t)cap * fsz * sizeof(double) > ((size_t)1 << 30)) cap /= 2;
+    if (cap > S2.cap) {
+        fk_dfree(S2.tt_all); fk_dfree(S2.work_all); fk_dfree(S2.res_all); fk_dfree(S2.fptr_dev);
+        S2.tt_all = (double *)fk_dalloc(sizeof(double) * fsz * (size_t)cap, who);
+        S2.work_all = (fk_work2d_t *)fk_dalloc(sizeof(fk_work2d_t) * (size_t)cap, who);
+        S2.res_all = (fk_result3d_t *)fk_dalloc(sizeof(fk_result3d_t) * (size_t)cap, who);
+        S2.fptr_dev = (void **)fk_dalloc(sizeof(void *) * (size_t)cap, who);
+        S2.cap = (S2.tt_all && S2.work_all && S2.res_all && S2.fptr_dev) ? cap : 0;
+        if (!S2.cap) return 1;
+    }
+    const int nrec = (fk_receiver.have && S2.tt_rec) ? fk_receiver.nrec : 0;
+    if (nrec > 0) {
+        if (fk_receiver_upload()) return 1;
+        if ((size_t)cap * nrec > (size_t)S2.rec_cap) {
+            fk_dfree(S2.rec_all);
+            S2.rec_all = (double *)fk_dalloc(sizeof(double) * (size_t)cap * nrec, who);
+            S2.rec_cap = S2.rec_all ? cap * nrec : 0;
+            if (!S2.rec_all) return 1;
+        }
+    }
+    if (!S2.tt) S2.tt = (double *)fk_dalloc(sizeof(double) * fsz, who);
+    if (!S2.grid_dev) S2.grid_dev = (fk_grid2d_t *)fk_dalloc(sizeof(fk_grid2d_t), who);
+    const double *slow = (const double *)fk_model_slow_dev(8);
+    if (!S2.tt || !S2.grid_dev || !slow) return 1;
+    fk_grid2d_t g = {nz, nx, zp, FK_PITCH(nz - 1), fk_model.dz, fk_model.dx, slow};
+    fk_work2d_t *w = (fk_work2d_t *)malloc(sizeof(fk_work2d_t) * (size_t)cap);
+    void **fp = (void **)malloc(sizeof(void *) * (size_t)cap);
+    fk_result3d_t *res = (fk_result3d_t *)malloc(sizeof(fk_result3d_t) * (size_t)cap);
+    cudaStream_t s = fk_stream();
+    int e = (w && fp && res) ? 0 : 1;
+    if (!e) e = (int)cudaMemcpyAsync(S2.grid_dev, &g, sizeof(g), cudaMemcpyHostToDevice, s);
+    for (int c0 = 0; !e && c0 < nsrc; c0 += cap) {
+        const int n = nsrc - c0 < cap ? nsrc - c0 : cap;
+        for (int i = 0; i < n; i++) {
+            set_work(&w[i], c0 + i + 1, S2.tt_all + fsz * (size_t)i);
+            fp[i] = S2.tt_all + fsz * (size_t)i;
+        }
+        e = (int)cudaMemcpyAsync(S2.work_all, w, sizeof(fk_work2d_t) * (size_t)n, cudaMemcpyHostToDevice, s);
+        if (!e) e = (int)cudaMemcpyAsync(S2.fptr_dev, fp, sizeof(void *) * (size_t)n, cudaMemcpyHostToDevice, s);
+        /* solver2D.F90:935-946: the reference's test never stops early */
+        if (!e) e = fk2d_solve(0, S2.grid_dev, S2.work_all, S2.res_all, n, nx, S2.eps, S2.nsweep, -1.0, 0, s);
+        if (!e && nrec > 0)
+            e = fk_receivers_batch2d(nx, zp, fk_model.dz, fk_model.dx, S2.fptr_dev, n, nrec, fk_receiver.ri_dev,
+                                     fk_receiver.rd_dev, S2.rec_all, s);
+        if (!e && nrec > 0)
+            e = (int)cudaMemcpyAsync(S2.tt_rec + (size_t)c0 * nrec, S2.rec_all, sizeof(double) * (size_t)n * nrec,
+                                     cudaMemcpyDeviceToHost, s);
+        if (!e) e = (int)cudaMemcpyAsync(res, S2.res_all, sizeof(fk_result3d_t) * (size_t)n, cudaMemcpyDeviceToHost, s);
+        /* the last source's field stays the current one, as after the reference's loop */
+        if (!e && c0 + n == nsrc)
+            e = (int)cudaMemcpyAsync(S2.tt, S2.tt_all + fsz * (size_t)(n - 1), sizeof(double) * fsz,
+                                     cudaMemcpyDeviceToDevice, s);
+        if (!e) e = (int)cudaStreamSynchronize(s);
+        for (int i = 0; !e && i < n; i++)
+            if (res[i].status) {
+                FK_ERR("fteik_solver2d_solveLSM: Error solving source %d", c0 + i + 1);
+                e = 1;
+            }
+    }
+    free(w);
+    free(fp);
+    free(res);
+    if (fk_check(e, who)) return 1;
+    S2.have_times = true;
+    S2.have_grad = false;
+    S2.src = nsrc;
+    return 0;
+}
+
 void fteik_solver2d_solveLSM(int *ierr)
 {
     /* solver2D.F90:740-773 */
     *ierr = 0;
+    S2.have_times = false;
     if (!fk_model.have_model) { FK_ERR("fteik_solver2d_solveLSM: Model not yet set"); *ierr = 1; return; }
     if (!fk_source.have || fk_source.nsrc < 1) {
         if (S2.verbose > 0) FK_ERR("fteik_solver2d_solveLSM: No sources");
         return;
     }
+    if (!S2.init || fk_dev_ready("fteik_solver2d_solveLSM")) { *ierr = 1; return; }
     alloc_rec();
-    for (int i = 1; i <= fk_source.nsrc; i++) {
-        fteik_solver2d_solveSourceLSM(i, ierr);
-        if (*ierr) { FK_ERR("fteik_solver2d_solveLSM: Error solving source %d", i); return; }
-    }
+    *ierr = solve_chunks("fteik_solver2d_solveLSM");
 }
 
 void fteik_solver2d_getTravelTimeField64f(int ngrd, int order, double tt[], int *ierr)
@@ -297,15 +393,62 @@ void fteik_solver2d_getTravelTimes64f(int ldr, double ttr[], int *ierr)
         memcpy(ttr + (size_t)i * ldr, S2.tt_rec + (size_t)i * nrec, sizeof(double) * (size_t)nrec);
 }
 
+/* solver2D.F90:984-1032 on the device, once per solved field. */
+static int gradient2(const char *who)
+{
+    if (S2.have_grad) return 0;
+    const size_t n = (size_t)fk_model.nz * fk_model.nx;
+    if (!S2.gx) S2.gx = (double *)fk_dalloc(sizeof(double) * n, who);
+    if (!S2.gz) S2.gz = (double *)fk_dalloc(sizeof(double) * n, who);
+    if (!S2.gx || !S2.gz) return 1;
+    int e = fk_gradient2d(fk_model.nz, fk_model.nx, FK_PITCH(fk_model.nz), fk_model.dz, fk_model.dx, S2.tt,
+                          S2.gx, S2.gz, fk_stream());
+    if (fk_check(e, who)) return 1;
+    S2.have_grad = true;
+    return 0;
+}
+
+void fteik_b200_solver2d_getTravelTimeGradient64f(int ngrd, double gradx[], double gradz[], int *ierr)
+{
+    const char *who = "fteik_b200_solver2d_getTravelTimeGradient64f";
+    *ierr = 1;
+    if (!S2.have_times) { FK_ERR("%s: Travel times not yet computed", who); return; }
+    if (ngrd != fk_model.nz * fk_model.nx) { FK_ERR("%s: ngrd=%d must be %d", who, ngrd, fk_model.nz * fk_model.nx); return; }
+    if (gradient2(who)) return;
+    cudaStream_t s = fk_stream();
+    int e = (int)cudaMemcpyAsync(gradx, S2.gx, sizeof(double) * (size_t)ngrd, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaMemcpyAsync(gradz, S2.gz, sizeof(double) * (size_t)ngrd, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    if (fk_check(e, who)) return;
+    *ierr = 0;
+}
+
 void fteik_solver2d_traceRaysToReceivers(int *ierr)
 {
-    FK_ERR("fteik_solver2d_traceRaysToReceivers: ray tracing is not part of this library");
-    *ierr = 1;
+    /* solver2D.F90:283-306 */
+    *ierr = 0;
+    if (!fk_receiver.have || fk_receiver.nrec < 1) {
+        FK_ERR("fteik_solver2d_traceRaysToReceivers: No receivers set");
+        *ierr = 1;
+        return;
+    }
+    fteik_solver2d_traceRaysToPoints(fk_receiver.nrec, fk_receiver.xrec, fk_receiver.zrec, ierr);
+    if (*ierr) { FK_ERR("fteik_solver2d_traceRaysToReceivers: Failed to compute rays"); *ierr = 1; }
 }
 
 void fteik_solver2d_traceRaysToPoints(int np, const double xp[], const double zp[], int *ierr)
 {
-    (void)np; (void)xp; (void)zp;
-    FK_ERR("fteik_solver2d_traceRaysToPoints: ray tracing is not part of this library");
-    *ierr = 1;
+    /* solver2D.F90:310-350: the gradient of the current field and the ray
+     * end points; the ray paths have no C accessor in the reference. */
+    *ierr = 0;
+    if (!S2.have_times) {
+        FK_ERR("fteik_solver2d_traceRaysToPoints: Travel time field not yet computed");
+        *ierr = 1;
+        return;
+    }
+    if (gradient2("fteik_solver2d_traceRaysToPoints")) { *ierr = 1; return; }
+    if (fk_check_ray_points(false, np, zp, xp, NULL)) {
+        FK_ERR("fteik_solver2d_traceRaysToPoints: Failed to set ray origins");
+        *ierr = 1;
+    }
 }

@@ -22,6 +22,8 @@ static struct {
     fk_tileplan_t plan;
     int plan_npass;
     fk_result3d_t last;
+    double *grad;           /* device [3 ngrd] gradient of the current field */
+    bool have_grad;
 } S3 = {.precision = 4};
 
 static void free_buffers(void)
@@ -32,6 +34,8 @@ static void free_buffers(void)
     fk_dfree(S3.work_dev); S3.work_dev = NULL;
     fk_dfree(S3.res_dev); S3.res_dev = NULL;
     fk_dfree(S3.group_dev); S3.group_dev = NULL;
+    fk_dfree(S3.grad); S3.grad = NULL;
+    S3.have_grad = false;
     fk_tileplan_free(&S3.plan);
     S3.plan_npass = 0;
 }
@@ -242,6 +246,7 @@ void fteik_solver3d_solveSourceLSM(int isrc, int *ierr)
         return;
     }
     S3.have_times = true;
+    S3.have_grad = false;
     S3.src = isrc;
 }
 
@@ -335,16 +340,62 @@ const void *fk_solver3d_field(int *precision)
     return S3.have_times ? S3.tt : NULL;
 }
 
+/* solver3D.F90:1249-1321 on the device, once per solved field. */
+static int gradient(const char *who)
+{
+    if (S3.have_grad) return 0;
+    const size_t n = (size_t)fk_model.nz * fk_model.nx * fk_model.ny;
+    if (!S3.grad) S3.grad = (double *)fk_dalloc(sizeof(double) * 3 * n, who);
+    if (!S3.grad) return 1;
+    int e = fk_gradient3d(S3.precision, fk_model.nz, fk_model.nx, fk_model.ny, FK_PITCH(fk_model.nz),
+                          fk_model.dz, fk_model.dx, fk_model.dy, S3.tt, S3.grad, fk_stream());
+    if (fk_check(e, who)) return 1;
+    S3.have_grad = true;
+    return 0;
+}
+
+void fteik_b200_solver3d_getTravelTimeGradient64f(int ngrd, double grad[], int *ierr)
+{
+    const char *who = "fteik_b200_solver3d_getTravelTimeGradient64f";
+    *ierr = 1;
+    if (!S3.have_times) { FK_ERR("%s: Travel times not yet computed", who); return; }
+    if (ngrd != fk_model.ngrd) { FK_ERR("%s: ngrd=%d must be %d", who, ngrd, fk_model.ngrd); return; }
+    if (gradient(who)) return;
+    cudaStream_t s = fk_stream();
+    int e = (int)cudaMemcpyAsync(grad, S3.grad, sizeof(double) * 3 * (size_t)ngrd, cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    if (fk_check(e, who)) return;
+    *ierr = 0;
+}
+
 void fteik_solver3d_traceRaysToReceivers(int *ierr)
 {
-    FK_ERR("fteik_solver3d_traceRaysToReceivers: ray tracing is not part of this library");
-    *ierr = 1;
+    /* solver3D.F90:756-782 */
+    *ierr = 0;
+    if (!fk_receiver.have || fk_receiver.nrec < 1) {
+        FK_ERR("fteik_solver3d_traceRaysToReceivers: No receivers set");
+        *ierr = 1;
+        return;
+    }
+    fteik_solver3d_traceRaysToPoints(fk_receiver.nrec, fk_receiver.zrec, fk_receiver.xrec, fk_receiver.yrec, ierr);
+    if (*ierr) { FK_ERR("fteik_solver3d_traceRaysToReceivers: Failed to compute rays"); *ierr = 1; }
 }
 
 void fteik_solver3d_traceRaysToPoints(int np, const double zp[], const double xp[],
                                       const double yp[], int *ierr)
 {
-    (void)np; (void)zp; (void)xp; (void)yp;
-    FK_ERR("fteik_solver3d_traceRaysToPoints: ray tracing is not part of this library");
-    *ierr = 1;
+    /* solver3D.F90:784-823: the gradient of the current field and the ray
+     * end points; the reference's 3D tracer (rays.F90:442-447) is a stub and
+     * its ray paths have no C accessor, so nothing more is observable. */
+    *ierr = 0;
+    if (!S3.have_times) {
+        FK_ERR("fteik_solver3d_traceRaysToPoints: Travel time field not yet computed");
+        *ierr = 1;
+        return;
+    }
+    if (gradient("fteik_solver3d_traceRaysToPoints")) { *ierr = 1; return; }
+    if (fk_check_ray_points(true, np, zp, xp, yp)) {
+        FK_ERR("fteik_solver3d_traceRaysToPoints: Failed to set ray origins");
+        *ierr = 1;
+    }
 }

@@ -145,11 +145,20 @@ void fteik_solver3d_getTravelTimeFieldCell64f(int ncell, int order,
                                               double tt[], int *ierr);
 /* solver3D.F90:990-1016 */
 void fteik_solver3d_getTravelTimes64f(int nrec, double ttr[], int *ierr);
-/* solver3D.F90:757-823: ray tracing is outside this library (ierr = 1) */
+/* solver3D.F90:756-823: as the reference, computes the travel-time gradient
+ * of the current field and checks the ray end points (ierr = 1 with no
+ * solved field, no points or a point outside the model); the reference's
+ * 3D tracer is a stub (rays.F90:442-447) and its rays have no C accessor. */
 void fteik_solver3d_traceRaysToReceivers(int *ierr);
 void fteik_solver3d_traceRaysToPoints(int np, const double zp[],
                                       const double xp[], const double yp[],
                                       int *ierr);
+/* The travel-time gradient of the current field, solver3D.F90:1249-1321
+ * (forward differences, backward on each axis' last node), in the layout of
+ * the reference's module array tgrad, which C callers cannot reach there:
+ * grad[3 m + 0, 1, 2] = dT/dx, dT/dy, dT/dz at node m (natural order, z
+ * fastest); ngrd = nz nx ny. */
+void fteik_b200_solver3d_getTravelTimeGradient64f(int ngrd, double grad[], int *ierr);
 
 /* ---- 2D solver: solver2D.F90 ---- */
 /* solver2D.F90:124-198 */
@@ -184,9 +193,18 @@ void fteik_solver2d_getTravelTimeFieldCell64f(int ncell, int order,
                                               double tt[], int *ierr);
 /* solver2D.F90:1410-1447: ttr[ldr*nsrc], receiver times of every source */
 void fteik_solver2d_getTravelTimes64f(int ldr, double ttr[], int *ierr);
+/* solver2D.F90:283-350: the travel-time gradient of the current field and a
+ * check of the ray end points, as the reference (its 2D rays have no C
+ * accessor) */
 void fteik_solver2d_traceRaysToReceivers(int *ierr);
 void fteik_solver2d_traceRaysToPoints(int np, const double xp[],
                                       const double zp[], int *ierr);
+/* The gradient of the current 2D field, solver2D.F90:984-1032 (backward
+ * differences, forward on each axis' first node): the reference's module
+ * arrays tgradx, tgradz (read by testing/test2d.F90 through USE), which C
+ * callers cannot reach there; node m = ix nz + iz, ngrd = nz nx. */
+void fteik_b200_solver2d_getTravelTimeGradient64f(int ngrd, double gradx[], double gradz[],
+                                                  int *ierr);
 
 /* ---- analytic solutions: analytic.F90 ---- */
 void fteik_analytic_initialize64f(int nz, int nx, int ny, double z0, double x0,

@@ -1411,3 +1411,82 @@ void orc_locate_l1_best64(int ngrd, int ldgrd, int ntf, const float *tables,
     *objOpt = bo[best];
     free(bo); free(bt); free(bg);
 }
+
+/* ============================================================ gradient == */
+/* solver3D.F90:1249-1321, loop by loop: interior forward differences along
+ * z, x and y, then the last node of each axis backward. */
+void orc_gradient3d(int nz, int nx, int ny, double dz, double dx, double dy,
+                    const double *tt, double *g)
+{
+    const long nzx = (long)nz * nx;
+    const long n = nzx * ny;
+    for (long m = 0; m < 3 * n; m++) g[m] = 0.0;
+    for (int iy = 0; iy < ny; iy++)
+        for (int ix = 0; ix < nx; ix++)
+            for (int iz = 0; iz < nz - 1; iz++) {
+                const long m1 = iy * nzx + (long)ix * nz + iz, m2 = m1 + 1;
+                g[3 * m1 + 2] = (tt[m2] - tt[m1]) / dz;
+            }
+    for (int iy = 0; iy < ny; iy++)
+        for (int ix = 0; ix < nx - 1; ix++)
+            for (int iz = 0; iz < nz; iz++) {
+                const long m1 = iy * nzx + (long)ix * nz + iz, m2 = m1 + nz;
+                g[3 * m1 + 0] = (tt[m2] - tt[m1]) / dx;
+            }
+    for (int iy = 0; iy < ny - 1; iy++)
+        for (int ix = 0; ix < nx; ix++)
+            for (int iz = 0; iz < nz; iz++) {
+                const long m1 = iy * nzx + (long)ix * nz + iz, m2 = m1 + nzx;
+                g[3 * m1 + 1] = (tt[m2] - tt[m1]) / dy;
+            }
+    if (nz > 1)
+        for (int iy = 0; iy < ny; iy++)
+            for (int ix = 0; ix < nx; ix++) {
+                const long m2 = iy * nzx + (long)ix * nz + nz - 1, m1 = m2 - 1;
+                g[3 * m2 + 2] = (tt[m2] - tt[m1]) / dz;
+            }
+    if (nx > 1)
+        for (int iy = 0; iy < ny; iy++)
+            for (int iz = 0; iz < nz; iz++) {
+                const long m2 = iy * nzx + (long)(nx - 1) * nz + iz, m1 = m2 - nz;
+                g[3 * m2 + 0] = (tt[m2] - tt[m1]) / dx;
+            }
+    if (ny > 1)
+        for (int ix = 0; ix < nx; ix++)
+            for (int iz = 0; iz < nz; iz++) {
+                const long m2 = (long)(ny - 1) * nzx + (long)ix * nz + iz, m1 = m2 - nzx;
+                g[3 * m2 + 1] = (tt[m2] - tt[m1]) / dy;
+            }
+}
+
+/* solver2D.F90:984-1032, loop by loop: interior backward differences, then
+ * the first node of each axis forward and the last backward. */
+void orc_gradient2d(int nz, int nx, double dz, double dx, const double *tt,
+                    double *gx, double *gz)
+{
+    for (long m = 0; m < (long)nz * nx; m++) gx[m] = gz[m] = 0.0;
+    for (int ix = 0; ix < nx; ix++)
+        for (int iz = 1; iz < nz - 1; iz++) {
+            const long m2 = (long)ix * nz + iz, m1 = m2 - 1;
+            gz[m2] = (tt[m2] - tt[m1]) / dz;
+        }
+    for (int ix = 1; ix < nx - 1; ix++)
+        for (int iz = 0; iz < nz; iz++) {
+            const long m2 = (long)ix * nz + iz, m1 = m2 - nz;
+            gx[m2] = (tt[m2] - tt[m1]) / dx;
+        }
+    if (nz > 1)
+        for (int ix = 0; ix < nx; ix++) {
+            long m1 = (long)ix * nz, m2 = m1 + 1;
+            gz[m1] = (tt[m2] - tt[m1]) / dz;
+            m1 = (long)ix * nz + nz - 2; m2 = m1 + 1;
+            gz[m2] = (tt[m2] - tt[m1]) / dz;
+        }
+    if (nx > 1)
+        for (int iz = 0; iz < nz; iz++) {
+            long m1 = iz, m2 = (long)nz + iz;
+            gx[m1] = (tt[m2] - tt[m1]) / dx;
+            m1 = (long)(nx - 2) * nz + iz; m2 = (long)(nx - 1) * nz + iz;
+            gx[m2] = (tt[m2] - tt[m1]) / dx;
+        }
+}

@@ -112,6 +112,16 @@ void orc_receiver_interp(int is3d, int nz, int nx, int ny,
 /* -------------------------------------------------------------- analytic -- */
 /* analytic.F90:618-662 (constant) and :456-528,844-890 (linear gradient).
  * Output in the solver's natural order (z fastest). */
+/* ------------------------------------------------------------- gradient -- */
+/* solver3D.F90:1249-1321: g[3 m + 0, 1, 2] = dT/dx, dT/dy, dT/dz at node m
+ * (natural order), forward differences, backward on each axis' last node. */
+void orc_gradient3d(int nz, int nx, int ny, double dz, double dx, double dy,
+                    const double *tt, double *g);
+/* solver2D.F90:984-1032: backward differences, forward on each axis' first
+ * node; gx[m], gz[m] with m = ix nz + iz. */
+void orc_gradient2d(int nz, int nx, double dz, double dx, const double *tt,
+                    double *gx, double *gz);
+
 void orc_analytic_constant(int nz, int nx, int ny, double z0, double x0,
                            double y0, double dz, double dx, double dy,
                            double vconst, double zs, double xs, double ys,

@@ -83,6 +83,12 @@ def load():
     lib.orc_locate_l2_points64.argtypes = [c_int, c_int, c_int, P(c_float), P(c_float),
                                            P(c_float), P(ctypes.c_ubyte), c_int, P(c_int),
                                            P(c_double), P(c_double)]
+    lib.orc_gradient3d.restype = None
+    lib.orc_gradient3d.argtypes = [c_int, c_int, c_int, c_double, c_double, c_double, P(c_double),
+                                   P(c_double)]
+    lib.orc_gradient2d.restype = None
+    lib.orc_gradient2d.argtypes = [c_int, c_int, c_double, c_double, P(c_double), P(c_double),
+                                   P(c_double)]
     _lib = lib
     return lib
 
@@ -239,3 +245,23 @@ def locate_l1_best64(tables, obs, wts, nthreads=0):
                              _ptr(wts, c_double), nth, ctypes.byref(oi), ctypes.byref(t0),
                              ctypes.byref(ob))
     return oi.value, t0.value, ob.value
+
+
+def gradient3d(n, h, tt):
+    """solver3D.F90:1249-1321 -> (ngrd, 3) array of dT/dx, dT/dy, dT/dz."""
+    lib = load()
+    nz, nx, ny = n
+    tt = np.ascontiguousarray(tt, np.float64).ravel()
+    g = np.empty(3 * tt.size, np.float64)
+    lib.orc_gradient3d(nz, nx, ny, *h, _ptr(tt, c_double), _ptr(g, c_double))
+    return g.reshape(-1, 3)
+
+
+def gradient2d(n, h, tt):
+    """solver2D.F90:984-1032 -> (gx, gz)."""
+    lib = load()
+    nz, nx = n
+    tt = np.ascontiguousarray(tt, np.float64).ravel()
+    gx, gz = np.empty(tt.size), np.empty(tt.size)
+    lib.orc_gradient2d(nz, nx, *h, _ptr(tt, c_double), _ptr(gx, c_double), _ptr(gz, c_double))
+    return gx, gz

@@ -70,3 +70,53 @@ def test_2d_linear_gradient_vs_analytic(fk):
     far = ta > 10 * h / 3000.0
     assert np.median(rel[far]) < 0.01
     s.free()
+
+
+def test_2d_solveLSM_batch_equals_source_loop(fk):
+    """solveLSM runs all sources in one launch; each source's receiver times
+    and the field left behind (the last source's) equal solveSourceLSM's."""
+    nz, nx, h = 41, 53, 15.0
+    rng = np.random.default_rng(8)
+    zc = (np.arange(nz - 1) + 0.5) * h
+    vel = (3000.0 + 1.5 * zc)[None, :] * (1.0 + 0.05 * rng.standard_normal((nx - 1, nz - 1)))
+    nsrc = 37
+    zs = rng.uniform(0, (nz - 1) * h, nsrc)
+    xs = rng.uniform(0, (nx - 1) * h, nsrc)
+    zs[0], xs[1] = 0.0, (nx - 1) * h            # surface source, source on the last node
+    zr, xr = rng.uniform(0, (nz - 1) * h, 11), rng.uniform(0, (nx - 1) * h, 11)
+    s = fk.fteik2d()
+    s.initialize(nx, nz, h, h, nsweep=2, eps=5.0)
+    s.setCellVelocityNatural(vel.ravel())
+    s.setSources(xs, zs)
+    s.setReceivers(xr, zr)
+    s.solveLSM()
+    batch = s.getTravelTimes().copy()
+    last = s.getTravelTimeField().copy()
+    for k in range(nsrc):
+        s.solveSourceLSM(k + 1)
+    loop = s.getTravelTimes()
+    assert np.array_equal(batch, loop)
+    assert np.array_equal(last, s.getTravelTimeField())
+    for k in (0, 1, nsrc - 1):
+        si, sa = O.source_snap(False, (nz, nx, 1), (0, 0, 0), (h, h, 1.0), (zs[k], xs[k], 0.0))
+        ref, _ = O.solve2d((nz, nx), (h, h), 1.0 / vel.ravel(), si[:2], sa[:2], 5.0, 2)
+        want, _ = O.receivers(False, (nz, nx, 1), (0, 0, 0), (h, h, 1.0), zr, xr, None, ref)
+        assert np.max(np.abs(batch[k] - want)) <= 1e-12 * np.max(want)
+    s.free()
+
+
+def test_2d_gradient_and_trace_entry_points(fk):
+    """solver2D.F90:984-1032 on the device equals the oracle's restatement
+    applied to the same field, bit for bit; traceRaysToPoints returns what
+    the reference's does (solver2D.F90:310-350)."""
+    nz, nx, h = 31, 29, 10.0
+    vel = linear_vz_cells(nz, nx, 2, h)[0]
+    s = _setup(fk, nz, nx, h, vel, (101.0, 77.0))
+    assert s.traceRaysToPoints([10.0], [10.0]) == 1                   # no field yet
+    s.solveSourceLSM(1)
+    gx, gz = s.getTravelTimeGradient()
+    wx, wz = O.gradient2d((nz, nx), (h, h), s.getTravelTimeField())
+    assert np.array_equal(gx, wx) and np.array_equal(gz, wz)
+    assert s.traceRaysToPoints([0.0, (nx - 1) * h], [(nz - 1) * h, 0.0]) == 0
+    assert s.traceRaysToPoints([1.0], [(nz - 1) * h + 0.5]) == 1       # below the model
+    s.free()

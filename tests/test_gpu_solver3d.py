@@ -217,3 +217,32 @@ def test_config2_converged_accuracy(fk):
     rel = np.abs(tt - ref) / ref.clip(1e-6)
     assert npass < 30 and res == 0.0
     assert np.max(rel) <= TOL32, (np.max(rel), np.sqrt(np.mean(rel ** 2)), npass)
+
+
+@pytest.mark.parametrize("precision", [8, 4])
+def test_gradient_and_trace_entry_points(fk, precision):
+    """solver3D.F90:1249-1321 on the device equals the oracle's restatement
+    applied to the same field, bit for bit; traceRaysTo* return what the
+    reference's do (solver3D.F90:756-823, rays.F90:271-347)."""
+    n, h, vel, src = _case("grf")
+    s = fk.fteik3d()
+    s.initialize(n[1], n[2], n[0], h[1], h[2], h[0], nsweep=2, eps=5.0, precision=precision)
+    s.setCellSlownessNatural(vel)
+    s.setSources(src[1], src[2], src[0])
+    assert s.traceRaysToPoints([10.0], [10.0], [10.0]) == 1          # no field yet
+    s.solveSourceLSM(1)
+    g = s.getTravelTimeGradient()
+    want = O.gradient3d(n, h, s.getTravelTimeField())
+    assert np.array_equal(g, want)
+    ext = [(n[i] - 1) * h[i] for i in range(3)]                       # z, x, y extents
+    assert s.traceRaysToPoints([0.0, ext[1]], [ext[2], 1.0], [ext[0], 0.0]) == 0
+    assert s.traceRaysToPoints([ext[1] + 1.0], [1.0], [1.0]) == 1     # outside in x
+    assert s.traceRaysToPoints([], [], []) == 1                       # no points
+    import ctypes
+    ierr = ctypes.c_int(0)
+    fk.lib().fteik_solver3d_traceRaysToReceivers(ctypes.byref(ierr))
+    assert ierr.value == 1                                            # no receivers
+    s.setReceivers([1.0, 2.0], [3.0, 4.0], [5.0, 6.0])
+    fk.lib().fteik_solver3d_traceRaysToReceivers(ctypes.byref(ierr))
+    assert ierr.value == 0
+    s.free()

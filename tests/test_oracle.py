@@ -166,3 +166,25 @@ def test_l1_oracle_matches_numpy():
     objs = 1.5 * np.abs(r - med).sum(axis=0)
     assert gi == int(np.argmin(objs))
     assert abs(ob - objs[gi]) <= 1e-12 * objs[gi] and abs(t0 - med[gi]) <= 1e-12
+
+
+def test_gradients_match_numpy_restatement():
+    """orc_gradient3d (solver3D.F90:1249-1321: forward differences, backward
+    on the last node) and orc_gradient2d (solver2D.F90:984-1032: backward
+    differences, forward on the first node) against numpy slicing."""
+    rng = np.random.default_rng(0)
+    nz, nx, ny, h = 5, 6, 7, (10.0, 20.0, 30.0)
+    t = rng.random(nz * nx * ny)
+    g = O.gradient3d((nz, nx, ny), h, t)
+    T = t.reshape(ny, nx, nz)
+    gz = np.empty_like(T); gz[:, :, :-1] = (T[:, :, 1:] - T[:, :, :-1]) / h[0]; gz[:, :, -1] = (T[:, :, -1] - T[:, :, -2]) / h[0]
+    gx = np.empty_like(T); gx[:, :-1] = (T[:, 1:] - T[:, :-1]) / h[1]; gx[:, -1] = (T[:, -1] - T[:, -2]) / h[1]
+    gy = np.empty_like(T); gy[:-1] = (T[1:] - T[:-1]) / h[2]; gy[-1] = (T[-1] - T[-2]) / h[2]
+    assert np.array_equal(g[:, 0], gx.ravel()) and np.array_equal(g[:, 1], gy.ravel())
+    assert np.array_equal(g[:, 2], gz.ravel())
+    t2 = rng.random(nz * nx)
+    ax, az = O.gradient2d((nz, nx), (h[0], h[1]), t2)
+    T2 = t2.reshape(nx, nz)
+    wz = np.empty_like(T2); wz[:, 1:] = (T2[:, 1:] - T2[:, :-1]) / h[0]; wz[:, 0] = (T2[:, 1] - T2[:, 0]) / h[0]
+    wx = np.empty_like(T2); wx[1:] = (T2[1:] - T2[:-1]) / h[1]; wx[0] = (T2[1] - T2[0]) / h[1]
+    assert np.array_equal(az, wz.ravel()) and np.array_equal(ax, wx.ravel())
