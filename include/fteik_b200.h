@@ -259,8 +259,11 @@ void locate_setNumberOfEvents(int nEvents, int *ierr);
 void locate_setNumberOfTravelTimeFields(int ntf, int *ierr);
 void locate_setNumberOfGridPointsF(int ngrd, int *ierr);
 
-/* ---- HDF5 archive (h5io.F90): not built into this library; each call
- * returns non-zero so python/fteik3d.py can bind its symbols ---- */
+/* ---- archive (h5io.F90:104-420) without HDF5: "name.h5" is written as the
+ * directory "name.h5.d/" with the reference's groups, each dataset a NumPy
+ * .npy file in the reference's layout (travel times FP32 x fastest, 2D
+ * flipped in z; velocities INT16 per cell; level schedules INT16 per node).
+ * Returns 0, -1 on misuse (as the reference), 1 on an I/O failure. ---- */
 int fteik_h5io_initializeF(const char *fileName);
 int fteik_h5io_finalizeF(void);
 int fteik_h5io_writeLevelSchedulesF(void);

@@ -97,8 +97,8 @@ def test_host_validation(fk):
     L.fteik_source_initialize64f(2, z.ctypes.data_as(PD), x.ctypes.data_as(PD),
                                  y.ctypes.data_as(PD), 0, ctypes.byref(ierr))
     assert ierr.value == 1          # y = 110.5 lies outside [0, 110]
-    assert L.fteik_h5io_initializeF(b"x.h5") != 0
     L.fteik_model_free()
+    assert L.fteik_h5io_initializeF(b"x.h5") == -1     # no model: h5io.F90:110-114
 
 
 def _no_gpu():
@@ -117,3 +117,41 @@ def test_compute_fails_loudly_without_gpu(fk):
     assert ierr.value == 1
     L.locate_initialize(1, 4, 100, ctypes.byref(ierr))
     assert ierr.value == 1
+
+
+def test_archive_levels_and_velocities(fk, tmp_path):
+    """The archive entry points (h5io.F90:104-420) write the reference's
+    datasets as .npy files: INT16 level schedules of the 8 sweeps
+    (graph3d.F90 levels, x fastest) and INT16 velocities per cell."""
+    L = fk.lib()
+    ierr = ctypes.c_int(0)
+    nz, nx, ny = 6, 7, 5
+    L.fteik_model_initializeGeometry(True, nz, nx, ny, 0.0, 0.0, 0.0, 10.0, 20.0, 30.0, ctypes.byref(ierr))
+    assert ierr.value == 0
+    rng = np.random.default_rng(3)
+    vel = rng.uniform(1500.0, 6000.0, (ny - 1) * (nx - 1) * (nz - 1))   # natural order, z fastest
+    L.fteik_model_setVelocityModel64f(vel.size, vel.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                      ctypes.byref(ierr))
+    assert ierr.value == 0
+    assert L.fteik_h5io_initializeF(str(tmp_path / "arch.txt").encode()) == -1   # not .h5/.hdf5
+    assert L.fteik_h5io_initializeF(str(tmp_path / "sub" / "arch.h5").encode()) == 0
+    d = tmp_path / "sub" / "arch.h5.d"
+    assert L.fteik_h5io_writeLevelSchedulesF() == 0
+    iz, iy, ix = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    for s in range(8):
+        pz = nz - 1 - iz if s >= 4 else iz
+        px = nx - 1 - ix if s % 2 else ix
+        py = ny - 1 - iy if (s // 2) % 2 else iy
+        got = np.load(d / "LevelSchedules" / f"Sweep_{s + 1}.npy")
+        assert got.dtype == np.int16 and np.array_equal(got, pz + px + py + 1)
+    assert L.fteik_h5io_writeVelocityModelF(b"model") == 0
+    assert L.fteik_h5io_writeVelocityModelF(b"model") == -1                       # name taken
+    got = np.load(d / "VelocityModels" / "model.npy")
+    want = np.floor(1.0 / (1.0 / vel) + 0.5).astype(np.int16).reshape(ny - 1, nx - 1, nz - 1)
+    assert np.array_equal(got, want.transpose(2, 0, 1))                         # x fastest
+    assert L.fteik_h5io_writeTravelTimesF(b"tt") == -1                            # no times
+    assert L.fteik_h5io_finalizeF() == 0
+    assert L.fteik_h5io_writeVelocityModelF(b"other") == -1                      # closed
+    geo = (d / "Geometry.txt").read_text().split()
+    assert [int(v) for v in geo[:3]] == [nz, nx, ny]
+    L.fteik_model_free()
