@@ -15,9 +15,11 @@
  *                        or, for lane 0, lane 31 of block k-1 through a
  *                        per-warp ring in shared memory (Zp - 31 >= 1 steps old)
  * (the initialisation sweeps start at the block holding x' = lox - 1)
- *   tn, ten              the y-upwind warp's step t - DL           (shared memory)
+ *   tn                   the y-upwind warp's step t - DL           (shared memory)
  *                        or, for the slab's first row, the upwind slab's
  *                        last row, final for this sweep            (global, L2)
+ *   ten                  lane l-1's tn of the previous step        (shuffle)
+ *                        or, for lane 0, lane 31's through the ring
  * Rows lag DL = 4 steps behind their upwind row, so the block synchronises
  * once per DL steps (the upwind row's values of the previous window are then
  * visible) instead of every step.  The skew ramp (31 + DL (TY - 1) steps) is
@@ -81,7 +83,7 @@ template <typename R, bool INIT, bool RESID, int S, int CHP>
 __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_grid3d_t &g, R *const (&ttp)[S],
                                            const R *__restrict__ slow, const Src &q, int s, int sweep_no,
                                            int P, int nslab, int *const (&prog)[S], R (*xr)[S][TY][32],
-                                           R (*xte)[S][TY][32], R *ring, int zring, int *s_flag,
+                                           R *ring, int zring, int *s_flag,
                                            double (&dmax)[S])
 {
     constexpr int CH = INIT ? CH_INIT : CHP;
@@ -218,13 +220,9 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
             const R te = (tx == 0) ? (from_ring ? ring_r[i * zring + zq] : HUGEV) : sh_r[i];
             R tn = HUGEV, ten = HUGEV, result = HUGEV;
             if (valid) {
-                if (oy == 0) {
-                    tn = cur.tn[i];
-                    ten = (tx == 0) ? (from_ring ? ring_tn[i * zring + zq] : HUGEV) : sh_tn[i];
-                } else {
-                    tn = xr[pp][i][wy][tx];
-                    ten = xte[pp][i][wy][tx];
-                }
+                tn = (oy == 0) ? cur.tn[i] : xr[pp][i][wy][tx];
+                /* lane l-1's y-upwind value one step ago is this node's ten */
+                ten = (tx == 0) ? (from_ring ? ring_tn[i * zring + zq] : HUGEV) : sh_tn[i];
                 const R told = cur.told[i];
                 result = told;
                 if (upd && ttp[i]) {
@@ -268,7 +266,6 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
                 ring_tn[i * zring + zq] = tn;
             }
             xr[cp][i][ty][tx] = result;
-            xte[cp][i][ty][tx] = te;
             r_last[i] = result;
             te_last[i] = te;
             tn_last[i] = tn;
@@ -298,7 +295,6 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
                                                                              int zring)
 {
     __shared__ R xr[NB][S][TY][32];
-    __shared__ R xte[NB][S][TY][32];
     __shared__ long long s_task;
     __shared__ int s_flag[2];
     __shared__ double s_max[S][TY];
@@ -378,7 +374,7 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
         for (int i = 0; i < S; ++i) dmax[i] = 0.0;
         if (!skip) {
             if (!slab_sweep<R, INIT, RESID, S, CHP>(P, g, ttp, reinterpret_cast<const R *>(g.slow), q, s, sweep_no, Pp,
-                                               nslab, prog, xr, xte, ring, zring, s_flag, dmax))
+                                               nslab, prog, xr, ring, zring, s_flag, dmax))
                 break;
         }
         __syncthreads();
