@@ -63,16 +63,26 @@ struct Pre {
     int addr;                        /* node offset in the fields */
 };
 
+/* Sleep between polls, doubling from 64 ns to 1 us: a waiting block's polls
+ * take issue slots and L2 requests from the working ones, and a wait ends
+ * at most ~1 us after its condition holds. */
+__device__ __forceinline__ void poll_backoff(unsigned &ns)
+{
+    __nanosleep(ns);
+    ns = ns < 1024u ? 2u * ns : 1024u;
+}
+
 /* Bounded acquire wait by one thread until *p >= need; false on timeout. */
 __device__ __forceinline__ bool wait_ge1(const int *p, int need, long long limit, int *error, int code)
 {
     long long it = 0;
+    unsigned ns = 64;
     while (fk3tw::ld_acquire(p) < need) {
         if (++it > limit) {
             atomicCAS(error, 0, code);
             return false;
         }
-        __nanosleep(64);
+        poll_backoff(ns);
     }
     return true;
 }
@@ -339,13 +349,14 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
             const int i = tid / 3, pq = Pp + tid % 3 - 1;
             if (prog[i] && pq >= 0 && pq < nslab) {
                 long long it = 0;
+                unsigned ns = 64;
                 while (fk3tw::ld_acquire(prog[i] + pq) < (s << SHIFT)) {
                     if (++it > P.spin_limit) {
                         atomicCAS(P.error, 0, 2000 + tid);
                         s_flag[1] = 0;
                         break;
                     }
-                    __nanosleep(64);
+                    poll_backoff(ns);
                 }
             }
         }
