@@ -358,6 +358,19 @@ def single_cpu_baselines(c1, c2, nthreads):
     c2["error_vs_fp64_oracle"] = field_errors(c2["_field"], tt3)
 
 
+def max_over_ranks(x, dist):
+    """The slowest rank's value of a per-rank time (every rank gets it); x
+    itself without a process group.  NCCL reduces on the GPU, gloo on the
+    host."""
+    if dist is None:
+        return x
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference(args, rank, world):
     grids = workload()
     nth = os.cpu_count() or 1
@@ -601,10 +614,7 @@ def main():
         ki.append(a)
         kp.append(c)
     init_ms, pass_ms = float(np.mean(ki)), float(np.mean(kp))
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     value = upd_total * world / (ms * 1e-3)
 
     # ---- end to end through the C ABI with host buffers ----
@@ -636,10 +646,7 @@ def main():
         torch.cuda.synchronize()
         barrier()
         te = (time.perf_counter() - t0) / ke
-        if dist is not None:
-            t = torch.tensor([te], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
+        te = max_over_ranks(te, dist)
         e2e = {"value": upd_total * world / te, "unit": "node-updates/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": te * 1e3}
 
