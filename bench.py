@@ -629,20 +629,26 @@ def main():
         d2h = sum(o.nbytes for o in outs)
 
         def e2e_step():
+            """Models and sources up, solve, tables down: the download is
+            queued on the library's copy stream and overlaps the next step's
+            uploads and solve; every step's copies are inside the timed
+            region (the last one waited for before the clock stops)."""
             for i, g in enumerate(grids, start=1):
                 b.setVelocityModel(i, vels[i - 1])
                 b.setSources(i, g["zs"], g["xs"], g["ys"])
             b.solve()
             for i in range(1, len(grids) + 1):
-                b.fields32(i, outs[i - 1])
+                b.fields32Async(i, outs[i - 1])
 
         e2e_step()
+        b.waitDownloads()
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
-        ke = max(1, min(args.steps, 3))
+        ke = max(1, args.steps)
         for _ in range(ke):
             e2e_step()
+        b.waitDownloads()
         torch.cuda.synchronize()
         barrier()
         te = (time.perf_counter() - t0) / ke

@@ -79,6 +79,9 @@ _SIGS = {
     "fteik_solver3d_getTravelTimeFieldCell64f": [c_int, c_int, _PD, _PI],
     "fteik_solver3d_getTravelTimes64f": [c_int, _PD, _PI],
     "fteik_solver3d_traceRaysToReceivers": [_PI],
+    "fteik_solver3d_traceRaysToPoints": [c_int, _PD, _PD, _PD, _PI],
+    "fteik_solver2d_traceRaysToReceivers": [_PI],
+    "fteik_solver2d_traceRaysToPoints": [c_int, _PD, _PD, _PI],
     # solver2D.F90
     "fteik_solver2d_initialize": [c_int, c_int] + [c_double] * 4 + [c_int, c_double, c_double, c_int, _PI],
     "fteik_solver2d_free": [],
@@ -129,6 +132,10 @@ _SIGS = {
     "fteik_b200_batch3d_solveAsync": [],
     "fteik_b200_batch3d_getTravelTimeField64f": [c_int, c_int, c_int, c_int, _PD, _PI],
     "fteik_b200_batch3d_getTravelTimeFields32f": [c_int, c_longlong, _PF, _PI],
+    "fteik_b200_batch3d_getTravelTimeFields32fAsync": [c_int, c_longlong, _PF, _PI],
+    "fteik_b200_batch3d_waitDownloads": [_PI],
+    "fteik_b200_solver3d_getTravelTimeGradient64f": [c_int, _PD, _PI],
+    "fteik_b200_solver2d_getTravelTimeGradient64f": [c_int, _PD, _PD, _PI],
     "fteik_b200_batch3d_getTravelTimes64f": [c_int, c_int, _PD, _PI],
     "fteik_b200_batch3d_getSolveInfo": [c_int, c_int, _PD, _PI, _PI],
     "fteik_b200_batch3d_exportToLocator": [c_int, c_int, _PI],
@@ -714,6 +721,22 @@ class Batch3D:
         self.lib.fteik_b200_batch3d_getTravelTimeFields32f(igrid, n, out.ctypes.data_as(_PF), byref(ierr))
         _check(ierr, "batch3d_getTravelTimeFields32f")
         return out
+
+    def fields32Async(self, igrid, out):
+        """Queue the download of fields32(igrid) into out (pinned host
+        memory, untouched until waitDownloads)."""
+        nz, nx, ny = self.grids[igrid - 1]
+        n = self.nsrc[igrid - 1] * nz * nx * ny
+        if out.dtype != np.float32 or out.size < n:
+            raise ValueError("out must hold nsrc * ngrd float32 values")
+        ierr = c_int(1)
+        self.lib.fteik_b200_batch3d_getTravelTimeFields32fAsync(igrid, n, out.ctypes.data_as(_PF), byref(ierr))
+        _check(ierr, "batch3d_getTravelTimeFields32fAsync")
+
+    def waitDownloads(self):
+        ierr = c_int(1)
+        self.lib.fteik_b200_batch3d_waitDownloads(byref(ierr))
+        _check(ierr, "batch3d_waitDownloads")
 
     def travelTimes(self, igrid):
         n = self.nsrc[igrid - 1] * self.nrec

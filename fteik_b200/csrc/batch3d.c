@@ -19,7 +19,8 @@
 typedef struct {
     int nz, nx, ny, ngrd, ncell, zp, zcp;
     double dz, dx, dy;
-    double *slow;           /* host FP64 natural */
+    double *vel_dev;        /* device FP64 cell velocities, natural order */
+    double *szero;          /* host [nsrc]: slowness of each source's cell */
     void *slow_dev;         /* device padded, batch precision */
     bool have_model;
     int nsrc;
@@ -30,6 +31,10 @@ typedef struct {
     int *ri_dev;
     double *rd_dev;
     int work0;              /* index of this grid's first work item */
+    float *dl_buf;          /* device dense FP32 tables being downloaded */
+    size_t dl_cap;
+    cudaEvent_t dl_ready, dl_done;  /* unpacked (library stream), copied (copy stream) */
+    bool have_dl_ev;
 } bgrid_t;
 
 static struct {
@@ -56,6 +61,7 @@ static struct {
     size_t stage_cap;
     cudaEvent_t ev[3];      /* in the graph: before init, after init, after passes */
     bool have_ev;
+    cudaStream_t copy_stream; /* asynchronous table downloads */
 } SB;
 
 static void *stage_buf(size_t bytes, const char *who)
@@ -69,9 +75,11 @@ static void *stage_buf(size_t bytes, const char *who)
 
 static void free_grid(bgrid_t *g)
 {
-    free(g->slow); free(g->zsi); free(g->xsi); free(g->ysi);
+    free(g->szero); free(g->zsi); free(g->xsi); free(g->ysi);
     free(g->zsa); free(g->xsa); free(g->ysa);
-    fk_dfree(g->slow_dev); fk_dfree(g->fields); fk_dfree(g->ri_dev); fk_dfree(g->rd_dev);
+    fk_dfree(g->vel_dev); fk_dfree(g->slow_dev); fk_dfree(g->fields); fk_dfree(g->ri_dev); fk_dfree(g->rd_dev);
+    fk_dfree(g->dl_buf);
+    if (g->have_dl_ev) { cudaEventDestroy(g->dl_ready); cudaEventDestroy(g->dl_done); }
     memset(g, 0, sizeof(*g));
 }
 
@@ -84,6 +92,7 @@ static void invalidate(void)
 
 void fteik_b200_batch3d_finalize(void)
 {
+    if (SB.copy_stream) cudaStreamSynchronize(SB.copy_stream);
     invalidate();
     for (int i = 0; i < SB.ngrid; i++) free_grid(&SB.g[i]);
     free(SB.g);
@@ -93,7 +102,9 @@ void fteik_b200_batch3d_finalize(void)
     fk_tileplan_free(&SB.plan);
     if (SB.have_ev) for (int i = 0; i < 3; i++) cudaEventDestroy(SB.ev[i]);
     free(SB.res_host); free(SB.work_order);
+    cudaStream_t cs = SB.copy_stream;   /* kept for the process's next batch */
     memset(&SB, 0, sizeof(SB));
+    SB.copy_stream = cs;
 }
 
 void fteik_b200_batch3d_initialize(int ngrid, const int nz[], const int nx[], const int ny[],
@@ -131,7 +142,6 @@ void fteik_b200_batch3d_initialize(int ngrid, const int nz[], const int nx[], co
         g->ncell = (nz[i] - 1) * (nx[i] - 1) * (ny[i] - 1);
         g->zp = FK_PITCH(nz[i]); g->zcp = FK_PITCH(nz[i] - 1);
         g->dz = dz[i]; g->dx = dx[i]; g->dy = dy[i];
-        g->slow = (double *)calloc((size_t)g->ncell, sizeof(double));
     }
     SB.precision = precision;
     SB.nsweep = nsweep;
@@ -155,19 +165,24 @@ void fteik_b200_batch3d_setVelocityModel64f(int igrid, int ncell, const double v
     bgrid_t *g = grid_of(igrid, who);
     if (!g) return;
     if (ncell != g->ncell) { FK_ERR("%s: ncell=%d, grid has %d cells", who, ncell, g->ncell); return; }
-    for (int i = 0; i < ncell; i++)
-        if (!(vel[i] > 0.0)) { FK_ERR("%s: velocities must be positive", who); return; }
-    for (int i = 0; i < ncell; i++) g->slow[i] = 1.0 / vel[i];
+    /* the velocities go up as given (pinned caller memory: one DMA) and are
+     * checked and inverted on the device */
     const size_t nelem = (size_t)g->zcp * (g->nx - 1) * (g->ny - 1);
     if (!g->slow_dev) g->slow_dev = fk_dalloc(nelem * (size_t)SB.precision, who);
-    double *tmp = (double *)stage_buf(sizeof(double) * (size_t)ncell, who);
-    if (!g->slow_dev || !tmp) return;
+    if (!g->vel_dev) g->vel_dev = (double *)fk_dalloc(sizeof(double) * (size_t)ncell, who);
+    int *bad_dev = (int *)stage_buf(sizeof(int), who);
+    if (!g->slow_dev || !g->vel_dev || !bad_dev) return;
+    g->have_model = false;
     cudaStream_t s = fk_stream();
+    int bad = 0;
     int e = (int)cudaMemsetAsync(g->slow_dev, 0, nelem * (size_t)SB.precision, s);
-    if (!e) e = (int)cudaMemcpyAsync(tmp, g->slow, sizeof(double) * (size_t)ncell, cudaMemcpyHostToDevice, s);
-    if (!e) e = fk_pack_slowness(SB.precision, 1, g->nz, g->nx, g->ny, g->zcp, tmp, g->slow_dev, s);
+    if (!e) e = (int)cudaMemsetAsync(bad_dev, 0, sizeof(int), s);
+    if (!e) e = (int)cudaMemcpyAsync(g->vel_dev, vel, sizeof(double) * (size_t)ncell, cudaMemcpyHostToDevice, s);
+    if (!e) e = fk_pack_velocity(SB.precision, g->nz, g->nx, g->ny, g->zcp, g->vel_dev, g->slow_dev, bad_dev, s);
+    if (!e) e = (int)cudaMemcpyAsync(&bad, bad_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (!e) e = (int)cudaStreamSynchronize(s);
     if (fk_check(e, who)) return;
+    if (bad) { FK_ERR("%s: velocities must be positive", who); return; }
     g->have_model = true;
     SB.solved = false;
     SB.work_dirty = true; /* szero of this grid's sources */
@@ -257,14 +272,45 @@ static void fill_work(fk_work3d_t *wh)
         wh[w].grid = i;
         wh[w].zsi = g->zsi[s]; wh[w].xsi = g->xsi[s]; wh[w].ysi = g->ysi[s];
         wh[w].zsa = g->zsa[s]; wh[w].xsa = g->xsa[s]; wh[w].ysa = g->ysa[s];
-        wh[w].szero = g->slow[((long)(g->ysi[s] - 1) * (g->nx - 1) + (g->xsi[s] - 1)) * (g->nz - 1) +
-                              (g->zsi[s] - 1)];
+        wh[w].szero = g->szero[s];
         wh[w].tt = (char *)g->fields + fbytes * (size_t)s;
     }
 }
 
+/* szero of every source: 1 / v of its cell (source.F90:429-464), the
+ * velocities gathered from the device copy of each grid's model. */
+static int update_szero(const char *who)
+{
+    cudaStream_t s = fk_stream();
+    int e = 0;
+    for (int i = 0; i < SB.ngrid && !e; i++) {
+        bgrid_t *g = &SB.g[i];
+        if (g->nsrc < 1) continue;
+        const int n = g->nsrc;
+        long long *idx = (long long *)malloc(sizeof(long long) * (size_t)n);
+        double *v = (double *)malloc(sizeof(double) * (size_t)n);
+        free(g->szero);
+        g->szero = (double *)malloc(sizeof(double) * (size_t)n);
+        char *dbuf = (char *)stage_buf((sizeof(long long) + sizeof(double)) * (size_t)n, who);
+        if (!idx || !v || !g->szero || !dbuf) { free(idx); free(v); return 1; }
+        for (int k = 0; k < n; k++)
+            idx[k] = ((long long)(g->ysi[k] - 1) * (g->nx - 1) + (g->xsi[k] - 1)) * (g->nz - 1) + (g->zsi[k] - 1);
+        long long *idx_dev = (long long *)dbuf;
+        double *v_dev = (double *)(dbuf + sizeof(long long) * (size_t)n);
+        e = (int)cudaMemcpyAsync(idx_dev, idx, sizeof(long long) * (size_t)n, cudaMemcpyHostToDevice, s);
+        if (!e) e = fk_gather64(g->vel_dev, idx_dev, n, v_dev, s);
+        if (!e) e = (int)cudaMemcpyAsync(v, v_dev, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s);
+        if (!e) e = (int)cudaStreamSynchronize(s);
+        for (int k = 0; !e && k < n; k++) g->szero[k] = 1.0 / v[k];
+        free(idx);
+        free(v);
+    }
+    return fk_check(e, who);
+}
+
 static int upload_work(const char *who)
 {
+    if (update_szero(who)) return 1;
     fk_work3d_t *wh = (fk_work3d_t *)malloc(sizeof(fk_work3d_t) * (size_t)SB.nwork);
     fill_work(wh);
     int e = (int)cudaMemcpy(SB.work_dev, wh, sizeof(fk_work3d_t) * (size_t)SB.nwork, cudaMemcpyHostToDevice);
@@ -286,6 +332,7 @@ static int build_work(const char *who)
         if (g->nz > max_nz) max_nz = g->nz;
     }
     if (nwork == 0) { FK_ERR("%s: no sources", who); return 1; }
+    if (update_szero(who)) return 1;
     fk_dfree(SB.grids_dev); fk_dfree(SB.work_dev); fk_dfree(SB.res_dev);
     free(SB.res_host); free(SB.work_order);
     SB.grids_dev = (fk_grid3d_t *)fk_dalloc(sizeof(fk_grid3d_t) * (size_t)SB.ngrid, who);
@@ -484,6 +531,52 @@ void fteik_b200_batch3d_getTravelTimeFields32f(int igrid, long long nval, float 
     }
     if (!e) e = (int)cudaStreamSynchronize(s);
     *ierr = fk_check(e, who);
+}
+
+void fteik_b200_batch3d_getTravelTimeFields32fAsync(int igrid, long long nval, float tt[], int *ierr)
+{
+    /* The tables unpacked into a per-grid device buffer on the library
+     * stream (after this grid's previous download has left that buffer),
+     * then copied to tt on a copy stream: the copy overlaps whatever the
+     * caller enqueues next, a new solve included, which may overwrite the
+     * fields as soon as the unpacking has run. */
+    const char *who = "fteik_b200_batch3d_getTravelTimeFields32fAsync";
+    *ierr = 1;
+    bgrid_t *g = grid_of(igrid, who);
+    if (!g) return;
+    if (!SB.solved) { FK_ERR("%s: not solved", who); return; }
+    if (SB.precision != 4) { FK_ERR("%s: the batch was solved in FP64", who); return; }
+    if (nval < (long long)g->nsrc * g->ngrd) { FK_ERR("%s: nval too small", who); return; }
+    const size_t bytes = (size_t)g->nsrc * g->ngrd * sizeof(float);
+    int e = 0;
+    if (!SB.copy_stream) e = (int)cudaStreamCreateWithFlags(&SB.copy_stream, cudaStreamNonBlocking);
+    if (!e && !g->have_dl_ev) {
+        e = (int)cudaEventCreateWithFlags(&g->dl_ready, cudaEventDisableTiming);
+        if (!e) e = (int)cudaEventCreateWithFlags(&g->dl_done, cudaEventDisableTiming);
+        g->have_dl_ev = !e;
+    }
+    if (fk_check(e, who)) return;
+    cudaStream_t s = fk_stream();
+    if (g->dl_cap < bytes) {
+        e = (int)cudaStreamSynchronize(SB.copy_stream);   /* the old buffer may still be read */
+        fk_dfree(g->dl_buf);
+        g->dl_buf = (float *)fk_dalloc(bytes, who);
+        g->dl_cap = g->dl_buf ? bytes : 0;
+        if (!g->dl_buf) return;
+    }
+    if (!e) e = (int)cudaStreamWaitEvent(s, g->dl_done, 0);
+    if (!e) e = fk_unpad_f32((const float *)g->fields, g->dl_buf, (size_t)g->nsrc * g->nx * g->ny, g->nz, g->zp, s);
+    if (!e) e = (int)cudaEventRecord(g->dl_ready, s);
+    if (!e) e = (int)cudaStreamWaitEvent(SB.copy_stream, g->dl_ready, 0);
+    if (!e) e = (int)cudaMemcpyAsync(tt, g->dl_buf, bytes, cudaMemcpyDeviceToHost, SB.copy_stream);
+    if (!e) e = (int)cudaEventRecord(g->dl_done, SB.copy_stream);
+    *ierr = fk_check(e, who);
+}
+
+void fteik_b200_batch3d_waitDownloads(int *ierr)
+{
+    *ierr = 0;
+    if (SB.copy_stream) *ierr = fk_check((int)cudaStreamSynchronize(SB.copy_stream), "fteik_b200_batch3d_waitDownloads");
 }
 
 void fteik_b200_batch3d_getTravelTimes64f(int igrid, int nval, double ttr[], int *ierr)

@@ -22,6 +22,30 @@ __global__ void pack_slow_kernel(int nzc, int nxc, int nyc, int zcp,
     }
 }
 
+/* Cell velocities (FP64, natural order) to padded slowness 1/v in the
+ * working precision; *bad = 1 if a velocity is not positive. */
+template <typename R>
+__global__ void pack_vel_kernel(int nzc, int nxc, int nyc, int zcp, const double *__restrict__ vel,
+                                R *__restrict__ out, int *__restrict__ bad)
+{
+    const size_t n = (size_t)nzc * nxc * nyc;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int iz = (int)(e % nzc);
+        const size_t col = e / nzc;
+        const double v = vel[e];
+        if (!(v > 0.0)) *bad = 1;
+        out[col * zcp + iz] = (R)(1.0 / v);
+    }
+}
+
+__global__ void gather64_kernel(const double *__restrict__ v, const long long *__restrict__ idx, int n,
+                                double *__restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = v[idx[i]];
+}
+
 /* order 0: natural, z fastest; 1: x fastest then y then z (XYZ, or XZ in 2D);
  * 2: z fastest, y, then x (ZYX). */
 template <typename R>
@@ -288,6 +312,26 @@ extern "C" int fk_pack_slowness(int precision, int is3d, int nz, int nx, int ny,
     else
         pack_slow_kernel<float><<<nblocks(n), 256, 0, s>>>(nz - 1, nx - 1, nyc, zcp, slow_nat,
                                                           (float *)slow_dev);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_pack_velocity(int precision, int nz, int nx, int ny, int zcp, const double *vel_nat,
+                                void *slow_dev, int *bad_dev, cudaStream_t s)
+{
+    const size_t n = (size_t)(nz - 1) * (nx - 1) * (ny - 1);
+    if (precision == 8)
+        pack_vel_kernel<double><<<nblocks(n), 256, 0, s>>>(nz - 1, nx - 1, ny - 1, zcp, vel_nat,
+                                                          (double *)slow_dev, bad_dev);
+    else
+        pack_vel_kernel<float><<<nblocks(n), 256, 0, s>>>(nz - 1, nx - 1, ny - 1, zcp, vel_nat,
+                                                         (float *)slow_dev, bad_dev);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_gather64(const double *v, const long long *idx, int n, double *out, cudaStream_t s)
+{
+    if (n <= 0) return 0;
+    gather64_kernel<<<(n + 255) / 256, 256, 0, s>>>(v, idx, n, out);
     return (int)cudaGetLastError();
 }
 

@@ -137,6 +137,12 @@ int fk2d_solve(int fsm, const fk_grid2d_t *grids, const fk_work2d_t *work,
  * the reference's natural layout. */
 int fk_pack_slowness(int precision, int is3d, int nz, int nx, int ny, int zcp,
                      const double *slow_nat, void *slow_dev, cudaStream_t s);
+/* 3D cell velocities (device, FP64 natural) -> padded slowness 1/v;
+ * *bad_dev = 1 when a velocity is not positive (bad_dev zeroed by the caller). */
+int fk_pack_velocity(int precision, int nz, int nx, int ny, int zcp, const double *vel_nat,
+                     void *slow_dev, int *bad_dev, cudaStream_t s);
+/* out[i] = v[idx[i]] on the device. */
+int fk_gather64(const double *v, const long long *idx, int n, double *out, cudaStream_t s);
 /* Copy a padded field (precision 4 or 8) to FP64 in the requested ordering:
  * 0 natural (z fastest), 1 XYZ / XZ (x fastest, z slowest), 2 ZYX. */
 int fk_field_to_f64(int precision, int is3d, int nz, int nx, int ny, int zp,

@@ -320,6 +320,15 @@ void fteik_b200_batch3d_getTravelTimeField64f(int igrid, int isrc, int ngrd,
 /* Fields of every source of a grid as FP32, natural order, [nsrc][ngrd]. */
 void fteik_b200_batch3d_getTravelTimeFields32f(int igrid, long long nval,
                                                float tt[], int *ierr);
+/* The same, returning once the copy is queued: the tables are unpacked on
+ * the library stream and copied to tt on a copy stream, so the copy runs
+ * while the caller uploads the next models and solves again.  tt should be
+ * pinned host memory and must stay untouched until
+ * fteik_b200_batch3d_waitDownloads returns. */
+void fteik_b200_batch3d_getTravelTimeFields32fAsync(int igrid, long long nval,
+                                                    float tt[], int *ierr);
+/* Wait for every queued table download. */
+void fteik_b200_batch3d_waitDownloads(int *ierr);
 /* Receiver times of every source of a grid: ttr[isrc*nrec + irec]. */
 void fteik_b200_batch3d_getTravelTimes64f(int igrid, int nval, double ttr[],
                                           int *ierr);
