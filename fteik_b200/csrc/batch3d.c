@@ -127,8 +127,8 @@ void fteik_b200_batch3d_initialize(int ngrid, const int nz[], const int nx[], co
             *ierr = 1;
             return;
         }
-        if (nx[i] > 1024) {
-            FK_ERR("fteik_b200_batch3d_initialize: grid %d has nx=%d > 1024", i + 1, nx[i]);
+        if (fk_schedule_walker() && nx[i] > 1024) {
+            FK_ERR("fteik_b200_batch3d_initialize: grid %d has nx=%d > 1024, the walker's limit", i + 1, nx[i]);
             *ierr = 1;
             return;
         }

@@ -433,6 +433,14 @@ inline int launch_slab_kernel(const fk3tw::Params &P, const int *pairs, int zrin
     int dev = 0, nsm = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (smem > 48 * 1024) { /* deep grids: the per-warp rings need the opt-in shared memory */
+        cudaError_t ea = cudaFuncSetAttribute(slab_kernel<R, INIT, RESID, S, CH_MANY>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (ea == cudaSuccess && !INIT)
+            ea = cudaFuncSetAttribute(slab_kernel<R, INIT, RESID, S, CH_FEW>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (ea != cudaSuccess) return (int)ea;
+    }
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, slab_kernel<R, INIT, RESID, S, CH_MANY>, NT, smem);
     if (per < 1) per = 1;
     /* fewer than 4 slab tasks per resident block and sweep: the upwind chains bound the time */
@@ -457,7 +465,6 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
     const long long steps = (long long)((pl->max_nx + 31) / 32) * zring + 31 + TY;
     if (steps >= (1LL << SHIFT) || 8 + 8 * (long long)npr + 1 >= (1LL << (31 - SHIFT)))
         return (int)cudaErrorInvalidValue;
-    if ((size_t)TY * 4 * zring * sizeof(R) > 48 * 1024) return (int)cudaErrorInvalidValue;
     cudaError_t e = cudaSuccess;
     e = cudaMemsetAsync(pl->done, 0, sizeof(int) * (size_t)pl->ntiles_total, st);
     if (!e) e = cudaMemsetAsync(pl->tickets, 0, 2 * sizeof(unsigned long long), st);

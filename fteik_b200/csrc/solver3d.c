@@ -116,7 +116,7 @@ void fteik_solver3d_initialize(int nz, int nx, int ny, double z0, double x0, dou
     fteik_solver3d_setSphereToCartEpsilon(eps, ierr);
     if (*ierr) { FK_ERR("fteik_solver3d_initialize: Failed to set epsilon"); return; }
     if (fk_dev_ready("fteik_solver3d_initialize")) { *ierr = 1; return; }
-    if (nx > 1024) {
+    if (fk_schedule_walker() && nx > 1024) {
         FK_ERR("fteik_solver3d_initialize: nx=%d exceeds the 1024 columns one CTA walks", nx);
         *ierr = 1;
         return;

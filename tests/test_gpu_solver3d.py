@@ -277,3 +277,28 @@ def test_batched_async_downloads(fk):
             assert np.array_equal(outs[step][ig], refs[step][ig])
     assert not np.array_equal(refs[0][0], refs[1][0])
     b.finalize()
+
+
+@pytest.mark.parametrize("precision", [8, 4])
+@pytest.mark.parametrize("shape", ["deep", "wide"])
+def test_deep_and_wide_grids(fk, shape, precision):
+    """Grids beyond the slab kernel's default shared memory (nz = 520: the
+    per-warp rings of the FP64 passes take 67 KB) and wider than 1024
+    columns, against the oracle."""
+    if shape == "deep":
+        n, h, eps = (520, 5, 6), (10.0, 12.0, 12.0), 5.0
+        src = (2511.3, 21.0, 33.0)
+        vel = layered_grf_cells(*n, seed=13, min_cells=1)
+    else:
+        n, h, eps = (4, 1500, 5), (10.0, 10.0, 10.0), 3.0
+        src = (11.0, 7403.7, 22.0)
+        rng = np.random.default_rng(13)
+        vel = linear_vz_cells(*n, h[0]) * (1.0 + 0.05 * rng.standard_normal((n[2] - 1, n[1] - 1, n[0] - 1)))
+    s = _gpu(fk, n, h, vel, src, precision=precision, eps=eps)
+    tt = s.getTravelTimeField()
+    ref = _oracle(n, h, vel, src, eps=eps)
+    if precision == 8:
+        assert np.max(np.abs(tt - ref)) <= 1e-12 * np.max(ref)
+    else:
+        assert np.max(np.abs(tt - ref) / np.maximum(ref, 1e-6)) <= TOL32
+    s.free()
