@@ -129,7 +129,7 @@ typedef struct {
 
 /* 2D LSM (fsm = 0) or FSM (fsm = 1) solve of every work item in FP64. */
 int fk2d_solve(int fsm, const fk_grid2d_t *grids, const fk_work2d_t *work,
-               fk_result3d_t *results, int nwork, int max_nx, double eps,
+               fk_result3d_t *results, int nwork, int max_nx, int max_nz, double eps,
                int nsweep, double conv_tol, int max_pass, cudaStream_t stream);
 
 /* ---- field utilities --------------------------------------------------- */

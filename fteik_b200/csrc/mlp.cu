@@ -30,7 +30,9 @@ __global__ void __launch_bounds__(NT) gemm_kernel(int M, int N, int K, const flo
     __shared__ float As[TK][TM + 4];
     __shared__ float Bs[TK][TN + 4];
     const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
-    /* split-K: slice blockIdx.z of gridDim.z; partial sums added atomically */
+    /* split-K: slice blockIdx.z of gridDim.z writes its partial tile to the
+     * workspace C + z M N (C is then the workspace, ldc = N); a second kernel
+     * adds the slices in a fixed order, so training is reproducible */
     const int kchunk = ((K + gridDim.z * TK - 1) / (gridDim.z * TK)) * TK;
     const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -84,12 +86,27 @@ __global__ void __launch_bounds__(NT) gemm_kernel(int M, int N, int K, const flo
             if (n >= N) continue;
             float *c = C + (size_t)m * ldc + n;
             if (gridDim.z > 1) {
-                atomicAdd(c, acc[i][j] + ((bias && blockIdx.z == 0) ? bias[n] : 0.0f));
+                C[((size_t)blockIdx.z * M + m) * N + n] = acc[i][j];
             } else {
                 const float v = acc[i][j] + (bias ? bias[n] : 0.0f);
                 *c = accumulate ? *c + v : v;
             }
         }
+    }
+}
+
+/* C[m][n] (+)= sum over the split slices in order + bias[n]. */
+__global__ void splitk_reduce_kernel(int M, int N, int split, const float *__restrict__ ws, float *__restrict__ C,
+                                     int ldc, const float *__restrict__ bias, int accumulate)
+{
+    const size_t n_el = (size_t)M * N;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n_el; e += (size_t)gridDim.x * blockDim.x) {
+        const int m = (int)(e / N), n = (int)(e % N);
+        float v = 0.0f;
+        for (int z = 0; z < split; ++z) v += ws[(size_t)z * n_el + e];
+        if (bias) v += bias[n];
+        float *c = C + (size_t)m * ldc + n;
+        *c = accumulate ? *c + v : v;
     }
 }
 
@@ -263,19 +280,28 @@ extern "C" int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta,
     /* long K with few output tiles (weight gradients): split K over CTAs */
     int split = 1;
     while (tiles * split < 128 && K / (split * 2) >= 256) split *= 2;
-    if (split > 1 && !accumulate) {
-        /* the slices add into C: start from zero */
-        if (ldc == N) {
-            const cudaError_t e = cudaMemsetAsync(C, 0, sizeof(float) * (size_t)M * N, s);
-            if (e != cudaSuccess) return (int)e;
-        } else {
-            const cudaError_t e = cudaMemset2DAsync(C, sizeof(float) * (size_t)ldc, 0, sizeof(float) * (size_t)N,
-                                                    (size_t)M, s);
-            if (e != cudaSuccess) return (int)e;
-        }
-    }
     dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM, split);
-    gemm_kernel<<<grid, NT, 0, s>>>(M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate);
+    if (split == 1) {
+        gemm_kernel<<<grid, NT, 0, s>>>(M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate);
+        return (int)cudaGetLastError();
+    }
+    /* partial tiles into the workspace, then an ordered reduction */
+    static float *ws = nullptr;
+    static size_t ws_cap = 0;
+    const size_t need = (size_t)split * M * N;
+    if (need > ws_cap) {
+        cudaError_t e = cudaStreamSynchronize(s);   /* the old workspace may still be read */
+        if (e == cudaSuccess && ws) e = cudaFree(ws);
+        ws = nullptr;
+        ws_cap = 0;
+        if (e == cudaSuccess) e = cudaMalloc((void **)&ws, sizeof(float) * need);
+        if (e != cudaSuccess) return (int)e;
+        ws_cap = need;
+    }
+    gemm_kernel<<<grid, NT, 0, s>>>(M, N, K, A, lda, ta, B, ldb, tb, ws, N, nullptr, 0);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return (int)e;
+    splitk_reduce_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>(M, N, split, ws, C, ldc, bias, accumulate);
     return (int)cudaGetLastError();
 }
 

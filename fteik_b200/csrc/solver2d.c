@@ -92,11 +92,6 @@ void fteik_solver2d_initialize(int nz, int nx, double z0, double x0, double dz, 
     fteik_solver2d_setSphereToCartEpsilon(eps, ierr);
     if (*ierr) { FK_ERR("fteik_solver2d_initialize64f: Failed to set epsilon"); return; }
     if (fk_dev_ready("fteik_solver2d_initialize")) { *ierr = 1; return; }
-    if (nx > 1024) {
-        FK_ERR("fteik_solver2d_initialize: nx=%d exceeds the 1024 columns one CTA walks", nx);
-        *ierr = 1;
-        return;
-    }
     S2.init = true;
     S2.src = -1;
 }
@@ -187,7 +182,7 @@ static int solve_one(int isrc, int fsm, const char *who)
     int e = (int)cudaMemcpyAsync(S2.grid_dev, &g, sizeof(g), cudaMemcpyHostToDevice, s);
     if (!e) e = (int)cudaMemcpyAsync(S2.work_dev, &w, sizeof(w), cudaMemcpyHostToDevice, s);
     /* solver2D.F90:935-946: the reference's test never stops early */
-    if (!e) e = fk2d_solve(fsm, S2.grid_dev, S2.work_dev, S2.res_dev, 1, nx, S2.eps, S2.nsweep,
+    if (!e) e = fk2d_solve(fsm, S2.grid_dev, S2.work_dev, S2.res_dev, 1, nx, nz, S2.eps, S2.nsweep,
                           -1.0, 0, s);
     if (!e) e = (int)cudaMemcpyAsync(&res, S2.res_dev, sizeof(res), cudaMemcpyDeviceToHost, s);
     if (!e) e = (int)cudaStreamSynchronize(s);
@@ -287,7 +282,7 @@ static int solve_chunks(const char *who)
         e = (int)cudaMemcpyAsync(S2.work_all, w, sizeof(fk_work2d_t) * (size_t)n, cudaMemcpyHostToDevice, s);
         if (!e) e = (int)cudaMemcpyAsync(S2.fptr_dev, fp, sizeof(void *) * (size_t)n, cudaMemcpyHostToDevice, s);
         /* solver2D.F90:935-946: the reference's test never stops early */
-        if (!e) e = fk2d_solve(0, S2.grid_dev, S2.work_all, S2.res_all, n, nx, S2.eps, S2.nsweep, -1.0, 0, s);
+        if (!e) e = fk2d_solve(0, S2.grid_dev, S2.work_all, S2.res_all, n, nx, nz, S2.eps, S2.nsweep, -1.0, 0, s);
         if (!e && nrec > 0)
             e = fk_receivers_batch2d(nx, zp, fk_model.dz, fk_model.dx, S2.fptr_dev, n, nrec, fk_receiver.ri_dev,
                                      fk_receiver.rd_dev, S2.rec_all, s);

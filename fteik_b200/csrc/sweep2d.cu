@@ -3,10 +3,13 @@
  * node updates localSolver.F90:123-289) and its natural-order twin
  * solveSourceFSM (solver2D.F90:1042-1280), in FP64.
  *
- * One CTA owns one (grid, source).  Each lane owns one logical x column and
- * walks z, lane x one step behind lane x-1, so tv is the lane's previous
- * result, te the previous result of lane x-1 (warp shuffle or the two-slot
- * hand-off between warps) and tev the lane's previous te.  Both reference
+ * One CTA owns one (grid, source).  Thread t owns the logical x columns
+ * b NT + t (b = 0, 1, ...: column blocks of NT <= 1024 threads) and walks
+ * their z positions, block after block, thread t one step behind thread t-1,
+ * so tv is the thread's previous result, te the previous result of thread
+ * t-1 (warp shuffle, the two-slot hand-off between warps, or for thread 0 of
+ * block b > 0 the last thread's result of block b-1 through a ring indexed
+ * by z, Zb >= NT steps old) and tev the thread's previous te.  Both reference
  * schedules are topological orders of the same dependency graph, so LSM and
  * FSM give identical fields here (the FSM's initialisation box clamp is
  * applied to both).  Compiled without multiply-add contraction.
@@ -120,7 +123,7 @@ struct Smem2 {
 };
 
 template <bool INIT>
-__device__ double sweep2(Smem2 &sm, const Src2 &q, const fk_grid2d_t &g,
+__device__ double sweep2(Smem2 &sm, double *ring, const Src2 &q, const fk_grid2d_t &g,
                          double *__restrict__ tt, const double *__restrict__ slow,
                          int sweep, int nthreads)
 {
@@ -133,19 +136,25 @@ __device__ double sweep2(Smem2 &sm, const Src2 &q, const fk_grid2d_t &g,
         lox = (sx > 0) ? max(1, q.xsi - 1) : max(1, nx - q.xsi - 1);
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int xl = threadIdx.x;
-    const bool xin = xl < nx;
-    const int ix = (sx > 0) ? xl : nx - 1 - xl;
-    const int cxU = (sx > 0) ? ix - 1 : ix;
-    const int cxD = min(max((sx > 0) ? ix : ix - 1, 0), nx - 2);
-    const int nsteps = nz + nthreads - 1;
+    const int t = threadIdx.x;
+    const int nblk = (nx + nthreads - 1) / nthreads;   /* column blocks */
+    /* steps per block: the ring between blocks needs >= nthreads; one block needs no ring */
+    const int zb = (nblk > 1 && nthreads > nz) ? nthreads : nz;
+    const int nsteps = nblk * zb + nthreads - 1;
     double r_last = FK_HUGE, te_last = FK_HUGE, dmax = 0.0;
     for (int s = 0; s < nsteps; ++s) {
+        const int j = s - t;
+        const int b = j >= 0 ? j / zb : -1;
+        const int il = j - b * zb;
+        const int xl = b * nthreads + t;
         double te = __shfl_up_sync(0xffffffffu, r_last, 1);
         if (lane == 0 && warp > 0) te = sm.xres[(s + 1) & 1][warp - 1];
-        const int il = s - xl;
+        if (t == 0) te = (b > 0 && il < nz) ? ring[il] : FK_HUGE;
         double result = r_last;
-        if (xin && il >= 0 && il < nz) {
+        if (j >= 0 && b < nblk && xl < nx && il < nz) {
+            const int ix = (sx > 0) ? xl : nx - 1 - xl;
+            const int cxU = (sx > 0) ? ix - 1 : ix;
+            const int cxD = min(max((sx > 0) ? ix : ix - 1, 0), nx - 2);
             const int iz = (sz > 0) ? il : nz - 1 - il;
             const size_t idx = (size_t)ix * zp + iz;
             const double told = tt[idx];
@@ -174,6 +183,7 @@ __device__ double sweep2(Smem2 &sm, const Src2 &q, const fk_grid2d_t &g,
         te_last = te;
         r_last = result;
         if (lane == 31) sm.xres[s & 1][warp] = result;
+        if (t == nthreads - 1 && j >= 0 && b < nblk && il < nz) ring[il] = result;
         bar(nthreads);
     }
     return dmax;
@@ -185,9 +195,10 @@ solve2d_kernel(const fk_grid2d_t *__restrict__ grids, const fk_work2d_t *__restr
                double conv_tol, int max_pass)
 {
     __shared__ Smem2 sm;
+    extern __shared__ double ring2[];                 /* [nz]: last thread -> thread 0 of the next block */
     const fk_work2d_t w = work[blockIdx.x];
     const fk_grid2d_t g = grids[w.grid];
-    const int nthreads = ((g.nx + 31) / 32) * 32;
+    const int nthreads = min(((g.nx + 31) / 32) * 32, (int)blockDim.x);
     if ((int)threadIdx.x >= nthreads) return;
     Src2 q;
     q.zsi = w.zsi; q.xsi = w.xsi; q.zsa = w.zsa; q.xsa = w.xsa; q.szero = w.szero;
@@ -213,7 +224,7 @@ solve2d_kernel(const fk_grid2d_t *__restrict__ grids, const fk_work2d_t *__restr
     }
     __threadfence_block();
     bar(nthreads);
-    for (int s = 1; s <= 4; ++s) sweep2<true>(sm, q, g, tt, g.slow, s, nthreads);
+    for (int s = 1; s <= 4; ++s) sweep2<true>(sm, ring2, q, g, tt, g.slow, s, nthreads);
     const bool converge = conv_tol >= 0.0 && max_pass > 0;
     const int npasses = converge ? max_pass : nsweep;
     double res = 0.0;
@@ -221,7 +232,7 @@ solve2d_kernel(const fk_grid2d_t *__restrict__ grids, const fk_work2d_t *__restr
     for (int it = 0; it < npasses; ++it) {
         double d = 0.0;
         for (int s = 1; s <= 4; ++s) {
-            double ds = sweep2<false>(sm, q, g, tt, g.slow, s, nthreads);
+            double ds = sweep2<false>(sm, ring2, q, g, tt, g.slow, s, nthreads);
             d = ds > d ? ds : d;
         }
         for (int o = 16; o > 0; o >>= 1) {
@@ -246,14 +257,18 @@ solve2d_kernel(const fk_grid2d_t *__restrict__ grids, const fk_work2d_t *__restr
 } // namespace
 
 extern "C" int fk2d_solve(int fsm, const fk_grid2d_t *grids, const fk_work2d_t *work,
-                          fk_result3d_t *results, int nwork, int max_nx, double eps,
+                          fk_result3d_t *results, int nwork, int max_nx, int max_nz, double eps,
                           int nsweep, double conv_tol, int max_pass, cudaStream_t stream)
 {
     (void)fsm; /* same dependency graph, same result: see the file comment */
     if (nwork <= 0) return 0;
-    if (max_nx > kMaxWarps * 32) return (int)cudaErrorInvalidValue;
-    const int nthreads = ((max_nx + 31) / 32) * 32;
-    solve2d_kernel<<<nwork, nthreads, 0, stream>>>(grids, work, results, eps, nsweep,
-                                                   conv_tol, max_pass);
+    const int nthreads = min(((max_nx + 31) / 32) * 32, kMaxWarps * 32);
+    const size_t smem = sizeof(double) * (size_t)(max_nz > 1 ? max_nz : 1);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(solve2d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
+    solve2d_kernel<<<nwork, nthreads, smem, stream>>>(grids, work, results, eps, nsweep,
+                                                      conv_tol, max_pass);
     return (int)cudaGetLastError();
 }

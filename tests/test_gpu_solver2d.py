@@ -120,3 +120,25 @@ def test_2d_gradient_and_trace_entry_points(fk):
     assert s.traceRaysToPoints([0.0, (nx - 1) * h], [(nz - 1) * h, 0.0]) == 0
     assert s.traceRaysToPoints([1.0], [(nz - 1) * h + 0.5]) == 1       # below the model
     s.free()
+
+
+@pytest.mark.parametrize("shape", [(30, 1300), (1100, 1050), (12, 2100)])
+def test_2d_more_than_1024_columns(fk, shape):
+    """Columns beyond one CTA's 1024 threads are walked block after block
+    (thread 0 of a block takes its x-upwind value from the previous block's
+    last thread through a ring): FP64 parity with the oracle."""
+    nz, nx = shape
+    h = 10.0
+    rng = np.random.default_rng(nx)
+    zc = (np.arange(nz - 1) + 0.5) * h
+    vel = ((3000.0 + 0.5 * zc)[None, :] * (1.0 + 0.03 * rng.standard_normal((nx - 1, nz - 1)))).ravel()
+    src = (0.37 * (nz - 1) * h, 0.61 * (nx - 1) * h)
+    s = _setup(fk, nz, nx, h, vel, src, eps=3.0)
+    s.solveSourceLSM(1)
+    tt = s.getTravelTimeField()
+    si, sa = O.source_snap(False, (nz, nx, 1), (0, 0, 0), (h, h, 1.0), (src[0], src[1], 0.0))
+    ref, _ = O.solve2d((nz, nx), (h, h), 1.0 / vel, si[:2], sa[:2], 3.0, 2)
+    # one-ulp differences of hypot (device vs libm) in the near-source
+    # analytic times propagate over a million nodes: 1e-11 of the largest time
+    assert np.max(np.abs(tt - ref)) <= 1e-11 * np.max(ref)
+    s.free()
