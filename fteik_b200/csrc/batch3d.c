@@ -244,8 +244,8 @@ void fteik_b200_batch3d_setReceivers64f(int igrid, int nrec, const double zrec[]
     g->rd_dev = (double *)fk_dalloc(3 * sizeof(double) * (size_t)nrec, who);
     int e = 1;
     if (g->ri_dev && g->rd_dev) {
-        e = (int)cudaMemcpy(g->ri_dev, ri, 3 * sizeof(int) * (size_t)nrec, cudaMemcpyHostToDevice);
-        if (!e) e = (int)cudaMemcpy(g->rd_dev, rd, 3 * sizeof(double) * (size_t)nrec, cudaMemcpyHostToDevice);
+        e = (int)fk_h2d(g->ri_dev, ri, 3 * sizeof(int) * (size_t)nrec);
+        if (!e) e = (int)fk_h2d(g->rd_dev, rd, 3 * sizeof(double) * (size_t)nrec);
         e = fk_check(e, who);
     }
     free(ri); free(rd);
@@ -313,7 +313,7 @@ static int upload_work(const char *who)
     if (update_szero(who)) return 1;
     fk_work3d_t *wh = (fk_work3d_t *)malloc(sizeof(fk_work3d_t) * (size_t)SB.nwork);
     fill_work(wh);
-    int e = (int)cudaMemcpy(SB.work_dev, wh, sizeof(fk_work3d_t) * (size_t)SB.nwork, cudaMemcpyHostToDevice);
+    int e = (int)fk_h2d(SB.work_dev, wh, sizeof(fk_work3d_t) * (size_t)SB.nwork);
     free(wh);
     SB.work_dirty = false;
     return fk_check(e, who);
@@ -371,9 +371,9 @@ static int build_work(const char *who)
     fk_dfree(SB.groups_dev);
     SB.groups_dev = (int *)fk_dalloc(sizeof(int) * (size_t)ng * S, who);
     int e = SB.groups_dev ? 0 : 1;
-    if (!e) e = (int)cudaMemcpy(SB.groups_dev, gr, sizeof(int) * (size_t)ng * S, cudaMemcpyHostToDevice);
-    if (!e) e = (int)cudaMemcpy(SB.grids_dev, gh, sizeof(fk_grid3d_t) * (size_t)SB.ngrid, cudaMemcpyHostToDevice);
-    if (!e) e = (int)cudaMemcpy(SB.work_dev, wh, sizeof(fk_work3d_t) * (size_t)nwork, cudaMemcpyHostToDevice);
+    if (!e) e = (int)fk_h2d(SB.groups_dev, gr, sizeof(int) * (size_t)ng * S);
+    if (!e) e = (int)fk_h2d(SB.grids_dev, gh, sizeof(fk_grid3d_t) * (size_t)SB.ngrid);
+    if (!e) e = (int)fk_h2d(SB.work_dev, wh, sizeof(fk_work3d_t) * (size_t)nwork);
     free(gr);
     SB.walker = fk_schedule_walker();
     if (!e && !SB.walker) {

@@ -84,6 +84,27 @@ int fk_sync(const char *who)
     return 0;
 }
 
+int fk_h2d(void *dst, const void *src, size_t bytes)
+{
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, g_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g_stream);
+    return (int)e;
+}
+
+int fk_d2h(void *dst, const void *src, size_t bytes)
+{
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, g_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g_stream);
+    return (int)e;
+}
+
+int fk_zero(void *dst, size_t bytes)
+{
+    cudaError_t e = cudaMemsetAsync(dst, 0, bytes, g_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g_stream);
+    return (int)e;
+}
+
 int fk_check_ray_points(bool is3d, int np, const double *z, const double *x, const double *y)
 {
     if (np < 1) {

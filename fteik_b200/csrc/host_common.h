@@ -21,6 +21,12 @@ void *fk_dalloc(size_t bytes, const char *who);
 void fk_dfree(void *p);
 int fk_check(int cuda_err, const char *who);  /* 0 on success, prints otherwise */
 int fk_sync(const char *who);
+/* Copies and zero fills on the library stream, complete on return (a
+ * cudaError_t).  The library stream is non-blocking: plain cudaMemcpy /
+ * cudaMemset run on the legacy stream, unordered with its kernels. */
+int fk_h2d(void *dst, const void *src, size_t bytes);
+int fk_d2h(void *dst, const void *src, size_t bytes);
+int fk_zero(void *dst, size_t bytes);
 
 /* ---- model (model.F90) ---- */
 typedef struct {

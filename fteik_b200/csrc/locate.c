@@ -157,7 +157,7 @@ void locate_initialize(int nEvents, int ntf, int ngrd, int *ierr)
     SL.l1ok = (unsigned char *)calloc((size_t)nEvents, 1);
     SL.norm = 2;
     if (!SL.tables || !SL.obs_dev || !SL.wts_dev) { *ierr = 1; return; }
-    if (fk_check((int)cudaMemset(SL.tables, 0, sizeof(float) * (size_t)ntf * SL.ldgrd),
+    if (fk_check((int)fk_zero(SL.tables, sizeof(float) * (size_t)ntf * SL.ldgrd),
                  "locate_initialize")) { *ierr = 1; return; }
     SL.init = true;
     SL.dirty = true;
@@ -468,7 +468,7 @@ void fteik_b200_locate_debugAccumulators(int enable, float *out, int *ierr)
         return;
     }
     if (SL.dbg_dev && out) {
-        int e = (int)cudaMemcpy(out, SL.dbg_dev, sizeof(float) * 256 * 128, cudaMemcpyDeviceToHost);
+        int e = (int)fk_d2h(out, SL.dbg_dev, sizeof(float) * 256 * 128);
         if (fk_check(e, "fteik_b200_locate_debugAccumulators")) *ierr = 1;
     }
     fk_dfree(SL.dbg_dev);
@@ -599,7 +599,7 @@ void fteik_b200_locate_setGeometry(int nz, int nx, int ny, double dz, double dx,
     }
     fk_dfree(SP.sta_dev);
     SP.sta_dev = (float *)fk_dalloc(sizeof(float) * 3 * (size_t)ntf, who);
-    int e = SP.sta_dev ? (int)cudaMemcpy(SP.sta_dev, h, sizeof(float) * 3 * (size_t)ntf, cudaMemcpyHostToDevice) : 1;
+    int e = SP.sta_dev ? (int)fk_h2d(SP.sta_dev, h, sizeof(float) * 3 * (size_t)ntf) : 1;
     free(h);
     if (fk_check(e, who)) return;
     SP.nz = nz; SP.nx = nx; SP.ny = ny;
@@ -728,8 +728,8 @@ void fteik_b200_locate_getSurrogateTable(int itf, int n, float out[], int *ierr)
     /* coarse surrogate travel times of table itf (coarse nodes z fastest) */
     *ierr = 1;
     if (!SP.ready || itf < 1 || itf > SL.ntf || n < SP.ngrd_c) { FK_ERR("fteik_b200_locate_getSurrogateTable: not built or bad arguments"); return; }
-    *ierr = fk_check((int)cudaMemcpy(out, SP.coarse + (size_t)(itf - 1) * SP.ldc, sizeof(float) * (size_t)SP.ngrd_c,
-                                     cudaMemcpyDeviceToHost), "fteik_b200_locate_getSurrogateTable");
+    *ierr = fk_check(fk_d2h(out, SP.coarse + (size_t)(itf - 1) * SP.ldc, sizeof(float) * (size_t)SP.ngrd_c),
+                     "fteik_b200_locate_getSurrogateTable");
 }
 
 /* Exhaustive tensor-core search of the events evs[0..m-1] (0-based). */

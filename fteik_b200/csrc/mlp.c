@@ -106,9 +106,9 @@ void fteik_b200_mlp_initialize(int width, int depth, unsigned long long seed, in
     NN.v = (float *)fk_dalloc(sizeof(float) * off, "mlp");
     NN.loss_dev = (double *)fk_dalloc(sizeof(double), "mlp");
     int e = (NN.w && NN.g && NN.m && NN.v && NN.loss_dev) ? 0 : 1;
-    if (!e) e = (int)cudaMemcpy(NN.w, h, sizeof(float) * off, cudaMemcpyHostToDevice);
-    if (!e) e = (int)cudaMemset(NN.m, 0, sizeof(float) * off);
-    if (!e) e = (int)cudaMemset(NN.v, 0, sizeof(float) * off);
+    if (!e) e = (int)fk_h2d(NN.w, h, sizeof(float) * off);
+    if (!e) e = (int)fk_zero(NN.m, sizeof(float) * off);
+    if (!e) e = (int)fk_zero(NN.v, sizeof(float) * off);
     free(h);
     if (fk_check(e, "fteik_b200_mlp_initialize")) return;
     NN.init = true;
@@ -125,7 +125,7 @@ void fteik_b200_mlp_getWeights(int n, float w[], int *ierr)
 {
     *ierr = 1;
     if (!NN.init || n < (int)NN.nparam) { FK_ERR("fteik_b200_mlp_getWeights: not initialized or n too small"); return; }
-    *ierr = fk_check((int)cudaMemcpy(w, NN.w, sizeof(float) * NN.nparam, cudaMemcpyDeviceToHost),
+    *ierr = fk_check((int)fk_d2h(w, NN.w, sizeof(float) * NN.nparam),
                      "fteik_b200_mlp_getWeights");
 }
 
@@ -133,11 +133,11 @@ void fteik_b200_mlp_setWeights(int n, const float w[], int *ierr)
 {
     *ierr = 1;
     if (!NN.init || n != (int)NN.nparam) { FK_ERR("fteik_b200_mlp_setWeights: not initialized or n /= %zu", NN.nparam); return; }
-    *ierr = fk_check((int)cudaMemcpy(NN.w, w, sizeof(float) * NN.nparam, cudaMemcpyHostToDevice),
+    *ierr = fk_check((int)fk_h2d(NN.w, w, sizeof(float) * NN.nparam),
                      "fteik_b200_mlp_setWeights");
     NN.adam_t = 0;
-    cudaMemset(NN.m, 0, sizeof(float) * NN.nparam);
-    cudaMemset(NN.v, 0, sizeof(float) * NN.nparam);
+    fk_zero(NN.m, sizeof(float) * NN.nparam);
+    fk_zero(NN.v, sizeof(float) * NN.nparam);
 }
 
 static int ensure_batch(int B)
@@ -320,8 +320,8 @@ void fteik_b200_mlp_train(int n, const float x[], const float y[], int steps, in
     float *xd = (float *)fk_dalloc(sizeof(float) * (size_t)n * MLP_IN, "mlp");
     float *yd = (float *)fk_dalloc(sizeof(float) * (size_t)n, "mlp");
     if (!xd || !yd) { fk_dfree(xd); fk_dfree(yd); return; }
-    int e = (int)cudaMemcpy(xd, x, sizeof(float) * (size_t)n * MLP_IN, cudaMemcpyHostToDevice);
-    if (!e) e = (int)cudaMemcpy(yd, y, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice);
+    int e = (int)fk_h2d(xd, x, sizeof(float) * (size_t)n * MLP_IN);
+    if (!e) e = (int)fk_h2d(yd, y, sizeof(float) * (size_t)n);
     d.x = xd;
     d.y = yd;
     if (!fk_check(e, "fteik_b200_mlp_train"))

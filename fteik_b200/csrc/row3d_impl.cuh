@@ -294,6 +294,218 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
     return true;
 }
 
+/* One Gauss-Seidel sweep over physical slab P in FP32: the walk of
+ * slab_sweep without the bookkeeping of the initialisation sweeps.  A pass
+ * has no source-limited box, so a lane's items are (column block k, z
+ * position zq) with zq wrapping at Zp and k = 0, 1, ...; the field and
+ * slowness indices are linear in both (the edge clamps are per-lane
+ * constants: x' = 0 is never updated and x' = nx - 1 has a zero x offset),
+ * and the steps run in windows of DL so the exchange-buffer slots are
+ * compile-time constants.  (Moving the two sources' row values as one 64-bit
+ * shared-memory word instead measured 14 % slower.)  A missing second source
+ * (odd number of sources on a grid) walks source 0's field without storing.
+ * The node updates, their order and the waits are those of slab_sweep, so
+ * the results are identical. */
+template <bool RESID, int S, int CHP>
+__device__ __forceinline__ bool slab_pass_f32(const fk3tw::Params &P_, const fk_grid3d_t &g,
+                                              float *const (&ttp)[S], const float *__restrict__ slow, int s,
+                                              int sweep_no, int P, int nslab, int *const (&prog)[S],
+                                              float (*xr)[S][TY][32], float *ring, int zring, int *s_flag,
+                                              double (&dmax)[S])
+{
+    constexpr int CH = CHP;
+    static_assert(CH % DL == 0 && NB == 2 * DL, "progress and buffer slots follow the DL windows");
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const unsigned FULL = 0xffffffffu;
+    const int nz = g.nz, nx = g.nx, ny = g.ny, zp = g.zp, zcp = g.zcp;
+    const int s0 = sweep_no - 1;
+    const int sz = (s0 < 4) ? 1 : -1;
+    const int sx = (s0 % 2 == 0) ? 1 : -1;
+    const int sy = ((s0 / 2) % 2 == 0) ? 1 : -1;
+    Mesh<float> mesh;
+    fk3::make_mesh<float>(mesh, g.dz, g.dx, g.dy);
+    const float HUGEV = (float)FK_HUGE;
+    const int th = min(TY, ny - TY * P);
+    const bool row = ty < th;
+    const int y = TY * P + ty;
+    const int oy = (sy > 0) ? ty : th - 1 - ty;
+    const int yl = (sy > 0) ? y : ny - 1 - y;
+    const bool rowupd = row && yl >= 1;
+    const int wy = ty - sy;
+    const int Z = nz;
+    const int Zp = Z > 32 ? Z : 32;
+    const int K = (nx + 31) / 32;
+    const int T = K * Zp + 31 + DL * (TY - 1);
+    const int Pu = P - sy;
+    const bool has_up = Pu >= 0 && Pu < nslab;
+    const int ylast_up = has_up ? ((sy > 0) ? TY * Pu + min(TY, ny - TY * Pu) - 1 : TY * Pu) : 0;
+    const bool wait_up = has_up && (((sy > 0) ? ylast_up : ny - 1 - ylast_up) >= 1);
+    const int yu = y - sy;
+    const bool has_yu = row && yu >= 0 && yu < ny;
+    const bool has2 = S == 2 && ttp[S - 1] != nullptr;
+    const float *const tt0 = ttp[0];
+    const float *const tt1 = has2 ? ttp[S - 1] : ttp[0];
+
+    /* item (k, zq) of this lane: node x = x0 + 32 sx k, z = iz0 + sz zq */
+    const int x0 = (sx > 0) ? tx : nx - 1 - tx;
+    const int iz0 = (sz > 0) ? 0 : nz - 1;
+    const int kl = row ? (nx - tx + 31) / 32 : 0;                  /* blocks with x' < nx */
+    const int kmin = rowupd ? (tx == 0 ? 1 : 0) : 0x7fffffff;       /* updated: x' >= 1, y' >= 1 */
+    const int kxl = (nx - 1 >= tx && (nx - 1 - tx) % 32 == 0) ? (nx - 1 - tx) / 32 : -1; /* x' = nx - 1 */
+    const int baseT = (y * nx + x0) * zp + iz0;
+    const int dkT = 32 * sx * zp;
+    const int dyT = sy * nx * zp;                                   /* to the y-upwind row */
+    /* slowness: cells (cxU | cxD, cyU | cyD, czD), czD = iz - (sz < 0) clamped to the grid */
+    const int cyU = (sy > 0) ? y - 1 : y;
+    const int cyD = min(max((sy > 0) ? y : y - 1, 0), ny - 2);
+    const int baseS = (cyU * (nx - 1) + x0 - (sx > 0 ? 1 : 0)) * zcp + ((sz > 0) ? 0 : nz - 2);
+    const int dkS = 32 * sx * zcp;
+    const int offY = (cyD - cyU) * (nx - 1) * zcp;
+    const int offX = sx * zcp;
+
+    struct Item {
+        float told[S], tn[S];
+        float duu, dud, ddu, ddd;   /* z-downwind slowness layer, s<z><x><y> with z = D */
+        int it, k, zq;
+    };
+    auto fetch = [&](Item &f, int kk, int zz) {
+        f.k = kk;
+        f.zq = zz;
+        f.it = baseT + kk * dkT + sz * zz;
+        const bool v = (unsigned)zz < (unsigned)Z && kk < kl;
+        if (v) {
+            f.told[0] = fk3tw::ldcg(tt0 + f.it);
+            if (S == 2) f.told[S - 1] = fk3tw::ldcg(tt1 + f.it);
+            if (oy == 0) {
+                f.tn[0] = has_yu ? fk3tw::ldcg(tt0 + (f.it - dyT)) : HUGEV;
+                if (S == 2) f.tn[S - 1] = has_yu ? fk3tw::ldcg(tt1 + (f.it - dyT)) : HUGEV;
+            }
+        }
+        if (v && kk >= kmin) {
+            const int is = baseS + kk * dkS + sz * min(zz, nz - 2);
+            const int ox = (kk == kxl) ? 0 : offX;
+            f.duu = __ldg(slow + is);
+            f.dud = __ldg(slow + (is + offY));
+            f.ddu = __ldg(slow + (is + ox));
+            f.ddd = __ldg(slow + (is + ox + offY));
+        }
+    };
+
+    const int *prog_up = prog[0] + (has_up ? Pu : P);
+    if (threadIdx.x == 0) {
+        s_flag[0] = 1;
+        if (wait_up && !wait_ge1(prog_up, (s << SHIFT) | min(T, CH + DL * (TY - 1) + 2), P_.spin_limit, P_.error,
+                                 3000))
+            s_flag[0] = 0;
+    }
+    __syncthreads();
+    if (!s_flag[0]) return false;
+
+    int nk = 0, nzq = -tx - DL * oy;     /* item of the next step */
+    Item nxt;
+#pragma unroll
+    for (int i = 0; i < S; ++i) nxt.told[i] = nxt.tn[i] = HUGEV;
+    nxt.duu = nxt.dud = nxt.ddu = nxt.ddd = 0.0f;
+    fetch(nxt, nk, nzq);
+    if (++nzq == Zp) { nzq = 0; ++nk; }
+    float zu_uu = 0.0f, zu_ud = 0.0f, zu_du = 0.0f, zu_dd = 0.0f;   /* z-upwind layer (previous step) */
+    float r_last[S], te_last[S], tn_last[S], ten_last[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) r_last[i] = te_last[i] = tn_last[i] = ten_last[i] = HUGEV;
+    float *ring_r = ring, *ring_tn = ring + S * zring;   /* [S][zring] each */
+    for (int t0 = 0; t0 < T; t0 += DL) {
+        if (wait_up && t0 > 0 && t0 % CH == 0) {
+            if (threadIdx.x == 0 &&
+                !wait_ge1(prog_up, (s << SHIFT) | min(T, t0 + CH + DL * (TY - 1) + 2), P_.spin_limit, P_.error,
+                          3001))
+                s_flag[0] = 0;
+            __syncthreads();
+            if (!s_flag[0]) return false;
+        }
+        const int half = (t0 / DL) & 1;   /* this window writes slots half DL + u, reads the other half */
+        float (*const xw)[S][TY][32] = xr + half * DL;
+        float (*const xrd)[S][TY][32] = xr + (1 - half) * DL;
+#pragma unroll
+        for (int u = 0; u < DL; ++u) {
+            float sh_r[S], sh_tn[S];
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                sh_r[i] = __shfl_up_sync(FULL, r_last[i], 1);
+                sh_tn[i] = __shfl_up_sync(FULL, tn_last[i], 1);
+            }
+            const Item cur = nxt;
+            fetch(nxt, nk, nzq);
+            if (++nzq == Zp) { nzq = 0; ++nk; }
+            const bool valid = (unsigned)cur.zq < (unsigned)Z && cur.k < kl;
+            const bool upd = valid && cur.zq >= 1 && cur.k >= kmin;
+            const bool from_ring = tx == 0 && cur.k > 0;   /* then 0 <= zq < Zp */
+            float rte[S], rten[S];
+#pragma unroll
+            for (int i = 0; i < S; ++i) rte[i] = rten[i] = HUGEV;
+            if (from_ring) {
+#pragma unroll
+                for (int i = 0; i < S; ++i) { rte[i] = ring_r[i * zring + cur.zq]; rten[i] = ring_tn[i * zring + cur.zq]; }
+            }
+            float tnw[S];
+            if (oy != 0) {
+#pragma unroll
+                for (int i = 0; i < S; ++i) tnw[i] = xrd[u][i][wy][tx];
+            }
+            const float s4 = fminf(zu_uu, zu_ud), s5 = fminf(zu_uu, zu_du), s6 = fminf(zu_uu, cur.duu);
+            const float s1 = fminf(s4, fminf(zu_du, zu_dd));
+            const float s2 = fminf(s4, fminf(cur.duu, cur.dud));
+            const float s3 = fminf(s5, fminf(cur.duu, cur.ddu));
+            const float s7 = zu_uu;
+            float res[S], tnv_[S];
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                const float te = (tx == 0) ? rte[i] : sh_r[i];
+                const float ten = (tx == 0) ? rten[i] : sh_tn[i];
+                const float tn = (oy == 0) ? cur.tn[i] : tnw[i];
+                const float told = cur.told[i];
+                float r = told;
+                if (upd) {
+                    /* one scalar evaluation per source: the float2 form (both
+                     * sources in packed instructions) measured 14 % slower */
+                    r = fk3::noinit_f32(mesh, r_last[i], te, tn, te_last[i], ten, tn_last[i], ten_last[i], s1, s2,
+                                        s3, s4, s5, s6, s7, told);
+                    if (r != told && (i == 0 || has2)) {
+                        (i == 0 ? ttp[0] : ttp[S - 1])[cur.it] = r;
+                        if (RESID) {
+                            const double d = fabs((double)r - (double)told);
+                            dmax[i] = d > dmax[i] ? d : dmax[i];
+                        }
+                    }
+                }
+                res[i] = r;
+                tnv_[i] = tn;
+                te_last[i] = te;
+                ten_last[i] = ten;
+            }
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                xw[u][i][ty][tx] = res[i];
+                if (tx == 31 && cur.zq >= 0) { ring_r[i * zring + cur.zq] = res[i]; ring_tn[i * zring + cur.zq] = tnv_[i]; }
+            }
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                r_last[i] = res[i];
+                tn_last[i] = tnv_[i];
+            }
+            zu_uu = cur.duu; zu_ud = cur.dud; zu_du = cur.ddu; zu_dd = cur.ddd;
+            if (u < DL - 1) __syncwarp();   /* lane 31 -> lane 0 ring */
+        }
+        __syncthreads();                    /* the window's row values become visible */
+        if (threadIdx.x == 0 && (t0 + DL) % CH == 0 && t0 + DL < T) {
+            __threadfence();
+#pragma unroll
+            for (int i = 0; i < S; ++i)
+                if (prog[i]) fk3tw::st_release(prog[i] + P, (s << SHIFT) | (t0 + DL));
+        }
+    }
+    return true;
+}
+
 /* Persistent slab-task kernel over sweeps [s_begin, s_end).  S = 2 runs
  * two sources of one grid in the same threads (the Gauss-Seidel passes,
  * whose walk does not depend on the source): the slowness, the indices and
@@ -384,9 +596,14 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
 #pragma unroll
         for (int i = 0; i < S; ++i) dmax[i] = 0.0;
         if (!skip) {
-            if (!slab_sweep<R, INIT, RESID, S, CHP>(P, g, ttp, reinterpret_cast<const R *>(g.slow), q, s, sweep_no, Pp,
-                                               nslab, prog, xr, ring, zring, s_flag, dmax))
-                break;
+            bool ok;
+            if constexpr (!INIT && sizeof(R) == 4)
+                ok = slab_pass_f32<RESID, S, CHP>(P, g, ttp, reinterpret_cast<const float *>(g.slow), s, sweep_no,
+                                                  Pp, nslab, prog, xr, ring, zring, s_flag, dmax);
+            else
+                ok = slab_sweep<R, INIT, RESID, S, CHP>(P, g, ttp, reinterpret_cast<const R *>(g.slow), q, s,
+                                                        sweep_no, Pp, nslab, prog, xr, ring, zring, s_flag, dmax);
+            if (!ok) break;
         }
         __syncthreads();
         if (RESID && !INIT) {

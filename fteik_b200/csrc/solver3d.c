@@ -180,7 +180,7 @@ static int ensure_buffers(void)
     if (!S3.res_dev) S3.res_dev = (fk_result3d_t *)fk_dalloc(sizeof(fk_result3d_t), "fteik_solver3d");
     if (!S3.group_dev) {
         S3.group_dev = (int *)fk_dalloc(sizeof(int), "fteik_solver3d");
-        if (S3.group_dev && fk_check((int)cudaMemset(S3.group_dev, 0, sizeof(int)), "fteik_solver3d"))
+        if (S3.group_dev && fk_check((int)fk_zero(S3.group_dev, sizeof(int)), "fteik_solver3d"))
             return 1;
     }
     return !(S3.tt && S3.grid_dev && S3.work_dev && S3.res_dev && S3.group_dev);

@@ -63,10 +63,8 @@ int fk_tileplan_build(fk_tileplan_t *pl, int nwork, const int *nx, const int *ny
     size_t total = off_cp + al(sizeof(int) * (size_t)nwork);
     char *m = (char *)fk_dalloc(total, who);
     int e = m ? 0 : 1;
-    if (!e) e = fk_check((int)cudaMemcpy(m + off_tasks, tasks, sizeof(int) * 2 * (size_t)ntiles,
-                                         cudaMemcpyHostToDevice), who);
-    if (!e) e = fk_check((int)cudaMemcpy(m + off_base, base, sizeof(int) * (size_t)nwork,
-                                         cudaMemcpyHostToDevice), who);
+    if (!e) e = fk_check((int)fk_h2d(m + off_tasks, tasks, sizeof(int) * 2 * (size_t)ntiles), who);
+    if (!e) e = fk_check((int)fk_h2d(m + off_base, base, sizeof(int) * (size_t)nwork), who);
     free(tasks); free(ntx); free(nty); free(base);
     if (e) { fk_dfree(m); return 1; }
     pl->mem = m;
@@ -161,14 +159,10 @@ static int rowplan_build(fk_tileplan_t *pl, int nwork, const int *nx, const int 
     size_t total = off_t2 + al(sizeof(int) * 2 * (size_t)ntask2);
     char *m = (char *)fk_dalloc(total, who);
     int e = m ? 0 : 1;
-    if (!e) e = fk_check((int)cudaMemcpy(m + off_tasks, tasks, sizeof(int) * 2 * (size_t)nslab,
-                                         cudaMemcpyHostToDevice), who);
-    if (!e) e = fk_check((int)cudaMemcpy(m + off_base, base, sizeof(int) * (size_t)nwork,
-                                         cudaMemcpyHostToDevice), who);
-    if (!e) e = fk_check((int)cudaMemcpy(m + off_pairs, pairs, sizeof(int) * 2 * (size_t)npair,
-                                         cudaMemcpyHostToDevice), who);
-    if (!e) e = fk_check((int)cudaMemcpy(m + off_t2, tasks2, sizeof(int) * 2 * (size_t)ntask2,
-                                         cudaMemcpyHostToDevice), who);
+    if (!e) e = fk_check((int)fk_h2d(m + off_tasks, tasks, sizeof(int) * 2 * (size_t)nslab), who);
+    if (!e) e = fk_check((int)fk_h2d(m + off_base, base, sizeof(int) * (size_t)nwork), who);
+    if (!e) e = fk_check((int)fk_h2d(m + off_pairs, pairs, sizeof(int) * 2 * (size_t)npair), who);
+    if (!e) e = fk_check((int)fk_h2d(m + off_t2, tasks2, sizeof(int) * 2 * (size_t)ntask2), who);
     free(tasks);
     free(tasks2);
     free(pairs);

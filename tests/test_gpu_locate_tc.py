@@ -97,7 +97,15 @@ def test_tc_matches_fp64_exhaustive(fk, shape, ntf, nev):
         if oi[e] - 1 != gi:
             # only an exact FP64 tie may pick a different node
             _, _, ob_here = O.locate_l2_best64(tables[:, [oi[e] - 1]], red[e], w)
-            assert abs(ob_here - gob) <= 1e-12 * max(gob, 1e-30), (e, oi[e] - 1, gi)
+            if abs(ob_here - gob) > 1e-12 * max(gob, 1e-30):
+                # report whether the miss repeats and how many events it hits
+                oi2, _, ob2 = loc.locateEvents(np.arange(1, nev + 1))
+                best = [O.locate_l2_best64(tables, red[k], w)[0] for k in range(nev)]
+                bad = [k for k in range(nev) if oi[k] - 1 != best[k]]
+                bad2 = [k for k in range(nev) if oi2[k] - 1 != best[k]]
+                raise AssertionError(f"event {e}: got node {oi[e] - 1} (misfit {ob[e]!r}, oracle there "
+                                     f"{ob_here!r}), oracle optimum {gi} ({gob!r}); events off: {bad}; "
+                                     f"second call: node {oi2[e] - 1} ({ob2[e]!r}), events off {bad2}")
             miss += 1
             continue
         assert abs(t0[e] - (gt0 + tep[e])) <= 1e-9 * max(1.0, abs(gt0 + tep[e]))
