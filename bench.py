@@ -664,7 +664,7 @@ def main():
     achieved = pass_bytes / (pass_ms * 1e-3) / 1e9
     traffic = None
     tp = os.path.join(ROOT, "profiles", "slab_pass_traffic.json")
-    if os.path.exists(tp):
+    if os.path.exists(tp) and sel == [1, 2, 3, 4]:   # captured on the 4-grid batch
         traffic = json.load(open(tp)).get("dram_bytes_per_launch")
     roofline = {"bound": "hbm", "kernel": "fk3rw::slab_kernel<float, passes, 2 sources per thread>",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
