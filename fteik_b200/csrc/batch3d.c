@@ -62,7 +62,38 @@ static struct {
     cudaEvent_t ev[3];      /* in the graph: before init, after init, after passes */
     bool have_ev;
     cudaStream_t copy_stream; /* asynchronous table downloads */
+    void *hmap, *hmap_dev;    /* mapped pinned host memory: small results kernels write */
+    size_t hmap_cap;
 } SB;
+
+/* Mapped pinned host memory for the small results the host waits for (the
+ * velocity check, the source-cell velocities): kernels write them straight
+ * to the host, so no copy queues behind table downloads still running on
+ * the copy stream.  *dev receives the device address. */
+static void *hmap_buf(size_t bytes, void **dev, const char *who)
+{
+    if (!SB.hmap || SB.hmap_cap < bytes) {
+        if (SB.hmap) {
+            cudaStreamSynchronize(fk_stream());
+            cudaFreeHost(SB.hmap);
+        }
+        SB.hmap = SB.hmap_dev = NULL;
+        SB.hmap_cap = 0;
+        void *p = NULL, *d = NULL;
+        cudaError_t e = cudaHostAlloc(&p, bytes, cudaHostAllocMapped);
+        if (e == cudaSuccess) e = cudaHostGetDevicePointer(&d, p, 0);
+        if (e != cudaSuccess) {
+            if (p) cudaFreeHost(p);
+            FK_ERR("%s: mapped host allocation of %zu bytes failed (%s)", who, bytes, cudaGetErrorString(e));
+            return NULL;
+        }
+        SB.hmap = p;
+        SB.hmap_dev = d;
+        SB.hmap_cap = bytes;
+    }
+    *dev = SB.hmap_dev;
+    return SB.hmap;
+}
 
 static void *stage_buf(size_t bytes, const char *who)
 {
@@ -102,6 +133,7 @@ void fteik_b200_batch3d_finalize(void)
     fk_tileplan_free(&SB.plan);
     if (SB.have_ev) for (int i = 0; i < 3; i++) cudaEventDestroy(SB.ev[i]);
     free(SB.res_host); free(SB.work_order);
+    if (SB.hmap) cudaFreeHost(SB.hmap);
     cudaStream_t cs = SB.copy_stream;   /* kept for the process's next batch */
     memset(&SB, 0, sizeof(SB));
     SB.copy_stream = cs;
@@ -170,19 +202,20 @@ void fteik_b200_batch3d_setVelocityModel64f(int igrid, int ncell, const double v
     const size_t nelem = (size_t)g->zcp * (g->nx - 1) * (g->ny - 1);
     if (!g->slow_dev) g->slow_dev = fk_dalloc(nelem * (size_t)SB.precision, who);
     if (!g->vel_dev) g->vel_dev = (double *)fk_dalloc(sizeof(double) * (size_t)ncell, who);
-    int *bad_dev = (int *)stage_buf(sizeof(int), who);
-    if (!g->slow_dev || !g->vel_dev || !bad_dev) return;
+    void *bad_dev = NULL;
+    volatile int *bad = (volatile int *)hmap_buf(sizeof(int), &bad_dev, who);
+    if (!g->slow_dev || !g->vel_dev || !bad) return;
     g->have_model = false;
     cudaStream_t s = fk_stream();
-    int bad = 0;
-    int e = (int)cudaMemsetAsync(g->slow_dev, 0, nelem * (size_t)SB.precision, s);
-    if (!e) e = (int)cudaMemsetAsync(bad_dev, 0, sizeof(int), s);
+    int e = (int)cudaStreamSynchronize(s);   /* no kernel of the stream uses the flag */
+    *bad = 0;
+    if (!e) e = (int)cudaMemsetAsync(g->slow_dev, 0, nelem * (size_t)SB.precision, s);
     if (!e) e = (int)cudaMemcpyAsync(g->vel_dev, vel, sizeof(double) * (size_t)ncell, cudaMemcpyHostToDevice, s);
-    if (!e) e = fk_pack_velocity(SB.precision, g->nz, g->nx, g->ny, g->zcp, g->vel_dev, g->slow_dev, bad_dev, s);
-    if (!e) e = (int)cudaMemcpyAsync(&bad, bad_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (!e) e = fk_pack_velocity(SB.precision, g->nz, g->nx, g->ny, g->zcp, g->vel_dev, g->slow_dev,
+                                 (int *)bad_dev, s);
     if (!e) e = (int)cudaStreamSynchronize(s);
     if (fk_check(e, who)) return;
-    if (bad) { FK_ERR("%s: velocities must be positive", who); return; }
+    if (*bad) { FK_ERR("%s: velocities must be positive", who); return; }
     g->have_model = true;
     SB.solved = false;
     SB.work_dirty = true; /* szero of this grid's sources */
@@ -287,23 +320,21 @@ static int update_szero(const char *who)
         bgrid_t *g = &SB.g[i];
         if (g->nsrc < 1) continue;
         const int n = g->nsrc;
-        long long *idx = (long long *)malloc(sizeof(long long) * (size_t)n);
-        double *v = (double *)malloc(sizeof(double) * (size_t)n);
         free(g->szero);
         g->szero = (double *)malloc(sizeof(double) * (size_t)n);
-        char *dbuf = (char *)stage_buf((sizeof(long long) + sizeof(double)) * (size_t)n, who);
-        if (!idx || !v || !g->szero || !dbuf) { free(idx); free(v); return 1; }
+        void *hdev = NULL;
+        e = (int)cudaStreamSynchronize(s);       /* no kernel of the stream uses the buffer */
+        char *hbuf = (char *)hmap_buf((sizeof(long long) + sizeof(double)) * (size_t)n, &hdev, who);
+        if (!g->szero || !hbuf) return 1;
+        /* cell indices in, velocities out, both in mapped host memory */
+        long long *idx = (long long *)hbuf;
+        volatile double *v = (volatile double *)(hbuf + sizeof(long long) * (size_t)n);
         for (int k = 0; k < n; k++)
             idx[k] = ((long long)(g->ysi[k] - 1) * (g->nx - 1) + (g->xsi[k] - 1)) * (g->nz - 1) + (g->zsi[k] - 1);
-        long long *idx_dev = (long long *)dbuf;
-        double *v_dev = (double *)(dbuf + sizeof(long long) * (size_t)n);
-        e = (int)cudaMemcpyAsync(idx_dev, idx, sizeof(long long) * (size_t)n, cudaMemcpyHostToDevice, s);
-        if (!e) e = fk_gather64(g->vel_dev, idx_dev, n, v_dev, s);
-        if (!e) e = (int)cudaMemcpyAsync(v, v_dev, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s);
+        if (!e) e = fk_gather64(g->vel_dev, (const long long *)hdev, n,
+                                (double *)((char *)hdev + sizeof(long long) * (size_t)n), s);
         if (!e) e = (int)cudaStreamSynchronize(s);
         for (int k = 0; !e && k < n; k++) g->szero[k] = 1.0 / v[k];
-        free(idx);
-        free(v);
     }
     return fk_check(e, who);
 }
