@@ -4,7 +4,7 @@
  * solveSourceFSM (solver2D.F90:1042-1280), in FP64.
  *
  * One CTA owns one (grid, source).  Thread t owns the logical x columns
- * b NT + t (b = 0, 1, ...: column blocks of NT <= 1024 threads) and walks
+ * b NT + t (b = 0, 1, ...: column blocks of NT <= 512 threads) and walks
  * their z positions, block after block, thread t one step behind thread t-1,
  * so tv is the thread's previous result, te the previous result of thread
  * t-1 (warp shuffle, the two-slot hand-off between warps, or for thread 0 of
@@ -19,7 +19,8 @@
 
 namespace {
 
-constexpr int kMaxWarps = 32;
+constexpr int kMaxWarps = 16;
+constexpr int kMaxThreads = kMaxWarps * 32;   /* 512: 128 registers per thread, no spills */
 
 struct Mesh2 {
     double dz, dx, dzi, dxi, dz2i, dx2i, dz2i_dx2i, dz2i_p_dx2i, dz2i_p_dx2i_inv;
@@ -141,40 +142,59 @@ __device__ double sweep2(Smem2 &sm, double *ring, const Src2 &q, const fk_grid2d
     /* steps per block: the ring between blocks needs >= nthreads; one block needs no ring */
     const int zb = (nblk > 1 && nthreads > nz) ? nthreads : nz;
     const int nsteps = nblk * zb + nthreads - 1;
+    /* The node and slowness loads of a thread's next item are issued one
+     * step ahead: within a sweep only this thread writes its columns. */
+    struct Item {
+        double told, sUU, sUD, sDU;
+        size_t idx;
+        int iz, ix, b, il;
+        bool valid, upd;
+    };
+    auto fetch = [&](int j, Item &f) {
+        f.b = j >= 0 ? j / zb : -1;
+        f.il = j - f.b * zb;
+        const int xl = f.b * nthreads + t;
+        f.valid = j >= 0 && f.b < nblk && xl < nx && f.il < nz;
+        f.upd = f.valid && f.il >= loz && xl >= lox;
+        if (!f.valid) return;
+        f.ix = (sx > 0) ? xl : nx - 1 - xl;
+        f.iz = (sz > 0) ? f.il : nz - 1 - f.il;
+        f.idx = (size_t)f.ix * zp + f.iz;
+        f.told = tt[f.idx];
+        if (f.upd) {
+            const int cxU = (sx > 0) ? f.ix - 1 : f.ix;
+            const int cxD = min(max((sx > 0) ? f.ix : f.ix - 1, 0), nx - 2);
+            const int czU = (sz > 0) ? f.iz - 1 : f.iz;
+            const int czD = min(max((sz > 0) ? f.iz : f.iz - 1, 0), nz - 2);
+            f.sUU = slow[(size_t)cxU * zcp + czU];
+            f.sUD = slow[(size_t)cxD * zcp + czU]; /* z U, x D */
+            f.sDU = slow[(size_t)cxU * zcp + czD]; /* z D, x U */
+        }
+    };
+    Item nxt;
+    fetch(-t, nxt);
     double r_last = FK_HUGE, te_last = FK_HUGE, dmax = 0.0;
     for (int s = 0; s < nsteps; ++s) {
-        const int j = s - t;
-        const int b = j >= 0 ? j / zb : -1;
-        const int il = j - b * zb;
-        const int xl = b * nthreads + t;
+        const Item cur = nxt;
+        fetch(s + 1 - t, nxt);
         double te = __shfl_up_sync(0xffffffffu, r_last, 1);
         if (lane == 0 && warp > 0) te = sm.xres[(s + 1) & 1][warp - 1];
-        if (t == 0) te = (b > 0 && il < nz) ? ring[il] : FK_HUGE;
+        if (t == 0) te = (cur.b > 0 && cur.il < nz) ? ring[cur.il] : FK_HUGE;
         double result = r_last;
-        if (j >= 0 && b < nblk && xl < nx && il < nz) {
-            const int ix = (sx > 0) ? xl : nx - 1 - xl;
-            const int cxU = (sx > 0) ? ix - 1 : ix;
-            const int cxD = min(max((sx > 0) ? ix : ix - 1, 0), nx - 2);
-            const int iz = (sz > 0) ? il : nz - 1 - il;
-            const size_t idx = (size_t)ix * zp + iz;
-            const double told = tt[idx];
+        if (cur.valid) {
+            const double told = cur.told;
             result = told;
-            if (il >= loz && xl >= lox) {
-                const int czU = (sz > 0) ? iz - 1 : iz;
-                const int czD = min(max((sz > 0) ? iz : iz - 1, 0), nz - 2);
-                const double sUU = slow[(size_t)cxU * zcp + czU];
-                const double sUD = slow[(size_t)cxD * zcp + czU]; /* z U, x D */
-                const double sDU = slow[(size_t)cxU * zcp + czD]; /* z D, x U */
-                const double s1 = dmin(sUU, sUD), s2 = dmin(sUU, sDU), s3 = sUU;
+            if (cur.upd) {
+                const double s1 = dmin(cur.sUU, cur.sUD), s2 = dmin(cur.sUU, cur.sDU), s3 = cur.sUU;
                 double tu;
                 if (INIT)
                     tu = init2(q, sm.mesh, sz, sx, r_last, te, te_last, told, s1, s2, s3,
-                               iz + 1, ix + 1);
+                               cur.iz + 1, cur.ix + 1);
                 else
                     tu = noinit2(sm.mesh, r_last, te, te_last, s1, s2, s3);
                 result = dmin(told, tu);
                 if (result != told) {
-                    tt[idx] = result;
+                    tt[cur.idx] = result;
                     double d = fabs(result - told);
                     dmax = d > dmax ? d : dmax;
                 }
@@ -183,13 +203,13 @@ __device__ double sweep2(Smem2 &sm, double *ring, const Src2 &q, const fk_grid2d
         te_last = te;
         r_last = result;
         if (lane == 31) sm.xres[s & 1][warp] = result;
-        if (t == nthreads - 1 && j >= 0 && b < nblk && il < nz) ring[il] = result;
+        if (t == nthreads - 1 && cur.b >= 0 && cur.b < nblk && cur.il < nz) ring[cur.il] = result;
         bar(nthreads);
     }
     return dmax;
 }
 
-__global__ void __launch_bounds__(1024, 1)
+__global__ void __launch_bounds__(kMaxThreads, 1)
 solve2d_kernel(const fk_grid2d_t *__restrict__ grids, const fk_work2d_t *__restrict__ work,
                fk_result3d_t *__restrict__ results, double eps, int nsweep,
                double conv_tol, int max_pass)
@@ -212,7 +232,7 @@ solve2d_kernel(const fk_grid2d_t *__restrict__ grids, const fk_work2d_t *__restr
         m.dz2i_p_dx2i = m.dz2i + m.dx2i;
         m.dz2i_p_dx2i_inv = 1.0 / (m.dz2i + m.dx2i);
     }
-    if (threadIdx.x < 2 * kMaxWarps) sm.xres[threadIdx.x >> 5][threadIdx.x & 31] = FK_HUGE;
+    if (threadIdx.x < 2 * kMaxWarps) sm.xres[threadIdx.x / kMaxWarps][threadIdx.x % kMaxWarps] = FK_HUGE;
     double *tt = w.tt;
     const size_t nfield = (size_t)g.nx * g.zp;
     for (size_t e = threadIdx.x; e < nfield; e += nthreads) tt[e] = FK_HUGE;
@@ -262,7 +282,7 @@ extern "C" int fk2d_solve(int fsm, const fk_grid2d_t *grids, const fk_work2d_t *
 {
     (void)fsm; /* same dependency graph, same result: see the file comment */
     if (nwork <= 0) return 0;
-    const int nthreads = min(((max_nx + 31) / 32) * 32, kMaxWarps * 32);
+    const int nthreads = min(((max_nx + 31) / 32) * 32, kMaxThreads);
     const size_t smem = sizeof(double) * (size_t)(max_nz > 1 ? max_nz : 1);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(solve2d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
