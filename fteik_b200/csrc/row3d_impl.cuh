@@ -20,9 +20,10 @@
  *                        last row, final for this sweep            (global, L2)
  *   ten                  lane l-1's tn of the previous step        (shuffle)
  *                        or, for lane 0, lane 31's through the ring
- * Rows lag DL = 4 steps behind their upwind row, so the block synchronises
+ * Rows lag DL = 2 steps behind their upwind row, so the block synchronises
  * once per DL steps (the upwind row's values of the previous window are then
- * visible) instead of every step.  The skew ramp (31 + DL (TY - 1) steps) is
+ * visible) instead of every step.  (DL = 1, 4 and 8 measured slower: a longer
+ * lag lengthens the chain of upwind slabs, a barrier every step costs issue.)  The skew ramp (31 + DL (TY - 1) steps) is
  * paid once per slab.
  *
  * Slabs publish their progress as (sweep << 20) | steps done every CH steps
@@ -52,7 +53,7 @@ constexpr int TY = FK_SLAB_Y;        /* rows (warps) per slab */
 constexpr int NT = TY * 32;
 constexpr int CH_INIT = 8;           /* progress granularity of the initialisation sweeps, steps */
 constexpr int CH_FEW = 8, CH_MANY = 32; /* passes: few tasks per sweep want a short lag, many few polls */
-constexpr int DL = 4;                /* row-to-row lag inside a slab = block barrier interval */
+constexpr int DL = 2;                /* row-to-row lag inside a slab = block barrier interval */
 constexpr int NB = 2 * DL;           /* row exchange buffer depth */
 constexpr int SHIFT = 20;            /* counter = (sweep << SHIFT) | steps */
 
@@ -679,7 +680,7 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
     const int npr = npass > 0 ? npass : 1;
     const int zring = pl->max_nz > 32 ? pl->max_nz : 32;
     /* counters hold (sweep << SHIFT) | steps: steps of a slab and sweep numbers must fit */
-    const long long steps = (long long)((pl->max_nx + 31) / 32) * zring + 31 + TY;
+    const long long steps = (long long)((pl->max_nx + 31) / 32) * zring + 31 + DL * TY;
     if (steps >= (1LL << SHIFT) || 8 + 8 * (long long)npr + 1 >= (1LL << (31 - SHIFT)))
         return (int)cudaErrorInvalidValue;
     cudaError_t e = cudaSuccess;
