@@ -182,6 +182,29 @@ def test_batched_multi_grid(fk):
         b.finalize()
 
 
+def test_source_pairs_match_single_source_bitwise(fk):
+    """The batch's Gauss-Seidel passes walk two sources of a grid in the
+    same threads (sharing indices, slowness and barriers, not arithmetic),
+    and an odd last source walks alone: every source's FP32 field equals the
+    one-source solve of that source bit for bit."""
+    n, h = (21, 45, 19), (25.0, 25.0, 25.0)
+    vel = layered_grf_cells(*n, seed=31, min_cells=2)
+    rng = np.random.default_rng(12)
+    srcs = [(rng.uniform(0, (n[0] - 1) * h[0]), rng.uniform(0, (n[1] - 1) * h[1]),
+             rng.uniform(0, (n[2] - 1) * h[2])) for _ in range(3)]
+    b = fk.Batch3D([(n[0], n[1], n[2], *h)], nsweep=2, eps=5.0, precision=4)
+    b.setVelocityModel(1, vel)
+    b.setSources(1, [s[0] for s in srcs], [s[1] for s in srcs], [s[2] for s in srcs])
+    b.solve()
+    f32 = b.fields32(1).reshape(len(srcs), -1)
+    b.finalize()
+    for k, src in enumerate(srcs):
+        s = _gpu(fk, n, h, vel, src, 4)
+        one = s.getTravelTimeField()
+        s.free()
+        assert np.array_equal(one.astype(np.float32), f32[k]), k
+
+
 def test_batched_converged(fk):
     grids = [(16, 18, 14, 25.0, 25.0, 25.0)]
     nz, nx, ny, dz, dx, dy = grids[0]
