@@ -150,12 +150,13 @@ class Clocks:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons}
 
 
-def cpu_reference(grids, steps, warmup, nthreads, sample_src=24):
+def cpu_reference(grids, steps, warmup, nthreads, sample_src=24, check=None):
     """CPU restatement of the reference (oracle/), timed on a bounded sample:
-    `sample_src` sources on the largest grid per step."""
+    `sample_src` sources on the 160x160x96 grid per step.  check(k, tt), if
+    given, receives each source's FP64 field outside the timed solves."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as O
-    g = grids[2]
+    g = next(g for g in grids if (g["nx"], g["ny"], g["nz"]) == (160, 160, 96))
     n = (g["nz"], g["nx"], g["ny"])
     slow = (1.0 / g["vel"]).ravel()
     upd = 0
@@ -167,11 +168,14 @@ def cpu_reference(grids, steps, warmup, nthreads, sample_src=24):
         upd += ni + NSWEEP * npass
     for _ in range(warmup):
         O.solve3d(n, (H, H, H), slow, *si_sa[0], EPS, NSWEEP, level_set=True, nthreads=nthreads)
-    t0 = time.perf_counter()
+    dt = 0.0
     for _ in range(steps):
-        for si, sa in si_sa:
-            O.solve3d(n, (H, H, H), slow, si, sa, EPS, NSWEEP, level_set=True, nthreads=nthreads)
-    dt = time.perf_counter() - t0
+        for k, (si, sa) in enumerate(si_sa):
+            t0 = time.perf_counter()
+            tt, _ = O.solve3d(n, (H, H, H), slow, si, sa, EPS, NSWEEP, level_set=True, nthreads=nthreads)
+            dt += time.perf_counter() - t0
+            if check is not None:
+                check(k, tt)
     return upd * steps / dt, dt, "%d source(s) on the %dx%dx%d grid per step, %d step(s)" % (
         sample_src, g["nx"], g["ny"], g["nz"], steps)
 
@@ -680,10 +684,30 @@ def main():
                               sur_steps=args.surrogate_steps)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, dt, sample = cpu_reference(grids, steps=1, warmup=0, nthreads=os.cpu_count() or 1)
+    batch_err = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and 3 in sel:
+        # the baseline's FP64 fields (160x160x96 grid) check the batch's FP32 fields of the same sources
+        f32 = b.fields32(sel.index(3) + 1).reshape(NSRC, -1)
+        acc = {"max_abs": 0.0, "sq_abs": 0.0, "n": 0, "max_rel": 0.0, "sq_rel": 0.0, "nrel": 0}
+
+        def check(k, tt):
+            d = np.abs(f32[k].astype(np.float64) - tt)
+            m = tt > 1e-3
+            rel = d[m] / tt[m]
+            acc["max_abs"] = max(acc["max_abs"], float(d.max()))
+            acc["sq_abs"] += float(np.dot(d, d))
+            acc["n"] += d.size
+            acc["max_rel"] = max(acc["max_rel"], float(rel.max()))
+            acc["sq_rel"] += float(np.dot(rel, rel))
+            acc["nrel"] += rel.size
+
+        v, dt, sample = cpu_reference(grids, steps=1, warmup=0, nthreads=os.cpu_count() or 1, check=check)
         cpu = {"value": v, "unit": "node-updates/s", "cores": os.cpu_count(), "kind": "port",
                "sample": sample}
+        batch_err = {"max_abs_s": acc["max_abs"], "rms_abs_s": (acc["sq_abs"] / acc["n"]) ** 0.5,
+                     "max_rel": acc["max_rel"], "rms_rel": (acc["sq_rel"] / acc["nrel"]) ** 0.5,
+                     "sample": "the FP32 batch fields of the baseline's %s, against its FP64 fields "
+                               "(relative figures over nodes more than 1 ms from the source)" % sample}
 
     b.finalize()            # the library holds one batch; the single-source section makes its own
     single = None
@@ -706,7 +730,7 @@ def main():
                            "node_updates_per_step": upd_total,
                            "l2": "fields 1.73 GB > L2 (inputs larger than L2)",
                            "parallelism": "replicas (one batch per GPU)" if world > 1 else "1 GPU"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "error_vs_fp64_oracle": batch_err,
                 "gpu_launches": 5 * args.steps, "clocks": clk.summary(), "locate": locate,
                 "single_source": single}
         print(json.dumps(line), flush=True)
