@@ -182,6 +182,25 @@ def test_batched_multi_grid(fk):
         b.finalize()
 
 
+def test_batch_rejects_nonpositive_velocity(fk):
+    """The batch checks velocities on the device (flag in mapped host
+    memory): a zero cell is refused, and the next valid model is accepted."""
+    n, h = (10, 12, 11), (20.0, 20.0, 20.0)
+    b = fk.Batch3D([(n[0], n[1], n[2], *h)], nsweep=1, eps=3.0, precision=4)
+    vel = np.full((n[0] - 1) * (n[1] - 1) * (n[2] - 1), 3000.0)
+    bad = vel.copy()
+    bad[123] = 0.0
+    with pytest.raises(fk.FteikError):
+        b.setVelocityModel(1, bad)
+    b.setVelocityModel(1, vel)
+    b.setSources(1, [0.0], [100.0], [100.0])
+    b.solve()
+    tt = b.field(1, 1)
+    ref = _oracle(n, h, vel, (0.0, 100.0, 100.0), nsweep=1, eps=3.0)
+    assert np.max(np.abs(tt - ref) / np.maximum(ref, 1e-6)) <= TOL32
+    b.finalize()
+
+
 def test_source_pairs_match_single_source_bitwise(fk):
     """The batch's Gauss-Seidel passes walk two sources of a grid in the
     same threads (sharing indices, slowness and barriers, not arithmetic),
