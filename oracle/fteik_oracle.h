@@ -24,7 +24,11 @@
  * gradient media, the locator's known true index, the index round trip) and
  * through an independent literal transcription of the level-set sweep
  * (tests/test_oracle_levelset.py) rather than against bit-level golden output
- * of the reference binary.
+ * of the reference binary.  The reference's own 2D check against a third-party
+ * 2D solver (testing/test2d.F90:25-87, within 1e-10) needs Fortran and that
+ * solver, neither of which is here, so it is not reproduced; the 2D solve is
+ * held to the analytic linear-gradient time (first-order convergence) and to
+ * the transcription instead.
  */
 #ifndef FTEIK_ORACLE_H
 #define FTEIK_ORACLE_H
