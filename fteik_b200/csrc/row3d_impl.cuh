@@ -305,8 +305,9 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
  * compile-time constants.  (Moving the two sources' row values as one 64-bit
  * shared-memory word instead measured 14 % slower.)  A missing second source
  * (odd number of sources on a grid) walks source 0's field without storing.
- * The node updates, their order and the waits are those of slab_sweep, so
- * the results are identical. */
+ * The nodes updated, their order and the waits are those of slab_sweep; the
+ * stencil is noinit_f32 (the contracted FP32 form), so a source gives the
+ * same bits whether it walks alone or paired. */
 template <bool RESID, int S, int CHP>
 __device__ __forceinline__ bool slab_pass_f32(const fk3tw::Params &P_, const fk_grid3d_t &g,
                                               float *const (&ttp)[S], const float *__restrict__ slow, int s,
