@@ -64,19 +64,6 @@ __device__ double init2(const Src2 &q, const Mesh2 &c, int sz, int sx, double tv
 {
     const double sgnrz = (double)sz, sgnrx = (double)sx;
     double t1d = dmin(tv + c.dz * sref1, te + c.dx * sref2);
-    /* tAnaD, localSolver.F90:74-112 */
-    double dz_ = ((double)iz - q.zsa) * c.dz, dx_ = ((double)ix - q.xsa) * c.dx;
-    double d0 = dz_ * dz_ + dx_ * dx_;
-    double t0c = 0.0, d0i_szero = 0.0;
-    if (d0 > 0.0) {
-        double sq = sqrt(d0);
-        t0c = q.szero * sq;
-        d0i_szero = q.szero / sq;
-    }
-    double tzc = d0i_szero * dz_, txc = d0i_szero * dx_;
-    double tauv = tv - tana2(q, c, iz - sz, ix);
-    double taue = te - tana2(q, c, iz, ix - sx);
-    double tauev = tev - tana2(q, c, iz - sz, ix - sx);
     double t1 = FK_HUGE, t2 = FK_HUGE, t3 = FK_HUGE;
     if (abs(iz - q.zsi) > q.eps || abs(ix - q.xsi) > q.eps) {
         if (tv <= te + c.dx * sref3 && te <= tv + c.dz * sref3 && te >= tev && tv >= tev) {
@@ -95,6 +82,20 @@ __device__ double init2(const Src2 &q, const Mesh2 &c, int sz, int sx, double tv
             t3 = tv + c.dz * sqrt(sref3 * sref3 - r * r);
         }
     } else {
+        /* tAnaD (localSolver.F90:74-112) and the perturbations, used only by
+         * the spherical operator near the source */
+        double dz_ = ((double)iz - q.zsa) * c.dz, dx_ = ((double)ix - q.xsa) * c.dx;
+        double d0 = dz_ * dz_ + dx_ * dx_;
+        double t0c = 0.0, d0i_szero = 0.0;
+        if (d0 > 0.0) {
+            double sq = sqrt(d0);
+            t0c = q.szero * sq;
+            d0i_szero = q.szero / sq;
+        }
+        double tzc = d0i_szero * dz_, txc = d0i_szero * dx_;
+        double tauv = tv - tana2(q, c, iz - sz, ix);
+        double taue = te - tana2(q, c, iz, ix - sx);
+        double tauev = tev - tana2(q, c, iz - sz, ix - sx);
         if (tv < te + c.dx * sref3 && te < tv + c.dz * sref3 && te >= tev && tv >= tev) {
             double ta = tauev + taue - tauv, tb = tauev - taue + tauv;
             double apoly = c.dz2i + c.dx2i;
