@@ -31,6 +31,24 @@ def test_library_exports_every_declared_symbol(fk):
         getattr(fk.lib(), s)
 
 
+def test_header_compiles_as_c_and_links(fk, tmp_path):
+    """A C caller: the public header compiles as C11 (gcc, warnings as
+    errors) and every function it declares resolves against the library at
+    link time.  Nothing is run."""
+    names = _declared()
+    src = tmp_path / "caller.c"
+    src.write_text('#include "fteik_b200.h"\n#include <stdio.h>\n'
+                   "int main(void)\n{\n    void (*const fns[])(void) = {\n" +
+                   "".join("        (void (*)(void))%s,\n" % n for n in names) +
+                   "    };\n    printf(\"%d\\n\", (int)(sizeof(fns) / sizeof(fns[0])));\n    return 0;\n}\n")
+    libdir = os.path.dirname(fteik_b200.LIB_PATH)
+    # the header needs nothing but the C standard library (no CUDA headers)
+    cmd = ["gcc", "-std=c11", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+           str(src), "-o", str(tmp_path / "caller"), "-L", libdir, "-lfteik_shared", "-Wl,-rpath," + libdir]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 def test_reference_python_wrapper_symbols_present(fk):
     """python/fteik3d.py, fteik2d.py and fteikAnalytic.py bind these at
     construction; every one must resolve."""
