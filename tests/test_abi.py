@@ -119,6 +119,31 @@ def test_host_validation(fk):
     assert L.fteik_h5io_initializeF(b"x.h5") == -1     # no model: h5io.F90:110-114
 
 
+def test_argument_checks_before_the_device(fk):
+    """Arguments the library refuses before touching a device."""
+    L = fk.lib()
+    ierr = ctypes.c_int(0)
+    L.locate_initialize(1, 65, 100, ctypes.byref(ierr))
+    assert ierr.value == 1                       # at most 64 tables per grid point
+    L.locate_initialize(0, 4, 100, ctypes.byref(ierr))
+    assert ierr.value == 1
+    for bad in (-1, 3):
+        L.fteik_b200_locate_setMethod(bad, ctypes.byref(ierr))
+        assert ierr.value == 1
+    L.fteik_b200_locate_setNorm(3, ctypes.byref(ierr))
+    assert ierr.value == 1
+    IA = ctypes.c_int * 1
+    DA = ctypes.c_double * 1
+    n, h = IA(10), DA(10.0)
+    args = (n, n, n, h, h, h)
+    for ngrid, nsweep, prec in ((0, 2, 4), (1, 2, 3), (1, -1, 4)):
+        ierr.value = 0
+        L.fteik_b200_batch3d_initialize(ngrid, *args, nsweep, ctypes.c_double(5.0), ctypes.c_double(-1.0), 0,
+                                        prec, ctypes.byref(ierr))
+        assert ierr.value == 1, (ngrid, nsweep, prec)
+    L.locate_finalize()
+
+
 def _no_gpu():
     try:
         import torch
