@@ -4,7 +4,7 @@
  * the GPU by these kernels (no library GEMM).
  *
  * The network has no counterpart in the reference; it ranks grid points for
- * the pruned grid search and is judged by the exhaustive search.
+ * the pruned grid search and is checked against the exhaustive search.
  *
  * GEMM: C[M][N] = sum_k A(m,k) B(k,n) (+ bias[n]) in FP32 on the CUDA cores,
  * 128 x 64 output tiles, K in steps of 16 through shared memory, 8 x 4

@@ -1,5 +1,5 @@
 """L1 grid search (locate norm 1) against the FP64 exhaustive L1 search of the
-CPU oracle.  The reference has no L1 misfit (parity is judged by the FP64
+CPU oracle.  The reference has no L1 misfit (parity is measured against the FP64
 search only)."""
 import numpy as np
 import pytest

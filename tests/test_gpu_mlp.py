@@ -1,6 +1,6 @@
 """Surrogate network on the GPU against the FP64 CPU oracle
 (oracle/mlp_oracle.py), and the surrogate-pruned grid search (locate
-method 2) against the exhaustive tensor-core search (method 1), its judge."""
+method 2) against the exhaustive tensor-core search (method 1), its reference."""
 import os
 import sys
 

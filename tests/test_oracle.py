@@ -128,7 +128,7 @@ def test_oracle_source_snap_rules():
 
 
 def test_mlp_oracle_gradient_matches_finite_differences():
-    """The FP64 network oracle (the judge of the GPU gradients) is pinned by
+    """The FP64 network oracle (the reference for the GPU gradients) is pinned by
     central differences of its own loss."""
     import sys, os
     sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
@@ -150,7 +150,7 @@ def test_mlp_oracle_gradient_matches_finite_differences():
 
 
 def test_l1_oracle_matches_numpy():
-    """The FP64 L1 search of the oracle (judge of the GPU L1 search) against a
+    """The FP64 L1 search of the oracle (the reference for the GPU L1 search) against a
     direct numpy evaluation on a small grid, with a skipped pick."""
     rng = np.random.default_rng(3)
     ntf, ngrd = 9, 500
