@@ -3,8 +3,8 @@
  *
  * A plain-C restatement of the reference fteik algorithms for the eikonal
  * solver and the grid-search locator.  Every function cites the reference
- * file:line it follows.  It is the checker for the CUDA product and the CPU
- * baseline timed beside it; the product never calls it.
+ * file:line it follows.  It is the oracle the CUDA product is tested
+ * against and the CPU baseline timed beside it; the product never calls it.
  */
 #include "fteik_oracle.h"
 
