@@ -2,10 +2,10 @@
  * fteik_oracle.h -- TEST INFRASTRUCTURE ONLY.
  *
  * CPU restatement of the reference fteik hot path (bakerb845/fteik), used as
- * the oracle the CUDA product is tested against and as the timed CPU baseline.  Nothing in
- * the product library links or calls this code: only tests/, the smoke check
- * in __graft_entry__.py and the cpu_baseline / reference legs of bench.py load
- * it (through ctypes).
+ * the oracle the CUDA product is tested against and as the timed CPU
+ * baseline.  Nothing in the product library links or calls this code: only
+ * tests/, the smoke check in __graft_entry__.py and the cpu_baseline /
+ * reference legs of bench.py load it (through ctypes).
  *
  * Precision follows the reference: the eikonal solvers are FP64, the locator
  * objective is FP32 with the reference's accumulation order.  The file is
