@@ -241,7 +241,7 @@ def test_batched_converged(fk):
     b.finalize()
 
 
-def test_config2_converged_accuracy(fk):
+def test_layered_128cubed_converged_accuracy(fk):
     """128^3, h = 25 m, 4 layers x (1 + 0.05 GRF), interior off-grid source,
     solved to convergence: FP32 GPU vs the FP64 oracle, relative error
     <= 1e-4 at every node."""
