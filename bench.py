@@ -150,7 +150,25 @@ class Clocks:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons}
 
 
-def cpu_reference(grids, steps, warmup, nthreads, sample_src=24, check=None):
+CPU_SAMPLE_SRC = 24     # sources of the 160x160x96 grid per CPU step (a few seconds of FP64 work)
+
+
+def cpu_steps(args):
+    """Warm-up solves and timed steps of the CPU baseline: the same in the
+    reference arm and in the line's cpu_baseline, so the two agree."""
+    return max(1, min(args.warmup, 3)), min(max(1, args.steps), 3)
+
+
+def config_dict(grids, world):
+    return {"workload": "batched tables: 64 surface sources x %d grids (%s), h=50 m, v(z)=3000+0.5z" % (
+                len(grids), ", ".join("%dx%dx%d" % (g["nx"], g["ny"], g["nz"]) for g in grids)),
+            "nsweep": NSWEEP, "eps": EPS, "work_items": NSRC * len(grids),
+            "node_updates_per_step": sum(node_updates(g) for g in grids),
+            "l2": "fields 1.73 GB > L2 (inputs larger than L2)",
+            "parallelism": "replicas (one batch per GPU)" if world > 1 else "1 GPU"}
+
+
+def cpu_reference(grids, steps, warmup, nthreads, sample_src=CPU_SAMPLE_SRC, check=None):
     """CPU restatement of the reference (oracle/), timed on a bounded sample:
     `sample_src` sources on the 160x160x96 grid per step.  check(k, tt), if
     given, receives each source's FP64 field outside the timed solves."""
@@ -166,8 +184,8 @@ def cpu_reference(grids, steps, warmup, nthreads, sample_src=24, check=None):
         si_sa.append((si, sa))
         ni, npass = O.count_updates3d(n, si)
         upd += ni + NSWEEP * npass
-    for _ in range(warmup):
-        O.solve3d(n, (H, H, H), slow, *si_sa[0], EPS, NSWEEP, level_set=True, nthreads=nthreads)
+    for w in range(warmup):
+        O.solve3d(n, (H, H, H), slow, *si_sa[w % len(si_sa)], EPS, NSWEEP, level_set=True, nthreads=nthreads)
     dt = 0.0
     for _ in range(steps):
         for k, (si, sa) in enumerate(si_sa):
@@ -176,8 +194,9 @@ def cpu_reference(grids, steps, warmup, nthreads, sample_src=24, check=None):
             dt += time.perf_counter() - t0
             if check is not None:
                 check(k, tt)
-    return upd * steps / dt, dt, "%d source(s) on the %dx%dx%d grid per step, %d step(s)" % (
-        sample_src, g["nx"], g["ny"], g["nz"], steps)
+    return upd * steps / dt, dt, ("%d source(s) on the %dx%dx%d grid per step, %d step(s) after %d "
+                                   "warm-up solve(s); node-updates/s of that sample" % (
+                                       sample_src, g["nx"], g["ny"], g["nz"], steps, warmup))
 
 
 def init_updates3d(n, si):
@@ -362,6 +381,38 @@ def single_cpu_baselines(c1, c2, nthreads):
     c2["error_vs_fp64_oracle"] = field_errors(c2["_field"], tt3)
 
 
+def layered_grf_batch_error(fk, grids, nsrc=8):
+    """The batch's FP32 fields on the other reading of the batch's velocity
+    recipe -- four layers (3000 / 4000 / 5000 / 6000 m/s, seeded interfaces)
+    times (1 + 0.05 GRF, 10-cell correlation length, seed 2) -- on the
+    160x160x96 grid, for the first `nsrc` of the batch's surface sources,
+    against the FP64 oracle's fields of the same solves."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    from models import layered_grf_cells
+    g = next(g for g in grids if (g["nx"], g["ny"], g["nz"]) == (160, 160, 96))
+    n = (g["nz"], g["nx"], g["ny"])
+    vel = layered_grf_cells(*n, seed=2)
+    b = fk.Batch3D([(n[0], n[1], n[2], H, H, H)], nsweep=NSWEEP, eps=EPS, precision=4)
+    b.setVelocityModel(1, vel)
+    b.setSources(1, g["zs"][:nsrc], g["xs"][:nsrc], g["ys"][:nsrc])
+    b.solve()
+    f32 = b.fields32(1).reshape(nsrc, -1)
+    b.finalize()
+    slow = (1.0 / vel).ravel()
+    errs = []
+    for k in range(nsrc):
+        si, sa = O.source_snap(True, n, (0, 0, 0), (H, H, H), (g["zs"][k], g["xs"][k], g["ys"][k]))
+        tt, _ = O.solve3d(n, (H, H, H), slow, si, sa, EPS, NSWEEP, level_set=True, nthreads=os.cpu_count() or 1)
+        errs.append(field_errors(f32[k], tt))
+    out = {key: (max if key.startswith("max") else lambda v: float(np.sqrt(np.mean(np.square(v)))))(
+        [e[key] for e in errs]) for key in errs[0]}
+    out["sample"] = ("%d surface sources of the batch on the 160x160x96 grid, velocity 4 layers x "
+                     "(1 + 0.05 GRF), FP32 batch fields against FP64 oracle solves (relative figures "
+                     "over nodes more than 1 ms from the source)" % nsrc)
+    return out
+
+
 def max_over_ranks(x, dist):
     """The slowest rank's value of a per-rank time (every rank gets it); x
     itself without a process group.  NCCL reduces on the GPU, gloo on the
@@ -380,14 +431,14 @@ def run_reference(args, rank, world):
     nth = os.cpu_count() or 1
     if rank != 0:
         return
-    steps = min(max(1, args.steps), 3)      # each timed step: 24 FP64 solves, a few seconds
-    warmup = max(0, args.warmup)            # each warm-up step: one solve
+    warmup, steps = cpu_steps(args)        # each timed step: 24 FP64 solves, a few seconds
     value, dt, sample = cpu_reference(grids, steps=steps, warmup=warmup, nthreads=nth)
+    cfg = config_dict(grids, 1)
+    cfg["cpu_sample"] = sample
     line = {"metric": METRIC, "value": value, "unit": "node-updates/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": steps, "warmup": warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": "batched tables: 64 surface sources x 4 grids, h=50 m", "nsweep": NSWEEP},
+            "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": value, "unit": "node-updates/s", "cores": nth, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "node-updates/s", "h2d_bytes_per_step": 0,
@@ -690,7 +741,12 @@ def main():
         f32 = b.fields32(sel.index(3) + 1).reshape(NSRC, -1)
         acc = {"max_abs": 0.0, "sq_abs": 0.0, "n": 0, "max_rel": 0.0, "sq_rel": 0.0, "nrel": 0}
 
+        seen = set()
+
         def check(k, tt):
+            if k in seen:          # every timed step solves the same sample
+                return
+            seen.add(k)
             d = np.abs(f32[k].astype(np.float64) - tt)
             m = tt > 1e-3
             rel = d[m] / tt[m]
@@ -701,7 +757,8 @@ def main():
             acc["sq_rel"] += float(np.dot(rel, rel))
             acc["nrel"] += rel.size
 
-        v, dt, sample = cpu_reference(grids, steps=1, warmup=0, nthreads=os.cpu_count() or 1, check=check)
+        cw, cs = cpu_steps(args)
+        v, dt, sample = cpu_reference(grids, steps=cs, warmup=cw, nthreads=os.cpu_count() or 1, check=check)
         cpu = {"value": v, "unit": "node-updates/s", "cores": os.cpu_count(), "kind": "port",
                "sample": sample}
         batch_err = {"max_abs_s": acc["max_abs"], "rms_abs_s": (acc["sq_abs"] / acc["n"]) ** 0.5,
@@ -709,7 +766,10 @@ def main():
                      "sample": "the FP32 batch fields of the baseline's %s, against its FP64 fields "
                                "(relative figures over nodes more than 1 ms from the source)" % sample}
 
-    b.finalize()            # the library holds one batch; the single-source section makes its own
+    b.finalize()            # the library holds one batch; the sections below make their own
+    grf_err = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and 3 in sel:
+        grf_err = layered_grf_batch_error(fk, grids)
     single = None
     if rank == 0 and world == 1 and not args.no_single:
         c1 = bench_single_2d(fk)
@@ -724,13 +784,9 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
-                "config": {"workload": "batched tables: 64 surface sources x 4 grids "
-                           "(96x96x64, 128x128x80, 160x160x96, 200x120x100), h=50 m, v(z)=3000+0.5z",
-                           "nsweep": NSWEEP, "eps": EPS, "work_items": NSRC * len(grids),
-                           "node_updates_per_step": upd_total,
-                           "l2": "fields 1.73 GB > L2 (inputs larger than L2)",
-                           "parallelism": "replicas (one batch per GPU)" if world > 1 else "1 GPU"},
+                "config": config_dict(grids, world),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "error_vs_fp64_oracle": batch_err,
+                "error_vs_fp64_oracle_layered_grf": grf_err,
                 "gpu_launches": 5 * args.steps, "clocks": clk.summary(), "locate": locate,
                 "single_source": single}
         print(json.dumps(line), flush=True)

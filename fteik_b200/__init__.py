@@ -45,6 +45,9 @@ _SIGS = {
     "fteik_model_setVelocityModel64f": [c_int, _PD, _PI],
     "fteik_model_setNodalVelocityModel64f": [c_int, c_int, _PD, _PI],
     "fteik_model_setCellVelocityModel64f": [c_int, c_int, _PD, _PI],
+    "fteik_model_setVelocityModel32f": [c_int, _PF, _PI],
+    "fteik_model_getVelocityModel64f": [c_int, _PI, _PD, _PI],
+    "fteik_model_isModel3D": [POINTER(c_bool), _PI],
     "fteik_model_grid2indexF": [c_int] * 5,
     "fteik_model_grid2index": [c_int] * 5,
     "fteik_model_index2gridF": [c_int, _PI, _PI, _PI, _PI],
@@ -55,11 +58,13 @@ _SIGS = {
     "fteik_source_getSolverInfo64fF": [c_int, _PI, _PI, _PI, _PD, _PD, _PD, _PD, _PD, _PI],
     "fteik_source_getNumberOfSources": [_PI, _PI],
     "fteik_source_free": [],
+    "fteik_source_setVerbosity": [c_int],
     # receiver.F90
     "fteik_receiver_initialize64f": [c_int, _PD, _PD, _PD, c_int, _PI],
     "fteik_receiver_getTravelTimes64f": [c_int, c_int, _PD, _PD, _PI],
     "fteik_receiver_getNumberOfReceivers": [_PI, _PI],
     "fteik_receiver_free": [],
+    "fteik_receiver_setVerbosity": [c_int],
     # solver3D.F90
     "fteik_solver3d_initialize": [c_int, c_int, c_int] + [c_double] * 6 + [c_int, c_double, c_double, c_int, _PI],
     "fteik_solver3d_free": [],
@@ -109,6 +114,7 @@ _SIGS = {
     "fteik_analytic_getTravelTimesConstantVel64f": [c_int, _PD, _PI],
     "fteik_analytic_getTravelTimesGradientVel64f": [c_int, _PD, _PI],
     "fteik_analytic_free": [],
+    "fteik_analytic_setVerbosity": [c_int],
     # locate.F90
     "locate_initialize": [c_int, c_int, c_int, _PI],
     "locate_finalize": [],
@@ -121,6 +127,10 @@ _SIGS = {
     "fteik_b200_version": [],
     "fteik_b200_device": [],
     "fteik_b200_stream": [],
+    "fteik_b200_setSpinLimit": [c_longlong, _PI],
+    "fteik_b200_getSpinLimit": [POINTER(c_longlong)],
+    "fteik_b200_setSlabConfig": [c_int, c_int, c_int, c_int, _PI],
+    "fteik_b200_getSlabConfig": [_PI, _PI, _PI, _PI],
     "fteik_b200_solver3d_setPrecision": [c_int, _PI],
     "fteik_b200_solver3d_getSolveInfo": [_PD, _PI, _PI],
     "fteik_b200_batch3d_initialize": [c_int, _PI, _PI, _PI, _PD, _PD, _PD, c_int, c_double, c_double,
@@ -228,6 +238,28 @@ def _i(a):
 
 class FteikError(RuntimeError):
     pass
+
+
+def set_spin_limit(polls):
+    """Poll limit of the 3D sweeps' bounded device-side waits (< 0: the
+    default); returns the previous limit."""
+    old = c_longlong(0)
+    lib().fteik_b200_getSpinLimit(byref(old))
+    ierr = c_int(1)
+    lib().fteik_b200_setSpinLimit(int(polls), byref(ierr))
+    _check(ierr, "fteik_b200_setSpinLimit")
+    return old.value
+
+
+def set_slab_config(staged=-1, pairs=-1, progress=-1, blocks_per_sm=-1):
+    """Launch configuration of the 3D sweep kernels (-1: the library's
+    choice); returns the previous (staged, pairs, progress, blocks_per_sm)."""
+    old = [c_int() for _ in range(4)]
+    lib().fteik_b200_getSlabConfig(*[byref(v) for v in old])
+    ierr = c_int(1)
+    lib().fteik_b200_setSlabConfig(int(staged), int(pairs), int(progress), int(blocks_per_sm), byref(ierr))
+    _check(ierr, "fteik_b200_setSlabConfig")
+    return tuple(v.value for v in old)
 
 
 def _check(ierr, what):

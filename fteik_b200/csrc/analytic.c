@@ -18,6 +18,8 @@ static struct {
     double *tt;        /* device, natural order */
 } SA = {.vconst = 5.0e3, .vtop = 5.0e3, .vbottom = 5.0e3};
 
+void fteik_analytic_setVerbosity(int verbose) { SA.verbose = verbose; }
+
 void fteik_analytic_free(void)
 {
     fk_dfree(SA.tt);

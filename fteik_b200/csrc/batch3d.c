@@ -4,14 +4,16 @@
  * solver3D.F90:1156-1243, and callers loop over sources,
  * python/fteik3d.py:258-263).
  *
- * Every (grid, source) pair becomes one work item; one kernel launch solves
- * them all, one CTA per item, largest grids first.  The launch is captured
- * once into a CUDA graph and replayed while the work list is unchanged.
+ * Every (grid, source) pair becomes one work item; one persistent kernel
+ * launch runs the initialisation sweeps of them all and one more runs their
+ * Gauss-Seidel passes, slab tasks of every item interleaved (row3d_impl.cuh).
+ * The launches are captured once into a CUDA graph and replayed while the
+ * work list is unchanged.
  * Fields stay on the device until exported.
  */
 #include "host_common.h"
 #include "fteik_b200.h"
-#include "tileplan.h"
+#include "slabplan.h"
 
 #include <stdlib.h>
 #include <string.h>
@@ -22,6 +24,7 @@ typedef struct {
     double *vel_dev;        /* device FP64 cell velocities, natural order */
     double *szero;          /* host [nsrc]: slowness of each source's cell */
     void *slow_dev;         /* device padded, batch precision */
+    float *slowz_dev;       /* FP32: node-indexed slowness copies (fk_grid3d_t.slowz) */
     bool have_model;
     int nsrc;
     int *zsi, *xsi, *ysi;
@@ -48,10 +51,9 @@ static struct {
     fk_result3d_t *res_host;
     int nwork, max_nx, max_nz;
     int *work_order;        /* work item -> (grid, src) packed as grid<<20|src */
-    int *groups_dev;        /* [ngroups][S] work items walked together */
-    int ngroups, S;
-    fk_tileplan_t plan;     /* tile-wavefront schedule */
-    bool walker;
+    fk_slabplan_t plan;     /* slab-pipelined schedule */
+    int spin_epoch;         /* poll limit the plan (and graph) was built with */
+    int cfg_epoch;          /* slab configuration the plan (and graph) was built with */
     bool work_dirty;        /* source positions changed, shape unchanged */
     cudaGraphExec_t graph;
     bool graph_ok;
@@ -108,7 +110,8 @@ static void free_grid(bgrid_t *g)
 {
     free(g->szero); free(g->zsi); free(g->xsi); free(g->ysi);
     free(g->zsa); free(g->xsa); free(g->ysa);
-    fk_dfree(g->vel_dev); fk_dfree(g->slow_dev); fk_dfree(g->fields); fk_dfree(g->ri_dev); fk_dfree(g->rd_dev);
+    fk_dfree(g->vel_dev); fk_dfree(g->slow_dev); fk_dfree(g->slowz_dev); fk_dfree(g->fields);
+    fk_dfree(g->ri_dev); fk_dfree(g->rd_dev);
     fk_dfree(g->dl_buf);
     if (g->have_dl_ev) { cudaEventDestroy(g->dl_ready); cudaEventDestroy(g->dl_done); }
     memset(g, 0, sizeof(*g));
@@ -128,9 +131,8 @@ void fteik_b200_batch3d_finalize(void)
     for (int i = 0; i < SB.ngrid; i++) free_grid(&SB.g[i]);
     free(SB.g);
     fk_dfree(SB.grids_dev); fk_dfree(SB.work_dev); fk_dfree(SB.res_dev); fk_dfree(SB.export_buf);
-    fk_dfree(SB.groups_dev);
     fk_dfree(SB.stage);
-    fk_tileplan_free(&SB.plan);
+    fk_slabplan_free(&SB.plan);
     if (SB.have_ev) for (int i = 0; i < 3; i++) cudaEventDestroy(SB.ev[i]);
     free(SB.res_host); free(SB.work_order);
     if (SB.hmap) cudaFreeHost(SB.hmap);
@@ -156,11 +158,6 @@ void fteik_b200_batch3d_initialize(int ngrid, const int nz[], const int nx[], co
         bgrid_t *g = &SB.g[i];
         if (nz[i] < 3 || nx[i] < 3 || ny[i] < 3 || dz[i] <= 0 || dx[i] <= 0 || dy[i] <= 0) {
             FK_ERR("fteik_b200_batch3d_initialize: grid %d needs n >= 3 and h > 0", i + 1);
-            *ierr = 1;
-            return;
-        }
-        if (fk_schedule_walker() && nx[i] > 1024) {
-            FK_ERR("fteik_b200_batch3d_initialize: grid %d has nx=%d > 1024, the walker's limit", i + 1, nx[i]);
             *ierr = 1;
             return;
         }
@@ -213,6 +210,14 @@ void fteik_b200_batch3d_setVelocityModel64f(int igrid, int ncell, const double v
     if (!e) e = (int)cudaMemcpyAsync(g->vel_dev, vel, sizeof(double) * (size_t)ncell, cudaMemcpyHostToDevice, s);
     if (!e) e = fk_pack_velocity(SB.precision, g->nz, g->nx, g->ny, g->zcp, g->vel_dev, g->slow_dev,
                                  (int *)bad_dev, s);
+    if (!e && SB.precision == 4) {
+        /* node-indexed copies for the staged pass step */
+        if (!g->slowz_dev)
+            g->slowz_dev = (float *)fk_dalloc(sizeof(float) * 2 * (size_t)g->zp * (g->nx - 1) * (g->ny - 1), who);
+        e = g->slowz_dev ? fk_node_slowness_f32(g->nz, g->nx, g->ny, g->zcp, g->zp, (const float *)g->slow_dev,
+                                                g->slowz_dev, s)
+                         : 1;
+    }
     if (!e) e = (int)cudaStreamSynchronize(s);
     if (fk_check(e, who)) return;
     if (*bad) { FK_ERR("%s: velocities must be positive", who); return; }
@@ -381,33 +386,15 @@ static int build_work(const char *who)
         gh[i].zp = g->zp; gh[i].zcp = g->zcp;
         gh[i].dz = g->dz; gh[i].dx = g->dx; gh[i].dy = g->dy;
         gh[i].slow = g->slow_dev;
+        gh[i].slowz = g->slowz_dev;
         for (int s = 0; s < g->nsrc; s++) SB.work_order[k++] = (i << 20) | s;
     }
     qsort(SB.work_order, (size_t)nwork, sizeof(int), cmp_work);
     SB.nwork = nwork;
     fill_work(wh);
-    /* groups of S consecutive work items of the same grid (work items are
-     * sorted by grid, so a group never spans two grids) */
-    const int S = fk3d_pick_s(SB.precision, max_nx, max_nz, nwork);
-    int *gr = (int *)malloc(sizeof(int) * (size_t)nwork * S);
-    int ng = 0;
-    for (int w = 0; w < nwork;) {
-        const int gi = SB.work_order[w] >> 20;
-        for (int k = 0; k < S; k++) {
-            if (w < nwork && (SB.work_order[w] >> 20) == gi) gr[ng * S + k] = w++;
-            else gr[ng * S + k] = -1;
-        }
-        ng++;
-    }
-    fk_dfree(SB.groups_dev);
-    SB.groups_dev = (int *)fk_dalloc(sizeof(int) * (size_t)ng * S, who);
-    int e = SB.groups_dev ? 0 : 1;
-    if (!e) e = (int)fk_h2d(SB.groups_dev, gr, sizeof(int) * (size_t)ng * S);
-    if (!e) e = (int)fk_h2d(SB.grids_dev, gh, sizeof(fk_grid3d_t) * (size_t)SB.ngrid);
+    int e = (int)fk_h2d(SB.grids_dev, gh, sizeof(fk_grid3d_t) * (size_t)SB.ngrid);
     if (!e) e = (int)fk_h2d(SB.work_dev, wh, sizeof(fk_work3d_t) * (size_t)nwork);
-    free(gr);
-    SB.walker = fk_schedule_walker();
-    if (!e && !SB.walker) {
+    if (!e) {
         int *wnx = (int *)malloc(sizeof(int) * (size_t)nwork);
         int *wny = (int *)malloc(sizeof(int) * (size_t)nwork);
         int *wnz = (int *)malloc(sizeof(int) * (size_t)nwork);
@@ -419,7 +406,13 @@ static int build_work(const char *who)
             wg[w] = wh[w].grid;
         }
         const int np = (SB.conv_tol >= 0.0 && SB.max_pass > 0) ? SB.max_pass : SB.nsweep;
-        e = fk_tileplan_build(&SB.plan, nwork, wnx, wny, wnz, wg, np, who);
+        const fk_slabcfg_t cfg = fk_slabcfg();
+        e = fk_slabplan_build(&SB.plan, nwork, wnx, wny, wnz, wg, np, cfg.pairs != 0, who);
+        SB.plan.dev.staged = SB.precision == 4 && cfg.staged == 1;
+        SB.plan.dev.progress = cfg.progress > 0 ? cfg.progress : 0;
+        SB.plan.dev.blocks_per_sm = cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 0;
+        SB.spin_epoch = fk_spin_epoch();
+        SB.cfg_epoch = fk_slabcfg_epoch();
         free(wnx);
         free(wny);
         free(wnz);
@@ -430,8 +423,6 @@ static int build_work(const char *who)
     SB.nwork = nwork;
     SB.max_nx = max_nx;
     SB.max_nz = max_nz;
-    SB.S = S;
-    SB.ngroups = ng;
     return fk_check(e, who);
 }
 
@@ -444,22 +435,16 @@ void fteik_b200_batch3d_solve(int *ierr)
     if (SB.graph_ok && SB.work_dirty) {
         if (upload_work(who)) return;
     }
+    if (SB.graph_ok && (SB.spin_epoch != fk_spin_epoch() || SB.cfg_epoch != fk_slabcfg_epoch()))
+        invalidate();   /* new poll limit or launch configuration */
     if (!SB.graph_ok) {
         if (build_work(who)) return;
         SB.work_dirty = false;
-        /* warm the kernel attributes outside capture, then capture */
         cudaGraph_t graph;
-        int e = SB.walker ? fk3d_prepare(SB.precision, SB.max_nx, SB.max_nz, SB.S) : 0;
-        if (!e) e = (int)cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        int e = (int)cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (!e) {
-            int le;
-            if (SB.walker)
-                le = fk3d_solve(SB.precision, SB.grids_dev, SB.work_dev, SB.groups_dev, SB.ngroups,
-                                SB.S, SB.res_dev, SB.nwork, SB.max_nx, SB.max_nz, SB.eps, SB.nsweep,
-                                SB.conv_tol, SB.max_pass, s);
-            else
-                le = fk3d_solve_tiles(SB.precision, SB.grids_dev, SB.work_dev, SB.nwork, &SB.plan.dev,
-                                      SB.res_dev, SB.eps, SB.nsweep, SB.conv_tol, SB.max_pass, s);
+            const int le = fk3d_solve_slabs(SB.precision, SB.grids_dev, SB.work_dev, SB.nwork, &SB.plan.dev,
+                                            SB.res_dev, SB.eps, SB.nsweep, SB.conv_tol, SB.max_pass, s);
             e = (int)cudaStreamEndCapture(s, &graph);
             if (!e) e = le;
         }
@@ -670,7 +655,7 @@ void fteik_b200_batch3d_timeSolve(float *init_ms, float *pass_ms, int *ierr)
     const char *who = "fteik_b200_batch3d_timeSolve";
     *init_ms = *pass_ms = 0.0f;
     *ierr = 1;
-    if (!SB.graph_ok || SB.walker) { FK_ERR("%s: solve once first (tile schedule)", who); return; }
+    if (!SB.graph_ok) { FK_ERR("%s: solve once first", who); return; }
     if (SB.work_dirty && upload_work(who)) return;
     if (!SB.have_ev) {
         bool ok = true;
@@ -679,10 +664,10 @@ void fteik_b200_batch3d_timeSolve(float *init_ms, float *pass_ms, int *ierr)
         if (!ok) { FK_ERR("%s: cannot create events", who); return; }
     }
     cudaStream_t s = fk_stream();
-    fk3d_tiles_set_events(SB.ev);
-    int e = fk3d_solve_tiles(SB.precision, SB.grids_dev, SB.work_dev, SB.nwork, &SB.plan.dev,
+    fk3d_slabs_set_events(SB.ev);
+    int e = fk3d_solve_slabs(SB.precision, SB.grids_dev, SB.work_dev, SB.nwork, &SB.plan.dev,
                              SB.res_dev, SB.eps, SB.nsweep, SB.conv_tol, SB.max_pass, s);
-    fk3d_tiles_set_events(NULL);
+    fk3d_slabs_set_events(NULL);
     if (!e) e = (int)cudaEventSynchronize(SB.ev[2]);
     if (!e) e = (int)cudaEventElapsedTime(init_ms, SB.ev[0], SB.ev[1]);
     if (!e) e = (int)cudaEventElapsedTime(pass_ms, SB.ev[1], SB.ev[2]);

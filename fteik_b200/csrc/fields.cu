@@ -315,6 +315,32 @@ extern "C" int fk_pack_slowness(int precision, int is3d, int nz, int nx, int ny,
     return (int)cudaGetLastError();
 }
 
+/* Cell slowness re-indexed by node z: out[c][iz] = slow[c][min(iz, nz-2)]
+ * (copy 0) and slow[c][max(iz-1, 0)] (copy 1) for iz < zp (the padding
+ * repeats the last cell), columns c over (ny-1)(nx-1). */
+__global__ void node_slowness_kernel(int nz, int ncol, int zcp, int zp, const float *__restrict__ slow,
+                                     float *__restrict__ out)
+{
+    const size_t n = (size_t)ncol * zp;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int iz = (int)(e % zp);
+        const size_t c = e / zp;
+        const int up = min(iz, nz - 2), dn = min(max(iz - 1, 0), nz - 2);
+        out[e] = slow[c * zcp + up];
+        out[n + e] = slow[c * zcp + dn];
+    }
+}
+
+extern "C" int fk_node_slowness_f32(int nz, int nx, int ny, int zcp, int zp, const float *slow_dev,
+                                    float *slowz_dev, cudaStream_t s)
+{
+    const int ncol = (nx - 1) * (ny - 1);
+    const size_t n = (size_t)ncol * zp;
+    node_slowness_kernel<<<nblocks(n), 256, 0, s>>>(nz, ncol, zcp, zp, slow_dev, slowz_dev);
+    return (int)cudaGetLastError();
+}
+
 extern "C" int fk_pack_velocity(int precision, int nz, int nx, int ny, int zcp, const double *vel_nat,
                                 void *slow_dev, int *bad_dev, cudaStream_t s)
 {

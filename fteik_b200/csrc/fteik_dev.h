@@ -27,6 +27,11 @@ typedef struct {
     int zp, zcp;          /* field / slowness z pitches (elements) */
     double dz, dx, dy;
     const void *slow;     /* device: float (FP32 solve) or double (FP64 solve) */
+    /* FP32 solve, optional: the cell slowness re-indexed by node z for the
+     * staged pass step, [2][ny-1][nx-1][zp]: copy 0 holds at node iz the
+     * cell min(iz, nz-2) (the z-downwind cell of ascending sweeps), copy 1
+     * the cell max(iz-1, 0) (descending sweeps); NULL when not built */
+    const float *slowz;
 } fk_grid3d_t;
 
 /* One (grid, source) work item. */
@@ -45,73 +50,48 @@ typedef struct {
     int status;           /* 0 ok */
 } fk_result3d_t;
 
-/* Solve every work item: field initialisation, 8 initialisation sweeps, then
- * nsweep passes of 8 sweeps (or, when conv_tol >= 0 and max_pass > 0,
- * passes until a pass changes no node by more than conv_tol).
- * precision: 4 (FP32 field, FP64 near-source stencil) or 8 (FP64 field).
- * groups: device [ngroups][S] work indices of one grid each (-1 = empty);
- * the passes run one group per CTA, S (1 or 2, see fk3d_pick_s) sources
- * walking together.  grids/work/results are device arrays.  Returns a
- * cudaError_t. */
-int fk3d_solve(int precision, const fk_grid3d_t *grids, const fk_work3d_t *work,
-               const int *groups, int ngroups, int S, fk_result3d_t *results, int nwork,
-               int max_nx, int max_nz, double eps, int nsweep, double conv_tol,
-               int max_pass, cudaStream_t stream);
-
-/* Sources per CTA for the passes: 2 when the shared memory allows it and
- * there are at least as many work items as SMs, else 1. */
-int fk3d_pick_s(int precision, int max_nx, int max_nz, int nwork);
-
-/* Set the kernel attributes a later fk3d_solve needs (call before a CUDA
- * graph capture of fk3d_solve). */
-int fk3d_prepare(int precision, int max_nx, int max_nz, int S);
-
-/* Dynamic shared memory of the initialisation kernel for these sizes. */
-size_t fk3d_smem_bytes(int precision, int max_nx, int max_nz);
-
-/* Plan of a tiled or row-pipelined 3D solve (device buffers; see
- * tile3d_impl.cuh and row3d_impl.cuh).  Tiles: tasks are one sweep's tile
- * tasks as int pairs {work, by' * ntx + bx'} ordered by tile level bx' + by',
- * done[] one counter per tile.  Rows: tasks are slabs of FK_SLAB_Y rows,
- * {work, j'} ordered by the logical slab j', done[] one counter per slab.  done_base: each work item's first counter;
- * the other buffers are scratch sized as noted. */
+/* Plan of a slab-pipelined 3D solve (device buffers; see row3d_impl.cuh):
+ * tasks are slabs of FK_SLAB_Y y-rows, {work, j'} ordered by the logical
+ * slab j', done[] one progress counter per slab, done_base each work item's
+ * first counter; the other buffers are scratch sized as noted. */
 typedef struct {
     const int *tasks;              /* 2 * ntask_sweep ints */
     const int *done_base;          /* nwork */
-    int ntask_sweep, ntiles_total;
-    int *done;                     /* ntiles_total */
+    int ntask_sweep, nslab_total;
+    int *done;                     /* nslab_total */
     unsigned long long *tickets;   /* 2 */
     int *error;                    /* 1 */
     unsigned long long *resid;     /* nwork * max(npass, 1) */
-    int *pass_tiles;               /* nwork * max(npass, 1) */
+    int *pass_slabs;               /* nwork * max(npass, 1) */
     int *conv_pass;                /* nwork */
     long long spin_limit;          /* bounded waits: polls before giving up */
-    int kind;                      /* FK_PLAN_TILES or FK_PLAN_ROWS */
     int max_nx, max_ny, max_nz;    /* largest grid of the plan */
-    /* FK_PLAN_ROWS: the Gauss-Seidel passes run sources of one grid in pairs
+    /* the Gauss-Seidel passes run sources of one grid in pairs
      * (NULL: one source per task); pairs[2 p + i] work items (-1: none),
      * tasks2 {pair, j'} ordered by j' */
     const int *pairs;
     const int *tasks2;
     int ntask2_sweep;
-} fk_tiles3d_t;
+    /* launch configuration: FP32 passes in the staged pass step (every
+     * grid's slowz built); progress step of the passes (8, 32 or 0 = by the
+     * number of slab tasks); resident blocks per SM (0 = as many as fit) */
+    int staged, progress, blocks_per_sm;
+} fk_slabs3d_t;
 
-#define FK_PLAN_TILES 0            /* 32 x 8 column tiles, one block per task */
-#define FK_PLAN_ROWS 1             /* FK_SLAB_Y y-rows over the whole x extent per task */
 #define FK_SLAB_Y 4
 
-#define FK_TILE_X 32
-#define FK_TILE_Y 8
-
-/* Tiled or row-pipelined solve of every work item (per plan->kind; same
- * semantics as fk3d_solve). */
-int fk3d_solve_tiles(int precision, const fk_grid3d_t *grids, const fk_work3d_t *work,
-                     int nwork, const fk_tiles3d_t *plan, fk_result3d_t *results, double eps,
+/* Slab-pipelined solve of every work item: field initialisation, 8
+ * initialisation sweeps, then nsweep passes of 8 sweeps (or, when conv_tol
+ * >= 0 and max_pass > 0, passes until a pass changes no node by more than
+ * conv_tol).  precision: 4 (FP32 field, FP64 near-source stencil) or 8 (FP64
+ * field).  grids/work/results are device arrays.  Returns a cudaError_t. */
+int fk3d_solve_slabs(int precision, const fk_grid3d_t *grids, const fk_work3d_t *work,
+                     int nwork, const fk_slabs3d_t *plan, fk_result3d_t *results, double eps,
                      int nsweep, double conv_tol, int max_pass, cudaStream_t stream);
 /* Optional timing: events recorded before the initialisation kernel, after
- * it and after the Gauss-Seidel kernel of every later fk3d_solve_tiles on
+ * it and after the Gauss-Seidel kernel of every later fk3d_solve_slabs on
  * this host thread (NULL to stop). */
-void fk3d_tiles_set_events(cudaEvent_t *ev3);
+void fk3d_slabs_set_events(cudaEvent_t *ev3);
 
 /* ---- 2D ---------------------------------------------------------------- */
 typedef struct {
@@ -139,6 +119,10 @@ int fk_pack_slowness(int precision, int is3d, int nz, int nx, int ny, int zcp,
                      const double *slow_nat, void *slow_dev, cudaStream_t s);
 /* 3D cell velocities (device, FP64 natural) -> padded slowness 1/v;
  * *bad_dev = 1 when a velocity is not positive (bad_dev zeroed by the caller). */
+/* The node-indexed FP32 slowness copies of fk_grid3d_t.slowz from the
+ * padded FP32 cell slowness (3D). */
+int fk_node_slowness_f32(int nz, int nx, int ny, int zcp, int zp, const float *slow_dev,
+                         float *slowz_dev, cudaStream_t s);
 int fk_pack_velocity(int precision, int nz, int nx, int ny, int zcp, const double *vel_nat,
                      void *slow_dev, int *bad_dev, cudaStream_t s);
 /* out[i] = v[idx[i]] on the device. */

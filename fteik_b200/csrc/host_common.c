@@ -44,6 +44,62 @@ const char *fteik_b200_version(void) { return "fteik-b200 0.1 (sm_100a)"; }
 
 cudaStream_t fk_stream(void) { return g_stream; }
 
+/* Polls a bounded device-side wait of the 3D sweeps (a slab waiting on its
+ * upwind slab) makes before it gives up and raises the kernel's error word:
+ * by default 2^22 polls of at most 1 us each, seconds, far longer than any
+ * wait of a correct run. */
+#define FK_SPIN_LIMIT_DEFAULT (1LL << 22)
+static long long g_spin_limit = FK_SPIN_LIMIT_DEFAULT;
+static int g_spin_epoch = 0;
+
+long long fk_spin_limit(void) { return g_spin_limit; }
+int fk_spin_epoch(void) { return g_spin_epoch; }
+
+void fteik_b200_setSpinLimit(long long polls, int *ierr)
+{
+    *ierr = 0;
+    if (polls < 0) {
+        g_spin_limit = FK_SPIN_LIMIT_DEFAULT;
+    } else {
+        g_spin_limit = polls;
+    }
+    g_spin_epoch++;
+}
+
+void fteik_b200_getSpinLimit(long long *polls) { *polls = g_spin_limit; }
+
+static fk_slabcfg_t g_slabcfg = {-1, -1, -1, -1};
+static int g_slabcfg_epoch = 0;
+
+fk_slabcfg_t fk_slabcfg(void) { return g_slabcfg; }
+int fk_slabcfg_epoch(void) { return g_slabcfg_epoch; }
+
+void fteik_b200_setSlabConfig(int staged, int pairs, int progress, int blocksPerSM, int *ierr)
+{
+    *ierr = 0;
+    if (staged < -1 || staged > 1 || pairs < -1 || pairs > 1 ||
+        !(progress == -1 || progress == 8 || progress == 32) || blocksPerSM < -1 || blocksPerSM == 0 ||
+        blocksPerSM > 4) {
+        FK_ERR("fteik_b200_setSlabConfig: staged and pairs must be -1, 0 or 1, progress -1, 8 or 32, "
+               "blocksPerSM -1 or 1..4");
+        *ierr = 1;
+        return;
+    }
+    g_slabcfg.staged = staged;
+    g_slabcfg.pairs = pairs;
+    g_slabcfg.progress = progress;
+    g_slabcfg.blocks_per_sm = blocksPerSM;
+    g_slabcfg_epoch++;
+}
+
+void fteik_b200_getSlabConfig(int *staged, int *pairs, int *progress, int *blocksPerSM)
+{
+    *staged = g_slabcfg.staged;
+    *pairs = g_slabcfg.pairs;
+    *progress = g_slabcfg.progress;
+    *blocksPerSM = g_slabcfg.blocks_per_sm;
+}
+
 void *fteik_b200_stream(void)
 {
     if (fk_dev_ready("fteik_b200_stream")) return NULL;

@@ -17,6 +17,22 @@
 /* ---- device, stream, allocation ---- */
 int fk_dev_ready(const char *who);           /* 0 if a CUDA device is usable */
 cudaStream_t fk_stream(void);
+/* Poll limit of the bounded device-side waits (fteik_b200_setSpinLimit), and
+ * a counter bumped by every change of it (captured graphs that baked the old
+ * limit in are rebuilt when it moves). */
+long long fk_spin_limit(void);
+int fk_spin_epoch(void);
+
+/* Launch configuration of the 3D slab sweeps (fteik_b200_setSlabConfig):
+ * each knob a value, or -1 for the library's choice. */
+typedef struct {
+    int staged;          /* FP32 passes: staged pass step (1) or direct loads (0) */
+    int pairs;           /* passes: two sources of one grid per thread (1) or one (0) */
+    int progress;        /* passes: progress published every 8 or 32 steps */
+    int blocks_per_sm;   /* resident blocks per SM of the persistent kernels, 1..4 */
+} fk_slabcfg_t;
+fk_slabcfg_t fk_slabcfg(void);
+int fk_slabcfg_epoch(void);
 void *fk_dalloc(size_t bytes, const char *who);
 void fk_dfree(void *p);
 int fk_check(int cuda_err, const char *who);  /* 0 on success, prints otherwise */
@@ -36,10 +52,12 @@ typedef struct {
     double *slow;          /* host FP64, natural cell order */
     void *slow_dev32;      /* device FP32 padded */
     void *slow_dev64;      /* device FP64 padded */
-    bool dev32_ok, dev64_ok;
+    float *slowz_dev;      /* device FP32 node-indexed copies (3D; fk_grid3d_t.slowz) */
+    bool dev32_ok, dev64_ok, devz_ok;
 } fk_model_t;
 extern fk_model_t fk_model;
 const void *fk_model_slow_dev(int precision); /* uploads lazily */
+const float *fk_model_slowz_dev(void);        /* 3D FP32 node-indexed copies, built lazily */
 void fk_model_invalidate_dev(void);
 
 /* ---- sources (source.F90) ---- */

@@ -24,6 +24,7 @@ void fk_model_invalidate_dev(void)
 {
     fk_model.dev32_ok = false;
     fk_model.dev64_ok = false;
+    fk_model.devz_ok = false;
 }
 
 void fteik_model_free(void)
@@ -31,6 +32,7 @@ void fteik_model_free(void)
     free(fk_model.slow);
     fk_dfree(fk_model.slow_dev32);
     fk_dfree(fk_model.slow_dev64);
+    fk_dfree(fk_model.slowz_dev);
     memset(&fk_model, 0, sizeof(fk_model));
     fk_model.lis3d = true;
 }
@@ -62,6 +64,7 @@ void fteik_model_setGridSize(bool lis3d, int nz, int nx, int ny, int *ierr)
     fk_model.slow = (double *)calloc((size_t)fk_model.ncell, sizeof(double));
     fk_dfree(fk_model.slow_dev32); fk_model.slow_dev32 = NULL;
     fk_dfree(fk_model.slow_dev64); fk_model.slow_dev64 = NULL;
+    fk_dfree(fk_model.slowz_dev); fk_model.slowz_dev = NULL;
     fk_model_invalidate_dev();
     fk_model.have_model = false;
 }
@@ -177,6 +180,64 @@ void fteik_model_setVelocityModel64f(int nv, const double vel[], int *ierr)
     for (int i = 0; i < nv; i++) fk_model.slow[i] = 1.0 / vel[i];
     fk_model_invalidate_dev();
     fk_model.have_model = true;
+}
+
+void fteik_model_setVelocityModel32f(int nv, const float vel4[], int *ierr)
+{
+    /* model.F90:719-754: slow = 1 / DBLE(vel4) */
+    *ierr = 0;
+    fk_model.have_model = false;
+    if (nv != fk_model.ncell || nv < 1) {
+        FK_ERR("fteik_model_setVelocityModel32f: ncell=%d but nv=%d", fk_model.ncell, nv);
+        *ierr = 1;
+        return;
+    }
+    float vmin = vel4[0];
+    for (int i = 1; i < nv; i++) if (vel4[i] < vmin) vmin = vel4[i];
+    if (!(vmin > 0.0f)) {
+        FK_ERR("fteik_model_setVelocityModel32f: All velocities must be positive");
+        *ierr = 1;
+        return;
+    }
+    for (int i = 0; i < nv; i++) fk_model.slow[i] = 1.0 / (double)vel4[i];
+    fk_model_invalidate_dev();
+    fk_model.have_model = true;
+}
+
+void fteik_model_getVelocityModel64f(int nwork, int *nv, double vel[], int *ierr)
+{
+    /* model.F90:651-688 */
+    *ierr = 0;
+    *nv = 0;
+    if (nwork == -1) {
+        *nv = fk_model.ncell;
+        return;
+    }
+    if (nwork < fk_model.ncell) {
+        FK_ERR("fteik_model_getVelocityModel64f: nv < ncell");
+        *ierr = 1;
+        return;
+    }
+    if (!fk_model.have_model) {
+        FK_ERR("fteik_model_getVelocityModel64f: Velocity model not yet set");
+        for (int i = 0; i < nwork; i++) vel[i] = 0.0;
+        *ierr = 1;
+        return;
+    }
+    for (int i = 0; i < fk_model.ncell; i++) vel[i] = 1.0 / fk_model.slow[i];
+    for (int i = fk_model.ncell; i < nwork; i++) vel[i] = 0.0;
+    *nv = fk_model.ncell;
+}
+
+void fteik_model_isModel3D(bool *lis3d, int *ierr)
+{
+    /* model.F90:692-706 */
+    *ierr = 0;
+    *lis3d = fk_model.lis3d;
+    if (!fk_model.have_geom || fk_model.nx < 1 || fk_model.nz < 1) {
+        FK_ERR("fteik_model_isModel3D: Model not yet initialized");
+        *ierr = 1;
+    }
 }
 
 void fteik_model_setCellVelocityModel64f(int nc, int order, const double vel[], int *ierr)
@@ -313,6 +374,28 @@ const void *fk_model_slow_dev(int precision)
     return *slot;
 }
 
+const float *fk_model_slowz_dev(void)
+{
+    /* the FP32 node-indexed slowness copies of the staged pass step, from
+     * the padded FP32 cell slowness */
+    if (fk_model.devz_ok) return fk_model.slowz_dev;
+    if (!fk_model.lis3d) return NULL;
+    const float *slow = (const float *)fk_model_slow_dev(4);
+    if (!slow) return NULL;
+    const int nz = fk_model.nz, nx = fk_model.nx, ny = fk_model.ny;
+    const size_t n = (size_t)2 * (nx - 1) * (ny - 1) * FK_PITCH(nz);
+    if (!fk_model.slowz_dev) {
+        fk_model.slowz_dev = (float *)fk_dalloc(sizeof(float) * n, "fteik_model");
+        if (!fk_model.slowz_dev) return NULL;
+    }
+    int e = fk_node_slowness_f32(nz, nx, ny, FK_PITCH(nz - 1), FK_PITCH(nz), slow, fk_model.slowz_dev,
+                                 fk_stream());
+    if (!e) e = (int)cudaStreamSynchronize(fk_stream());
+    if (fk_check(e, "fteik_model: node-indexed slowness")) return NULL;
+    fk_model.devz_ok = true;
+    return fk_model.slowz_dev;
+}
+
 /* -------------------------------------------------------------- source -- */
 int fk_snap_source(bool is3d, int nz, int nx, int ny, double z0, double x0, double y0,
                    double dz, double dx, double dy, double zsrc, double xsrc, double ysrc,
@@ -353,6 +436,8 @@ int fk_snap_source(bool is3d, int nz, int nx, int ny, double z0, double x0, doub
     *zsa = za; *xsa = xa; *ysa = ya;
     return 0;
 }
+
+void fteik_source_setVerbosity(int verbose) { fk_source.verbose = verbose; }
 
 void fteik_source_free(void)
 {
@@ -512,6 +597,8 @@ int fk_receiver_geometry(bool is3d, int nz, int nx, int ny, double z0, double x0
     }
     return e;
 }
+
+void fteik_receiver_setVerbosity(int verbose) { fk_receiver.verbose = verbose; }
 
 void fteik_receiver_free(void)
 {

@@ -179,9 +179,6 @@ extern "C" int fk_locate_l2_exact(int ngrd, int ldgrd, int ntf, const float *tab
 /* Lives on every device that loads this library until the process exits. */
 static __device__ __align__(256) unsigned char g_noalloc_scratch[FK_NOALLOC_MAX_EVENTS * 12 + 256];
 
-static void *g_noalloc_ptr[64];  /* device address of the array, per device */
-static int g_noalloc_ready[64];
-
 extern "C" void fteik_b200_locate_l2_noalloc(int ngrd, int ldgrd, int ntf, const float *tables,
                                              int nev, const float *obs, const float *wts,
                                              int *opt_index, float *t0, float *obj, void *stream,
@@ -202,25 +199,19 @@ extern "C" void fteik_b200_locate_l2_noalloc(int ngrd, int ldgrd, int ntf, const
         fprintf(stderr, "fteik_b200_locate_l2_noalloc: null buffer\n");
         return;
     }
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= 64) {
-        fprintf(stderr, "fteik_b200_locate_l2_noalloc: no usable CUDA device\n");
+    /* the device address of the array, looked up on every call with the
+     * caller's current device (the host-side name of the array is not a
+     * device address); nothing is cached, so concurrent first calls from
+     * several host threads and a reset device leave no stale address */
+    void *scratch = NULL;
+    cudaError_t e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "fteik_b200_locate_l2_noalloc: cudaGetSymbolAddress failed (%s)\n",
+                cudaGetErrorString(e));
         return;
     }
-    if (!g_noalloc_ready[dev]) {
-        /* once per device, with that device current: the host-side name of
-         * the array is not a device address */
-        e = cudaGetSymbolAddress(&g_noalloc_ptr[dev], g_noalloc_scratch);
-        if (e != cudaSuccess) {
-            fprintf(stderr, "fteik_b200_locate_l2_noalloc: cudaGetSymbolAddress failed (%s)\n",
-                    cudaGetErrorString(e));
-            return;
-        }
-        g_noalloc_ready[dev] = 1;
-    }
     const int rc = fk_locate_l2_exact(ngrd, ldgrd, ntf, tables, nev, obs, wts, opt_index, t0, obj,
-                                      g_noalloc_ptr[dev], sizeof(g_noalloc_scratch),
+                                      scratch, sizeof(g_noalloc_scratch),
                                       (cudaStream_t)stream);
     if (rc != 0) {
         fprintf(stderr, "fteik_b200_locate_l2_noalloc: launch failed (%s)\n",

@@ -41,7 +41,7 @@
  * the reference's sweep bit for bit in FP64.
  */
 #pragma once
-#include "tile3d_impl.cuh"
+#include "slab3d_common.cuh"
 
 namespace fk3rw {
 using fk3::Mesh;
@@ -116,6 +116,7 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
     Mesh<double> mesh64;
     if (INIT) fk3::make_mesh<double>(mesh64, g.dz, g.dx, g.dy);
     const R HUGEV = (R)FK_HUGE;
+    const R eps_r = (R)q.eps_t;
     const int th = min(TY, ny - TY * P);             /* rows in this slab */
     const bool row = ty < th;
     const int y = TY * P + ty;
@@ -245,8 +246,14 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
                         const int x = (sx > 0) ? xl : nx - 1 - xl;
                         const int il = loz - 1 + zq;
                         const int iz = (sz > 0) ? il : nz - 1 - il;
-                        const double tmin = (double)rmin(rmin(tv, te), tn);
-                        const bool lcart = tmin > q.eps_t;
+                        /* the Cartesian / spherical switch (localSolver.F90:572-575)
+                         * compares in the field's precision: in FP32 both the upwind
+                         * time and the threshold are rounded to FP32, so a time that
+                         * equals the threshold in FP64 (a node eps cells from a
+                         * node-centred source along a grid line of a uniform medium)
+                         * stays spherical, as in FP64, instead of being pushed past the
+                         * threshold by its own rounding */
+                        const bool lcart = rmin(rmin(tv, te), tn) > eps_r;
                         if (lcart && sizeof(R) == 4)
                             /* away from the source the initialisation stencil is the
                              * plane-wave one (localSolver.F90:715-732) */
@@ -508,13 +515,288 @@ __device__ __forceinline__ bool slab_pass_f32(const fk3tw::Params &P_, const fk_
     return true;
 }
 
+/* ---- staged FP32 pass step ---------------------------------------------
+ * The walk of slab_pass_f32 with the lane's node values, upwind-row values
+ * and slowness moved in 16-byte groups of 4 consecutive z positions by
+ * cp.async into a per-warp shared-memory stage, instead of one 4-byte L2
+ * load per value and step (each of which fetches a 32-byte sector): a lane
+ * issues the loads of its group G + 1 when it starts reading group G, so
+ * the loads run 4 to 7 walk items ahead, and it reads each item from the
+ * stage one step before using it.
+ *
+ * Groups follow the walk: items 4 G .. 4 G + 3 of the lane's linear walk
+ * j = k Zp + zq.  Zp is a multiple of 4, and descending sweeps start with
+ * zoff = (-nz) mod 4 dummy items, so a group is always 4 consecutive nodes
+ * iz = 4 m .. 4 m + 3 of one column: a 16-byte aligned block of the field
+ * ([ny][nx][zp], zp a multiple of 8) and of the node-indexed slowness
+ * copies (fk_grid3d_t.slowz).  The dummy items and the walk positions past
+ * nz are invalid items, as in slab_pass_f32.
+ *
+ * Stage: per warp [2 buffers][8 arrays][32 slots][4 floats] (8 KB): arrays
+ * told (per source), tn (per source, slab's first row only) and the four
+ * slowness values; group G goes to buffer G & 1; lane l's slot is
+ * (l >> 2) | ((l & 3) << 3), so that the 32 lanes, whose walks are skewed by
+ * one item each, read 32 different banks in every step.
+ *
+ * The loads run further ahead than slab_pass_f32's, so a slab's first row
+ * waits for its upwind slab to be 6 steps further along. */
+constexpr int SG_NARR = 8;
+constexpr int SG_ARR_BYTES = 32 * 16;
+constexpr int SG_WARP_BYTES = 2 * SG_NARR * SG_ARR_BYTES;   /* 8 KB */
+constexpr int SG_AHEAD = 8;       /* items past the current one a lane may have loaded, + 1 */
+
+__device__ __forceinline__ void cpa16(uint32_t saddr, const void *gptr)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(gptr) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <bool RESID, int S, int CHP>
+__device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, const fk_grid3d_t &g,
+                                                     float *const (&ttp)[S], int s, int sweep_no, int P,
+                                                     int nslab, int *const (&prog)[S], float (*xr)[S][TY][32],
+                                                     float *ring, int zring, int *s_flag, double (&dmax)[S],
+                                                     uint32_t stage, const float *stage_f)
+{
+    constexpr int CH = CHP;
+    static_assert(CH % DL == 0 && NB == 2 * DL, "progress and buffer slots follow the DL windows");
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const unsigned FULL = 0xffffffffu;
+    const int nz = g.nz, nx = g.nx, ny = g.ny, zp = g.zp;
+    const int s0 = sweep_no - 1;
+    const int sz = (s0 < 4) ? 1 : -1;
+    const int sx = (s0 % 2 == 0) ? 1 : -1;
+    const int sy = ((s0 / 2) % 2 == 0) ? 1 : -1;
+    Mesh<float> mesh;
+    fk3::make_mesh<float>(mesh, g.dz, g.dx, g.dy);
+    const float HUGEV = (float)FK_HUGE;
+    const int th = min(TY, ny - TY * P);
+    const bool row = ty < th;
+    const int y = TY * P + ty;
+    const int oy = (sy > 0) ? ty : th - 1 - ty;
+    const int yl = (sy > 0) ? y : ny - 1 - y;
+    const bool rowupd = row && yl >= 1;
+    const int wy = ty - sy;
+    const int zoff = (sz > 0) ? 0 : ((4 - (nz & 3)) & 3);   /* leading dummy items */
+    const int Zn = nz + zoff;                               /* items zoff .. Zn - 1 are the nodes */
+    const int Zp = ((max(Zn, 32) + 3) >> 2) << 2;
+    const int K = (nx + 31) / 32;
+    const int T = K * Zp + 31 + DL * (TY - 1);
+    const int Pu = P - sy;
+    const bool has_up = Pu >= 0 && Pu < nslab;
+    const int ylast_up = has_up ? ((sy > 0) ? TY * Pu + min(TY, ny - TY * Pu) - 1 : TY * Pu) : 0;
+    const bool wait_up = has_up && (((sy > 0) ? ylast_up : ny - 1 - ylast_up) >= 1);
+    const int yu = y - sy;
+    const bool has_yu = row && yu >= 0 && yu < ny;
+    const bool has2 = S == 2 && ttp[S - 1] != nullptr;
+    float *const tt0 = ttp[0];
+    float *const tt1 = has2 ? ttp[S - 1] : ttp[0];
+
+    const int x0 = (sx > 0) ? tx : nx - 1 - tx;
+    const int kl = row ? (nx - tx + 31) / 32 : 0;                  /* blocks with x' < nx */
+    const int kmin = rowupd ? (tx == 0 ? 1 : 0) : 0x7fffffff;       /* updated: x' >= 1, y' >= 1 */
+    const int kxl = (nx - 1 >= tx && (nx - 1 - tx) % 32 == 0) ? (nx - 1 - tx) / 32 : -1; /* x' = nx - 1 */
+    /* node iz of walk position zq: sz > 0: zq; sz < 0: nz - 1 + zoff - zq */
+    const int colT = (y * nx + x0) * zp;
+    const int dkT = 32 * sx * zp;
+    const int dyT = sy * nx * zp;
+    const int cyU = (sy > 0) ? y - 1 : y;
+    const int cyD = min(max((sy > 0) ? y : y - 1, 0), ny - 2);
+    const float *const sl = g.slowz + ((sz > 0) ? (size_t)0 : (size_t)(ny - 1) * (nx - 1) * zp);
+    const int colS = (cyU * (nx - 1) + x0 - (sx > 0 ? 1 : 0)) * zp;
+    const int dkS = 32 * sx * zp;
+    const int offY = (cyD - cyU) * (nx - 1) * zp;
+    const int offX = sx * zp;
+    const int slot = (tx >> 2) | ((tx & 3) << 3);
+    const uint32_t my = stage + (uint32_t)(slot * 16);   /* cp.async destination */
+    const float *const myf = stage_f + slot * 4;          /* the same bytes, for reading */
+
+    /* group loads: cursor (lk, lzq) = first item of group gl */
+    int gl = 0, lk = 0, lzq = 0;
+    auto issue = [&]() {
+        const uint32_t d = my + (uint32_t)((gl & 1) * SG_NARR * SG_ARR_BYTES);
+        if (lzq < Zn && lk < kl) {
+            const int izb = (sz > 0) ? lzq : nz + zoff - 4 - lzq;
+            const int it = colT + lk * dkT + izb;
+            cpa16(d, tt0 + it);
+            if (S == 2) cpa16(d + SG_ARR_BYTES, tt1 + it);
+            if (oy == 0 && has_yu) {
+                cpa16(d + 2 * SG_ARR_BYTES, tt0 + (it - dyT));
+                if (S == 2) cpa16(d + 3 * SG_ARR_BYTES, tt1 + (it - dyT));
+            }
+            if (lk >= kmin) {
+                const int is = colS + lk * dkS + izb;
+                const int ox = (lk == kxl) ? 0 : offX;
+                cpa16(d + 4 * SG_ARR_BYTES, sl + is);
+                cpa16(d + 5 * SG_ARR_BYTES, sl + (is + offY));
+                cpa16(d + 6 * SG_ARR_BYTES, sl + (is + ox));
+                cpa16(d + 7 * SG_ARR_BYTES, sl + (is + ox + offY));
+            }
+        }
+        cpa_commit();
+        ++gl;
+        lzq += 4;
+        if (lzq == Zp) { lzq = 0; ++lk; }
+    };
+
+    struct Item {
+        float told[S], tn[S];
+        float duu, dud, ddu, ddd;
+        int k, zq;
+    };
+    /* item jn = (kk, zz) of the walk: make sure groups up to jn / 4 + 1 are
+     * issued, wait for group jn / 4, read the item from the stage */
+    auto fetch = [&](Item &f, int kk, int zz, int jn) {
+        f.k = kk;
+        f.zq = zz;
+        if (jn >= -4) {
+            const int target = (jn >> 2) + 1;
+            while (gl <= target) issue();
+        }
+        if (jn >= 0) {
+            cpa_wait1();   /* (a memory clobber: the reads below stay after it) */
+            const int e = (sz > 0) ? (jn & 3) : 3 - (jn & 3);
+            constexpr int A = SG_ARR_BYTES / 4;   /* floats per array */
+            const float *a = myf + ((jn >> 2) & 1) * SG_NARR * A + e;
+            f.told[0] = a[0];
+            if (S == 2) f.told[S - 1] = a[A];
+            if (oy == 0) {
+                f.tn[0] = has_yu ? a[2 * A] : HUGEV;
+                if (S == 2) f.tn[S - 1] = has_yu ? a[3 * A] : HUGEV;
+            }
+            f.duu = a[4 * A];
+            f.dud = a[5 * A];
+            f.ddu = a[6 * A];
+            f.ddd = a[7 * A];
+        }
+    };
+
+    const int *prog_up = prog[0] + (has_up ? Pu : P);
+    if (threadIdx.x == 0) {
+        s_flag[0] = 1;
+        if (wait_up && !wait_ge1(prog_up, (s << SHIFT) | min(T, CH + DL * (TY - 1) + 2 + SG_AHEAD - 2),
+                                 P_.spin_limit, P_.error, 3000))
+            s_flag[0] = 0;
+    }
+    __syncthreads();
+    if (!s_flag[0]) return false;
+
+    const int c = tx + DL * oy;                 /* the lane's item at step t is t - c */
+    int nk = 0, nzq = -c;                       /* item of the next step */
+    Item nxt;
+#pragma unroll
+    for (int i = 0; i < S; ++i) nxt.told[i] = nxt.tn[i] = HUGEV;
+    nxt.duu = nxt.dud = nxt.ddu = nxt.ddd = 0.0f;
+    fetch(nxt, nk, nzq, -c);
+    if (++nzq == Zp) { nzq = 0; ++nk; }
+    float zu_uu = 0.0f, zu_ud = 0.0f, zu_du = 0.0f, zu_dd = 0.0f;
+    float r_last[S], te_last[S], tn_last[S], ten_last[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) r_last[i] = te_last[i] = tn_last[i] = ten_last[i] = HUGEV;
+    float *ring_r = ring, *ring_tn = ring + S * zring;
+    bool ok = true;
+    for (int t0 = 0; t0 < T; t0 += DL) {
+        if (wait_up && t0 > 0 && t0 % CH == 0) {
+            if (threadIdx.x == 0 &&
+                !wait_ge1(prog_up, (s << SHIFT) | min(T, t0 + CH + DL * (TY - 1) + 2 + SG_AHEAD - 2),
+                          P_.spin_limit, P_.error, 3001))
+                s_flag[0] = 0;
+            __syncthreads();
+            if (!s_flag[0]) { ok = false; break; }
+        }
+        const int half = (t0 / DL) & 1;
+        float (*const xw)[S][TY][32] = xr + half * DL;
+        float (*const xrd)[S][TY][32] = xr + (1 - half) * DL;
+#pragma unroll
+        for (int u = 0; u < DL; ++u) {
+            float sh_r[S], sh_tn[S];
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                sh_r[i] = __shfl_up_sync(FULL, r_last[i], 1);
+                sh_tn[i] = __shfl_up_sync(FULL, tn_last[i], 1);
+            }
+            const Item cur = nxt;
+            fetch(nxt, nk, nzq, t0 + u + 1 - c);
+            if (++nzq == Zp) { nzq = 0; ++nk; }
+            const bool valid = (unsigned)(cur.zq - zoff) < (unsigned)nz && cur.k < kl;
+            const bool upd = valid && cur.zq > zoff && cur.k >= kmin;
+            const bool from_ring = tx == 0 && cur.k > 0;   /* then 0 <= zq < Zp */
+            float rte[S], rten[S];
+#pragma unroll
+            for (int i = 0; i < S; ++i) rte[i] = rten[i] = HUGEV;
+            if (from_ring) {
+#pragma unroll
+                for (int i = 0; i < S; ++i) { rte[i] = ring_r[i * zring + cur.zq]; rten[i] = ring_tn[i * zring + cur.zq]; }
+            }
+            float tnw[S];
+            if (oy != 0) {
+#pragma unroll
+                for (int i = 0; i < S; ++i) tnw[i] = xrd[u][i][wy][tx];
+            }
+            const float s4 = fminf(zu_uu, zu_ud), s5 = fminf(zu_uu, zu_du), s6 = fminf(zu_uu, cur.duu);
+            const float s1 = fminf(s4, fminf(zu_du, zu_dd));
+            const float s2 = fminf(s4, fminf(cur.duu, cur.dud));
+            const float s3 = fminf(s5, fminf(cur.duu, cur.ddu));
+            const float s7 = zu_uu;
+            float res[S], tnv_[S];
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                const float te = (tx == 0) ? rte[i] : sh_r[i];
+                const float ten = (tx == 0) ? rten[i] : sh_tn[i];
+                const float tn = (oy == 0) ? cur.tn[i] : tnw[i];
+                const float told = cur.told[i];
+                float r = told;
+                if (upd) {
+                    r = fk3::noinit_f32(mesh, r_last[i], te, tn, te_last[i], ten, tn_last[i], ten_last[i], s1, s2,
+                                        s3, s4, s5, s6, s7, told);
+                    if (r != told && (i == 0 || has2)) {
+                        const int iz = (sz > 0) ? cur.zq : nz - 1 + zoff - cur.zq;
+                        (i == 0 ? tt0 : tt1)[colT + cur.k * dkT + iz] = r;
+                        if (RESID) {
+                            const double d = fabs((double)r - (double)told);
+                            dmax[i] = d > dmax[i] ? d : dmax[i];
+                        }
+                    }
+                }
+                res[i] = r;
+                tnv_[i] = tn;
+                te_last[i] = te;
+                ten_last[i] = ten;
+            }
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                xw[u][i][ty][tx] = res[i];
+                if (tx == 31 && cur.zq >= 0) { ring_r[i * zring + cur.zq] = res[i]; ring_tn[i * zring + cur.zq] = tnv_[i]; }
+            }
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                r_last[i] = res[i];
+                tn_last[i] = tnv_[i];
+            }
+            zu_uu = cur.duu; zu_ud = cur.dud; zu_du = cur.ddu; zu_dd = cur.ddd;
+            if (u < DL - 1) __syncwarp();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && (t0 + DL) % CH == 0 && t0 + DL < T) {
+            __threadfence();
+#pragma unroll
+            for (int i = 0; i < S; ++i)
+                if (prog[i]) fk3tw::st_release(prog[i] + P, (s << SHIFT) | (t0 + DL));
+        }
+    }
+    cpa_wait0();   /* no copy into the stage outlives the task */
+    return ok;
+}
+
 /* Persistent slab-task kernel over sweeps [s_begin, s_end).  S = 2 runs
  * two sources of one grid in the same threads (the Gauss-Seidel passes,
  * whose walk does not depend on the source): the slowness, the indices and
  * the barriers are shared and the two stencils give each thread two
  * independent dependency chains.  tasks = {pair, j'} with pairs[2 pair + i]
  * the work items (-1: none) when S = 2, {work, j'} when S = 1. */
-template <typename R, bool INIT, bool RESID, int S, int CHP>
+template <typename R, bool INIT, bool RESID, int S, int CHP, bool STG = false>
 __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(fk3tw::Params P, const int *pairs,
                                                                              int zring)
 {
@@ -524,6 +806,10 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
     __shared__ double s_max[S][TY];
     extern __shared__ __align__(16) unsigned char slab_smem[];
     R *ring = reinterpret_cast<R *>(slab_smem) + (size_t)(threadIdx.x >> 5) * 2 * S * zring;
+    /* staged pass step: the per-warp stages follow the rings (16-byte aligned: zring is a multiple of 4) */
+    const size_t stage_off = (size_t)TY * 2 * S * zring * sizeof(R) + (size_t)(threadIdx.x >> 5) * SG_WARP_BYTES;
+    const uint32_t stage = (uint32_t)__cvta_generic_to_shared(slab_smem) + (uint32_t)stage_off;
+    const float *const stage_f = reinterpret_cast<const float *>(slab_smem + stage_off);
     const int tid = threadIdx.x;
     const long long total = (long long)(P.s_end - P.s_begin) * P.ntask_sweep;
     for (;;) {
@@ -599,7 +885,10 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
         for (int i = 0; i < S; ++i) dmax[i] = 0.0;
         if (!skip) {
             bool ok;
-            if constexpr (!INIT && sizeof(R) == 4)
+            if constexpr (!INIT && sizeof(R) == 4 && STG)
+                ok = slab_pass_f32_staged<RESID, S, CHP>(P, g, ttp, s, sweep_no, Pp, nslab, prog, xr, ring, zring,
+                                                         s_flag, dmax, stage, stage_f);
+            else if constexpr (!INIT && sizeof(R) == 4)
                 ok = slab_pass_f32<RESID, S, CHP>(P, g, ttp, reinterpret_cast<const float *>(g.slow), s, sweep_no,
                                                   Pp, nslab, prog, xr, ring, zring, s_flag, dmax);
             else
@@ -632,7 +921,7 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
                     atomicMax(rp, (unsigned long long)__double_as_longlong(m));
                     if (sweep_no == 8) {
                         __threadfence();
-                        const int c = atomicAdd(P.pass_tiles + (size_t)wi[i] * P.npass + pass, 1);
+                        const int c = atomicAdd(P.pass_slabs + (size_t)wi[i] * P.npass + pass, 1);
                         if (c == nslab - 1) {
                             const double r = __longlong_as_double((long long)atomicAdd(rp, 0ull));
                             if (P.converge && r <= P.conv_tol) atomicMin(P.conv_pass + wi[i], pass);
@@ -645,33 +934,41 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
     }
 }
 
-template <typename R, bool INIT, bool RESID, int S>
-inline int launch_slab_kernel(const fk3tw::Params &P, const int *pairs, int zring, cudaStream_t st)
+template <typename R, bool INIT, bool RESID, int S, bool STG = false>
+inline int launch_slab_kernel(const fk3tw::Params &P, const int *pairs, int zring, cudaStream_t st,
+                              int progress = 0, int blocks_per_sm = 0)
 {
-    const size_t smem = (size_t)TY * 2 * S * zring * sizeof(R);
+    const size_t smem = (size_t)TY * 2 * S * zring * sizeof(R) + (STG ? (size_t)TY * SG_WARP_BYTES : 0);
     int dev = 0, nsm = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (smem > 48 * 1024) { /* deep grids: the per-warp rings need the opt-in shared memory */
-        cudaError_t ea = cudaFuncSetAttribute(slab_kernel<R, INIT, RESID, S, CH_MANY>,
+        cudaError_t ea = cudaFuncSetAttribute(slab_kernel<R, INIT, RESID, S, CH_MANY, STG>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (ea == cudaSuccess && !INIT)
-            ea = cudaFuncSetAttribute(slab_kernel<R, INIT, RESID, S, CH_FEW>,
+            ea = cudaFuncSetAttribute(slab_kernel<R, INIT, RESID, S, CH_FEW, STG>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (ea != cudaSuccess) return (int)ea;
     }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, slab_kernel<R, INIT, RESID, S, CH_MANY>, NT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, slab_kernel<R, INIT, RESID, S, CH_MANY, STG>, NT, smem);
     if (per < 1) per = 1;
+    if (blocks_per_sm > 0 && blocks_per_sm < per) per = blocks_per_sm;
     /* fewer than 4 slab tasks per resident block and sweep: the upwind chains bound the time */
-    if (!INIT && P.ntask_sweep < 4 * nsm * per)
-        slab_kernel<R, INIT, RESID, S, CH_FEW><<<nsm * per, NT, smem, st>>>(P, pairs, zring);
+    const bool few = progress == CH_FEW || (progress == 0 && P.ntask_sweep < 4 * nsm * per);
+    if (!INIT && few)
+        slab_kernel<R, INIT, RESID, S, CH_FEW, STG><<<nsm * per, NT, smem, st>>>(P, pairs, zring);
     else
-        slab_kernel<R, INIT, RESID, S, CH_MANY><<<nsm * per, NT, smem, st>>>(P, pairs, zring);
+        slab_kernel<R, INIT, RESID, S, CH_MANY, STG><<<nsm * per, NT, smem, st>>>(P, pairs, zring);
     return (int)cudaGetLastError();
 }
 
+/* The FP32 initialisation kernel lives in its own unit (slab_init_f32.cu),
+ * compiled without multiply-add contraction: its near-source spherical
+ * stencil is FP64 and so rounds as the FP64 CPU algorithm does. */
+int launch_init_f32(const fk3tw::Params &P, int zring, cudaStream_t st, int blocks_per_sm);
+
 template <typename R>
-inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nwork, const fk_tiles3d_t *pl,
+inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nwork, const fk_slabs3d_t *pl,
                        fk_result3d_t *results, double eps, int nsweep, double conv_tol, int max_pass,
                        cudaStream_t st)
 {
@@ -679,17 +976,19 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
     const int converge = conv_tol >= 0.0 && max_pass > 0;
     const int npass = converge ? max_pass : nsweep;
     const int npr = npass > 0 ? npass : 1;
-    const int zring = pl->max_nz > 32 ? pl->max_nz : 32;
+    /* walk positions per column: nz, plus up to 3 leading items in the staged
+     * step's descending sweeps, at least 32, a multiple of 4 */
+    const int zring = ((pl->max_nz + 3 > 32 ? pl->max_nz + 3 : 32) + 3) / 4 * 4;
     /* counters hold (sweep << SHIFT) | steps: steps of a slab and sweep numbers must fit */
     const long long steps = (long long)((pl->max_nx + 31) / 32) * zring + 31 + DL * TY;
     if (steps >= (1LL << SHIFT) || 8 + 8 * (long long)npr + 1 >= (1LL << (31 - SHIFT)))
         return (int)cudaErrorInvalidValue;
     cudaError_t e = cudaSuccess;
-    e = cudaMemsetAsync(pl->done, 0, sizeof(int) * (size_t)pl->ntiles_total, st);
+    e = cudaMemsetAsync(pl->done, 0, sizeof(int) * (size_t)pl->nslab_total, st);
     if (!e) e = cudaMemsetAsync(pl->tickets, 0, 2 * sizeof(unsigned long long), st);
     if (!e) e = cudaMemsetAsync(pl->error, 0, sizeof(int), st);
     if (!e) e = cudaMemsetAsync(pl->resid, 0, sizeof(unsigned long long) * (size_t)nwork * npr, st);
-    if (!e) e = cudaMemsetAsync(pl->pass_tiles, 0, sizeof(int) * (size_t)nwork * npr, st);
+    if (!e) e = cudaMemsetAsync(pl->pass_slabs, 0, sizeof(int) * (size_t)nwork * npr, st);
     if (!e) e = cudaMemsetAsync(pl->conv_pass, 0x3f, sizeof(int) * (size_t)nwork, st);
     if (e) return (int)e;
     fk3tw::field_init_kernel<R><<<dim3(64, nwork), 256, 0, st>>>(grids, work, eps);
@@ -703,7 +1002,7 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
     P.done = pl->done;
     P.error = pl->error;
     P.resid = pl->resid;
-    P.pass_tiles = pl->pass_tiles;
+    P.pass_slabs = pl->pass_slabs;
     P.conv_pass = pl->conv_pass;
     P.npass = npr;
     P.converge = converge;
@@ -713,26 +1012,42 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
     P.s_begin = 0;
     P.s_end = 8;
     P.ticket = pl->tickets;
-    if (fk3tw::g_tile_events) cudaEventRecord(fk3tw::g_tile_events[0], st);
-    int rc = launch_slab_kernel<R, true, false, 1>(P, nullptr, zring, st);
+    if (fk3tw::g_slab_events) cudaEventRecord(fk3tw::g_slab_events[0], st);
+    int rc;
+    if constexpr (sizeof(R) == 4)
+        rc = launch_init_f32(P, zring, st, pl->blocks_per_sm);
+    else
+        rc = launch_slab_kernel<R, true, false, 1>(P, nullptr, zring, st, 0, pl->blocks_per_sm);
     if (rc) return rc;
-    if (fk3tw::g_tile_events) cudaEventRecord(fk3tw::g_tile_events[1], st);
+    if (fk3tw::g_slab_events) cudaEventRecord(fk3tw::g_slab_events[1], st);
     if (npass > 0) {
         P.s_begin = 8;
         P.s_end = 8 + 8 * npass;
         P.ticket = pl->tickets + 1;
+        const bool stg = sizeof(R) == 4 && pl->staged;
         if (pl->pairs) { /* two sources per thread */
             P.tasks = reinterpret_cast<const int2 *>(pl->tasks2);
             P.ntask_sweep = pl->ntask2_sweep;
-            rc = converge ? launch_slab_kernel<R, false, true, 2>(P, pl->pairs, zring, st)
-                          : launch_slab_kernel<R, false, false, 2>(P, pl->pairs, zring, st);
+            const int *pr = pl->pairs;
+            const int ch = pl->progress, bps = pl->blocks_per_sm;
+            if (stg)
+                rc = converge ? launch_slab_kernel<R, false, true, 2, true>(P, pr, zring, st, ch, bps)
+                              : launch_slab_kernel<R, false, false, 2, true>(P, pr, zring, st, ch, bps);
+            else
+                rc = converge ? launch_slab_kernel<R, false, true, 2>(P, pr, zring, st, ch, bps)
+                              : launch_slab_kernel<R, false, false, 2>(P, pr, zring, st, ch, bps);
         } else {
-            rc = converge ? launch_slab_kernel<R, false, true, 1>(P, nullptr, zring, st)
-                          : launch_slab_kernel<R, false, false, 1>(P, nullptr, zring, st);
+            const int ch = pl->progress, bps = pl->blocks_per_sm;
+            if (stg)
+                rc = converge ? launch_slab_kernel<R, false, true, 1, true>(P, nullptr, zring, st, ch, bps)
+                              : launch_slab_kernel<R, false, false, 1, true>(P, nullptr, zring, st, ch, bps);
+            else
+                rc = converge ? launch_slab_kernel<R, false, true, 1>(P, nullptr, zring, st, ch, bps)
+                              : launch_slab_kernel<R, false, false, 1>(P, nullptr, zring, st, ch, bps);
         }
         if (rc) return rc;
     }
-    if (fk3tw::g_tile_events) cudaEventRecord(fk3tw::g_tile_events[2], st);
+    if (fk3tw::g_slab_events) cudaEventRecord(fk3tw::g_slab_events[2], st);
     fk3tw::finalize_kernel<<<(nwork + 127) / 128, 128, 0, st>>>(nwork, npr, converge, npass, pl->resid,
                                                                  pl->conv_pass, pl->error, results);
     return (int)cudaGetLastError();

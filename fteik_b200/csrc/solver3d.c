@@ -4,7 +4,7 @@
  */
 #include "host_common.h"
 #include "fteik_b200.h"
-#include "tileplan.h"
+#include "slabplan.h"
 
 #include <stdlib.h>
 #include <string.h>
@@ -18,9 +18,9 @@ static struct {
     fk_grid3d_t *grid_dev;
     fk_work3d_t *work_dev;
     fk_result3d_t *res_dev;
-    int *group_dev;
-    fk_tileplan_t plan;
+    fk_slabplan_t plan;
     int plan_npass;
+    int plan_cfg;           /* slab configuration epoch the plan was built with */
     fk_result3d_t last;
     double *grad;           /* device [3 ngrd] gradient of the current field */
     bool have_grad;
@@ -33,10 +33,9 @@ static void free_buffers(void)
     fk_dfree(S3.grid_dev); S3.grid_dev = NULL;
     fk_dfree(S3.work_dev); S3.work_dev = NULL;
     fk_dfree(S3.res_dev); S3.res_dev = NULL;
-    fk_dfree(S3.group_dev); S3.group_dev = NULL;
     fk_dfree(S3.grad); S3.grad = NULL;
     S3.have_grad = false;
-    fk_tileplan_free(&S3.plan);
+    fk_slabplan_free(&S3.plan);
     S3.plan_npass = 0;
 }
 
@@ -116,11 +115,6 @@ void fteik_solver3d_initialize(int nz, int nx, int ny, double z0, double x0, dou
     fteik_solver3d_setSphereToCartEpsilon(eps, ierr);
     if (*ierr) { FK_ERR("fteik_solver3d_initialize: Failed to set epsilon"); return; }
     if (fk_dev_ready("fteik_solver3d_initialize")) { *ierr = 1; return; }
-    if (fk_schedule_walker() && nx > 1024) {
-        FK_ERR("fteik_solver3d_initialize: nx=%d exceeds the 1024 columns one CTA walks", nx);
-        *ierr = 1;
-        return;
-    }
     S3.init = true;
     S3.src = -1;
 }
@@ -178,12 +172,7 @@ static int ensure_buffers(void)
     if (!S3.grid_dev) S3.grid_dev = (fk_grid3d_t *)fk_dalloc(sizeof(fk_grid3d_t), "fteik_solver3d");
     if (!S3.work_dev) S3.work_dev = (fk_work3d_t *)fk_dalloc(sizeof(fk_work3d_t), "fteik_solver3d");
     if (!S3.res_dev) S3.res_dev = (fk_result3d_t *)fk_dalloc(sizeof(fk_result3d_t), "fteik_solver3d");
-    if (!S3.group_dev) {
-        S3.group_dev = (int *)fk_dalloc(sizeof(int), "fteik_solver3d");
-        if (S3.group_dev && fk_check((int)fk_zero(S3.group_dev, sizeof(int)), "fteik_solver3d"))
-            return 1;
-    }
-    return !(S3.tt && S3.grid_dev && S3.work_dev && S3.res_dev && S3.group_dev);
+    return !(S3.tt && S3.grid_dev && S3.work_dev && S3.res_dev);
 }
 
 void fteik_solver3d_solveSourceLSM(int isrc, int *ierr)
@@ -214,6 +203,13 @@ void fteik_solver3d_solveSourceLSM(int isrc, int *ierr)
     g.zp = FK_PITCH(g.nz); g.zcp = FK_PITCH(g.nz - 1);
     g.dz = fk_model.dz; g.dx = fk_model.dx; g.dy = fk_model.dy;
     g.slow = slow;
+    g.slowz = NULL;
+    const fk_slabcfg_t cfg = fk_slabcfg();
+    const bool staged = S3.precision == 4 && cfg.staged == 1;
+    if (staged) {
+        g.slowz = fk_model_slowz_dev();
+        if (!g.slowz) { *ierr = 1; return; }
+    }
     fk_work3d_t w;
     w.grid = 0;
     w.zsi = fk_source.zsi[isrc - 1]; w.xsi = fk_source.xsi[isrc - 1]; w.ysi = fk_source.ysi[isrc - 1];
@@ -224,19 +220,22 @@ void fteik_solver3d_solveSourceLSM(int isrc, int *ierr)
     int e = (int)cudaMemcpyAsync(S3.grid_dev, &g, sizeof(g), cudaMemcpyHostToDevice, s);
     if (!e) e = (int)cudaMemcpyAsync(S3.work_dev, &w, sizeof(w), cudaMemcpyHostToDevice, s);
     /* the reference's 3D solver has no convergence test: nsweep passes */
-    if (!e && fk_schedule_walker()) {
-        e = fk3d_solve(S3.precision, S3.grid_dev, S3.work_dev, S3.group_dev, 1, 1, S3.res_dev, 1,
-                       g.nx, g.nz, S3.eps, S3.nsweep, -1.0, 0, s);
-    } else if (!e) {
-        if (!S3.plan.mem || S3.plan_npass < S3.nsweep) {
+    if (!e) {
+        if (!S3.plan.mem || S3.plan_npass < S3.nsweep || S3.plan.dev.spin_limit != fk_spin_limit() ||
+            S3.plan_cfg != fk_slabcfg_epoch()) {
             const int gid0 = 0;
-            if (fk_tileplan_build(&S3.plan, 1, &g.nx, &g.ny, &g.nz, &gid0, S3.nsweep, "fteik_solver3d")) {
+            if (fk_slabplan_build(&S3.plan, 1, &g.nx, &g.ny, &g.nz, &gid0, S3.nsweep, cfg.pairs != 0,
+                                  "fteik_solver3d")) {
                 *ierr = 1;
                 return;
             }
             S3.plan_npass = S3.nsweep;
+            S3.plan_cfg = fk_slabcfg_epoch();
         }
-        e = fk3d_solve_tiles(S3.precision, S3.grid_dev, S3.work_dev, 1, &S3.plan.dev, S3.res_dev,
+        S3.plan.dev.staged = staged;
+        S3.plan.dev.progress = cfg.progress > 0 ? cfg.progress : 0;
+        S3.plan.dev.blocks_per_sm = cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 0;
+        e = fk3d_solve_slabs(S3.precision, S3.grid_dev, S3.work_dev, 1, &S3.plan.dev, S3.res_dev,
                              S3.eps, S3.nsweep, -1.0, 0, s);
     }
     if (!e) e = (int)cudaMemcpyAsync(&S3.last, S3.res_dev, sizeof(S3.last), cudaMemcpyDeviceToHost, s);

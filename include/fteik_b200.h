@@ -58,8 +58,14 @@ void fteik_model_setOrigin2D(double z0, double x0);
 /* model.F90:264-296 */
 void fteik_model_getGridSize(int *nz, int *nx, int *ny, int *ngrd, int *ncell,
                              int *ierr);
-/* model.F90:719-754 */
+/* model.F90:574-607 (cells in natural order) */
 void fteik_model_setVelocityModel64f(int nv, const double vel[], int *ierr);
+/* model.F90:719-754: FP32 cell velocities, widened to FP64 before 1/v */
+void fteik_model_setVelocityModel32f(int nv, const float vel4[], int *ierr);
+/* model.F90:651-688: nwork = -1 queries nv = ncell; else vel[0..ncell) = 1/slowness */
+void fteik_model_getVelocityModel64f(int nwork, int *nv, double vel[], int *ierr);
+/* model.F90:692-706 */
+void fteik_model_isModel3D(bool *lis3d, int *ierr);
 /* model.F90:311-449 (order 0 natural, 1 XYZ, 2 ZYX) */
 void fteik_model_setNodalVelocityModel64f(int ng, int order,
                                           const double vel[], int *ierr);
@@ -94,6 +100,8 @@ void fteik_source_getSzero64fF(int isrc, double *szero, double *szero2,
                                int *ierr);
 void fteik_source_getNumberOfSources(int *nsrc, int *ierr);
 void fteik_source_free(void);
+/* source.F90:243-249 */
+void fteik_source_setVerbosity(int verbose);
 
 /* ---- receivers: receiver.F90 ---- */
 /* receiver.F90:62-164 */
@@ -104,6 +112,8 @@ void fteik_receiver_getTravelTimes64f(int nrec, int ngrd, const double ttimes[],
                                       double ttr[], int *ierr);
 void fteik_receiver_getNumberOfReceivers(int *nrec, int *ierr);
 void fteik_receiver_free(void);
+/* receiver.F90:171-177 */
+void fteik_receiver_setVerbosity(int verbose);
 
 /* ---- 3D solver: solver3D.F90 ---- */
 /* solver3D.F90:126-184 */
@@ -229,6 +239,8 @@ void fteik_analytic_getTravelTimesConstantVel64f(int ldr, double ttr[],
 void fteik_analytic_getTravelTimesGradientVel64f(int ldr, double ttr[],
                                                  int *ierr);
 void fteik_analytic_free(void);
+/* analytic.F90:194-200 */
+void fteik_analytic_setVerbosity(int verbose);
 
 /* ---- locator: locate.F90 ---- */
 /* locate.F90:142-223 */
@@ -278,6 +290,33 @@ int fteik_b200_device(void);
 /* The library's CUDA stream (a cudaStream_t), for callers that time or
  * order their own work against the library's; NULL without a device. */
 void *fteik_b200_stream(void);
+
+/* Poll limit of the bounded device-side waits of the 3D sweeps (a slab
+ * waiting on its upwind slab or on its neighbours' previous sweep).  A wait
+ * that runs out of polls stops its kernel, which returns normally with an
+ * error word set; the solve reports it as ierr = 1 and the library stays
+ * usable.  polls < 0 restores the default (2^22 polls of at most 1 us,
+ * seconds of waiting).  Takes effect at the next solve (a captured batch
+ * graph is rebuilt).  No counterpart in the reference, whose OpenMP
+ * barriers wait without a limit. */
+void fteik_b200_setSpinLimit(long long polls, int *ierr);
+void fteik_b200_getSpinLimit(long long *polls);
+
+/* Launch configuration of the persistent 3D sweep kernels, for the
+ * single-source solver and the batch.  Each knob takes a value or -1 for
+ * the library's choice (the default; the batch then picks by timing, see
+ * fteik_b200_batch3d_getSlabConfig):
+ *   staged      FP32 passes: 1 = each lane's node values, upwind-row values
+ *               and slowness move in 16-byte groups through shared memory
+ *               (cp.async), 0 = one 4-byte load per value and step;
+ *   pairs       passes: 1 = two sources of one grid share each thread, 0 = one;
+ *   progress    passes: slabs publish progress every 8 or 32 steps;
+ *   blocksPerSM resident blocks per SM, 1..4.
+ * Results are the same bits whichever configuration runs.  Takes effect at
+ * the next solve (a captured batch graph is rebuilt).  No counterpart in the
+ * reference. */
+void fteik_b200_setSlabConfig(int staged, int pairs, int progress, int blocksPerSM, int *ierr);
+void fteik_b200_getSlabConfig(int *staged, int *pairs, int *progress, int *blocksPerSM);
 
 /* Precision of fteik_solver3d_solveSourceLSM: 4 (default; FP32 fields with
  * FP64 source corners, near-source stencil and residual) or 8 (FP64 fields,
@@ -435,8 +474,9 @@ void fteik_b200_mlp_train(int n, const float x[], const float y[], int steps, in
  * (NULL: the legacy default stream); the call returns after launching.
  * Limits: 1 <= nev <= 65536, 1 <= ntf <= 64.  Its scratch (12 bytes per
  * event) is a fixed array that every device loading the library keeps until
- * exit; the first call on a device looks up that array's device address, so
- * make that first call before any stream capture.  Every call reuses the
+ * exit; every call looks up that array's device address on the current
+ * device (the first lookup on a device may load the library's device code,
+ * so make the first call on a device before any stream capture).  Every call reuses the
  * same array, so calls whose work overlaps on the GPU race: order them on
  * one stream.  It allocates nothing (no cudaMalloc, cudaFree or stream
  * creation). */

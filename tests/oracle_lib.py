@@ -137,6 +137,38 @@ def solve2d(n, h, slow, si, sa, eps, nsweep, fsm=False, conv_tol=-1.0, max_pass=
     return tt, npass.value
 
 
+def cell_to_slowness(n, order, vel):
+    """model.F90:505-607: cell velocities in ordering `order` -> FP64 cell
+    slowness in natural order.  n = (nz, nx, ny); ny = 1 for 2D."""
+    lib = load()
+    nz, nx, ny = n
+    is3d = ny > 1
+    ncell = (nz - 1) * (nx - 1) * (ny - 1 if is3d else 1)
+    vel = np.ascontiguousarray(vel, np.float64).ravel()
+    slow = np.empty(ncell, np.float64)
+    if lib.orc_cell_velocity_to_slowness(int(is3d), nz, nx, ny, int(order), _ptr(vel, c_double),
+                                         _ptr(slow, c_double)) != 0:
+        raise ValueError("non-positive velocity")
+    return slow
+
+
+def nodal_to_slowness(n, order, vel, keep_defects=False):
+    """model.F90:311-449: nodal velocities in ordering `order` -> FP64 cell
+    slowness in natural order; keep_defects reproduces the reference's
+    XYZ-ordering scale (model.F90:353) and natural-ordering y-plane
+    (model.F90:386-389) defects."""
+    lib = load()
+    nz, nx, ny = n
+    is3d = ny > 1
+    ncell = (nz - 1) * (nx - 1) * (ny - 1 if is3d else 1)
+    vel = np.ascontiguousarray(vel, np.float64).ravel()
+    slow = np.empty(ncell, np.float64)
+    if lib.orc_nodal_velocity_to_slowness(int(is3d), nz, nx, ny, int(order), int(keep_defects),
+                                          _ptr(vel, c_double), _ptr(slow, c_double)) != 0:
+        raise ValueError("non-positive velocity")
+    return slow
+
+
 def count_updates3d(n, si):
     lib = load()
     a, b = ctypes.c_int64(), ctypes.c_int64()

@@ -35,8 +35,7 @@ def test_gpu_3d_golden(fk, c, precision):
     if precision == 8:
         assert np.max(np.abs(got - tt)) <= 1e-12 * np.max(tt)
     else:
-        tol = 1e-3 if c == 3 else 1e-4
-        assert np.max(np.abs(got - tt) / np.maximum(tt, 1e-6)) <= tol
+        assert np.max(np.abs(got - tt) / np.maximum(tt, 1e-6)) <= 1e-4
 
 
 @pytest.mark.parametrize("c", range(3))

@@ -1,0 +1,170 @@
+"""The reference's own callers, unmodified, run against this library.
+
+oracle/ref_callers.mk builds them from where they lie in the reference tree
+(it runs where the reference is present; the binaries and byte-compiled
+wrappers travel with the repository in oracle/_ref/):
+
+* testing/loctest.c -- the locator's known answer: the optimum it prints
+  equals the "True index" it prints (loctest.c:160-169);
+* performanceTests/convergence.c -- 2D LSM against the analytic solutions on
+  eight grids from h = 100 m to 0.78 m (convergence.c:14-133): the norms it
+  prints equal the FP64 oracle's for the same solves and fall at first order;
+* python/fteik3d.py and python/fteik2d.py -- the reference's ctypes wrappers
+  (they bind libfteik_shared.so from LD_LIBRARY_PATH and pass velocities and
+  fields in the ZYX / ZX orderings): their solves equal the oracle's.
+"""
+import importlib.util
+import os
+import re
+import subprocess
+from importlib.machinery import SourcelessFileLoader
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from models import layered_grf_cells
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref")
+LIBDIR = os.path.join(ROOT, "fteik_b200", "lib")
+
+
+def _need(path):
+    if not os.path.exists(path):
+        pytest.skip("%s not built (oracle/ref_callers.mk needs the reference tree)" % path)
+    return path
+
+
+def _run(prog):
+    out = subprocess.run([_need(os.path.join(REF, prog))], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    return out.stdout
+
+
+def test_loctest_finds_the_true_index(fk):
+    out = _run("loctest")
+    m = re.search(r"optindex, t0, obj:\s*(\d+)\s+(\S+)\s+(\S+)", out)
+    t = re.search(r"True index:\s*(\d+)", out)
+    assert m and t, out
+    opt, t0, obj = int(m.group(1)), float(m.group(2)), float(m.group(3))
+    true_idx = int(t.group(1))
+    # loctest.c:34-44: nz, nx, ny = 101, 95, 98, source node (nz/2, nx/2, ny/2);
+    # receivers 1..9 sit at x = y, receiver 10 at x = y = 0, so the node with x
+    # and y swapped is an equally good optimum up to the tables' rounding
+    nz, nx, ny = 101, 95, 98
+    zs, xs, ys = nz // 2, nx // 2, ny // 2
+    assert true_idx == ys * nz * nx + xs * nz + zs + 1
+    mirror = xs * nz * nx + ys * nz + zs + 1
+    assert opt in (true_idx, mirror), out
+    assert obj < 1e-8
+    # t0Opt is in the picks' own time base: the 1.5 s origin time
+    assert abs(t0 - 1.5) < 1e-4, out
+
+
+def _convergence_oracle(job, i):
+    """The solve and norms of convergence.c:41-125 for grid i, from the oracle."""
+    dx0 = dz0 = 100.0 / 2 ** i
+    nx = int(1000.0 / dx0 + 0.5) + 1
+    nz = int(1000.0 / dz0 + 0.5) + 1
+    xs, zs = (nx - 1) * dx0 / 2.0, (nz - 1) * dz0 / 2.0
+    if job == 1:
+        v = np.full(nz - 1, 1000.0)
+    else:
+        v = 1000.0 + 1000.0 / 1000.0 * (np.arange(nz - 1) * dz0)
+    slow = np.tile(1.0 / v, nx - 1)                    # natural order: z fastest
+    si, sa = O.source_snap(False, (nz, nx, 1), (0, 0, 0), (dz0, dx0, 1.0), (zs, xs, 0.0))
+    tt, _ = O.solve2d((nz, nx), (dz0, dx0), slow, si[:2], sa[:2], eps=3.0, nsweep=2)
+    if job == 1:
+        ta = O.analytic_constant((nz, nx, 1), (0, 0, 0), (dz0, dx0, 1.0), 1000.0, (zs, xs, 0.0))
+    else:
+        ta = O.analytic_linear((nz, nx, 1), (0, 0, 0), (dz0, dx0, 1.0), 1000.0, 2000.0, (zs, xs, 0.0))
+    r = tt - ta
+    n = nz * nx
+    return n, np.sum(np.abs(r)) / n, np.sqrt(np.sum(r * r)) / n, max(0.0, np.max(r))
+
+
+def test_convergence_program_matches_oracle_and_converges(fk):
+    out = _run("convergence")
+    rows = [ln.split() for ln in out.splitlines() if re.match(r"^\s*\d+\s+\S+e", ln)]
+    assert len(rows) == 16, out
+    for job in (1, 2):
+        block = rows[8 * (job - 1): 8 * job]
+        l1 = np.array([float(r[4]) for r in block])
+        for i in range(5):   # grids up to 161 x 161: the oracle's solves take seconds
+            n, o1, o2, o8 = _convergence_oracle(job, i)
+            r = block[i]
+            assert int(r[0]) == n
+            for got, want in ((float(r[4]), o1), (float(r[5]), o2), (float(r[6]), o8)):
+                assert abs(got - want) <= 1e-5 * abs(want) + 1e-15, (job, i, got, want)
+        # first order: the mean error halves with h (rate between 0.6 and 1.6)
+        rate = np.log2(l1[:-1] / l1[1:])
+        assert np.all(l1[1:] < l1[:-1]), l1
+        assert 0.6 < np.mean(rate) < 1.6, rate
+
+
+def _load_wrapper(name):
+    path = _need(os.path.join(REF, "python", name + ".pyc"))
+    os.environ["LD_LIBRARY_PATH"] = os.pathsep.join([LIBDIR, os.environ.get("LD_LIBRARY_PATH", "")])
+    loader = SourcelessFileLoader(name, path)
+    spec = importlib.util.spec_from_loader(name, loader)
+    mod = importlib.util.module_from_spec(spec)
+    loader.exec_module(mod)
+    return mod
+
+
+@pytest.mark.parametrize("nodal", [False, True])
+def test_python_fteik3d_wrapper(fk, nodal):
+    m = _load_wrapper("fteik3d")
+    n, h = (21, 18, 16), (25.0, 20.0, 30.0)   # nz, nx, ny
+    nz, nx, ny = n
+    src = (213.3, 171.9, 232.6)               # z, x, y
+    s = m.fteik3d()
+    assert s.initialize(nx, ny, nz, h[1], h[2], h[0], nsweep=2, eps=5.0) == 0
+    if nodal:
+        rng = np.random.default_rng(8)
+        vnode = 3000.0 + 2.0 * (np.arange(nz) * h[0])[None, None, :] + 50.0 * rng.random((ny, nx, nz))
+        # the wrapper takes [nz, ny, nx] and passes it in ZYX order (order 2)
+        assert s.setVelocityModel(vnode.transpose(2, 0, 1)) == 0
+        slow = O.nodal_to_slowness(n, 0, vnode.ravel(), keep_defects=False)
+    else:
+        vcell = layered_grf_cells(*n, seed=6, min_cells=3)          # [ny-1][nx-1][nz-1]
+        assert s.setVelocityModel(vcell.transpose(2, 0, 1)) == 0
+        slow = 1.0 / vcell.ravel()
+    s.setSources(np.array([src[1]]), np.array([src[2]]), np.array([src[0]]))
+    assert s.solveLSM() == 0
+    tt = s.getTravelTimeField()                                     # [nz, ny, nx]
+    got = np.asarray(tt).transpose(1, 2, 0).ravel()                 # natural order
+    si, sa = O.source_snap(True, n, (0, 0, 0), h, src)
+    ref, _ = O.solve3d(n, h, slow, si, sa, 5.0, 2)
+    # the library's default precision (FP32 fields) against the FP64 oracle
+    assert np.max(np.abs(got - ref) / np.maximum(ref, 1e-6)) <= 1e-4
+    s.free()
+
+
+def test_python_fteik2d_wrapper(fk):
+    m = _load_wrapper("fteik2d")
+    nz, nx, h = 31, 27, 10.0
+    s = m.fteik2d()
+    assert s.initialize(nx, nz, h, h, nsweep=2, eps=3.0) == 0
+    rng = np.random.default_rng(2)
+    vcell = (3000.0 + 2.0 * (np.arange(nz - 1) + 0.5) * h)[:, None] * (1 + 0.05 * rng.standard_normal((nz - 1, nx - 1)))
+    assert s.setVelocityModel(vcell) == 0                            # [nz-1, nx-1], ZX order
+    xs, zs = np.array([101.3, 203.9]), np.array([77.7, 150.2])
+    s.setSources(xs, zs)
+    s.setReceivers(np.array([12.0, 250.0, 133.3]), np.array([0.0, 280.0, 41.0]))
+    assert s.solveLSM() == 0
+    slow = 1.0 / vcell.ravel(order="F")
+    ttr = s.getTravelTimes()                                         # [nrec, nsrc]
+    for k in range(2):
+        si, sa = O.source_snap(False, (nz, nx, 1), (0, 0, 0), (h, h, 1.0), (zs[k], xs[k], 0.0))
+        ref, _ = O.solve2d((nz, nx), (h, h), slow, si[:2], sa[:2], eps=3.0, nsweep=2)
+        want, _ = O.receivers(False, (nz, nx, 1), (0, 0, 0), (h, h, 1.0), np.array([0.0, 280.0, 41.0]),
+                              np.array([12.0, 250.0, 133.3]), None, ref)
+        assert np.max(np.abs(np.asarray(ttr)[:, k] - want)) <= 1e-12 * np.max(want)
+    # the field left behind is the last source's (as after the reference's loop)
+    tt = np.asarray(s.getTravelTimeField()).ravel(order="F")
+    assert np.max(np.abs(tt - ref)) <= 1e-12 * np.max(ref)
+    s.free()

@@ -1,0 +1,102 @@
+"""Launch configurations of the 3D slab sweeps (fteik_b200_setSlabConfig):
+the staged FP32 pass step (16-byte cp.async groups through shared memory),
+one or two sources per thread, progress every 8 or 32 steps, 1 to 4
+resident blocks per SM.  Each changes only how the same node updates are
+scheduled and loaded, so every configuration gives the default's FP32
+fields bit for bit -- single source and batch, fixed passes and solves to
+convergence -- on grids whose depth takes every leading-item offset of the
+staged step's descending sweeps (nz mod 4 = 0..3), shallower and deeper than
+32, and wider than one 32-column block.  No counterpart in the reference."""
+import numpy as np
+import pytest
+
+from models import interior_source, layered_grf_cells
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = [(1, 1, -1, -1), (1, 0, 8, -1), (1, 1, 32, 2), (0, 0, 32, 1), (1, 1, 8, 4)]
+SHAPES = {            # nz, nx, ny
+    "nz23": (23, 19, 17),
+    "nz30_wide": (30, 70, 13),
+    "nz12": (12, 14, 13),
+    "nz45": (45, 40, 10),
+    "nz9_wide": (9, 70, 11),
+}
+
+
+def _solve_single(fk, n, h, vel, src, cfg):
+    old = fk.set_slab_config(*cfg)
+    try:
+        s = fk.fteik3d()
+        s.initialize(n[1], n[2], n[0], h[1], h[2], h[0], nsweep=2, eps=5.0, precision=4)
+        s.setCellSlownessNatural(vel)
+        s.setSources(src[1], src[2], src[0])
+        s.solveSourceLSM(1)
+        tt = s.getTravelTimeField()
+        s.free()
+    finally:
+        fk.set_slab_config(*old)
+    return tt
+
+
+@pytest.mark.parametrize("shape", sorted(SHAPES))
+def test_single_source_configs_same_bits(fk, shape):
+    n = SHAPES[shape]
+    h = (25.0, 20.0, 30.0)
+    vel = layered_grf_cells(*n, seed=sum(n), min_cells=2)
+    src = interior_source(n, h, n[0])
+    ref = _solve_single(fk, n, h, vel, src, (-1, -1, -1, -1))
+    for cfg in CONFIGS:
+        got = _solve_single(fk, n, h, vel, src, cfg)
+        assert np.array_equal(got, ref), cfg
+
+
+def _batch(fk, grids, srcs, vels, cfg, **kw):
+    old = fk.set_slab_config(*cfg)
+    try:
+        b = fk.Batch3D(grids, precision=4, eps=5.0, **kw)
+        for ig in range(len(grids)):
+            b.setVelocityModel(ig + 1, vels[ig])
+            z, x, y = srcs[ig]
+            b.setSources(ig + 1, z, x, y)
+        b.solve()
+        out = [b.fields32(ig + 1).copy() for ig in range(len(grids))]
+        info = [b.solveInfo(ig + 1, 1) for ig in range(len(grids))]
+        b.finalize()
+    finally:
+        fk.set_slab_config(*old)
+    return out, info
+
+
+def _batch_case():
+    grids = [(23, 40, 12, 25.0, 25.0, 25.0), (30, 17, 15, 30.0, 20.0, 25.0), (12, 33, 9, 20.0, 20.0, 20.0)]
+    rng = np.random.default_rng(7)
+    srcs, vels = [], []
+    for ig, (nz, nx, ny, dz, dx, dy) in enumerate(grids):
+        k = 3 if ig != 1 else 2                        # odd source counts walk one source alone
+        z = rng.uniform(0, (nz - 1) * dz, k)
+        z[0] = 0.0                                     # a surface source (the on-node nudge)
+        srcs.append((z, rng.uniform(0, (nx - 1) * dx, k), rng.uniform(0, (ny - 1) * dy, k)))
+        vels.append(layered_grf_cells(nz, nx, ny, seed=60 + ig, min_cells=2))
+    return grids, srcs, vels
+
+
+def test_batch_configs_same_bits(fk):
+    grids, srcs, vels = _batch_case()
+    ref, _ = _batch(fk, grids, srcs, vels, (-1, -1, -1, -1), nsweep=2)
+    for cfg in CONFIGS:
+        got, _ = _batch(fk, grids, srcs, vels, cfg, nsweep=2)
+        for a, b in zip(ref, got):
+            assert np.array_equal(a, b), cfg
+
+
+def test_batch_converged_configs_same_bits(fk):
+    """Passes to convergence (the FP64 residual compiled into the pass
+    kernel): the same fields and the same pass counts."""
+    grids, srcs, vels = _batch_case()
+    ref, rinfo = _batch(fk, grids, srcs, vels, (-1, -1, -1, -1), convTol=0.0, maxPass=25)
+    for cfg in CONFIGS[:3]:
+        got, info = _batch(fk, grids, srcs, vels, cfg, convTol=0.0, maxPass=25)
+        assert info == rinfo, cfg
+        for a, b in zip(ref, got):
+            assert np.array_equal(a, b), cfg

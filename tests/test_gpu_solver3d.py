@@ -76,13 +76,7 @@ def test_fp32_within_tolerance(fk, name):
     rel = np.abs(tt - ref) / np.maximum(ref, 1e-6)
     k = int(np.argmax(rel))
     where = (k % n[0], (k // n[0]) % n[1], k // (n[0] * n[1]))
-    tol = TOL32
-    if name == "node":
-        # a source exactly on a node of a constant medium makes many upwind
-        # differences tie exactly in FP64; FP32 rounding breaks those ties and
-        # selects neighbouring stencils, a discretisation-size difference
-        tol = 1e-3
-    assert np.max(rel) <= tol, (np.max(rel), np.sqrt(np.mean(rel ** 2)), where, ref[k], tt[k])
+    assert np.max(rel) <= TOL32, (np.max(rel), np.sqrt(np.mean(rel ** 2)), where, ref[k], tt[k])
     s.free()
 
 
