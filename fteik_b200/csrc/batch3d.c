@@ -15,6 +15,7 @@
 #include "fteik_b200.h"
 #include "slabplan.h"
 
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -54,6 +55,9 @@ static struct {
     fk_slabplan_t plan;     /* slab-pipelined schedule */
     int spin_epoch;         /* poll limit the plan (and graph) was built with */
     int cfg_epoch;          /* slab configuration the plan (and graph) was built with */
+    int tuned[5];           /* configuration in use: staged, pairs, progress, blocks/SM passes, init */
+    float tune_ms[2];       /* its init / pass kernel times when tuned (0: not timed) */
+    int tune_runs;          /* candidate solves the last tuning ran (0: cache hit or nothing to tune) */
     bool work_dirty;        /* source positions changed, shape unchanged */
     cudaGraphExec_t graph;
     bool graph_ok;
@@ -408,9 +412,6 @@ static int build_work(const char *who)
         const int np = (SB.conv_tol >= 0.0 && SB.max_pass > 0) ? SB.max_pass : SB.nsweep;
         const fk_slabcfg_t cfg = fk_slabcfg();
         e = fk_slabplan_build(&SB.plan, nwork, wnx, wny, wnz, wg, np, cfg.pairs != 0, who);
-        SB.plan.dev.staged = SB.precision == 4 && cfg.staged == 1;
-        SB.plan.dev.progress = cfg.progress > 0 ? cfg.progress : 0;
-        SB.plan.dev.blocks_per_sm = cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 0;
         SB.spin_epoch = fk_spin_epoch();
         SB.cfg_epoch = fk_slabcfg_epoch();
         free(wnx);
@@ -424,6 +425,189 @@ static int build_work(const char *who)
     SB.max_nx = max_nx;
     SB.max_nz = max_nz;
     return fk_check(e, who);
+}
+
+/* ------------------------------------------------------------------ tuner --
+ * Launch configuration of the two persistent sweep kernels, chosen per work
+ * list by timing (no counterpart in the reference, whose OpenMP loops have a
+ * fixed chunk size, constants.F90:23).  The knobs (fteik_b200_setSlabConfig)
+ * the caller left at -1 are searched on the first solve of a new work list,
+ * eagerly, with CUDA events around each kernel:
+ *   1. staged x pairs x progress (8 | 32), all resident blocks;
+ *   2. the best of 1 at 3 and 2 resident blocks per SM;
+ * the pass kernel takes the fastest pass time, the initialisation kernel the
+ * blocks per SM of the fastest initialisation time.  Every candidate is run
+ * twice and timed by its faster run.  Every configuration gives the same
+ * fields bit for bit, so the search changes only the time.  The choice is
+ * kept per work list (grid shapes, sources per grid, precision, passes) in
+ * memory and, when FTEIK_B200_TUNE_CACHE names a file, in that file, so
+ * later processes skip the search. */
+static void tune_apply(const int t[5])
+{
+    SB.plan.dev.staged = SB.precision == 4 && t[0] == 1;
+    SB.plan.dev.pairs = t[1] ? SB.plan.pairs_all : NULL;
+    SB.plan.dev.progress = t[2];
+    SB.plan.dev.blocks_per_sm = t[3];
+    SB.plan.dev.init_blocks_per_sm = t[4];
+    memcpy(SB.tuned, t, sizeof(SB.tuned));
+}
+
+static void tune_key(char *key, size_t cap)
+{
+    struct cudaDeviceProp prop;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+        prop.name[0] = 0;
+        prop.multiProcessorCount = 0;
+    }
+    size_t o = (size_t)snprintf(key, cap, "%s|sm%d|p%d|n%d|c%d:%d|", prop.name, prop.multiProcessorCount,
+                                SB.precision, SB.nsweep, SB.conv_tol >= 0.0, SB.max_pass);
+    for (int i = 0; i < SB.ngrid && o < cap; i++)
+        o += (size_t)snprintf(key + o, cap - o, "%dx%dx%dx%d;", SB.g[i].nz, SB.g[i].nx, SB.g[i].ny, SB.g[i].nsrc);
+    for (char *c = key; *c; c++)
+        if (*c == ' ' || *c == '\t' || *c == '\n') *c = '_';
+}
+
+#define TUNE_MEM 16
+static char g_tune_key[TUNE_MEM][512];
+static int g_tune_val[TUNE_MEM][5];
+static int g_tune_n = 0;
+
+static int tune_lookup(const char *key, int t[5])
+{
+    for (int i = 0; i < g_tune_n; i++)
+        if (strcmp(g_tune_key[i], key) == 0) { memcpy(t, g_tune_val[i], 5 * sizeof(int)); return 1; }
+    const char *path = getenv("FTEIK_B200_TUNE_CACHE");
+    if (!path || !*path) return 0;
+    FILE *f = fopen(path, "r");
+    if (!f) return 0;
+    char line[700], k[600];
+    int found = 0;
+    while (fgets(line, sizeof(line), f))
+        if (sscanf(line, "%599s %d %d %d %d %d", k, &t[0], &t[1], &t[2], &t[3], &t[4]) == 6 && strcmp(k, key) == 0)
+            found = 1;   /* the last line for a key wins */
+    fclose(f);
+    return found;
+}
+
+static void tune_store(const char *key, const int t[5])
+{
+    const int i = g_tune_n < TUNE_MEM ? g_tune_n++ : TUNE_MEM - 1;
+    snprintf(g_tune_key[i], sizeof(g_tune_key[i]), "%s", key);
+    memcpy(g_tune_val[i], t, 5 * sizeof(int));
+    const char *path = getenv("FTEIK_B200_TUNE_CACHE");
+    if (!path || !*path) return;
+    FILE *f = fopen(path, "a");
+    if (!f) return;
+    fprintf(f, "%s %d %d %d %d %d\n", key, t[0], t[1], t[2], t[3], t[4]);
+    fclose(f);
+}
+
+/* One eager solve of the current plan with events around both kernels. */
+static int tune_time(float *init_ms, float *pass_ms)
+{
+    cudaStream_t s = fk_stream();
+    fk3d_slabs_set_events(SB.ev);
+    int e = fk3d_solve_slabs(SB.precision, SB.grids_dev, SB.work_dev, SB.nwork, &SB.plan.dev, SB.res_dev,
+                             SB.eps, SB.nsweep, SB.conv_tol, SB.max_pass, s);
+    fk3d_slabs_set_events(NULL);
+    if (!e) e = (int)cudaEventSynchronize(SB.ev[2]);
+    if (!e) e = (int)cudaEventElapsedTime(init_ms, SB.ev[0], SB.ev[1]);
+    if (!e) e = (int)cudaEventElapsedTime(pass_ms, SB.ev[1], SB.ev[2]);
+    if (!e) e = (int)cudaMemcpyAsync(SB.res_host, SB.res_dev, sizeof(fk_result3d_t) * (size_t)SB.nwork,
+                                    cudaMemcpyDeviceToHost, s);
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    for (int w = 0; !e && w < SB.nwork; w++)
+        if (SB.res_host[w].status) e = (int)cudaErrorLaunchFailure;
+    return e;
+}
+
+static int ensure_events(void)
+{
+    if (SB.have_ev) return 0;
+    bool ok = true;
+    for (int i = 0; i < 3; i++) ok = ok && cudaEventCreate(&SB.ev[i]) == cudaSuccess;
+    SB.have_ev = ok;
+    return ok ? 0 : 1;
+}
+
+static int tune(const char *who)
+{
+    const fk_slabcfg_t cfg = fk_slabcfg();
+    int t[5] = {SB.precision == 4 && cfg.staged == 1, cfg.pairs != 0, cfg.progress > 0 ? cfg.progress : 0,
+                cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 0, cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 0};
+    /* a knob at 0 is explicit: progress by task count, all resident blocks */
+    SB.tune_ms[0] = SB.tune_ms[1] = 0.0f;
+    SB.tune_runs = 0;
+    const bool search = (cfg.staged < 0 && SB.precision == 4) || cfg.pairs < 0 || cfg.progress < 0 ||
+                        cfg.blocks_per_sm < 0;
+    if (!search) { tune_apply(t); return 0; }
+    char key[512];
+    tune_key(key, sizeof(key));
+    if (tune_lookup(key, t)) { tune_apply(t); return 0; }
+    if (ensure_events()) { FK_ERR("%s: cannot create events", who); return 1; }
+    const int st_n = (cfg.staged < 0 && SB.precision == 4) ? 2 : 1;
+    const int pr_n = cfg.pairs < 0 ? 2 : 1;
+    const int ch_n = cfg.progress < 0 ? 2 : 1;
+    float best_pass = 3.4e38f, best_init[5];
+    int best[5];
+    for (int b = 0; b < 5; b++) best_init[b] = 3.4e38f;
+    for (int a = 0; a < st_n * pr_n * ch_n; a++) {
+        int c[5] = {st_n == 2 ? a % 2 : t[0], pr_n == 2 ? 1 - (a / st_n) % 2 : t[1],
+                    ch_n == 2 ? ((a / (st_n * pr_n)) % 2 ? 32 : 8) : t[2], t[3], t[4]};
+        tune_apply(c);
+        float im = 3.4e38f, pm = 3.4e38f;
+        for (int r = 0; r < 2; r++) {
+            float i1, p1;
+            if (fk_check(tune_time(&i1, &p1), who)) return 1;
+            im = i1 < im ? i1 : im;
+            pm = p1 < pm ? p1 : pm;
+            SB.tune_runs++;
+        }
+        if (im < best_init[c[4]]) best_init[c[4]] = im;
+        if (pm < best_pass) { best_pass = pm; memcpy(best, c, sizeof(best)); }
+    }
+    if (cfg.blocks_per_sm < 0) {
+        for (int bps = 3; bps >= 2; bps--) {
+            int c[5] = {best[0], best[1], best[2], bps, bps};
+            tune_apply(c);
+            float im = 3.4e38f, pm = 3.4e38f;
+            for (int r = 0; r < 2; r++) {
+                float i1, p1;
+                if (fk_check(tune_time(&i1, &p1), who)) return 1;
+                im = i1 < im ? i1 : im;
+                pm = p1 < pm ? p1 : pm;
+                SB.tune_runs++;
+            }
+            if (im < best_init[bps]) best_init[bps] = im;
+            if (pm < best_pass) { best_pass = pm; memcpy(best, c, sizeof(best)); }
+        }
+        int bi = 0;
+        for (int b = 0; b < 5; b++) if (best_init[b] < best_init[bi]) bi = b;
+        best[4] = bi;
+    }
+    tune_apply(best);
+    SB.tune_ms[0] = best_init[best[4]];
+    SB.tune_ms[1] = best_pass;
+    tune_store(key, best);
+    return 0;
+}
+
+void fteik_b200_batch3d_getSlabConfig(int *staged, int *pairs, int *progress, int *blocksPerSM,
+                                      int *initBlocksPerSM, float *initMs, float *passMs, int *tuneRuns,
+                                      int *ierr)
+{
+    *ierr = SB.graph_ok ? 0 : 1;
+    if (!SB.graph_ok) FK_ERR("fteik_b200_batch3d_getSlabConfig: solve once first");
+    *staged = SB.tuned[0];
+    *pairs = SB.tuned[1];
+    *progress = SB.tuned[2];
+    *blocksPerSM = SB.tuned[3];
+    *initBlocksPerSM = SB.tuned[4];
+    *initMs = SB.tune_ms[0];
+    *passMs = SB.tune_ms[1];
+    *tuneRuns = SB.tune_runs;
 }
 
 void fteik_b200_batch3d_solve(int *ierr)
@@ -440,6 +624,7 @@ void fteik_b200_batch3d_solve(int *ierr)
     if (!SB.graph_ok) {
         if (build_work(who)) return;
         SB.work_dirty = false;
+        if (tune(who)) return;
         cudaGraph_t graph;
         int e = (int)cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (!e) {
@@ -657,12 +842,7 @@ void fteik_b200_batch3d_timeSolve(float *init_ms, float *pass_ms, int *ierr)
     *ierr = 1;
     if (!SB.graph_ok) { FK_ERR("%s: solve once first", who); return; }
     if (SB.work_dirty && upload_work(who)) return;
-    if (!SB.have_ev) {
-        bool ok = true;
-        for (int i = 0; i < 3; i++) ok = ok && cudaEventCreate(&SB.ev[i]) == cudaSuccess;
-        SB.have_ev = ok;
-        if (!ok) { FK_ERR("%s: cannot create events", who); return; }
-    }
+    if (ensure_events()) { FK_ERR("%s: cannot create events", who); return; }
     cudaStream_t s = fk_stream();
     fk3d_slabs_set_events(SB.ev);
     int e = fk3d_solve_slabs(SB.precision, SB.grids_dev, SB.work_dev, SB.nwork, &SB.plan.dev,

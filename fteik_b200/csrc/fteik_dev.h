@@ -74,8 +74,9 @@ typedef struct {
     int ntask2_sweep;
     /* launch configuration: FP32 passes in the staged pass step (every
      * grid's slowz built); progress step of the passes (8, 32 or 0 = by the
-     * number of slab tasks); resident blocks per SM (0 = as many as fit) */
-    int staged, progress, blocks_per_sm;
+     * number of slab tasks); resident blocks per SM of the pass and of the
+     * initialisation kernel (0 = as many as fit) */
+    int staged, progress, blocks_per_sm, init_blocks_per_sm;
 } fk_slabs3d_t;
 
 #define FK_SLAB_Y 4

@@ -78,10 +78,10 @@ void fteik_b200_setSlabConfig(int staged, int pairs, int progress, int blocksPer
 {
     *ierr = 0;
     if (staged < -1 || staged > 1 || pairs < -1 || pairs > 1 ||
-        !(progress == -1 || progress == 8 || progress == 32) || blocksPerSM < -1 || blocksPerSM == 0 ||
+        !(progress == -1 || progress == 0 || progress == 8 || progress == 32) || blocksPerSM < -1 ||
         blocksPerSM > 4) {
-        FK_ERR("fteik_b200_setSlabConfig: staged and pairs must be -1, 0 or 1, progress -1, 8 or 32, "
-               "blocksPerSM -1 or 1..4");
+        FK_ERR("fteik_b200_setSlabConfig: staged and pairs must be -1, 0 or 1, progress -1, 0, 8 or 32, "
+               "blocksPerSM -1, 0 or 1..4");
         *ierr = 1;
         return;
     }

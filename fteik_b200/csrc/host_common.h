@@ -28,8 +28,8 @@ int fk_spin_epoch(void);
 typedef struct {
     int staged;          /* FP32 passes: staged pass step (1) or direct loads (0) */
     int pairs;           /* passes: two sources of one grid per thread (1) or one (0) */
-    int progress;        /* passes: progress published every 8 or 32 steps */
-    int blocks_per_sm;   /* resident blocks per SM of the persistent kernels, 1..4 */
+    int progress;        /* passes: progress every 8 or 32 steps, 0 = by the number of slab tasks */
+    int blocks_per_sm;   /* resident blocks per SM of the persistent kernels, 1..4, 0 = all that fit */
 } fk_slabcfg_t;
 fk_slabcfg_t fk_slabcfg(void);
 int fk_slabcfg_epoch(void);

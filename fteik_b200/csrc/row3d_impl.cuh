@@ -1015,9 +1015,9 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
     if (fk3tw::g_slab_events) cudaEventRecord(fk3tw::g_slab_events[0], st);
     int rc;
     if constexpr (sizeof(R) == 4)
-        rc = launch_init_f32(P, zring, st, pl->blocks_per_sm);
+        rc = launch_init_f32(P, zring, st, pl->init_blocks_per_sm);
     else
-        rc = launch_slab_kernel<R, true, false, 1>(P, nullptr, zring, st, 0, pl->blocks_per_sm);
+        rc = launch_slab_kernel<R, true, false, 1>(P, nullptr, zring, st, 0, pl->init_blocks_per_sm);
     if (rc) return rc;
     if (fk3tw::g_slab_events) cudaEventRecord(fk3tw::g_slab_events[1], st);
     if (npass > 0) {

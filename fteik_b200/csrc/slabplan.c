@@ -55,7 +55,7 @@ int fk_slabplan_build(fk_slabplan_t *pl, int nwork, const int *nx, const int *ny
     for (int w = 0; w < nwork; w++) {
         pairs[2 * npair] = w;
         pairs[2 * npair + 1] = -1;
-        if (pairing && w + 1 < nwork && gid[w + 1] == gid[w]) pairs[2 * npair + 1] = ++w;
+        if (w + 1 < nwork && gid[w + 1] == gid[w]) pairs[2 * npair + 1] = ++w;
         npair++;
     }
     long ntask2 = 0;
@@ -110,7 +110,8 @@ int fk_slabplan_build(fk_slabplan_t *pl, int nwork, const int *nx, const int *ny
     pl->dev.max_nx = maxnx;
     pl->dev.max_ny = maxny;
     pl->dev.max_nz = maxnz;
-    pl->dev.pairs = pairing ? (const int *)(m + off_pairs) : NULL;
+    pl->pairs_all = (const int *)(m + off_pairs);
+    pl->dev.pairs = pairing ? pl->pairs_all : NULL;
     pl->dev.tasks2 = (const int *)(m + off_t2);
     pl->dev.ntask2_sweep = (int)ntask2;
     return 0;

@@ -235,6 +235,7 @@ void fteik_solver3d_solveSourceLSM(int isrc, int *ierr)
         S3.plan.dev.staged = staged;
         S3.plan.dev.progress = cfg.progress > 0 ? cfg.progress : 0;
         S3.plan.dev.blocks_per_sm = cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 0;
+        S3.plan.dev.init_blocks_per_sm = S3.plan.dev.blocks_per_sm;
         e = fk3d_solve_slabs(S3.precision, S3.grid_dev, S3.work_dev, 1, &S3.plan.dev, S3.res_dev,
                              S3.eps, S3.nsweep, -1.0, 0, s);
     }

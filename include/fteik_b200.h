@@ -310,8 +310,10 @@ void fteik_b200_getSpinLimit(long long *polls);
  *               and slowness move in 16-byte groups through shared memory
  *               (cp.async), 0 = one 4-byte load per value and step;
  *   pairs       passes: 1 = two sources of one grid share each thread, 0 = one;
- *   progress    passes: slabs publish progress every 8 or 32 steps;
- *   blocksPerSM resident blocks per SM, 1..4.
+ *   progress    passes: slabs publish progress every 8 or 32 steps, or 0 =
+ *               8 when a sweep has fewer than 4 slab tasks per resident
+ *               block, else 32;
+ *   blocksPerSM resident blocks per SM, 1..4, or 0 = as many as fit.
  * Results are the same bits whichever configuration runs.  Takes effect at
  * the next solve (a captured batch graph is rebuilt).  No counterpart in the
  * reference. */
@@ -371,6 +373,17 @@ void fteik_b200_batch3d_waitDownloads(int *ierr);
 /* Receiver times of every source of a grid: ttr[isrc*nrec + irec]. */
 void fteik_b200_batch3d_getTravelTimes64f(int igrid, int nval, double ttr[],
                                           int *ierr);
+/* The launch configuration the batch runs (see fteik_b200_setSlabConfig):
+ * knobs left at -1 are chosen by timing the candidates on the first solve of
+ * a new work list (grid shapes, sources per grid, precision, passes); the
+ * choice is remembered in the process and, when the environment variable
+ * FTEIK_B200_TUNE_CACHE names a file, appended to that file for later
+ * processes.  initMs / passMs: the chosen kernels' times during the search
+ * (0 when nothing was searched), tuneRuns the candidate solves it ran (0 on
+ * a cache hit).  No counterpart in the reference. */
+void fteik_b200_batch3d_getSlabConfig(int *staged, int *pairs, int *progress, int *blocksPerSM,
+                                      int *initBlocksPerSM, float *initMs, float *passMs, int *tuneRuns,
+                                      int *ierr);
 /* Run one solve outside its CUDA graph with events around the
  * initialisation kernel and the Gauss-Seidel kernel and return their device
  * times (ms); the fields end as after fteik_b200_batch3d_solve. */

@@ -100,3 +100,75 @@ def test_batch_converged_configs_same_bits(fk):
         assert info == rinfo, cfg
         for a, b in zip(ref, got):
             assert np.array_equal(a, b), cfg
+
+
+def _timed(fk, b, k=5):
+    import torch
+    stream = torch.cuda.ExternalStream(fk.lib().fteik_b200_stream())
+    for _ in range(2):
+        b.solveAsync()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e30
+    for _ in range(3):
+        e0.record(stream)
+        for _ in range(k):
+            b.solveAsync()
+        e1.record(stream)
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / k)
+    return best
+
+
+@pytest.mark.parametrize("kind", ["batch", "one_grid"])
+def test_tuned_configuration_not_slower_than_fixed(fk, kind, tmp_path, monkeypatch):
+    """The configuration the batch picks by timing (knobs at -1) is not
+    slower than the fixed configuration the library ran before it had a
+    tuner (direct loads, source pairs, progress step by task count, all
+    resident blocks), on a multi-grid batch and on one grid; the choice goes
+    to the cache file, and a second batch of the same work list reuses it
+    instead of searching again."""
+    monkeypatch.setenv("FTEIK_B200_TUNE_CACHE", str(tmp_path / "tune.txt"))
+    if kind == "batch":
+        grids = [(48, 96, 64, 50.0, 50.0, 50.0), (64, 80, 72, 50.0, 50.0, 50.0)]
+        nsrc = 16
+    else:
+        grids = [(64, 128, 96, 50.0, 50.0, 50.0)]
+        nsrc = 1
+    rng = np.random.default_rng(5)
+
+    def make():
+        b = fk.Batch3D(grids, nsweep=2, eps=5.0, precision=4)
+        for ig, (nz, nx, ny, dz, dx, dy) in enumerate(grids, start=1):
+            b.setVelocityModel(ig, layered_grf_cells(nz, nx, ny, seed=ig, min_cells=3))
+            r = np.random.default_rng(ig)
+            b.setSources(ig, np.zeros(nsrc), r.uniform(0, (nx - 1) * dx, nsrc), r.uniform(0, (ny - 1) * dy, nsrc))
+        return b
+
+    old = fk.set_slab_config(0, 1, 0, 0)
+    try:
+        b = make()
+        b.solve()
+        fixed = _timed(fk, b)
+        f_fixed = [b.fields32(ig + 1).copy() for ig in range(len(grids))]
+        b.finalize()
+    finally:
+        fk.set_slab_config(*old)
+    fk.set_slab_config(-1, -1, -1, -1)
+    b = make()
+    b.solve()
+    cfg = b.slabConfig()
+    tuned = _timed(fk, b)
+    assert cfg["tune_runs"] > 0
+    for ig in range(len(grids)):
+        assert np.array_equal(b.fields32(ig + 1), f_fixed[ig])
+    b.finalize()
+    assert tuned <= fixed * 1.03, (tuned, fixed, cfg)
+    b = make()
+    b.solve()
+    again = b.slabConfig()
+    b.finalize()
+    assert again["tune_runs"] == 0
+    assert (tmp_path / "tune.txt").read_text().count("\n") >= 1
+    assert [again[k] for k in ("staged", "pairs", "progress", "blocks_per_sm", "init_blocks_per_sm")] == \
+        [cfg[k] for k in ("staged", "pairs", "progress", "blocks_per_sm", "init_blocks_per_sm")]
