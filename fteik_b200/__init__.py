@@ -146,6 +146,11 @@ _SIGS = {
     "fteik_b200_batch3d_waitDownloads": [_PI],
     "fteik_b200_solver3d_getTravelTimeGradient64f": [c_int, _PD, _PI],
     "fteik_b200_solver2d_getTravelTimeGradient64f": [c_int, _PD, _PD, _PI],
+    "fteik_rays_setODEIntegrator": [c_int, _PI],
+    "fteik_b200_solver2d_getNumberOfRays": [_PI, _PI],
+    "fteik_b200_solver2d_getRayTimes": [c_int, _PD, _PD, _PD, _PI, _PI],
+    "fteik_b200_solver2d_getRayPath": [c_int, c_int, _PD, _PD, _PI, _PI],
+    "fteik_b200_solver2d_getRayCells": [c_int, c_int, _PI, _PD, _PI, _PI],
     "fteik_b200_batch3d_getTravelTimes64f": [c_int, c_int, _PD, _PI],
     "fteik_b200_batch3d_getSolveInfo": [c_int, c_int, _PD, _PI, _PI],
     "fteik_b200_batch3d_exportToLocator": [c_int, c_int, _PI],
@@ -471,6 +476,43 @@ class fteik2d:
         ierr = c_int(1)
         self.lib.fteik_solver2d_traceRaysToPoints(x.size, px, pz, byref(ierr))
         return ierr.value
+
+    def setODEIntegrator(self, integrator):
+        """rays.F90:215-229: 1 Euler, 2 midpoint, 3 RK4; returns ierr."""
+        ierr = c_int(1)
+        self.lib.fteik_rays_setODEIntegrator(int(integrator), byref(ierr))
+        return ierr.value
+
+    def getRays(self):
+        """The traced rays: list of dicts with the path (x, z), the cells
+        and lengths, the times along the steps / from the field / from the
+        cells, and the status."""
+        n, ierr = c_int(), c_int(1)
+        self.lib.fteik_b200_solver2d_getNumberOfRays(byref(n), byref(ierr))
+        nr = n.value
+        if nr < 1:
+            return []
+        ts, tf, tc = np.zeros(nr), np.zeros(nr), np.zeros(nr)
+        st = np.zeros(nr, np.int32)
+        self.lib.fteik_b200_solver2d_getRayTimes(nr, ts.ctypes.data_as(_PD), tf.ctypes.data_as(_PD),
+                                                 tc.ctypes.data_as(_PD), st.ctypes.data_as(_PI), byref(ierr))
+        _check(ierr, "getRayTimes")
+        rays = []
+        for r in range(1, nr + 1):
+            npts, nseg = c_int(), c_int()
+            self.lib.fteik_b200_solver2d_getRayPath(r, 0, None, None, byref(npts), byref(ierr))
+            x, z = np.zeros(npts.value), np.zeros(npts.value)
+            self.lib.fteik_b200_solver2d_getRayPath(r, npts.value, x.ctypes.data_as(_PD), z.ctypes.data_as(_PD),
+                                                    byref(npts), byref(ierr))
+            _check(ierr, "getRayPath")
+            self.lib.fteik_b200_solver2d_getRayCells(r, 0, None, None, byref(nseg), byref(ierr))
+            c, ln = np.zeros(nseg.value, np.int32), np.zeros(nseg.value)
+            self.lib.fteik_b200_solver2d_getRayCells(r, nseg.value, c.ctypes.data_as(_PI), ln.ctypes.data_as(_PD),
+                                                     byref(nseg), byref(ierr))
+            _check(ierr, "getRayCells")
+            rays.append({"x": x, "z": z, "cells": c, "lengths": ln, "t_step": ts[r - 1], "t_field": tf[r - 1],
+                         "t_cell": tc[r - 1], "status": int(st[r - 1])})
+        return rays
 
     def getTravelTimes(self):
         out = np.zeros(max(self.nrec * self.nsrc, 1))

@@ -113,6 +113,16 @@ int fk2d_solve(int fsm, const fk_grid2d_t *grids, const fk_work2d_t *work,
                fk_result3d_t *results, int nwork, int max_nx, int max_nz, double eps,
                int nsweep, double conv_tol, int max_pass, cudaStream_t stream);
 
+/* 2D ray paths (rays2d.cu): pass 1 counts points and (cell, length) pieces
+ * and writes npts / nseg / status / tn / tne per ray; pass 2 writes the
+ * points and pieces at pts_off / seg_off.  Positions relative to the model
+ * origin; slow [nx-1][zcp], tt [nx][zp], gx / gz [nx][nz] device arrays. */
+int fk_rays2d(int pass, int nz, int nx, int zp, int zcp, double dz, double dx, const double *slow,
+              const double *tt, const double *gx, const double *gz, int integrator, double xs, double zs,
+              int nray, const double *xr, const double *zr, int *npts, int *nseg, int *status,
+              double *tn, double *tne, const long long *pts_off, const long long *seg_off, double *px,
+              double *pz, int *cells, double *lens, cudaStream_t s);
+
 /* ---- field utilities --------------------------------------------------- */
 /* Fill a padded slowness array (precision 4 or 8) from FP64 cell slowness in
  * the reference's natural layout. */

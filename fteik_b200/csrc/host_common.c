@@ -187,3 +187,23 @@ int fk_check_ray_points(bool is3d, int np, const double *z, const double *x, con
     }
     return ierr;
 }
+
+/* rays.F90:93-104, :215-229: the ray-path integrator, reset to Euler when a
+ * solver is initialised or freed (fteik_rays_initialize calls
+ * fteik_rays_free, rays.F90:143,176-199). */
+static int g_ray_integrator = FK_RAYS_EULER;
+
+int fk_rays_integrator(void) { return g_ray_integrator; }
+void fk_rays_reset(void) { g_ray_integrator = FK_RAYS_EULER; }
+
+void fteik_rays_setODEIntegrator(int integrator, int *ierr)
+{
+    *ierr = 0;
+    g_ray_integrator = FK_RAYS_EULER;
+    if (integrator < FK_RAYS_EULER || integrator > FK_RAYS_RK4) {
+        FK_ERR("fteik_rays_setODEIntegrator: Invalid integrator = %d using Euler", integrator);
+        *ierr = 1;
+        return;
+    }
+    g_ray_integrator = integrator;
+}

@@ -33,6 +33,13 @@ typedef struct {
 } fk_slabcfg_t;
 fk_slabcfg_t fk_slabcfg(void);
 int fk_slabcfg_epoch(void);
+
+/* ---- ray paths (rays.F90) ---- */
+#define FK_RAYS_EULER 1
+#define FK_RAYS_MIDPOINT 2
+#define FK_RAYS_RK4 3
+int fk_rays_integrator(void);
+void fk_rays_reset(void);
 void *fk_dalloc(size_t bytes, const char *who);
 void fk_dfree(void *p);
 int fk_check(int cuda_err, const char *who);  /* 0 on success, prints otherwise */

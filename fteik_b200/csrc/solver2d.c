@@ -5,6 +5,7 @@
 #include "host_common.h"
 #include "fteik_b200.h"
 
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -31,6 +32,23 @@ static struct {
     bool have_grad;
 } S2;
 
+/* Ray paths of the last traceRaysTo* (host copies). */
+static struct {
+    int nray;
+    int *npts, *nseg, *status;
+    double *tn, *tne, *tcell;
+    long long *pts_off, *seg_off;
+    double *px, *pz, *lens;   /* positions relative to the model origin */
+    int *cells;               /* 1-based natural cell index */
+} R2;
+
+static void rays_free(void)
+{
+    free(R2.npts); free(R2.nseg); free(R2.status); free(R2.tn); free(R2.tne); free(R2.tcell);
+    free(R2.pts_off); free(R2.seg_off); free(R2.px); free(R2.pz); free(R2.lens); free(R2.cells);
+    memset(&R2, 0, sizeof(R2));
+}
+
 void fteik_solver2d_free(void)
 {
     fk_dfree(S2.tt); fk_dfree(S2.export_buf);
@@ -40,6 +58,8 @@ void fteik_solver2d_free(void)
     free(S2.tt_rec);
     memset(&S2, 0, sizeof(S2));
     S2.src = -1;
+    rays_free();
+    fk_rays_reset();
     fteik_receiver_free();
     fteik_source_free();
     fteik_model_free();
@@ -431,10 +451,98 @@ void fteik_solver2d_traceRaysToReceivers(int *ierr)
     if (*ierr) { FK_ERR("fteik_solver2d_traceRaysToReceivers: Failed to compute rays"); *ierr = 1; }
 }
 
+/* rays.F90:449-670 on the device: every ray of the points at once, one
+ * thread each (rays2d.cu), counted then written; results kept on the host. */
+static int trace2d(int np, const double *xp, const double *zp, const char *who)
+{
+    rays_free();
+    const int nz = fk_model.nz, nx = fk_model.nx, zp_ = FK_PITCH(nz), zcp = FK_PITCH(nz - 1);
+    const double *slow = (const double *)fk_model_slow_dev(8);
+    if (!slow) return 1;
+    const double xs = (double)(fk_source.xsi[S2.src - 1] - 1) * fk_model.dx;   /* source.F90:180-181 */
+    const double zs = (double)(fk_source.zsi[S2.src - 1] - 1) * fk_model.dz;
+    const int integ = fk_rays_integrator();
+    R2.nray = np;
+    R2.npts = (int *)malloc(sizeof(int) * (size_t)np);
+    R2.nseg = (int *)malloc(sizeof(int) * (size_t)np);
+    R2.status = (int *)malloc(sizeof(int) * (size_t)np);
+    R2.tn = (double *)malloc(sizeof(double) * (size_t)np);
+    R2.tne = (double *)malloc(sizeof(double) * (size_t)np);
+    R2.tcell = (double *)malloc(sizeof(double) * (size_t)np);
+    R2.pts_off = (long long *)malloc(sizeof(long long) * (size_t)np);
+    R2.seg_off = (long long *)malloc(sizeof(long long) * (size_t)np);
+    double *rel = (double *)malloc(sizeof(double) * 2 * (size_t)np);
+    for (int i = 0; i < np; i++) {
+        rel[i] = xp[i] - fk_model.x0;
+        rel[np + i] = zp[i] - fk_model.z0;
+    }
+    /* device: [xr zr tn tne] doubles, [npts nseg status] ints, then the two offset arrays */
+    const size_t nd = 4 * (size_t)np, ni = 3 * (size_t)np;
+    char *d = (char *)fk_dalloc(sizeof(double) * nd + sizeof(int) * ni + sizeof(long long) * 2 * (size_t)np + 64, who);
+    if (!d) { free(rel); return 1; }
+    double *d_xr = (double *)d, *d_zr = d_xr + np, *d_tn = d_zr + np, *d_tne = d_tn + np;
+    int *d_npts = (int *)(d_tne + np), *d_nseg = d_npts + np, *d_st = d_nseg + np;
+    long long *d_po = (long long *)(((uintptr_t)(d_st + np) + 15) & ~(uintptr_t)15), *d_so = d_po + np;
+    cudaStream_t st = fk_stream();
+    int e = (int)cudaMemcpyAsync(d_xr, rel, sizeof(double) * 2 * (size_t)np, cudaMemcpyHostToDevice, st);
+    if (!e) e = fk_rays2d(1, nz, nx, zp_, zcp, fk_model.dz, fk_model.dx, slow, S2.tt, S2.gx, S2.gz, integ, xs, zs,
+                          np, d_xr, d_zr, d_npts, d_nseg, d_st, d_tn, d_tne, NULL, NULL, NULL, NULL, NULL, NULL, st);
+    if (!e) e = (int)cudaMemcpyAsync(R2.npts, d_npts, sizeof(int) * (size_t)np, cudaMemcpyDeviceToHost, st);
+    if (!e) e = (int)cudaMemcpyAsync(R2.nseg, d_nseg, sizeof(int) * (size_t)np, cudaMemcpyDeviceToHost, st);
+    if (!e) e = (int)cudaMemcpyAsync(R2.status, d_st, sizeof(int) * (size_t)np, cudaMemcpyDeviceToHost, st);
+    if (!e) e = (int)cudaMemcpyAsync(R2.tn, d_tn, sizeof(double) * (size_t)np, cudaMemcpyDeviceToHost, st);
+    if (!e) e = (int)cudaMemcpyAsync(R2.tne, d_tne, sizeof(double) * (size_t)np, cudaMemcpyDeviceToHost, st);
+    if (!e) e = (int)cudaStreamSynchronize(st);
+    free(rel);
+    if (fk_check(e, who)) { fk_dfree(d); return 1; }
+    long long tp = 0, ts = 0;
+    for (int i = 0; i < np; i++) {
+        R2.pts_off[i] = tp;
+        R2.seg_off[i] = ts;
+        tp += R2.npts[i];
+        ts += R2.nseg[i];
+    }
+    R2.px = (double *)malloc(sizeof(double) * (size_t)(tp ? tp : 1));
+    R2.pz = (double *)malloc(sizeof(double) * (size_t)(tp ? tp : 1));
+    R2.lens = (double *)malloc(sizeof(double) * (size_t)(ts ? ts : 1));
+    R2.cells = (int *)malloc(sizeof(int) * (size_t)(ts ? ts : 1));
+    char *o = (char *)fk_dalloc(sizeof(double) * (size_t)(2 * tp + ts) + sizeof(int) * (size_t)ts + 64, who);
+    if (!o) { fk_dfree(d); return 1; }
+    double *d_px = (double *)o, *d_pz = d_px + tp, *d_len = d_pz + tp;
+    int *d_cells = (int *)(d_len + ts);
+    e = (int)cudaMemcpyAsync(d_po, R2.pts_off, sizeof(long long) * (size_t)np, cudaMemcpyHostToDevice, st);
+    if (!e) e = (int)cudaMemcpyAsync(d_so, R2.seg_off, sizeof(long long) * (size_t)np, cudaMemcpyHostToDevice, st);
+    if (!e) e = fk_rays2d(2, nz, nx, zp_, zcp, fk_model.dz, fk_model.dx, slow, S2.tt, S2.gx, S2.gz, integ, xs, zs,
+                          np, d_xr, d_zr, d_npts, d_nseg, d_st, d_tn, d_tne, d_po, d_so, d_px, d_pz, d_cells,
+                          d_len, st);
+    if (!e && tp) e = (int)cudaMemcpyAsync(R2.px, d_px, sizeof(double) * (size_t)tp, cudaMemcpyDeviceToHost, st);
+    if (!e && tp) e = (int)cudaMemcpyAsync(R2.pz, d_pz, sizeof(double) * (size_t)tp, cudaMemcpyDeviceToHost, st);
+    if (!e && ts) e = (int)cudaMemcpyAsync(R2.lens, d_len, sizeof(double) * (size_t)ts, cudaMemcpyDeviceToHost, st);
+    if (!e && ts) e = (int)cudaMemcpyAsync(R2.cells, d_cells, sizeof(int) * (size_t)ts, cudaMemcpyDeviceToHost, st);
+    if (!e) e = (int)cudaStreamSynchronize(st);
+    fk_dfree(o);
+    fk_dfree(d);
+    if (fk_check(e, who)) return 1;
+    /* the time of each ray from its (cell, length) pieces (rays.F90:650) */
+    int bad = 0;
+    for (int i = 0; i < np; i++) {
+        double t = 0.0;
+        for (int k = 0; k < R2.nseg[i]; k++) t += R2.lens[R2.seg_off[i] + k] * fk_model.slow[R2.cells[R2.seg_off[i] + k] - 1];
+        R2.tcell[i] = t;
+        if (R2.status[i]) {
+            FK_ERR("fteik_rays_trace2d: Ray path %d failed to terminate", i + 1);
+            bad = 1;
+        }
+    }
+    return bad;
+}
+
 void fteik_solver2d_traceRaysToPoints(int np, const double xp[], const double zp[], int *ierr)
 {
-    /* solver2D.F90:310-350: the gradient of the current field and the ray
-     * end points; the ray paths have no C accessor in the reference. */
+    /* solver2D.F90:310-350: the gradient of the current field, the ray end
+     * points, then the ray paths (rays.F90:406-670), which the reference
+     * keeps in module variables and this library returns through
+     * fteik_b200_solver2d_getRay*. */
     *ierr = 0;
     if (!S2.have_times) {
         FK_ERR("fteik_solver2d_traceRaysToPoints: Travel time field not yet computed");
@@ -445,5 +553,63 @@ void fteik_solver2d_traceRaysToPoints(int np, const double xp[], const double zp
     if (fk_check_ray_points(false, np, zp, xp, NULL)) {
         FK_ERR("fteik_solver2d_traceRaysToPoints: Failed to set ray origins");
         *ierr = 1;
+        return;
     }
+    if (trace2d(np, xp, zp, "fteik_solver2d_traceRaysToPoints")) {
+        FK_ERR("fteik_solver2d_traceRaysToPoints: Failed to compute rays");
+        *ierr = 1;
+    }
+}
+
+void fteik_b200_solver2d_getNumberOfRays(int *nray, int *ierr)
+{
+    *nray = R2.nray;
+    *ierr = 0;
+}
+
+void fteik_b200_solver2d_getRayTimes(int nray, double tstep[], double tfield[], double tcell[], int status[],
+                                     int *ierr)
+{
+    *ierr = 1;
+    if (nray != R2.nray || R2.nray < 1) {
+        FK_ERR("fteik_b200_solver2d_getRayTimes: nray=%d but %d rays are traced", nray, R2.nray);
+        return;
+    }
+    for (int i = 0; i < nray; i++) {
+        tstep[i] = R2.tn[i];
+        tfield[i] = R2.tne[i];
+        tcell[i] = R2.tcell[i];
+        status[i] = R2.status[i];
+    }
+    *ierr = 0;
+}
+
+void fteik_b200_solver2d_getRayPath(int ir, int maxpts, double x[], double z[], int *npts, int *ierr)
+{
+    *ierr = 1;
+    *npts = 0;
+    if (ir < 1 || ir > R2.nray) { FK_ERR("fteik_b200_solver2d_getRayPath: ray %d not traced", ir); return; }
+    *npts = R2.npts[ir - 1];
+    if (maxpts == 0) { *ierr = 0; return; }          /* size query */
+    if (maxpts < *npts) { FK_ERR("fteik_b200_solver2d_getRayPath: maxpts=%d < %d", maxpts, *npts); return; }
+    for (int k = 0; k < *npts; k++) {
+        x[k] = R2.px[R2.pts_off[ir - 1] + k] + fk_model.x0;
+        z[k] = R2.pz[R2.pts_off[ir - 1] + k] + fk_model.z0;
+    }
+    *ierr = 0;
+}
+
+void fteik_b200_solver2d_getRayCells(int ir, int maxseg, int cells[], double lengths[], int *nseg, int *ierr)
+{
+    *ierr = 1;
+    *nseg = 0;
+    if (ir < 1 || ir > R2.nray) { FK_ERR("fteik_b200_solver2d_getRayCells: ray %d not traced", ir); return; }
+    *nseg = R2.nseg[ir - 1];
+    if (maxseg == 0) { *ierr = 0; return; }          /* size query */
+    if (maxseg < *nseg) { FK_ERR("fteik_b200_solver2d_getRayCells: maxseg=%d < %d", maxseg, *nseg); return; }
+    for (int k = 0; k < *nseg; k++) {
+        cells[k] = R2.cells[R2.seg_off[ir - 1] + k];
+        lengths[k] = R2.lens[R2.seg_off[ir - 1] + k];
+    }
+    *ierr = 0;
 }

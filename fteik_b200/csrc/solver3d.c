@@ -47,6 +47,7 @@ void fteik_solver3d_free(void)
     memset(&S3, 0, sizeof(S3));
     S3.precision = prec;
     S3.src = -1;
+    fk_rays_reset();
     fteik_receiver_free();
     fteik_source_free();
     fteik_model_free();

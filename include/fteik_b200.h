@@ -282,6 +282,13 @@ int fteik_h5io_writeLevelSchedulesF(void);
 int fteik_h5io_writeVelocityModelF(const char *velName);
 int fteik_h5io_writeTravelTimesF(const char *ttName);
 
+/* ---- ray paths: rays.F90 ---- */
+/* rays.F90:215-229: integrator of the ray-path equation for the next
+ * traceRaysTo* call: 1 Euler (default), 2 midpoint, 3 the reference's RK4;
+ * an invalid value sets Euler and ierr = 1.  Initialising or freeing a
+ * solver resets it to Euler, as in the reference. */
+void fteik_rays_setODEIntegrator(int integrator, int *ierr);
+
 /* =====================  Part 2: additions (fteik_b200_)  ================= */
 
 /* Library version string and the CUDA device in use (-1 if none). */
@@ -474,6 +481,23 @@ void fteik_b200_mlp_gradient(int n, const float x[], const float y[], double *lo
                              int *ierr);
 void fteik_b200_mlp_train(int n, const float x[], const float y[], int steps, int batch, double lr,
                           double *loss, int *ierr);
+
+/* The 2D ray paths of the last fteik_solver2d_traceRaysToPoints /
+ * ToReceivers (rays.F90:449-670, which keeps them in module variables no C
+ * caller can read).  Ray ir (1-based) runs from its end point to the
+ * source's grid point: its integration points (x, z, model coordinates,
+ * getRayPath), and the cells it crosses with the length inside each (cells:
+ * 1-based natural cell index (ix - 1)(nz - 1) + iz, getRayCells).
+ * maxpts / maxseg = 0 only returns the count.  getRayTimes: per ray the
+ * time along the steps (step length x slowness of its starting cell), the
+ * drop of the travel-time field along the path, the time from the cell
+ * pieces (length x cell slowness), and status 1 when the ray did not reach
+ * the source in nx nz steps.  No counterpart in the reference's C API. */
+void fteik_b200_solver2d_getNumberOfRays(int *nray, int *ierr);
+void fteik_b200_solver2d_getRayTimes(int nray, double tstep[], double tfield[], double tcell[], int status[],
+                                     int *ierr);
+void fteik_b200_solver2d_getRayPath(int ir, int maxpts, double x[], double z[], int *npts, int *ierr);
+void fteik_b200_solver2d_getRayCells(int ir, int maxseg, int cells[], double lengths[], int *nseg, int *ierr);
 
 /* Allocation-free grid search (no counterpart in the reference).  For
  * callers that cannot let a library allocate device memory -- a host that

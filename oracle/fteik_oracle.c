@@ -1490,3 +1490,202 @@ void orc_gradient2d(int nz, int nx, double dz, double dx, const double *tt,
             gx[m2] = (tt[m2] - tt[m1]) / dx;
         }
 }
+
+/* ============================================================== rays 2D == */
+/* rays.F90:449-670 (fteik_rays_trace2d), the integrators of :671-825
+ * (Euler, midpoint and the reference's RK4, whose k2 is evaluated at
+ * x_n + k1 and then halved) and evalf2d / bilinear (:843-999), for one ray
+ * traced from its end point (xr, zr) to the source grid point (xs, zs), all
+ * relative to the model origin.  Cell (ix, iz) of a position: 1-based,
+ * INT(x/dx + 1) clamped to [1, n-1].  The reference's segmentation of the
+ * path into cells (:560-640) overwrites its x coordinates and stops after
+ * the first ray (a debugging PAUSE); here every integration step is split
+ * exactly at the cell boundaries it crosses, consecutive pieces in one cell
+ * merged, which is the (cell, length) list those lines intend.  Returns 0,
+ * 1 when the ray does not reach the source within nx*nz steps (the
+ * reference's limit), 2 when a capacity is too small. */
+#define RAY_EPS 2.220446049250313e-16
+
+static inline int ray_cell_ix(double x, double d, int n)
+{
+    int i = (int)(x / d + 1.0);
+    return i < 1 ? 1 : (i > n - 1 ? n - 1 : i);
+}
+
+static inline double ray_bilinear(double x, double z, double x1, double z1, double x2, double z2,
+                                  double c11, double c12, double c21, double c22)
+{
+    /* rays.F90:969-999 */
+    double den = (x1 - x2) * (z1 - z2);
+    double a0 = (c11 * x2 * z2 - c12 * x2 * z1 - c21 * x1 * z2 + c22 * x1 * z1) / den;
+    double a1 = (-c11 * z2 + c12 * z1 + c21 * z2 - c22 * z1) / den;
+    double a2 = (-c11 * x2 + c12 * x2 + c21 * x1 - c22 * x1) / den;
+    double a3 = (c11 - c12 - c21 + c22) / den;
+    return a0 + a1 * x + a2 * z + a3 * x * z;
+}
+
+typedef struct {
+    int nz, nx;
+    double dz, dx;
+    const double *slow, *gx, *gz;
+} ray_grid_t;
+
+/* rays.F90:857-894 (evalf2d) */
+static void ray_evalf(const ray_grid_t *g, double xn, double zn, double *d1, double *d3)
+{
+    const int ix = ray_cell_ix(xn, g->dx, g->nx), iz = ray_cell_ix(zn, g->dz, g->nz);
+    const long icell = (long)(ix - 1) * (g->nz - 1) + iz;
+    const double x1 = (double)(ix - 1) * g->dx, x2 = (double)ix * g->dx;
+    const double z1 = (double)(iz - 1) * g->dz, z2 = (double)iz * g->dz;
+    const long i11 = (long)(ix - 1) * g->nz + iz, i12 = i11 + 1, i21 = (long)ix * g->nz + iz, i22 = i21 + 1;
+    double dtdx = ray_bilinear(xn, zn, x1, z1, x2, z2, g->gx[i11 - 1], g->gx[i12 - 1], g->gx[i21 - 1],
+                               g->gx[i22 - 1]);
+    double dtdz = ray_bilinear(xn, zn, x1, z1, x2, z2, g->gz[i11 - 1], g->gz[i12 - 1], g->gz[i21 - 1],
+                               g->gz[i22 - 1]);
+    *d1 = -dtdx / g->slow[icell - 1];
+    *d3 = -dtdz / g->slow[icell - 1];
+}
+
+/* rays.F90:813-825 (updatePosition2D) */
+static void ray_update(const ray_grid_t *g, double xn, double zn, double ds, double d1, double d3,
+                       double *x1, double *z1)
+{
+    double a = xn + ds * d1, b = zn + ds * d3;
+    double xmax = (double)(g->nx - 1) * g->dx - RAY_EPS, zmax = (double)(g->nz - 1) * g->dz - RAY_EPS;
+    a = a > RAY_EPS ? a : RAY_EPS;
+    *x1 = a < xmax ? a : xmax;
+    b = b > RAY_EPS ? b : RAY_EPS;
+    *z1 = b < zmax ? b : zmax;
+}
+
+static void ray_step(const ray_grid_t *g, int integrator, double ds, double xn, double zn, double *x1,
+                     double *z1)
+{
+    double d1, d3;
+    if (integrator == 2) {
+        /* rays.F90:765-787 (updateMidpoint2D) */
+        double xm, zm;
+        ray_evalf(g, xn, zn, &d1, &d3);
+        ray_update(g, xn, zn, 0.5 * ds, d1, d3, &xm, &zm);
+        ray_evalf(g, xm, zm, &d1, &d3);
+        ray_update(g, xn, zn, ds, d1, d3, x1, z1);
+    } else if (integrator == 3) {
+        /* rays.F90:671-712 (updateRK42D) */
+        static const double dsscal[3] = {0.5, 0.5, 1.0};
+        double k[4][2], xk, zk;
+        ray_evalf(g, xn, zn, &k[0][0], &k[0][1]);
+        k[0][0] = ds * k[0][0];
+        k[0][1] = ds * k[0][1];
+        ray_update(g, xn, zn, 1.0, k[0][0], k[0][1], &xk, &zk);
+        for (int i = 1; i < 4; i++) {
+            ray_evalf(g, xk, zk, &k[i][0], &k[i][1]);
+            k[i][0] = ds * dsscal[i - 1] * k[i][0];
+            k[i][1] = ds * dsscal[i - 1] * k[i][1];
+            ray_update(g, xn, zn, 1.0, k[i][0], k[i][1], &xk, &zk);
+        }
+        d1 = 1.0 / 6.0 * (k[0][0] + 2.0 * (k[1][0] + k[2][0]) + k[3][0]);
+        d3 = 1.0 / 6.0 * (k[0][1] + 2.0 * (k[1][1] + k[2][1]) + k[3][1]);
+        ray_update(g, xn, zn, 1.0, d1, d3, x1, z1);
+    } else {
+        /* rays.F90:735-748 (updateEuler2D) */
+        ray_evalf(g, xn, zn, &d1, &d3);
+        ray_update(g, xn, zn, ds, d1, d3, x1, z1);
+    }
+}
+
+/* Split the straight step (xa, za) -> (xb, zb) at the cell boundaries it
+ * crosses; append (cell, length) pieces, merging a piece into the last entry
+ * when it lies in the same cell. */
+static int ray_split(const ray_grid_t *g, double xa, double za, double xb, double zb, int maxseg, int *cells,
+                     double *lens, int *nseg)
+{
+    const double ddx = xb - xa, ddz = zb - za;
+    const double L = sqrt(ddx * ddx + ddz * ddz);
+    if (!(L > 0.0)) return 0;
+    double tx[8], tz[8];
+    int nxc = 0, nzc = 0;
+    if (ddx != 0.0) {
+        const double lo = xa < xb ? xa : xb, hi = xa < xb ? xb : xa;
+        const int m0 = (int)floor(lo / g->dx) + 1, m1 = (int)ceil(hi / g->dx) - 1;
+        for (int m = m0; m <= m1 && nxc < 8; m++) tx[nxc++] = ((double)m * g->dx - xa) / ddx;
+        if (ddx < 0.0)
+            for (int i = 0; i < nxc / 2; i++) { double t = tx[i]; tx[i] = tx[nxc - 1 - i]; tx[nxc - 1 - i] = t; }
+    }
+    if (ddz != 0.0) {
+        const double lo = za < zb ? za : zb, hi = za < zb ? zb : za;
+        const int m0 = (int)floor(lo / g->dz) + 1, m1 = (int)ceil(hi / g->dz) - 1;
+        for (int m = m0; m <= m1 && nzc < 8; m++) tz[nzc++] = ((double)m * g->dz - za) / ddz;
+        if (ddz < 0.0)
+            for (int i = 0; i < nzc / 2; i++) { double t = tz[i]; tz[i] = tz[nzc - 1 - i]; tz[nzc - 1 - i] = t; }
+    }
+    double tprev = 0.0;
+    int i = 0, j = 0;
+    for (;;) {
+        double tnext;
+        if (i < nxc && (j >= nzc || tx[i] <= tz[j])) tnext = tx[i++];
+        else if (j < nzc) tnext = tz[j++];
+        else tnext = 1.0;
+        if (tnext > tprev) {
+            const double tm = 0.5 * (tprev + tnext);
+            const double xm = xa + tm * ddx, zm = za + tm * ddz;
+            const int ix = ray_cell_ix(xm, g->dx, g->nx), iz = ray_cell_ix(zm, g->dz, g->nz);
+            const int c = (ix - 1) * (g->nz - 1) + iz;
+            const double len = (tnext - tprev) * L;
+            if (*nseg > 0 && cells[*nseg - 1] == c) {
+                lens[*nseg - 1] += len;
+            } else {
+                if (*nseg >= maxseg) return 2;
+                cells[*nseg] = c;
+                lens[*nseg] = len;
+                (*nseg)++;
+            }
+            tprev = tnext;
+        }
+        if (tnext >= 1.0) break;
+    }
+    return 0;
+}
+
+int orc_ray2d(int nz, int nx, double dz, double dx, const double *slow, const double *tt, const double *gx,
+              const double *gz, double xs, double zs, int integrator, double xr, double zr, int maxpts,
+              double *px, double *pz, int *npts, int maxseg, int *cells, double *lens, int *nseg, double *tn,
+              double *tne)
+{
+    const ray_grid_t g = {nz, nx, dz, dx, slow, gx, gz};
+    const double ds = (dx < dz ? dx : dz) / 2.0;
+    const double rad2 = (dx * dx + dz * dz) / 2.0;
+    double xn = xr, zn = zr, t_n = 0.0, t_e = 0.0;
+    int np = 0, ns = 0, done = 0;
+    if (maxpts < 1) return 2;
+    px[np] = xn; pz[np] = zn; np++;
+    const long maxk = (long)nx * nz;
+    for (long k = 1; k <= maxk; k++) {
+        const int ix = ray_cell_ix(xn, dx, nx), iz = ray_cell_ix(zn, dz, nz);
+        const double x1 = (double)(ix - 1) * dx, x2 = (double)ix * dx;
+        const double z1 = (double)(iz - 1) * dz, z2 = (double)iz * dz;
+        const long i11 = (long)(ix - 1) * nz + iz, i12 = i11 + 1, i21 = (long)ix * nz + iz, i22 = i21 + 1;
+        const double c11 = tt[i11 - 1], c12 = tt[i12 - 1], c21 = tt[i21 - 1], c22 = tt[i22 - 1];
+        double xn1, zn1;
+        ray_step(&g, integrator, ds, xn, zn, &xn1, &zn1);
+        if ((xn1 - xs) * (xn1 - xs) + (zn1 - zs) * (zn1 - zs) < rad2) {
+            done = 1;
+            xn1 = xs;
+            zn1 = zs;
+        }
+        const long icell = (long)(ix - 1) * (nz - 1) + iz;
+        t_e = t_e - (ray_bilinear(xn1, zn1, x1, z1, x2, z2, c11, c12, c21, c22) -
+                     ray_bilinear(xn, zn, x1, z1, x2, z2, c11, c12, c21, c22));
+        t_n = t_n + sqrt((xn1 - xn) * (xn1 - xn) + (zn1 - zn) * (zn1 - zn)) * slow[icell - 1];
+        if (ray_split(&g, xn, zn, xn1, zn1, maxseg, cells, lens, &ns)) return 2;
+        xn = xn1;
+        zn = zn1;
+        if (np >= maxpts) return 2;
+        px[np] = xn; pz[np] = zn; np++;
+        if (done) break;
+    }
+    *npts = np;
+    *nseg = ns;
+    *tn = t_n;
+    *tne = t_e;
+    return done ? 0 : 1;
+}

@@ -126,6 +126,17 @@ void orc_gradient3d(int nz, int nx, int ny, double dz, double dx, double dy,
 void orc_gradient2d(int nz, int nx, double dz, double dx, const double *tt,
                     double *gx, double *gz);
 
+/* rays.F90:449-825: one 2D ray from (xr, zr) to the source grid point (xs,
+ * zs), positions relative to the model origin; slow [(nx-1)(nz-1)], tt, gx,
+ * gz [nx nz] z fastest; integrator 1 Euler, 2 midpoint, 3 RK4.  Outputs the
+ * integration points, the (cell, length) pieces (1-based natural cell
+ * index), the time along the steps (tn) and from the field (tne).  Returns
+ * 0, 1 (did not reach the source in nx nz steps) or 2 (capacity). */
+int orc_ray2d(int nz, int nx, double dz, double dx, const double *slow, const double *tt, const double *gx,
+              const double *gz, double xs, double zs, int integrator, double xr, double zr, int maxpts,
+              double *px, double *pz, int *npts, int maxseg, int *cells, double *lens, int *nseg, double *tn,
+              double *tne);
+
 void orc_analytic_constant(int nz, int nx, int ny, double z0, double x0,
                            double y0, double dz, double dx, double dy,
                            double vconst, double zs, double xs, double ys,

@@ -52,6 +52,10 @@ def load():
     lib.orc_sweep3d.argtypes = [c_int, c_int, c_int, c_int, c_int, c_double, c_double, c_double,
                                 P(c_double), c_int, c_int, c_int, c_double, c_double, c_double,
                                 c_double, P(c_double)]
+    lib.orc_ray2d.restype = c_int
+    lib.orc_ray2d.argtypes = [c_int, c_int, c_double, c_double] + [P(c_double)] * 4 + \
+        [c_double, c_double, c_int, c_double, c_double, c_int, P(c_double), P(c_double), P(c_int), c_int,
+         P(c_int), P(c_double), P(c_int), P(c_double), P(c_double)]
     lib.orc_count_updates3d.restype = None
     lib.orc_count_updates3d.argtypes = [c_int, c_int, c_int, c_int, c_int, c_int,
                                         P(ctypes.c_int64), P(ctypes.c_int64)]
@@ -167,6 +171,26 @@ def nodal_to_slowness(n, order, vel, keep_defects=False):
                                           _ptr(vel, c_double), _ptr(slow, c_double)) != 0:
         raise ValueError("non-positive velocity")
     return slow
+
+
+def ray2d(n, h, slow, tt, gx, gz, src_grid, integrator, end):
+    """rays.F90:449-825 for one ray: n = (nz, nx), h = (dz, dx), FP64 arrays
+    z fastest, src_grid and end = (x, z) relative to the model origin.
+    Returns (status, x, z, cells, lengths, t_step, t_field)."""
+    lib = load()
+    nz, nx = n
+    cap = nz * nx + 2
+    px, pz = np.zeros(cap), np.zeros(cap)
+    cells, lens = np.zeros(4 * cap, np.int32), np.zeros(4 * cap)
+    npts, nseg, tn, tne = c_int(), c_int(), c_double(), c_double()
+    a = [np.ascontiguousarray(v, np.float64) for v in (slow, tt, gx, gz)]
+    st = lib.orc_ray2d(nz, nx, h[0], h[1], *[_ptr(v, c_double) for v in a], float(src_grid[0]),
+                       float(src_grid[1]), int(integrator), float(end[0]), float(end[1]), cap,
+                       _ptr(px, c_double), _ptr(pz, c_double), ctypes.byref(npts), 4 * cap,
+                       _ptr(cells, c_int), _ptr(lens, c_double), ctypes.byref(nseg), ctypes.byref(tn),
+                       ctypes.byref(tne))
+    k, m = npts.value, nseg.value
+    return st, px[:k], pz[:k], cells[:m], lens[:m], tn.value, tne.value
 
 
 def count_updates3d(n, si):

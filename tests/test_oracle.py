@@ -188,3 +188,25 @@ def test_gradients_match_numpy_restatement():
     wz = np.empty_like(T2); wz[:, 1:] = (T2[:, 1:] - T2[:, :-1]) / h[0]; wz[:, 0] = (T2[:, 1] - T2[:, 0]) / h[0]
     wx = np.empty_like(T2); wx[1:] = (T2[1:] - T2[:-1]) / h[1]; wx[0] = (T2[1] - T2[0]) / h[1]
     assert np.array_equal(az, wz.ravel()) and np.array_equal(ax, wx.ravel())
+
+
+@pytest.mark.parametrize("integrator", [1, 2, 3])
+def test_oracle_rays_straight_in_a_constant_medium(integrator):
+    """rays.F90:449-825 restated: in a uniform medium, with the exact travel
+    times' finite-difference gradient, every integrator walks a nearly
+    straight path to the source grid point; the cell pieces add up to the
+    path length and the step time is length / v."""
+    nz, nx, h, v = 31, 41, 10.0, 3000.0
+    xs, zs = 150.0, 100.0
+    X, Z = np.meshgrid(np.arange(nx) * h, np.arange(nz) * h, indexing="ij")
+    tt = (np.hypot(X - xs, Z - zs) / v).ravel()
+    gx, gz = O.gradient2d((nz, nx), (h, h), tt)
+    slow = np.full((nz - 1) * (nx - 1), 1.0 / v)
+    for end in [(380.0, 290.0), (0.0, 0.0), (400.0, 3.0)]:
+        st, px, pz, cells, lens, tn, tne = O.ray2d((nz, nx), (h, h), slow, tt, gx, gz, (xs, zs), integrator, end)
+        d = np.hypot(end[0] - xs, end[1] - zs)
+        assert st == 0 and (px[-1], pz[-1]) == (xs, zs)
+        assert np.sum(lens) == pytest.approx(np.sum(np.hypot(np.diff(px), np.diff(pz))), rel=1e-12)
+        assert np.sum(lens) == pytest.approx(d, rel=5e-3)   # the steps bend slightly near the source
+        assert tn * v == pytest.approx(np.sum(lens), rel=1e-12)
+        assert np.all((cells >= 1) & (cells <= (nz - 1) * (nx - 1)))
