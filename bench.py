@@ -590,6 +590,9 @@ def main():
                     help="solve only the 160x160x96 grid once and run the grid-search section")
     ap.add_argument("--locate-events", type=int, default=LOC_NEV)
     ap.add_argument("--surrogate-steps", type=int, default=SUR_STEPS)
+    ap.add_argument("--slab-config", default=None,
+                    help="staged,pairs,progress,blocks_per_sm for the 3D sweep kernels "
+                         "(fteik_b200_setSlabConfig; default: chosen by the library's tuner)")
     ap.add_argument("--grids", default="1,2,3,4",
                     help="subset of the 4 batched grids (1-based, comma separated) for profiling")
     args = ap.parse_args()
@@ -613,6 +616,8 @@ def main():
     if not os.path.exists(fk.LIB_PATH):
         fk.build()
 
+    if args.slab_config:
+        fk.set_slab_config(*[int(v) for v in args.slab_config.split(",")])
     grids = workload()
     if args.locate_only:
         g = grids[LOC_GRID - 1]

@@ -99,9 +99,11 @@ def test_convergence_program_matches_oracle_and_converges(fk):
             assert int(r[0]) == n
             for got, want in ((float(r[4]), o1), (float(r[5]), o2), (float(r[6]), o8)):
                 assert abs(got - want) <= 1e-5 * abs(want) + 1e-15, (job, i, got, want)
-        # first order: the mean error halves with h (rate between 0.6 and 1.6)
-        rate = np.log2(l1[:-1] / l1[1:])
-        assert np.all(l1[1:] < l1[:-1]), l1
+        # first order once the grid resolves the source region (h <= 50 m; at
+        # h = 100 m the mean error happens to be below the next grid's, in the
+        # oracle as here): the mean error halves with h
+        rate = np.log2(l1[1:-1] / l1[2:])
+        assert np.all(l1[2:] < l1[1:-1]), l1
         assert 0.6 < np.mean(rate) < 1.6, rate
 
 
