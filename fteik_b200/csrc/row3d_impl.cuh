@@ -516,41 +516,39 @@ __device__ __forceinline__ bool slab_pass_f32(const fk3tw::Params &P_, const fk_
 }
 
 /* ---- staged FP32 pass step ---------------------------------------------
- * The walk of slab_pass_f32 with the lane's node values, upwind-row values
- * and slowness moved in 16-byte groups of 4 consecutive z positions by
- * cp.async into a per-warp shared-memory stage, instead of one 4-byte L2
- * load per value and step (each of which fetches a 32-byte sector): a lane
- * issues the loads of its group G + 1 when it starts reading group G, so
- * the loads run 4 to 7 walk items ahead, and it reads each item from the
- * stage one step before using it.
+ * The walk of slab_pass_f32 with the lane's own node values and slowness
+ * moved in 16-byte groups of 4 consecutive z positions by cp.async into a
+ * per-warp shared-memory stage, instead of one 4-byte L2 load per value and
+ * step (each of which fetches a whole 32-byte sector).
  *
  * Groups follow the walk: items 4 G .. 4 G + 3 of the lane's linear walk
  * j = k Zp + zq.  Zp is a multiple of 4, and descending sweeps start with
  * zoff = (-nz) mod 4 dummy items, so a group is always 4 consecutive nodes
  * iz = 4 m .. 4 m + 3 of one column: a 16-byte aligned block of the field
- * ([ny][nx][zp], zp a multiple of 8) and of the node-indexed slowness
- * copies (fk_grid3d_t.slowz).  The dummy items and the walk positions past
- * nz are invalid items, as in slab_pass_f32.
+ * ([ny][nx][zp], zp a multiple of 8) and of the node-indexed slowness copies
+ * (fk_grid3d_t.slowz).  The dummy items and the walk positions past nz are
+ * invalid items, as in slab_pass_f32.
  *
- * Stage: per warp [2 buffers][8 arrays][32 slots][4 floats] (8 KB): arrays
- * told (per source), tn (per source, slab's first row only) and the four
- * slowness values; group G goes to buffer G & 1; lane l's slot is
- * (l >> 2) | ((l & 3) << 3), so that the 32 lanes, whose walks are skewed by
- * one item each, read 32 different banks in every step.
- *
- * The loads run further ahead than slab_pass_f32's, so a slab's first row
- * waits for its upwind slab to be 6 steps further along. */
-constexpr int SG_NARR = 8;
+ * Loads are warp-uniform: every 4 steps all 32 lanes issue one group each,
+ * two groups ahead of the one they read next (the lanes' walks are skewed by
+ * one item, so their groups start at different steps), after waiting for
+ * the batch issued 4 steps before; a lane reads an item from the stage one
+ * step before using it.  A group lives in buffer G mod 3: the two groups a
+ * lane reads in the next 4 steps and the one in flight.  Stage per warp:
+ * [3 buffers][6 arrays: told per source, the 4 slowness values][32 slots]
+ * [4 floats] (9 KB); lane l's slot is (l >> 2) | ((l & 3) << 3), so the 32
+ * lanes read 32 different banks in every step.  The slab's first row still
+ * loads its upwind row's values directly, one step ahead. */
+constexpr int SG_NARR = 6;
+constexpr int SG_NBUF = 3;
 constexpr int SG_ARR_BYTES = 32 * 16;
-constexpr int SG_WARP_BYTES = 2 * SG_NARR * SG_ARR_BYTES;   /* 8 KB */
-constexpr int SG_AHEAD = 8;       /* items past the current one a lane may have loaded, + 1 */
+constexpr int SG_WARP_BYTES = SG_NBUF * SG_NARR * SG_ARR_BYTES;   /* 9 KB */
 
 __device__ __forceinline__ void cpa16(uint32_t saddr, const void *gptr)
 {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(gptr) : "memory");
 }
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cpa_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cpa_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 template <bool RESID, int S, int CHP>
@@ -561,7 +559,7 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
                                                      uint32_t stage, const float *stage_f)
 {
     constexpr int CH = CHP;
-    static_assert(CH % DL == 0 && NB == 2 * DL, "progress and buffer slots follow the DL windows");
+    static_assert(CH % DL == 0 && NB == 2 * DL && (2 * DL) % 4 == 0, "windows, progress and load batches align");
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
     const int nz = g.nz, nx = g.nx, ny = g.ny, zp = g.zp;
@@ -602,6 +600,7 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
     const int colT = (y * nx + x0) * zp;
     const int dkT = 32 * sx * zp;
     const int dyT = sy * nx * zp;
+    const int izw = (sz > 0) ? 0 : nz - 1 + zoff;                  /* iz = izw + sz zq */
     const int cyU = (sy > 0) ? y - 1 : y;
     const int cyD = min(max((sy > 0) ? y : y - 1, 0), ny - 2);
     const float *const sl = g.slowz + ((sz > 0) ? (size_t)0 : (size_t)(ny - 1) * (nx - 1) * zp);
@@ -612,33 +611,37 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
     const int slot = (tx >> 2) | ((tx & 3) << 3);
     const uint32_t my = stage + (uint32_t)(slot * 16);   /* cp.async destination */
     const float *const myf = stage_f + slot * 4;          /* the same bytes, for reading */
+    constexpr int A = SG_ARR_BYTES / 4;                   /* floats per array */
+    constexpr int BUFF = SG_NARR * A;                     /* floats per buffer */
+    const bool loads_slow = rowupd;                       /* a row that updates reads slowness */
 
-    /* group loads: cursor (lk, lzq) = first item of group gl */
-    int gl = 0, lk = 0, lzq = 0;
+    const int c = tx + DL * oy;                 /* the lane's item at step t is t - c */
+    /* group loads: batch b (step 4 b) issues group G_b = ((4 b + 1 - c) >> 2) + 2, i.e. two groups
+     * past the one holding item 4 b + 1 - c, the first read after the batch; G_{b+1} = G_b + 1.
+     * Cursor (lk, lzq) = (column block, walk position) of the group's first item. */
+    int gl = ((1 - 8 - c) >> 2) + 2;            /* G_{-2}: the prologue issues G_{-2}, G_{-1} */
+    int lk = 0, lzq = 4 * gl;
+    while (lzq >= Zp) { lzq -= Zp; ++lk; }
     auto issue = [&]() {
-        const uint32_t d = my + (uint32_t)((gl & 1) * SG_NARR * SG_ARR_BYTES);
-        if (lzq < Zn && lk < kl) {
+        const uint32_t d = my + (uint32_t)(((gl + 3 * 0x2000000) % 3) * (SG_NARR * SG_ARR_BYTES));
+        if (lzq >= 0 && lzq < Zn && lk < kl) {
             const int izb = (sz > 0) ? lzq : nz + zoff - 4 - lzq;
             const int it = colT + lk * dkT + izb;
             cpa16(d, tt0 + it);
             if (S == 2) cpa16(d + SG_ARR_BYTES, tt1 + it);
-            if (oy == 0 && has_yu) {
-                cpa16(d + 2 * SG_ARR_BYTES, tt0 + (it - dyT));
-                if (S == 2) cpa16(d + 3 * SG_ARR_BYTES, tt1 + (it - dyT));
-            }
-            if (lk >= kmin) {
+            if (loads_slow && lk >= kmin) {
                 const int is = colS + lk * dkS + izb;
                 const int ox = (lk == kxl) ? 0 : offX;
-                cpa16(d + 4 * SG_ARR_BYTES, sl + is);
-                cpa16(d + 5 * SG_ARR_BYTES, sl + (is + offY));
-                cpa16(d + 6 * SG_ARR_BYTES, sl + (is + ox));
-                cpa16(d + 7 * SG_ARR_BYTES, sl + (is + ox + offY));
+                cpa16(d + 2 * SG_ARR_BYTES, sl + is);
+                cpa16(d + 3 * SG_ARR_BYTES, sl + (is + offY));
+                cpa16(d + 4 * SG_ARR_BYTES, sl + (is + ox));
+                cpa16(d + 5 * SG_ARR_BYTES, sl + (is + ox + offY));
             }
         }
         cpa_commit();
         ++gl;
         lzq += 4;
-        if (lzq == Zp) { lzq = 0; ++lk; }
+        if (lzq >= Zp) { lzq -= Zp; ++lk; }
     };
 
     struct Item {
@@ -646,44 +649,41 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
         float duu, dud, ddu, ddd;
         int k, zq;
     };
-    /* item jn = (kk, zz) of the walk: make sure groups up to jn / 4 + 1 are
-     * issued, wait for group jn / 4, read the item from the stage */
+    /* item jn = (kk, zz) of the walk from the stage (its group is resident) */
     auto fetch = [&](Item &f, int kk, int zz, int jn) {
         f.k = kk;
         f.zq = zz;
-        if (jn >= -4) {
-            const int target = (jn >> 2) + 1;
-            while (gl <= target) issue();
-        }
         if (jn >= 0) {
-            cpa_wait1();   /* (a memory clobber: the reads below stay after it) */
             const int e = (sz > 0) ? (jn & 3) : 3 - (jn & 3);
-            constexpr int A = SG_ARR_BYTES / 4;   /* floats per array */
-            const float *a = myf + ((jn >> 2) & 1) * SG_NARR * A + e;
+            const float *a = myf + (((jn >> 2) + 3 * 0x2000000) % 3) * BUFF + e;
             f.told[0] = a[0];
             if (S == 2) f.told[S - 1] = a[A];
-            if (oy == 0) {
-                f.tn[0] = has_yu ? a[2 * A] : HUGEV;
-                if (S == 2) f.tn[S - 1] = has_yu ? a[3 * A] : HUGEV;
+            f.duu = a[2 * A];
+            f.dud = a[3 * A];
+            f.ddu = a[4 * A];
+            f.ddd = a[5 * A];
+            if (oy == 0) {   /* the upwind slab's last row, final for this sweep: direct loads */
+                const int it = colT + kk * dkT + izw + sz * zz;
+                const bool v = (unsigned)(zz - zoff) < (unsigned)nz && kk < kl;
+                f.tn[0] = (v && has_yu) ? fk3tw::ldcg(tt0 + (it - dyT)) : HUGEV;
+                if (S == 2) f.tn[S - 1] = (v && has_yu) ? fk3tw::ldcg(tt1 + (it - dyT)) : HUGEV;
             }
-            f.duu = a[4 * A];
-            f.dud = a[5 * A];
-            f.ddu = a[6 * A];
-            f.ddd = a[7 * A];
         }
     };
 
     const int *prog_up = prog[0] + (has_up ? Pu : P);
     if (threadIdx.x == 0) {
         s_flag[0] = 1;
-        if (wait_up && !wait_ge1(prog_up, (s << SHIFT) | min(T, CH + DL * (TY - 1) + 2 + SG_AHEAD - 2),
-                                 P_.spin_limit, P_.error, 3000))
+        if (wait_up && !wait_ge1(prog_up, (s << SHIFT) | min(T, CH + DL * (TY - 1) + 2), P_.spin_limit, P_.error,
+                                 3000))
             s_flag[0] = 0;
     }
     __syncthreads();
     if (!s_flag[0]) return false;
 
-    const int c = tx + DL * oy;                 /* the lane's item at step t is t - c */
+    issue();                                    /* G_{-2} */
+    issue();                                    /* G_{-1} */
+    cpa_wait0();
     int nk = 0, nzq = -c;                       /* item of the next step */
     Item nxt;
 #pragma unroll
@@ -700,11 +700,15 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
     for (int t0 = 0; t0 < T; t0 += DL) {
         if (wait_up && t0 > 0 && t0 % CH == 0) {
             if (threadIdx.x == 0 &&
-                !wait_ge1(prog_up, (s << SHIFT) | min(T, t0 + CH + DL * (TY - 1) + 2 + SG_AHEAD - 2),
-                          P_.spin_limit, P_.error, 3001))
+                !wait_ge1(prog_up, (s << SHIFT) | min(T, t0 + CH + DL * (TY - 1) + 2), P_.spin_limit, P_.error,
+                          3001))
                 s_flag[0] = 0;
             __syncthreads();
             if (!s_flag[0]) { ok = false; break; }
+        }
+        if ((t0 & 3) == 0) {                    /* load batch: warp-uniform */
+            cpa_wait0();                        /* the batch of 4 steps ago has landed */
+            issue();
         }
         const int half = (t0 / DL) & 1;
         float (*const xw)[S][TY][32] = xr + half * DL;
@@ -752,8 +756,7 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
                     r = fk3::noinit_f32(mesh, r_last[i], te, tn, te_last[i], ten, tn_last[i], ten_last[i], s1, s2,
                                         s3, s4, s5, s6, s7, told);
                     if (r != told && (i == 0 || has2)) {
-                        const int iz = (sz > 0) ? cur.zq : nz - 1 + zoff - cur.zq;
-                        (i == 0 ? tt0 : tt1)[colT + cur.k * dkT + iz] = r;
+                        (i == 0 ? tt0 : tt1)[colT + cur.k * dkT + izw + sz * cur.zq] = r;
                         if (RESID) {
                             const double d = fabs((double)r - (double)told);
                             dmax[i] = d > dmax[i] ? d : dmax[i];

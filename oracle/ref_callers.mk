@@ -5,7 +5,7 @@
 #
 #   testing/loctest.c              -> _ref/loctest       (locator known answer)
 #   performanceTests/convergence.c -> _ref/convergence   (2D first-order convergence)
-#   python/fteik3d.py, fteik2d.py  -> _ref/python/*.pyc  (byte-compiled, loaded sourceless)
+#   python/fteik3d.py, fteik2d.py  -> _ref/python/*.bytecode (byte-compiled, loaded sourceless)
 #
 # The C programs include "fteik/fteik_fortran.h", found in ../include; they
 # link ../fteik_b200/lib/libfteik_shared.so through an $ORIGIN-relative rpath,
@@ -22,7 +22,7 @@ ifeq ($(wildcard $(REF)/testing/loctest.c),)
 all:
 	@echo "ref_callers.mk: no reference tree at $(REF); the callers are not built"
 else
-all: $(OUT)/loctest $(OUT)/convergence $(OUT)/python/fteik3d.pyc $(OUT)/python/fteik2d.pyc
+all: $(OUT)/loctest $(OUT)/convergence $(OUT)/python/fteik3d.bytecode $(OUT)/python/fteik2d.bytecode
 endif
 
 $(OUT):
@@ -34,7 +34,7 @@ $(OUT)/loctest: $(REF)/testing/loctest.c $(ROOT)/include/fteik_b200.h | $(OUT)
 $(OUT)/convergence: $(REF)/performanceTests/convergence.c $(ROOT)/include/fteik_b200.h | $(OUT)
 	$(CC) $(CFLAGS) -o $@ $< $(LDFLAGS)
 
-$(OUT)/python/%.pyc: $(REF)/python/%.py | $(OUT)
+$(OUT)/python/%.bytecode: $(REF)/python/%.py | $(OUT)
 	$(PY) -c "import py_compile, sys; py_compile.compile(sys.argv[1], cfile=sys.argv[2], doraise=True)" $< $@
 
 .PHONY: all

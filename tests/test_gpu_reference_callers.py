@@ -108,7 +108,7 @@ def test_convergence_program_matches_oracle_and_converges(fk):
 
 
 def _load_wrapper(name):
-    path = _need(os.path.join(REF, "python", name + ".pyc"))
+    path = _need(os.path.join(REF, "python", name + ".bytecode"))
     os.environ["LD_LIBRARY_PATH"] = os.pathsep.join([LIBDIR, os.environ.get("LD_LIBRARY_PATH", "")])
     loader = SourcelessFileLoader(name, path)
     spec = importlib.util.spec_from_loader(name, loader)

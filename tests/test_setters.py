@@ -120,7 +120,7 @@ def test_velocity_setters_32f_and_natural(fk):
 
 
 def _wrapper(name):
-    path = os.path.join(ROOT, "oracle", "_ref", "python", name + ".pyc")
+    path = os.path.join(ROOT, "oracle", "_ref", "python", name + ".bytecode")
     if not os.path.exists(path):
         pytest.skip("%s not built (oracle/ref_callers.mk needs the reference tree)" % path)
     os.environ["LD_LIBRARY_PATH"] = os.pathsep.join([os.path.dirname(fteik_lib_path()),
