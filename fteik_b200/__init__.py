@@ -156,7 +156,7 @@ _SIGS = {
     "fteik_b200_batch3d_exportToLocator": [c_int, c_int, _PI],
     "fteik_b200_batch3d_finalize": [],
     "fteik_b200_batch3d_timeSolve": [POINTER(c_float), POINTER(c_float), _PI],
-    "fteik_b200_batch3d_getSlabConfig": [_PI, _PI, _PI, _PI, _PI, POINTER(c_float), POINTER(c_float), _PI, _PI],
+    "fteik_b200_batch3d_getSlabConfig": [_PI, _PI, _PI, _PI, _PI, _PI, POINTER(c_float), POINTER(c_float), _PI, _PI],
     "fteik_b200_locate_locateEvents": [c_int, _PI, _PI, _PD, _PD, _PI],
     "fteik_b200_locate_setMethod": [c_int, _PI],
     "fteik_b200_locate_setNorm": [c_int, _PI],
@@ -836,13 +836,13 @@ class Batch3D:
     def slabConfig(self):
         """The launch configuration in use (tuned on the first solve of a new
         work list where left to the library)."""
-        v = [c_int() for _ in range(5)]
+        v = [c_int() for _ in range(6)]
         im, pm, runs, ierr = c_float(), c_float(), c_int(), c_int(1)
         self.lib.fteik_b200_batch3d_getSlabConfig(*[byref(x) for x in v], byref(im), byref(pm), byref(runs),
                                                   byref(ierr))
         _check(ierr, "batch3d_getSlabConfig")
         return {"staged": v[0].value, "pairs": v[1].value, "progress": v[2].value,
-                "blocks_per_sm": v[3].value, "init_blocks_per_sm": v[4].value,
+                "blocks_per_sm": v[3].value, "init_blocks_per_sm": v[4].value, "init_pairs": v[5].value,
                 "init_ms": im.value, "pass_ms": pm.value, "tune_runs": runs.value}
 
     def exportToLocator(self, igrid, itf0=1):

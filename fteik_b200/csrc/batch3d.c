@@ -55,7 +55,7 @@ static struct {
     fk_slabplan_t plan;     /* slab-pipelined schedule */
     int spin_epoch;         /* poll limit the plan (and graph) was built with */
     int cfg_epoch;          /* slab configuration the plan (and graph) was built with */
-    int tuned[5];           /* configuration in use: staged, pairs, progress, blocks/SM passes, init */
+    int tuned[6];           /* configuration in use: staged, pairs, progress, blocks/SM passes, init, init pairs */
     float tune_ms[2];       /* its init / pass kernel times when tuned (0: not timed) */
     int tune_runs;          /* candidate solves the last tuning ran (0: cache hit or nothing to tune) */
     bool work_dirty;        /* source positions changed, shape unchanged */
@@ -442,13 +442,14 @@ static int build_work(const char *who)
  * kept per work list (grid shapes, sources per grid, precision, passes) in
  * memory and, when FTEIK_B200_TUNE_CACHE names a file, in that file, so
  * later processes skip the search. */
-static void tune_apply(const int t[5])
+static void tune_apply(const int t[6])
 {
     SB.plan.dev.staged = SB.precision == 4 && t[0] == 1;
     SB.plan.dev.pairs = t[1] ? SB.plan.pairs_all : NULL;
     SB.plan.dev.progress = t[2];
     SB.plan.dev.blocks_per_sm = t[3];
     SB.plan.dev.init_blocks_per_sm = t[4];
+    SB.plan.dev.init_pairs = (SB.precision == 4 && t[5]) ? SB.plan.pairs_all : NULL;
     memcpy(SB.tuned, t, sizeof(SB.tuned));
 }
 
@@ -471,13 +472,13 @@ static void tune_key(char *key, size_t cap)
 
 #define TUNE_MEM 16
 static char g_tune_key[TUNE_MEM][512];
-static int g_tune_val[TUNE_MEM][5];
+static int g_tune_val[TUNE_MEM][6];
 static int g_tune_n = 0;
 
-static int tune_lookup(const char *key, int t[5])
+static int tune_lookup(const char *key, int t[6])
 {
     for (int i = 0; i < g_tune_n; i++)
-        if (strcmp(g_tune_key[i], key) == 0) { memcpy(t, g_tune_val[i], 5 * sizeof(int)); return 1; }
+        if (strcmp(g_tune_key[i], key) == 0) { memcpy(t, g_tune_val[i], 6 * sizeof(int)); return 1; }
     const char *path = getenv("FTEIK_B200_TUNE_CACHE");
     if (!path || !*path) return 0;
     FILE *f = fopen(path, "r");
@@ -485,22 +486,23 @@ static int tune_lookup(const char *key, int t[5])
     char line[700], k[600];
     int found = 0;
     while (fgets(line, sizeof(line), f))
-        if (sscanf(line, "%599s %d %d %d %d %d", k, &t[0], &t[1], &t[2], &t[3], &t[4]) == 6 && strcmp(k, key) == 0)
+        if (sscanf(line, "%599s %d %d %d %d %d %d", k, &t[0], &t[1], &t[2], &t[3], &t[4], &t[5]) == 7 &&
+            strcmp(k, key) == 0)
             found = 1;   /* the last line for a key wins */
     fclose(f);
     return found;
 }
 
-static void tune_store(const char *key, const int t[5])
+static void tune_store(const char *key, const int t[6])
 {
     const int i = g_tune_n < TUNE_MEM ? g_tune_n++ : TUNE_MEM - 1;
     snprintf(g_tune_key[i], sizeof(g_tune_key[i]), "%s", key);
-    memcpy(g_tune_val[i], t, 5 * sizeof(int));
+    memcpy(g_tune_val[i], t, 6 * sizeof(int));
     const char *path = getenv("FTEIK_B200_TUNE_CACHE");
     if (!path || !*path) return;
     FILE *f = fopen(path, "a");
     if (!f) return;
-    fprintf(f, "%s %d %d %d %d %d\n", key, t[0], t[1], t[2], t[3], t[4]);
+    fprintf(f, "%s %d %d %d %d %d %d\n", key, t[0], t[1], t[2], t[3], t[4], t[5]);
     fclose(f);
 }
 
@@ -535,9 +537,10 @@ static int ensure_events(void)
 static int tune(const char *who)
 {
     const fk_slabcfg_t cfg = fk_slabcfg();
-    int t[5] = {SB.precision == 4 && cfg.staged == 1, cfg.pairs != 0, cfg.progress > 0 ? cfg.progress : 0,
-                cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 0, cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 0};
     /* a knob at 0 is explicit: progress by task count, all resident blocks */
+    int t[6] = {SB.precision == 4 && cfg.staged == 1, cfg.pairs != 0, cfg.progress > 0 ? cfg.progress : 0,
+                cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 0, cfg.blocks_per_sm > 0 ? cfg.blocks_per_sm : 0,
+                SB.precision == 4 && cfg.pairs != 0};
     SB.tune_ms[0] = SB.tune_ms[1] = 0.0f;
     SB.tune_runs = 0;
     const bool search = (cfg.staged < 0 && SB.precision == 4) || cfg.pairs < 0 || cfg.progress < 0 ||
@@ -550,12 +553,15 @@ static int tune(const char *who)
     const int st_n = (cfg.staged < 0 && SB.precision == 4) ? 2 : 1;
     const int pr_n = cfg.pairs < 0 ? 2 : 1;
     const int ch_n = cfg.progress < 0 ? 2 : 1;
-    float best_pass = 3.4e38f, best_init[5];
-    int best[5];
-    for (int b = 0; b < 5; b++) best_init[b] = 3.4e38f;
+    /* the two kernels are chosen apart: the passes by their time, the
+     * initialisation sweeps (pairs, blocks per SM) by theirs */
+    float best_pass = 3.4e38f, best_init = 3.4e38f;
+    int best[6], best_i[2] = {t[4], t[5]};
+    memcpy(best, t, sizeof(best));
     for (int a = 0; a < st_n * pr_n * ch_n; a++) {
-        int c[5] = {st_n == 2 ? a % 2 : t[0], pr_n == 2 ? 1 - (a / st_n) % 2 : t[1],
-                    ch_n == 2 ? ((a / (st_n * pr_n)) % 2 ? 32 : 8) : t[2], t[3], t[4]};
+        const int pr = pr_n == 2 ? 1 - (a / st_n) % 2 : t[1];
+        int c[6] = {st_n == 2 ? a % 2 : t[0], pr, ch_n == 2 ? ((a / (st_n * pr_n)) % 2 ? 32 : 8) : t[2], t[3], t[4],
+                    SB.precision == 4 && pr};
         tune_apply(c);
         float im = 3.4e38f, pm = 3.4e38f;
         for (int r = 0; r < 2; r++) {
@@ -565,12 +571,12 @@ static int tune(const char *who)
             pm = p1 < pm ? p1 : pm;
             SB.tune_runs++;
         }
-        if (im < best_init[c[4]]) best_init[c[4]] = im;
+        if (im < best_init) { best_init = im; best_i[0] = c[4]; best_i[1] = c[5]; }
         if (pm < best_pass) { best_pass = pm; memcpy(best, c, sizeof(best)); }
     }
     if (cfg.blocks_per_sm < 0) {
         for (int bps = 3; bps >= 2; bps--) {
-            int c[5] = {best[0], best[1], best[2], bps, bps};
+            int c[6] = {best[0], best[1], best[2], bps, bps, best_i[1]};
             tune_apply(c);
             float im = 3.4e38f, pm = 3.4e38f;
             for (int r = 0; r < 2; r++) {
@@ -580,24 +586,24 @@ static int tune(const char *who)
                 pm = p1 < pm ? p1 : pm;
                 SB.tune_runs++;
             }
-            if (im < best_init[bps]) best_init[bps] = im;
+            if (im < best_init) { best_init = im; best_i[0] = bps; best_i[1] = c[5]; }
             if (pm < best_pass) { best_pass = pm; memcpy(best, c, sizeof(best)); }
         }
-        int bi = 0;
-        for (int b = 0; b < 5; b++) if (best_init[b] < best_init[bi]) bi = b;
-        best[4] = bi;
     }
+    best[4] = best_i[0];
+    best[5] = best_i[1];
     tune_apply(best);
-    SB.tune_ms[0] = best_init[best[4]];
+    SB.tune_ms[0] = best_init;
     SB.tune_ms[1] = best_pass;
     tune_store(key, best);
     return 0;
 }
 
 void fteik_b200_batch3d_getSlabConfig(int *staged, int *pairs, int *progress, int *blocksPerSM,
-                                      int *initBlocksPerSM, float *initMs, float *passMs, int *tuneRuns,
-                                      int *ierr)
+                                      int *initBlocksPerSM, int *initPairs, float *initMs, float *passMs,
+                                      int *tuneRuns, int *ierr)
 {
+    *initPairs = SB.tuned[5];
     *ierr = SB.graph_ok ? 0 : 1;
     if (!SB.graph_ok) FK_ERR("fteik_b200_batch3d_getSlabConfig: solve once first");
     *staged = SB.tuned[0];

@@ -77,6 +77,9 @@ typedef struct {
      * number of slab tasks); resident blocks per SM of the pass and of the
      * initialisation kernel (0 = as many as fit) */
     int staged, progress, blocks_per_sm, init_blocks_per_sm;
+    /* FP32 initialisation sweeps: the source pairs walked together (the
+     * union of their boxes), or NULL for one source per thread */
+    const int *init_pairs;
 } fk_slabs3d_t;
 
 #define FK_SLAB_Y 4

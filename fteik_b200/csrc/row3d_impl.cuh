@@ -90,9 +90,14 @@ __device__ __forceinline__ bool wait_ge1(const int *p, int need, long long limit
 
 /* One sweep over physical slab P.  Returns false on a wait timeout (the
  * whole block returns false). */
+/* One sweep over physical slab P.  In the initialisation sweeps each source
+ * updates only its own box (solver3D.F90:493-565); with two sources per
+ * thread the walk covers the union of the two boxes and a source's nodes
+ * outside its own box keep their values, which is what that source's own
+ * walk would read there. */
 template <typename R, bool INIT, bool RESID, int S, int CHP>
 __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_grid3d_t &g, R *const (&ttp)[S],
-                                           const R *__restrict__ slow, const Src &q, int s, int sweep_no,
+                                           const R *__restrict__ slow, const Src (&qs)[S], int s, int sweep_no,
                                            int P, int nslab, int *const (&prog)[S], R (*xr)[S][TY][32],
                                            R *ring, int zring, int *s_flag,
                                            double (&dmax)[S])
@@ -105,18 +110,30 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
     const int sz = (s0 < 4) ? 1 : -1;
     const int sx = (s0 % 2 == 0) ? 1 : -1;
     const int sy = ((s0 / 2) % 2 == 0) ? 1 : -1;
-    int loz = 1, lox = 1, loy = 1;
-    if (INIT) { /* solver3D.F90:493-565, flipped bound clamped to the grid */
-        loz = (sz > 0) ? max(1, q.zsi - 1) : max(1, nz - q.zsi - 1);
-        lox = (sx > 0) ? max(1, q.xsi - 1) : max(1, nx - q.xsi - 1);
-        loy = (sy > 0) ? max(1, q.ysi - 1) : max(1, ny - q.ysi - 1);
+    int loz = 1, lox = 1, loy = 1;            /* the walk's box: the union of the sources' boxes */
+    int lozi[S], loxi[S], loyi[S];
+    R eps_r[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) {
+        lozi[i] = loxi[i] = loyi[i] = 1;
+        eps_r[i] = (R)qs[i].eps_t;
+        if (INIT) { /* solver3D.F90:493-565, flipped bound clamped to the grid */
+            lozi[i] = (sz > 0) ? max(1, qs[i].zsi - 1) : max(1, nz - qs[i].zsi - 1);
+            loxi[i] = (sx > 0) ? max(1, qs[i].xsi - 1) : max(1, nx - qs[i].xsi - 1);
+            loyi[i] = (sy > 0) ? max(1, qs[i].ysi - 1) : max(1, ny - qs[i].ysi - 1);
+        }
+    }
+    if (INIT) {
+        loz = lozi[0]; lox = loxi[0]; loy = loyi[0];
+#pragma unroll
+        for (int i = 1; i < S; ++i)
+            if (ttp[i]) { loz = min(loz, lozi[i]); lox = min(lox, loxi[i]); loy = min(loy, loyi[i]); }
     }
     Mesh<R> mesh;
     fk3::make_mesh<R>(mesh, g.dz, g.dx, g.dy);
     Mesh<double> mesh64;
     if (INIT) fk3::make_mesh<double>(mesh64, g.dz, g.dx, g.dy);
     const R HUGEV = (R)FK_HUGE;
-    const R eps_r = (R)q.eps_t;
     const int th = min(TY, ny - TY * P);             /* rows in this slab */
     const bool row = ty < th;
     const int y = TY * P + ty;
@@ -237,7 +254,11 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
                 ten = (tx == 0) ? (from_ring ? ring_tn[i * zring + zq] : HUGEV) : sh_tn[i];
                 const R told = cur.told[i];
                 result = told;
-                if (upd && ttp[i]) {
+                /* a source updates only inside its own box (the walk's box for S = 1) */
+                const bool updi = S == 1 || !INIT ||
+                                  (yl >= loyi[i] && xl >= loxi[i] && loz - 1 + zq >= lozi[i]);
+                if (upd && updi && ttp[i]) {
+                    const Src &q = qs[i];
                     const R tv = r_last[i], tev = te_last[i], tnv = tn_last[i], tnve = ten_last[i];
                     R r;
                     if (!INIT) {
@@ -253,7 +274,7 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
                          * node-centred source along a grid line of a uniform medium)
                          * stays spherical, as in FP64, instead of being pushed past the
                          * threshold by its own rounding */
-                        const bool lcart = rmin(rmin(tv, te), tn) > eps_r;
+                        const bool lcart = rmin(rmin(tv, te), tn) > eps_r[i];
                         if (lcart && sizeof(R) == 4)
                             /* away from the source the initialisation stencil is the
                              * plane-wave one (localSolver.F90:715-732) */
@@ -874,14 +895,19 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
             for (int i = 0; i < S; ++i)
                 if (wi[i] >= 0) skip = skip && *((volatile int *)(P.conv_pass + wi[i])) < pass;
         }
-        Src q;
-        fk3tw::tw_setup_src(q, w0, g, P.eps);
+        Src qs[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) fk3tw::tw_setup_src(qs[i], i == 0 ? w0 : P.work[wi[i] >= 0 ? wi[i] : wi[0]], g, P.eps);
         if (INIT) {
-            /* slabs wholly before this sweep's source-limited rows keep their values */
-            const int loy = (sy > 0) ? max(1, q.ysi - 1) : max(1, g.ny - q.ysi - 1);
+            /* slabs wholly before every source's rows of this sweep keep their values */
             const int ylast = (sy > 0) ? min(g.ny, TY * (Pp + 1)) - 1 : TY * Pp;
             const int yl_max = (sy > 0) ? ylast : g.ny - 1 - ylast;
-            skip = yl_max < loy;
+            skip = true;
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                const int loy = (sy > 0) ? max(1, qs[i].ysi - 1) : max(1, g.ny - qs[i].ysi - 1);
+                if (wi[i] >= 0 && yl_max >= loy) skip = false;
+            }
         }
         double dmax[S];
 #pragma unroll
@@ -895,7 +921,7 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
                 ok = slab_pass_f32<RESID, S, CHP>(P, g, ttp, reinterpret_cast<const float *>(g.slow), s, sweep_no,
                                                   Pp, nslab, prog, xr, ring, zring, s_flag, dmax);
             else
-                ok = slab_sweep<R, INIT, RESID, S, CHP>(P, g, ttp, reinterpret_cast<const R *>(g.slow), q, s,
+                ok = slab_sweep<R, INIT, RESID, S, CHP>(P, g, ttp, reinterpret_cast<const R *>(g.slow), qs, s,
                                                         sweep_no, Pp, nslab, prog, xr, ring, zring, s_flag, dmax);
             if (!ok) break;
         }
@@ -968,7 +994,7 @@ inline int launch_slab_kernel(const fk3tw::Params &P, const int *pairs, int zrin
 /* The FP32 initialisation kernel lives in its own unit (slab_init_f32.cu),
  * compiled without multiply-add contraction: its near-source spherical
  * stencil is FP64 and so rounds as the FP64 CPU algorithm does. */
-int launch_init_f32(const fk3tw::Params &P, int zring, cudaStream_t st, int blocks_per_sm);
+int launch_init_f32(const fk3tw::Params &P, int zring, cudaStream_t st, int blocks_per_sm, const int *pairs);
 
 template <typename R>
 inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nwork, const fk_slabs3d_t *pl,
@@ -1017,8 +1043,16 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
     P.ticket = pl->tickets;
     if (fk3tw::g_slab_events) cudaEventRecord(fk3tw::g_slab_events[0], st);
     int rc;
-    if constexpr (sizeof(R) == 4)
-        rc = launch_init_f32(P, zring, st, pl->init_blocks_per_sm);
+    if constexpr (sizeof(R) == 4) {
+        if (pl->init_pairs) { /* two sources per thread over the union of their boxes */
+            fk3tw::Params Pi = P;
+            Pi.tasks = reinterpret_cast<const int2 *>(pl->tasks2);
+            Pi.ntask_sweep = pl->ntask2_sweep;
+            rc = launch_init_f32(Pi, zring, st, pl->init_blocks_per_sm, pl->init_pairs);
+        } else {
+            rc = launch_init_f32(P, zring, st, pl->init_blocks_per_sm, nullptr);
+        }
+    }
     else
         rc = launch_slab_kernel<R, true, false, 1>(P, nullptr, zring, st, 0, pl->init_blocks_per_sm);
     if (rc) return rc;

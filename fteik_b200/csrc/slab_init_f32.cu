@@ -8,8 +8,9 @@
 #include "row3d_impl.cuh"
 
 namespace fk3rw {
-int launch_init_f32(const fk3tw::Params &P, int zring, cudaStream_t st, int blocks_per_sm)
+int launch_init_f32(const fk3tw::Params &P, int zring, cudaStream_t st, int blocks_per_sm, const int *pairs)
 {
+    if (pairs) return launch_slab_kernel<float, true, false, 2>(P, pairs, zring, st, 0, blocks_per_sm);
     return launch_slab_kernel<float, true, false, 1>(P, nullptr, zring, st, 0, blocks_per_sm);
 }
 } // namespace fk3rw

@@ -383,14 +383,16 @@ void fteik_b200_batch3d_getTravelTimes64f(int igrid, int nval, double ttr[],
 /* The launch configuration the batch runs (see fteik_b200_setSlabConfig):
  * knobs left at -1 are chosen by timing the candidates on the first solve of
  * a new work list (grid shapes, sources per grid, precision, passes); the
+ * initialisation kernel takes its own blocks per SM and source pairing
+ * (initPairs: two sources per thread over the union of their boxes).  The
  * choice is remembered in the process and, when the environment variable
  * FTEIK_B200_TUNE_CACHE names a file, appended to that file for later
  * processes.  initMs / passMs: the chosen kernels' times during the search
  * (0 when nothing was searched), tuneRuns the candidate solves it ran (0 on
  * a cache hit).  No counterpart in the reference. */
 void fteik_b200_batch3d_getSlabConfig(int *staged, int *pairs, int *progress, int *blocksPerSM,
-                                      int *initBlocksPerSM, float *initMs, float *passMs, int *tuneRuns,
-                                      int *ierr);
+                                      int *initBlocksPerSM, int *initPairs, float *initMs, float *passMs,
+                                      int *tuneRuns, int *ierr);
 /* Run one solve outside its CUDA graph with events around the
  * initialisation kernel and the Gauss-Seidel kernel and return their device
  * times (ms); the fields end as after fteik_b200_batch3d_solve. */

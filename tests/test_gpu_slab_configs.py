@@ -170,5 +170,5 @@ def test_tuned_configuration_not_slower_than_fixed(fk, kind, tmp_path, monkeypat
     b.finalize()
     assert again["tune_runs"] == 0
     assert (tmp_path / "tune.txt").read_text().count("\n") >= 1
-    assert [again[k] for k in ("staged", "pairs", "progress", "blocks_per_sm", "init_blocks_per_sm")] == \
-        [cfg[k] for k in ("staged", "pairs", "progress", "blocks_per_sm", "init_blocks_per_sm")]
+    keys = ("staged", "pairs", "progress", "blocks_per_sm", "init_blocks_per_sm", "init_pairs")
+    assert [again[k] for k in keys] == [cfg[k] for k in keys]
