@@ -180,6 +180,8 @@ _SIGS = {
     "fteik_b200_mlp_forward": [c_int, _PF, _PF, _PI],
     "fteik_b200_mlp_gradient": [c_int, _PF, _PF, _PD, _PF, _PI],
     "fteik_b200_mlp_train": [c_int, _PF, _PF, c_int, c_int, c_double, _PD, _PI],
+    "fteik_b200_mlp_setTensorProducts": [c_int, _PI],
+    "fteik_b200_mlp_getTensorProducts": [_PI],
     "fteik_b200_locate_l2_noalloc": [c_int, c_int, c_int, ctypes.c_void_p, c_int, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, _PI],
@@ -266,6 +268,17 @@ def set_slab_config(staged=-1, pairs=-1, progress=-1, blocks_per_sm=-1):
     lib().fteik_b200_setSlabConfig(int(staged), int(pairs), int(progress), int(blocks_per_sm), byref(ierr))
     _check(ierr, "fteik_b200_setSlabConfig")
     return tuple(v.value for v in old)
+
+
+def set_mlp_tensor_products(products):
+    """Hidden-layer GEMMs of the surrogate: 0 FP32 CUDA cores, 1 BF16
+    tensor cores, 3 split-BF16 tensor cores; returns the previous value."""
+    old = c_int()
+    lib().fteik_b200_mlp_getTensorProducts(byref(old))
+    ierr = c_int(1)
+    lib().fteik_b200_mlp_setTensorProducts(int(products), byref(ierr))
+    _check(ierr, "fteik_b200_mlp_setTensorProducts")
+    return old.value
 
 
 def _check(ierr, what):

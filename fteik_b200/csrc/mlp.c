@@ -23,6 +23,35 @@ int fk_mlp_colsum(int M, int N, const float *dz, float *db, cudaStream_t s);
 int fk_mlp_mse(int n, const float *pred, const float *y, float *dpred, double *loss, cudaStream_t s);
 int fk_mlp_adam(size_t n, float *w, const float *g, float *m, float *v, float lr, float b1,
                 float b2, float eps, float c1, float c2, cudaStream_t s);
+void fk_mlp_set_tensor(int products);
+int fk_mlp_get_tensor(void);
+int fk_mlp_tc_status(cudaStream_t s);
+
+void fteik_b200_mlp_setTensorProducts(int products, int *ierr)
+{
+    *ierr = 0;
+    if (products != 0 && products != 1 && products != 3) {
+        FK_ERR("fteik_b200_mlp_setTensorProducts: products must be 0, 1 or 3");
+        *ierr = 1;
+        return;
+    }
+    fk_mlp_set_tensor(products);
+}
+
+void fteik_b200_mlp_getTensorProducts(int *products) { *products = fk_mlp_get_tensor(); }
+
+/* 0, or the CUDA error / tensor-core wait timeout of the work queued so far */
+static int tc_check(int e, const char *who)
+{
+    if (!e) {
+        const int st = fk_mlp_tc_status(fk_stream());
+        if (st) {
+            FK_ERR("%s: a tensor-core GEMM gave up waiting (%d)", who, st);
+            return 1;
+        }
+    }
+    return fk_check(e, who);
+}
 
 #define MLP_IN 6
 #define MLP_MAXL 16
@@ -218,7 +247,7 @@ void fteik_b200_mlp_forward(int n, const float x[], float tau[], int *ierr)
         if (!e) e = (int)cudaMemcpyAsync(tau + r0, NN.x[NN.nlayer], sizeof(float) * (size_t)B,
                                          cudaMemcpyDeviceToHost, s);
         if (!e) e = (int)cudaStreamSynchronize(s);
-        if (fk_check(e, "fteik_b200_mlp_forward")) return;
+        if (tc_check(e, "fteik_b200_mlp_forward")) return;
     }
     *ierr = 0;
 }
@@ -241,7 +270,7 @@ void fteik_b200_mlp_gradient(int n, const float x[], const float y[], double *lo
     if (!e) e = (int)cudaMemcpyAsync(loss, NN.loss_dev, sizeof(double), cudaMemcpyDeviceToHost, s);
     if (!e) e = (int)cudaStreamSynchronize(s);
     fk_dfree(ydev);
-    *ierr = fk_check(e, "fteik_b200_mlp_gradient");
+    *ierr = tc_check(e, "fteik_b200_mlp_gradient");
 }
 
 /* Adam steps over batches produced by next_batch (device x / y).  The
@@ -277,7 +306,7 @@ int fk_mlp_train_device(fk_batch_fn next_batch, void *ctx, long long steps, int 
     }
     fk_dfree(ydev);
     if (last_loss) *last_loss = lcount ? lsum / (double)lcount : 0.0;
-    return fk_check(e, "mlp training");
+    return tc_check(e, "mlp training");
 }
 
 typedef struct {

@@ -272,10 +272,70 @@ using namespace fkmlp;
 
 static int grid1d(size_t n) { size_t b = (n + 255) / 256; return (int)(b < 4096 ? (b ? b : 1) : 4096); }
 
+extern "C" int fk_mlp_gemm_tc(int prod, int M, int N, int K, const float *A, int lda, int ta, const float *B,
+                              int ldb, int tb, float *C, int ldc, const float *bias, int accumulate, int split,
+                              float *ws, int *error, cudaStream_t s);
+
+/* 0: every GEMM on the CUDA cores in FP32; 1 or 3: GEMMs with N and K of at
+ * least 64 (the hidden layers) on the tensor cores with that many BF16
+ * products (mlp_tc.cu) */
+static int g_tensor = 1;
+static int *g_tc_error = nullptr;
+
+extern "C" void fk_mlp_set_tensor(int products) { g_tensor = products; }
+extern "C" int fk_mlp_get_tensor(void) { return g_tensor; }
+
+/* the tensor-core kernels' error word (a wait that timed out), read and cleared */
+extern "C" int fk_mlp_tc_status(cudaStream_t s)
+{
+    if (!g_tc_error) return 0;
+    int v = 0;
+    cudaError_t e = cudaMemcpyAsync(&v, g_tc_error, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && v) e = cudaMemsetAsync(g_tc_error, 0, sizeof(int), s);
+    return e != cudaSuccess ? (int)e : v;
+}
+
+static float *g_ws = nullptr;
+static size_t g_ws_cap = 0;
+
+static int workspace(size_t need, cudaStream_t s)
+{
+    if (need <= g_ws_cap) return 0;
+    cudaError_t e = cudaStreamSynchronize(s);   /* the old workspace may still be read */
+    if (e == cudaSuccess && g_ws) e = cudaFree(g_ws);
+    g_ws = nullptr;
+    g_ws_cap = 0;
+    if (e == cudaSuccess) e = cudaMalloc((void **)&g_ws, sizeof(float) * need);
+    if (e != cudaSuccess) return (int)e;
+    g_ws_cap = need;
+    return 0;
+}
+
 extern "C" int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta, const float *B, int ldb,
                            int tb, float *C, int ldc, const float *bias, int accumulate, cudaStream_t s)
 {
     if (M <= 0 || N <= 0) return 0;
+    if (g_tensor && N >= 64 && N <= 256 && K >= 64 && M >= 64) {
+        if (!g_tc_error) {
+            cudaError_t e = cudaMalloc((void **)&g_tc_error, sizeof(int));
+            if (e == cudaSuccess) e = cudaMemsetAsync(g_tc_error, 0, sizeof(int), s);
+            if (e != cudaSuccess) return (int)e;
+        }
+        /* long K with few 128-row tiles (weight gradients): split K over CTAs */
+        const int mt = (M + 127) / 128;
+        int split = 1;
+        while (mt * split < 148 && K / (split * 2) >= 128) split *= 2;
+        if (split > 1) {
+            const int e = workspace((size_t)split * M * N, s);
+            if (e) return e;
+        }
+        int e = fk_mlp_gemm_tc(g_tensor, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate, split, g_ws,
+                               g_tc_error, s);
+        if (e || split == 1) return e;
+        splitk_reduce_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>(M, N, split, g_ws, C, ldc, bias, accumulate);
+        return (int)cudaGetLastError();
+    }
     const int tiles = ((N + TN - 1) / TN) * ((M + TM - 1) / TM);
     /* long K with few output tiles (weight gradients): split K over CTAs */
     int split = 1;
@@ -286,22 +346,12 @@ extern "C" int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta,
         return (int)cudaGetLastError();
     }
     /* partial tiles into the workspace, then an ordered reduction */
-    static float *ws = nullptr;
-    static size_t ws_cap = 0;
-    const size_t need = (size_t)split * M * N;
-    if (need > ws_cap) {
-        cudaError_t e = cudaStreamSynchronize(s);   /* the old workspace may still be read */
-        if (e == cudaSuccess && ws) e = cudaFree(ws);
-        ws = nullptr;
-        ws_cap = 0;
-        if (e == cudaSuccess) e = cudaMalloc((void **)&ws, sizeof(float) * need);
-        if (e != cudaSuccess) return (int)e;
-        ws_cap = need;
-    }
-    gemm_kernel<<<grid, NT, 0, s>>>(M, N, K, A, lda, ta, B, ldb, tb, ws, N, nullptr, 0);
+    const int ew = workspace((size_t)split * M * N, s);
+    if (ew) return ew;
+    gemm_kernel<<<grid, NT, 0, s>>>(M, N, K, A, lda, ta, B, ldb, tb, g_ws, N, nullptr, 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return (int)e;
-    splitk_reduce_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>(M, N, split, ws, C, ldc, bias, accumulate);
+    splitk_reduce_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>(M, N, split, g_ws, C, ldc, bias, accumulate);
     return (int)cudaGetLastError();
 }
 

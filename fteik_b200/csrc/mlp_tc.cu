@@ -1,0 +1,333 @@
+/*
+ * mlp_tc.cu -- the surrogate network's GEMMs on the tensor cores (tcgen05,
+ * BF16 operands, FP32 accumulators in tensor memory).  No counterpart in the
+ * reference.
+ *
+ * C[M][N] = sum_k A(m,k) B(k,n) (+ bias[n]) with the operand accessors of
+ * the CUDA-core kernel (mlp.cu): A(m,k) = A[m lda + k] (ta = 0) or
+ * A[k lda + m] (ta = 1); B(k,n) = B[k ldb + n] (tb = 0) or B[n ldb + k]
+ * (tb = 1).  A CTA computes one 128 x 256 tile (M x N; N up to 256) over a
+ * range of K (split K: partial tiles go to a workspace that a second kernel
+ * adds in a fixed order).
+ *
+ * Each K block of 64 is staged by all 256 threads: FP32 values from global
+ * memory, rounded to BF16 (PROD = 1) or split into BF16 hi + lo parts
+ * (PROD = 3: products hi hi + hi lo + lo hi, about FP32 accuracy), written
+ * into shared memory in the 128-byte-swizzled K-major layout the MMA reads.
+ * One thread issues the MMAs (kind::f16, 128 x 256 x 16 each) and commits
+ * them to the stage's mbarrier; the next stage is staged meanwhile (two
+ * stages).  The epilogue reads the accumulators from tensor memory with
+ * tcgen05.ld (warp w: lanes 32 (w mod 4) .. +31, columns 128 (w / 4) ..
+ * +127) and writes C.  Every mbarrier wait is bounded; on a timeout the CTA
+ * sets the error word, lets its MMAs drain and frees its tensor memory.
+ */
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fteik_dev.h"
+
+namespace fkmtc {
+
+constexpr int BM = 128, BN = 256, BK = 64;
+constexpr int NT = 256;
+constexpr int A_TILE = BM * BK * 2;   /* 16 KB of BF16 */
+constexpr int B_TILE = BN * BK * 2;   /* 32 KB */
+constexpr uint32_t TMEM_COLS = 256;
+constexpr long long WAIT_LIMIT = 1ll << 24;
+
+/* kind::f16 instruction descriptor: D FP32, A and B BF16, both K-major,
+ * N >> 3 at bit 17, M >> 4 at bit 24 */
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+
+template <int PROD>
+struct Cfg {
+    static constexpr int NP = PROD == 3 ? 2 : 1;          /* hi (+ lo) copies */
+    static constexpr int STAGE = NP * (A_TILE + B_TILE);
+    static constexpr int SMEM = 2 * STAGE + 1024;         /* + alignment slack */
+};
+
+/* byte offset of element (row, k) in a swizzled K-major tile (rows of 128 B) */
+__device__ __forceinline__ uint32_t swz(int row, int k)
+{
+    return (uint32_t)row * 128u + ((uint32_t)(((k >> 3) ^ (row & 7))) << 4) + (uint32_t)(k & 7) * 2u;
+}
+
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (long long i = 0; i < WAIT_LIMIT; ++i)
+        if (mbar_try(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(IDESC), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+#define FKM_R8(i) "=r"(r[i]), "=r"(r[i + 1]), "=r"(r[i + 2]), "=r"(r[i + 3]), "=r"(r[i + 4]), \
+                  "=r"(r[i + 5]), "=r"(r[i + 6]), "=r"(r[i + 7])
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *r)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : FKM_R8(0), FKM_R8(8), FKM_R8(16), FKM_R8(24)
+        : "r"(taddr)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+/* one value into the hi (and lo) tiles */
+template <int PROD>
+__device__ __forceinline__ void put(uint8_t *hi, uint8_t *lo, uint32_t off, float v)
+{
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    *reinterpret_cast<__nv_bfloat16 *>(hi + off) = h;
+    if (PROD == 3) *reinterpret_cast<__nv_bfloat16 *>(lo + off) = __float2bfloat16_rn(v - __bfloat162float(h));
+}
+
+/* Stage the K block [k0, k0 + 64) of A (rows m0 ..) and B (columns n0 ..);
+ * out-of-range elements are zero. */
+template <int PROD>
+__device__ __forceinline__ void stage(uint8_t *sA, uint8_t *sB, int M, int N, int K, const float *__restrict__ A,
+                                      int lda, int ta, const float *__restrict__ B, int ldb, int tb, int m0, int n0,
+                                      int k0, int k1)
+{
+    uint8_t *aLo = sA + A_TILE, *bLo = sB + B_TILE;
+    const int t = threadIdx.x;
+    if (!ta) {
+        /* A[m][k], k contiguous: thread -> row t / 2, 32 consecutive k */
+        const int row = t >> 1, kb = (t & 1) * 32, m = m0 + row;
+#pragma unroll 8
+        for (int i = 0; i < 32; ++i) {
+            const int k = k0 + kb + i;
+            const float v = (m < M && k < k1) ? A[(size_t)m * lda + k] : 0.0f;
+            put<PROD>(sA, aLo, swz(row, kb + i), v);
+        }
+    } else {
+        /* A[k][m], m contiguous: thread -> k = t / 4, 32 consecutive m */
+        const int kk = t >> 2, mb = (t & 3) * 32, k = k0 + kk;
+#pragma unroll 8
+        for (int i = 0; i < 32; ++i) {
+            const int m = m0 + mb + i;
+            const float v = (m < M && k < k1) ? A[(size_t)k * lda + m] : 0.0f;
+            put<PROD>(sA, aLo, swz(mb + i, kk), v);
+        }
+    }
+    if (tb) {
+        /* B[n][k], k contiguous: thread -> row n = t, 64 consecutive k */
+        const int n = n0 + t;
+#pragma unroll 8
+        for (int i = 0; i < 64; ++i) {
+            const int k = k0 + i;
+            const float v = (n < N && k < k1) ? B[(size_t)n * ldb + k] : 0.0f;
+            put<PROD>(sB, bLo, swz(t, i), v);
+        }
+    } else {
+        /* B[k][n], n contiguous: thread -> k = t / 4, 64 consecutive n */
+        const int kk = t >> 2, nb = (t & 3) * 64, k = k0 + kk;
+#pragma unroll 8
+        for (int i = 0; i < 64; ++i) {
+            const int n = n0 + nb + i;
+            const float v = (n < N && k < k1) ? B[(size_t)k * ldb + n] : 0.0f;
+            put<PROD>(sB, bLo, swz(nb + i, kk), v);
+        }
+    }
+    /* the generic-proxy writes become visible to the tensor cores' reads */
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+template <int PROD>
+__global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, const float *__restrict__ A, int lda,
+                                                        int ta, const float *__restrict__ B, int ldb, int tb,
+                                                        float *__restrict__ C, int ldc,
+                                                        const float *__restrict__ bias, int accumulate,
+                                                        int kchunk, int *error)
+{
+    using G = Cfg<PROD>;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    uint8_t *base = reinterpret_cast<uint8_t *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
+    const int nkb = (ke - kb + BK - 1) / BK;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t bar0 = (uint32_t)__cvta_generic_to_shared(&bars[0]);
+    if (threadIdx.x == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_fail = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(&s_tmem)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    int committed = 0;
+    for (int b = 0; b < nkb; ++b) {
+        const int buf = b & 1;
+        uint8_t *sA = base + buf * G::STAGE;
+        uint8_t *sB = sA + G::NP * A_TILE;
+        if (b >= 2 && !mbar_wait(bar0 + 8u * buf, ((b - 2) >> 1) & 1)) {   /* the MMAs of b - 2 read this stage */
+            if (threadIdx.x == 0) { atomicCAS(error, 0, 1); s_fail = 1; }
+        }
+        __syncthreads();
+        if (s_fail) break;
+        stage<PROD>(sA, sB, M, N, K, A, lda, ta, B, ldb, tb, m0, n0, kb + b * BK, ke);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc_fence_after();
+            const uint32_t a_hi = (uint32_t)__cvta_generic_to_shared(sA), a_lo = a_hi + A_TILE;
+            const uint32_t b_hi = (uint32_t)__cvta_generic_to_shared(sB), b_lo = b_hi + B_TILE;
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) {
+                const uint32_t ko = (uint32_t)kk * 32u;
+                mma_bf16(tmem, sdesc_sw128(a_hi + ko), sdesc_sw128(b_hi + ko), (b > 0 || kk > 0) ? 1u : 0u);
+                if (PROD == 3) {
+                    mma_bf16(tmem, sdesc_sw128(a_hi + ko), sdesc_sw128(b_lo + ko), 1u);
+                    mma_bf16(tmem, sdesc_sw128(a_lo + ko), sdesc_sw128(b_hi + ko), 1u);
+                }
+            }
+            mma_commit(bar0 + 8u * buf);
+        }
+        committed = b + 1;
+    }
+    /* every MMA of this CTA has completed: the last commit covers them all */
+    bool ok = !s_fail;
+    if (committed > 0) {
+        const int last = committed - 1;
+        if (!mbar_wait(bar0 + 8u * (last & 1), (last >> 1) & 1)) {
+            ok = false;
+            if (threadIdx.x == 0) atomicCAS(error, 0, 2);
+        }
+    }
+    tc_fence_after();
+    if (ok && committed == 0 && gridDim.z > 1) {
+        /* a split-K slice past the end of K: its partial tile is zero */
+        for (int e = threadIdx.x; e < BM * BN; e += NT) {
+            const int m = m0 + e / BN, n = n0 + e % BN;
+            if (m < M && n < N) C[((size_t)blockIdx.z * M + m) * N + n] = 0.0f;
+        }
+    }
+    if (ok && committed > 0) {
+        /* epilogue: this warp's 32 TMEM lanes, 128 of the 256 columns */
+        const int q = warp & 3, half = warp >> 2;
+        const int m = m0 + q * 32 + lane;
+#pragma unroll 1
+        for (int c = 0; c < 128; c += 32) {
+            uint32_t r[32];
+            tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(half * 128 + c), r);
+            tmem_wait_ld();
+            if (m < M) {
+                const int nb = n0 + half * 128 + c;
+                if (gridDim.z > 1) {
+                    float *w = C + ((size_t)blockIdx.z * M + m) * N;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        if (nb + j < N) w[nb + j] = __uint_as_float(r[j]);
+                } else {
+                    float *crow = C + (size_t)m * ldc;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int n = nb + j;
+                        if (n < N) {
+                            const float v = __uint_as_float(r[j]) + (bias ? bias[n] : 0.0f);
+                            crow[n] = accumulate ? crow[n] + v : v;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+} // namespace fkmtc
+
+/* Launch one tensor-core GEMM (PROD 1 or 3); ws: split-K workspace of split
+ * M N floats, or NULL for split = 1; error: device word set on a wait
+ * timeout.  Returns a cudaError_t. */
+extern "C" int fk_mlp_gemm_tc(int prod, int M, int N, int K, const float *A, int lda, int ta, const float *B,
+                              int ldb, int tb, float *C, int ldc, const float *bias, int accumulate, int split,
+                              float *ws, int *error, cudaStream_t s)
+{
+    using namespace fkmtc;
+    if (M <= 0 || N <= 0 || K <= 0) return 0;
+    if (N > BN || (prod != 1 && prod != 3) || (split > 1 && !ws)) return (int)cudaErrorInvalidValue;
+    const int kchunk = ((K + split * BK - 1) / (split * BK)) * BK;
+    const dim3 grid(1, (M + BM - 1) / BM, split);
+    cudaError_t e;
+    if (prod == 3) {
+        const int smem = Cfg<3>::SMEM;
+        e = cudaFuncSetAttribute(gemm_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return (int)e;
+        gemm_tc_kernel<3><<<grid, NT, smem, s>>>(M, N, K, A, lda, ta, B, ldb, tb, split > 1 ? ws : C,
+                                                 split > 1 ? N : ldc, split > 1 ? nullptr : bias,
+                                                 split > 1 ? 0 : accumulate, kchunk, error);
+    } else {
+        const int smem = Cfg<1>::SMEM;
+        e = cudaFuncSetAttribute(gemm_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return (int)e;
+        gemm_tc_kernel<1><<<grid, NT, smem, s>>>(M, N, K, A, lda, ta, B, ldb, tb, split > 1 ? ws : C,
+                                                 split > 1 ? N : ldc, split > 1 ? nullptr : bias,
+                                                 split > 1 ? 0 : accumulate, kchunk, error);
+    }
+    return (int)cudaGetLastError();
+}

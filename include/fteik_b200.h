@@ -483,6 +483,15 @@ void fteik_b200_mlp_gradient(int n, const float x[], const float y[], double *lo
                              int *ierr);
 void fteik_b200_mlp_train(int n, const float x[], const float y[], int steps, int batch, double lr,
                           double *loss, int *ierr);
+/* Arithmetic of the network's hidden-layer products (forward, input and
+ * weight gradients, inference): 1 (default) = tensor cores (tcgen05), BF16
+ * operands, FP32 accumulation; 3 = tensor cores, each FP32 operand split
+ * into BF16 hi + lo and the products hi hi + hi lo + lo hi (about FP32
+ * accuracy, three times the tensor work); 0 = FP32 on the CUDA cores.  The
+ * first and last layers (6 inputs, 1 output) always run on the CUDA cores;
+ * weights, Adam and losses stay FP32. */
+void fteik_b200_mlp_setTensorProducts(int products, int *ierr);
+void fteik_b200_mlp_getTensorProducts(int *products);
 
 /* The 2D ray paths of the last fteik_solver2d_traceRaysToPoints /
  * ToReceivers (rays.F90:449-670, which keeps them in module variables no C
