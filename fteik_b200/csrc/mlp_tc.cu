@@ -129,8 +129,29 @@ __device__ __forceinline__ void put(uint8_t *hi, uint8_t *lo, uint32_t off, floa
     if (PROD == 3) *reinterpret_cast<__nv_bfloat16 *>(lo + off) = __float2bfloat16_rn(v - __bfloat162float(h));
 }
 
+/* 8 consecutive-k values (two float4) as one 16-byte swizzle unit of the hi
+ * (and lo) tiles */
+template <int PROD>
+__device__ __forceinline__ void put8(uint8_t *hi, uint8_t *lo, uint32_t off, float4 a, float4 b)
+{
+    const float v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const __nv_bfloat162 p = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+        h[i] = *reinterpret_cast<const uint32_t *>(&p);
+        if (PROD == 3) {
+            const __nv_bfloat162 q = __floats2bfloat162_rn(v[2 * i] - __low2float(p), v[2 * i + 1] - __high2float(p));
+            l[i] = *reinterpret_cast<const uint32_t *>(&q);
+        }
+    }
+    *reinterpret_cast<uint4 *>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+    if (PROD == 3) *reinterpret_cast<uint4 *>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
 /* Stage the K block [k0, k0 + 64) of A (rows m0 ..) and B (columns n0 ..);
- * out-of-range elements are zero. */
+ * out-of-range elements are zero.  Rows with k contiguous in memory move in
+ * 16-byte loads when the whole block is in range and aligned. */
 template <int PROD>
 __device__ __forceinline__ void stage(uint8_t *sA, uint8_t *sB, int M, int N, int K, const float *__restrict__ A,
                                       int lda, int ta, const float *__restrict__ B, int ldb, int tb, int m0, int n0,
@@ -138,7 +159,17 @@ __device__ __forceinline__ void stage(uint8_t *sA, uint8_t *sB, int M, int N, in
 {
     uint8_t *aLo = sA + A_TILE, *bLo = sB + B_TILE;
     const int t = threadIdx.x;
-    if (!ta) {
+    const bool kfull = k0 + BK <= k1;
+    if (!ta && kfull && (lda & 3) == 0 && ((uintptr_t)A & 15) == 0) {
+        const int row = t >> 1, kb = (t & 1) * 32, m = m0 + row;
+        const float4 *src = reinterpret_cast<const float4 *>(A + (size_t)m * lda + k0 + kb);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+            if (m < M) { a = src[2 * c]; b = src[2 * c + 1]; }
+            put8<PROD>(sA, aLo, swz(row, kb + 8 * c), a, b);
+        }
+    } else if (!ta) {
         /* A[m][k], k contiguous: thread -> row t / 2, 32 consecutive k */
         const int row = t >> 1, kb = (t & 1) * 32, m = m0 + row;
 #pragma unroll 8
@@ -157,7 +188,16 @@ __device__ __forceinline__ void stage(uint8_t *sA, uint8_t *sB, int M, int N, in
             put<PROD>(sA, aLo, swz(mb + i, kk), v);
         }
     }
-    if (tb) {
+    if (tb && kfull && (ldb & 3) == 0 && ((uintptr_t)B & 15) == 0) {
+        const int n = n0 + t;
+        const float4 *src = reinterpret_cast<const float4 *>(B + (size_t)n * ldb + k0);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+            if (n < N) { a = src[2 * c]; b = src[2 * c + 1]; }
+            put8<PROD>(sB, bLo, swz(t, 8 * c), a, b);
+        }
+    } else if (tb) {
         /* B[n][k], k contiguous: thread -> row n = t, 64 consecutive k */
         const int n = n0 + t;
 #pragma unroll 8
