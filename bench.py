@@ -475,6 +475,13 @@ def locate_workload(b, g, nev, igrid=LOC_GRID):
     return picks
 
 
+def _mlp_products(fk):
+    from ctypes import byref, c_int
+    v = c_int()
+    fk.lib().fteik_b200_mlp_getTensorProducts(byref(v))
+    return v.value
+
+
 def bench_locate(fk, b, grids, stream, steps, nev=LOC_NEV, igrid=LOC_GRID, sur_steps=SUR_STEPS):
     import torch
     g = grids[LOC_GRID - 1]
@@ -508,6 +515,7 @@ def bench_locate(fk, b, grids, stream, steps, nev=LOC_NEV, igrid=LOC_GRID, sur_s
     # exactly
     loc.setGeometry(g["nz"], g["nx"], g["ny"], H, H, H, g["zs"], g["xs"], g["ys"])
     fk.MLP(SUR_WIDTH, SUR_DEPTH, seed=7)
+    mlp_products = _mlp_products(fk)
     torch.cuda.synchronize()
     t_tr = time.perf_counter()
     sur_loss = loc.trainSurrogate(nsamples=SUR_SAMPLES, steps=sur_steps, batch=SUR_BATCH, lr=2e-3,
@@ -560,7 +568,10 @@ def bench_locate(fk, b, grids, stream, steps, nev=LOC_NEV, igrid=LOC_GRID, sur_s
                 "fine_blocks_examined_per_event": nblk / max(1, nev - nfb),
                 "stage_ms": {"coarse_ranking": stage[0], "pruned_rescore": stage[1],
                              "results_to_host": stage[2]},
-                "network": "6 -> %d x %d SiLU -> tau, FP32 CUDA-core kernels" % (SUR_DEPTH, SUR_WIDTH),
+                "network": "6 -> %d x %d SiLU -> tau; hidden-layer GEMMs on the tensor cores (tcgen05, %s), "
+                           "first / last layer, SiLU, Adam on the CUDA cores in FP32" % (
+                               SUR_DEPTH, SUR_WIDTH, {0: "off: FP32 CUDA cores", 1: "BF16 operands, FP32 accumulators",
+                                                      3: "split-BF16 operands, FP32 accumulators"}[mlp_products]),
                 "training": {"samples": SUR_SAMPLES, "steps": sur_steps, "batch": SUR_BATCH,
                              "seconds": t_tr, "final_mse_tau": sur_loss,
                              "tflops": 3.0 * flops_row * sur_steps * SUR_BATCH / t_tr / 1e12},

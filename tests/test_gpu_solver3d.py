@@ -110,6 +110,45 @@ def test_orderings_and_cells(fk):
     s.free()
 
 
+@pytest.mark.parametrize("precision", [8, 4])
+@pytest.mark.parametrize("setter", ["nodal0", "nodal1", "nodal2", "cell32f"])
+def test_velocity_setters_solve_like_oracle(fk, setter, precision):
+    """Nodal velocities in each ordering (model.F90:311-449) and FP32 cell
+    velocities (model.F90:719-754) set through the C ABI and solved on the
+    GPU, against the oracle solving the slowness its own restatement of the
+    setter builds."""
+    import ctypes
+    from ctypes import byref, c_int
+    n, h = (14, 12, 11), (20.0, 25.0, 30.0)
+    nz, nx, ny = n
+    rng = np.random.default_rng(21)
+    src = interior_source(n, h, 3)
+    s = fk.fteik3d()
+    s.initialize(nx, ny, nz, h[1], h[2], h[0], precision=precision)
+    ierr = c_int(1)
+    if setter.startswith("nodal"):
+        order = int(setter[-1])
+        vel = rng.uniform(2000.0, 5000.0, nz * nx * ny)
+        s.lib.fteik_solver3d_setNodalVelocityModel64f(vel.size, order,
+                                                      vel.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                      byref(ierr))
+        slow = O.nodal_to_slowness(n, order, vel)
+    else:
+        v32 = rng.uniform(2000.0, 5000.0, (nz - 1) * (nx - 1) * (ny - 1)).astype(np.float32)
+        s.lib.fteik_model_setVelocityModel32f(v32.size, v32.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                              byref(ierr))
+        slow = 1.0 / v32.astype(np.float64)
+    assert ierr.value == 0
+    s.setSources(src[1], src[2], src[0])
+    s.solveSourceLSM(1)
+    got = s.getTravelTimeField()
+    si, sa = O.source_snap(True, n, (0, 0, 0), h, src)
+    want, _ = O.solve3d(n, h, slow, si, sa, 5.0, 2)
+    err = np.max(np.abs(got - want)) / np.max(want)
+    assert err <= (1e-12 if precision == 8 else TOL32), err
+    s.free()
+
+
 def test_receivers_match_oracle(fk):
     n, h, vel, src = _case("grf")
     rng = np.random.default_rng(4)
