@@ -580,7 +580,7 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
                                                      uint32_t stage, const float *stage_f)
 {
     constexpr int CH = CHP;
-    static_assert(CH % DL == 0 && NB == 2 * DL && (2 * DL) % 4 == 0, "windows, progress and load batches align");
+    static_assert(CH % DL == 0 && NB == 2 * DL, "windows and progress align");
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
     const int nz = g.nz, nx = g.nx, ny = g.ny, zp = g.zp;
@@ -727,15 +727,15 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
             __syncthreads();
             if (!s_flag[0]) { ok = false; break; }
         }
-        if ((t0 & 3) == 0) {                    /* load batch: warp-uniform */
-            cpa_wait0();                        /* the batch of 4 steps ago has landed */
-            issue();
-        }
         const int half = (t0 / DL) & 1;
         float (*const xw)[S][TY][32] = xr + half * DL;
         float (*const xrd)[S][TY][32] = xr + (1 - half) * DL;
 #pragma unroll
         for (int u = 0; u < DL; ++u) {
+            if (((t0 + u) & 3) == 0) {          /* load batch every 4 steps: warp-uniform */
+                cpa_wait0();                    /* the batch of 4 steps ago has landed */
+                issue();
+            }
             float sh_r[S], sh_tn[S];
 #pragma unroll
             for (int i = 0; i < S; ++i) {
@@ -971,7 +971,12 @@ inline int launch_slab_kernel(const fk3tw::Params &P, const int *pairs, int zrin
     int dev = 0, nsm = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (smem > 48 * 1024) { /* deep grids: the per-warp rings need the opt-in shared memory */
+    /* deep grids: the per-warp rings (and the stage) need the opt-in shared
+     * memory once they and the kernel's static arrays pass the default 48 KB */
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, slab_kernel<R, INIT, RESID, S, CH_MANY, STG>) != cudaSuccess)
+        return (int)cudaGetLastError();
+    if (smem + fa.sharedSizeBytes > 48 * 1024) {
         cudaError_t ea = cudaFuncSetAttribute(slab_kernel<R, INIT, RESID, S, CH_MANY, STG>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (ea == cudaSuccess && !INIT)

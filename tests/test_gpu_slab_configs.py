@@ -6,7 +6,8 @@ scheduled and loaded, so every configuration gives the default's FP32
 fields bit for bit -- single source and batch, fixed passes and solves to
 convergence -- on grids whose depth takes every leading-item offset of the
 staged step's descending sweeps (nz mod 4 = 0..3), shallower and deeper than
-32, and wider than one 32-column block.  No counterpart in the reference."""
+32, deep enough to need the opt-in shared memory, and wider than one
+32-column block.  No counterpart in the reference."""
 import numpy as np
 import pytest
 
@@ -21,6 +22,7 @@ SHAPES = {            # nz, nx, ny
     "nz12": (12, 14, 13),
     "nz45": (45, 40, 10),
     "nz9_wide": (9, 70, 11),
+    "nz150_deep": (150, 20, 9),   # rings + stage + static arrays above the default 48 KB
 }
 
 

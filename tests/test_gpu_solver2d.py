@@ -142,3 +142,35 @@ def test_2d_more_than_1024_columns(fk, shape):
     # analytic times propagate over a million nodes: 1e-11 of the largest time
     assert np.max(np.abs(tt - ref)) <= 1e-11 * np.max(ref)
     s.free()
+
+
+@pytest.mark.parametrize("kind,order", [("nodal", 0), ("nodal", 1), ("cell", 0), ("cell", 1)])
+def test_2d_velocity_setters_solve_like_oracle(fk, kind, order):
+    """2D nodal and cell velocities in the ZX (0) and XZ (1) orderings
+    (model.F90:311-607) set through the C ABI and solved on the GPU, against
+    the oracle solving the slowness its restatement of the setter builds."""
+    import ctypes
+    from ctypes import byref, c_int
+    nz, nx, h = 27, 31, 10.0
+    src = (113.3, 171.9)
+    rng = np.random.default_rng(12 + order)
+    s = fk.fteik2d()
+    s.initialize(nx, nz, h, h, nsweep=2, eps=5.0)
+    n = nz * nx if kind == "nodal" else (nz - 1) * (nx - 1)
+    vel = rng.uniform(2000.0, 5000.0, n)
+    p = vel.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    ierr = c_int(1)
+    if kind == "nodal":
+        s.lib.fteik_solver2d_setNodalVelocityModel64f(n, order, p, byref(ierr))
+        slow = O.nodal_to_slowness((nz, nx, 1), order, vel)
+    else:
+        s.lib.fteik_solver2d_setCellVelocityModel64f(n, order, p, byref(ierr))
+        slow = O.cell_to_slowness((nz, nx, 1), order, vel)
+    assert ierr.value == 0
+    s.setSources(src[1], src[0])
+    s.solveSourceLSM(1)
+    tt = s.getTravelTimeField()
+    si, sa = O.source_snap(False, (nz, nx, 1), (0, 0, 0), (h, h, 1.0), (src[0], src[1], 0.0))
+    ref, _ = O.solve2d((nz, nx), (h, h), slow, si[:2], sa[:2], 5.0, 2)
+    assert np.max(np.abs(tt - ref)) <= 1e-12 * np.max(ref)
+    s.free()
