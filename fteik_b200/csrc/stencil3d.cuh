@@ -156,10 +156,10 @@ __device__ __forceinline__ V noinit_v(const Mesh<float> &c, V tv, V te, V tn, V 
     return out;
 }
 
-/* noinit_v<float> with the compiler free to contract products into
- * multiply-adds: the same operators.  The Gauss-Seidel pass step uses this
- * form (14 % faster there); the initialisation sweeps use noinit_v<float>
- * (9 % faster there).  With d = te - tv etc. the
+/* noinit_v<float> written with scalar operations: the same roundings in
+ * the same order (every multiply-add explicit), so both give the same bits.
+ * The direct Gauss-Seidel pass step uses this form (14 % faster there than
+ * noinit_v<float2>).  With d = te - tv etc. the
  * plane operator is  t = tev + d (dx2i - dz2i)/B + (2/B) sqrt(s^2 B - C d^2),
  * B = dz2i + dx2i, C = dz2i dx2i, and the 3D operator's differences are
  * ta - tb = 1.5 (te - tv + ten - tnv), tb - tc = 1.5 (tv - tn + tev - ten),
@@ -190,7 +190,7 @@ __device__ __forceinline__ float noinit_f32(const Mesh<float> &c, float tv, floa
     const float tab = 1.5f * (temtv + (ten - tnv));
     const float tbc = 1.5f * (tvmtn + (tev - ten));
     const float tac = tab + tbc;
-    const float tb = tv + 0.5f * ((tnv - tn) + (tev - te)) - ten + tnve;
+    const float tb = fmaf((tnv - tn) + (tev - te), 0.5f, tv) - ten + tnve;
     const float t2 = (s7 * s7) * c.dsum_nine;
     const float t3 = fmaf(c.dz2dx2, tab * tab, fmaf(c.dz2dy2, tbc * tbc, c.dx2dy2 * (tac * tac)));
     const float t3c = fmaf(c.dsumi, rsqrt_(t2 - t3), fmaf(c.dsumi, fmaf(tab, c.dx2i, -tbc * c.dy2i), tb));
