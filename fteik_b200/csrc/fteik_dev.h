@@ -59,7 +59,7 @@ typedef struct {
     const int *done_base;          /* nwork */
     int ntask_sweep, nslab_total;
     int *done;                     /* nslab_total */
-    unsigned long long *tickets;   /* 2 */
+    unsigned long long *tickets;   /* 2: initialisation and pass launches */
     int *error;                    /* 1 */
     unsigned long long *resid;     /* nwork * max(npass, 1) */
     int *pass_slabs;               /* nwork * max(npass, 1) */
@@ -80,6 +80,13 @@ typedef struct {
     /* FP32 initialisation sweeps: the source pairs walked together (the
      * union of their boxes), or NULL for one source per thread */
     const int *init_pairs;
+    /* initialisation sweeps with one source per thread: tasks_init = one
+     * {work, -1} task per work item (the whole sweep of a box at most
+     * FK_SLAB_Y z positions deep, walked with the axes turned) followed by
+     * the slab tasks; done_t one counter per work item for those tasks */
+    const int *tasks_init;
+    int ntask_init_sweep;
+    int *done_t;                   /* nwork */
 } fk_slabs3d_t;
 
 #define FK_SLAB_Y 4

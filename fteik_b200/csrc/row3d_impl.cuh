@@ -328,6 +328,164 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
     return true;
 }
 
+/* Logical z positions of the box of initialisation sweep `sweep_no` of
+ * source q (solver3D.F90:493-565): the read-only layer loz - 1 and the
+ * updated layers loz .. nz - 1. */
+__device__ __forceinline__ int init_box_depth(const Src &q, int nz, int sweep_no)
+{
+    const int loz = (sweep_no <= 4) ? max(1, q.zsi - 1) : max(1, nz - q.zsi - 1);
+    return nz - loz + 1;
+}
+
+/* One initialisation sweep of one source over a box at most TY z positions
+ * deep (a source within two cells of the surface in the upward sweeps, of
+ * the bottom in the downward ones), walked with the axes turned: warp ty is
+ * the box's logical z layer loz - 1 + ty, lanes walk x as in slab_sweep,
+ * and the walk runs along y, so one task covers the whole box.  slab_sweep
+ * walks such a box with at least 32 z steps per column block for its 2 or 3
+ * layers; here a column block takes as many steps as the box has rows.  A
+ * node's seven upwind values arrive through the same channels in other
+ * roles -- its own previous step is the y-upwind node, the row above the
+ * z-upwind one, lane l-1 the x-upwind one -- and go to the stencil in their
+ * physical roles with the same slowness cells, so every node gets the bits
+ * slab_sweep gives it.  No other task reads the box while it runs: no
+ * progress counters, no waits. */
+template <typename R>
+__device__ __forceinline__ void slab_sweep_zrows(const fk_grid3d_t &g, R *tt, const R *__restrict__ slow,
+                                                 const Src &q, int sweep_no, R (*xr)[1][TY][32], R *ring,
+                                                 int zring)
+{
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const unsigned FULL = 0xffffffffu;
+    const int nz = g.nz, nx = g.nx, ny = g.ny, zp = g.zp, zcp = g.zcp;
+    const int s0 = sweep_no - 1;
+    const int sz = (s0 < 4) ? 1 : -1;
+    const int sx = (s0 % 2 == 0) ? 1 : -1;
+    const int sy = ((s0 / 2) % 2 == 0) ? 1 : -1;
+    /* solver3D.F90:493-565, flipped bounds clamped to the grid */
+    const int loz = (sz > 0) ? max(1, q.zsi - 1) : max(1, nz - q.zsi - 1);
+    const int lox = (sx > 0) ? max(1, q.xsi - 1) : max(1, nx - q.xsi - 1);
+    const int loy = (sy > 0) ? max(1, q.ysi - 1) : max(1, ny - q.ysi - 1);
+    Mesh<R> mesh;
+    fk3::make_mesh<R>(mesh, g.dz, g.dx, g.dy);
+    Mesh<double> mesh64;
+    fk3::make_mesh<double>(mesh64, g.dz, g.dx, g.dy);
+    const R HUGEV = (R)FK_HUGE;
+    const R eps_r = (R)q.eps_t;
+    const int Zr = nz - loz + 1;                     /* rows: logical z loz - 1 .. nz - 1 */
+    const bool row = ty < Zr;
+    const int iz = (sz > 0) ? loz - 1 + ty : nz - loz - ty;
+    const bool rowupd = row && ty >= 1;              /* logical z >= loz */
+    const int Y = ny - loy + 1;                      /* walk positions: logical y loy - 1 .. ny - 1 */
+    const int Yp = Y > 32 ? Y : 32;
+    const int K = (nx + 31) / 32;
+    const int k0 = (lox - 1) / 32;
+    const int T = (K - k0) * Yp + 31 + DL * (TY - 1);
+    /* slowness cells: z fixed by the row (U: the layer above, D: this one,
+     * clamped), x by the lane's column, y by the step: each step fetches its
+     * y-downwind layer, the previous step's is its y-upwind one */
+    const int czU = (sz > 0) ? iz - 1 : iz;
+    const int czD = min(max((sz > 0) ? iz : iz - 1, 0), nz - 2);
+
+    struct Item {
+        R told;
+        R uud, udd, dud, ddd;   /* y-downwind layer, s<z><x><y> with y = D */
+        int addr;
+    };
+    auto fetch = [&](int kk, int jj, Item &f) {
+        const int xl = 32 * kk + tx;
+        if (!(row && jj >= 0 && jj < Y && kk < K && xl < nx)) return;
+        const int x = (sx > 0) ? xl : nx - 1 - xl;
+        const int yl = loy - 1 + jj;
+        const int y = (sy > 0) ? yl : ny - 1 - yl;
+        f.addr = (y * nx + x) * zp + iz;
+        f.told = fk3tw::ldcg(tt + f.addr);
+        if (rowupd && xl >= lox) {
+            const int cxU = (sx > 0) ? x - 1 : x;
+            const int cxD = min(max((sx > 0) ? x : x - 1, 0), nx - 2);
+            const int rD = min(max((sy > 0) ? y : y - 1, 0), ny - 2) * (nx - 1);
+            f.uud = __ldg(slow + ((rD + cxU) * zcp + czU));
+            f.udd = __ldg(slow + ((rD + cxD) * zcp + czU));
+            f.dud = __ldg(slow + ((rD + cxU) * zcp + czD));
+            f.ddd = __ldg(slow + ((rD + cxD) * zcp + czD));
+        }
+    };
+
+    int kn = k0, jn = -tx - DL * ty;     /* item of the next step */
+    Item cur, nxt;
+    nxt.told = HUGEV;
+    nxt.uud = nxt.udd = nxt.dud = nxt.ddd = (R)0;
+    nxt.addr = 0;
+    fetch(kn, jn, nxt);
+    R yu_uu = 0, yu_ud = 0, yu_du = 0, yu_dd = 0;   /* y-upwind layer (previous step) */
+    /* previous step's: own result (y-upwind node), x-upwind value, z-upwind
+     * value, and x-upwind's z-upwind value */
+    R r_last = HUGEV, te_last = HUGEV, tv_last = HUGEV, tev_last = HUGEV;
+    R *ring_r = ring, *ring_tv = ring + zring;
+    for (int t = 0; t < T; ++t) {
+        const int pp = (t + NB - DL) % NB, cp = t % NB;   /* the row above's step t - DL */
+        const R sh_r = __shfl_up_sync(FULL, r_last, 1);
+        const R sh_tv = __shfl_up_sync(FULL, tv_last, 1);
+        const int k = kn, j = jn;
+        cur = nxt;
+        if (++jn == Yp) { jn = 0; ++kn; }
+        fetch(kn, jn, nxt);
+        const int xl = 32 * k + tx;
+        const bool valid = row && j >= 0 && j < Y && k < K && xl < nx;
+        const bool from_ring = k > k0 && j >= 0 && j < Yp;
+        const bool upd = valid && rowupd && xl >= lox && j >= 1;   /* logical y >= loy */
+        /* the seven cells in the names of slab_sweep: uuu = (zU, xU, yU) ... */
+        const R uuu = yu_uu, udu = yu_ud, duu = yu_du, ddu = yu_dd;
+        const R uud = cur.uud, udd = cur.udd, dud = cur.dud;
+        const R s4 = rmin(uuu, uud), s5 = rmin(uuu, udu), s6 = rmin(uuu, duu);
+        const R s1 = rmin(s4, rmin(udu, udd));
+        const R s2 = rmin(s4, rmin(duu, dud));
+        const R s3 = rmin(s5, rmin(duu, ddu));
+        const R s7 = uuu;
+        const R te = (tx == 0) ? (from_ring ? ring_r[j] : HUGEV) : sh_r;
+        R tv = HUGEV, tev = HUGEV, result = HUGEV;
+        if (valid) {
+            tv = (ty == 0) ? HUGEV : xr[pp][0][ty - 1][tx];
+            tev = (tx == 0) ? (from_ring ? ring_tv[j] : HUGEV) : sh_tv;
+            const R told = cur.told;
+            result = told;
+            if (upd) {
+                const R tn = r_last, ten = te_last, tnv = tv_last, tnve = tev_last;
+                const int x = (sx > 0) ? xl : nx - 1 - xl;
+                const int yl = loy - 1 + j;
+                const int y = (sy > 0) ? yl : ny - 1 - yl;
+                /* as in slab_sweep: the switch compares in the field's precision */
+                const bool lcart = rmin(rmin(tv, te), tn) > eps_r;
+                R r;
+                if (lcart && sizeof(R) == 4)
+                    r = fk3::noinit(mesh, tv, te, tn, tev, ten, tnv, tnve, s1, s2, s3, s4, s5, s6, s7, told);
+                else if (lcart || sizeof(R) == 8)
+                    r = fk3::init_node<R>(q, mesh, lcart, tv, te, tn, tev, ten, tnv, tnve, told, s1, s2, s3, s4, s5,
+                                          s6, s7, iz + 1, x + 1, y + 1, sz, sx, sy);
+                else
+                    r = (R)fk3::init_node<double>(q, mesh64, lcart, (double)tv, (double)te, (double)tn, (double)tev,
+                                                  (double)ten, (double)tnv, (double)tnve, (double)told, (double)s1,
+                                                  (double)s2, (double)s3, (double)s4, (double)s5, (double)s6,
+                                                  (double)s7, iz + 1, x + 1, y + 1, sz, sx, sy);
+                if (r != told) tt[cur.addr] = r;
+                result = r;
+            }
+        }
+        if (tx == 31 && j >= 0 && j < Yp) {
+            ring_r[j] = result;
+            ring_tv[j] = tv;
+        }
+        xr[cp][0][ty][tx] = result;
+        r_last = result;
+        te_last = te;
+        tv_last = tv;
+        tev_last = tev;
+        if (valid && rowupd && xl >= lox) { yu_uu = cur.uud; yu_ud = cur.udd; yu_du = cur.dud; yu_dd = cur.ddd; }
+        if ((t + 1) % DL == 0) __syncthreads();   /* the window's row values become visible */
+        else __syncwarp();                        /* lane 31 -> lane 0 ring */
+    }
+}
+
 /* The Gauss-Seidel stencil of the FP32 pass steps for the S sources of a
  * thread (they share the slowness): with PACKED the two sources in packed
  * float2 instructions (noinit_v<float2>; 5 % faster in the staged step,
@@ -925,7 +1083,11 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
         const int sweep_no = s % 8 + 1;
         const int s0 = sweep_no - 1;
         const int sy = ((s0 / 2) % 2 == 0) ? 1 : -1;
-        const int Pp = (sy > 0) ? tk.y : nslab - 1 - tk.y;   /* physical slab */
+        /* initialisation, one source per thread (P.done_t set): task {w, -1}
+         * walks the sweep of a box at most TY z positions deep with the axes
+         * turned, and then the slab tasks of that sweep have nothing to do */
+        const bool turned_task = INIT && S == 1 && P.done_t != nullptr && tk.y < 0;
+        const int Pp = turned_task ? 0 : (sy > 0) ? tk.y : nslab - 1 - tk.y;   /* physical slab */
         int *prog[S];
         R *ttp[S];
 #pragma unroll
@@ -933,20 +1095,35 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
             prog[i] = wi[i] >= 0 ? P.done + P.done_base[wi[i]] : nullptr;
             ttp[i] = wi[i] >= 0 ? reinterpret_cast<R *>(i == 0 ? w0.tt : P.work[wi[i]].tt) : nullptr;
         }
-        /* slabs P-1, P, P+1 of every source done with the previous sweep */
-        if (tid < 3 * S) {
-            const int i = tid / 3, pq = Pp + tid % 3 - 1;
-            if (prog[i] && pq >= 0 && pq < nslab) {
+        /* done with the previous sweep: slabs P-1, P, P+1 of every source,
+         * and the turned-axes task of the source; a turned-axes task waits for
+         * every slab of its source and its own previous task (all of them
+         * hold smaller tickets, so the waits cannot cycle) */
+        {
+            auto wait_done = [&](const int *c) {   /* bounded acquire wait for (sweep s - 1) done */
                 long long it = 0;
                 unsigned ns = 64;
-                while (fk3tw::ld_acquire(prog[i] + pq) < (s << SHIFT)) {
+                while (fk3tw::ld_acquire(c) < (s << SHIFT)) {
                     if (++it > P.spin_limit) {
                         atomicCAS(P.error, 0, 2000 + tid);
                         s_flag[1] = 0;
-                        break;
+                        return false;
                     }
                     poll_backoff(ns);
                 }
+                return true;
+            };
+            if (!turned_task) {
+                if (tid < 3 * S) {
+                    const int i = tid / 3, pq = Pp + tid % 3 - 1;
+                    if (prog[i] && pq >= 0 && pq < nslab) wait_done(prog[i] + pq);
+                } else if (tid == 3 * S && INIT && S == 1 && P.done_t != nullptr) {
+                    wait_done(P.done_t + wi[0]);
+                }
+            } else {
+                /* every slab q of the source (q = tid, tid + NT, ...), and q = nslab its previous turned task */
+                for (int q = tid; q <= nslab; q += NT)
+                    if (!wait_done(q < nslab ? prog[0] + q : P.done_t + wi[0])) break;
             }
         }
         __syncthreads();
@@ -963,6 +1140,7 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
         Src qs[S];
 #pragma unroll
         for (int i = 0; i < S; ++i) fk3tw::tw_setup_src(qs[i], i == 0 ? w0 : P.work[wi[i] >= 0 ? wi[i] : wi[0]], g, P.eps);
+        const bool thin = INIT && S == 1 && P.done_t != nullptr && init_box_depth(qs[0], g.nz, sweep_no) <= TY;
         if (INIT) {
             /* slabs wholly before every source's rows of this sweep keep their values */
             const int ylast = (sy > 0) ? min(g.ny, TY * (Pp + 1)) - 1 : TY * Pp;
@@ -973,11 +1151,18 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
                 const int loy = (sy > 0) ? max(1, qs[i].ysi - 1) : max(1, g.ny - qs[i].ysi - 1);
                 if (wi[i] >= 0 && yl_max >= loy) skip = false;
             }
+            /* a thin box is the turned-axes task's alone */
+            if (turned_task) skip = !thin;
+            else if (thin) skip = true;
         }
         double dmax[S];
 #pragma unroll
         for (int i = 0; i < S; ++i) dmax[i] = 0.0;
-        if (!skip) {
+        if (!skip && turned_task) {
+            if constexpr (INIT && S == 1)
+                slab_sweep_zrows<R>(g, ttp[0], reinterpret_cast<const R *>(g.slow), qs[0], sweep_no,
+                                    reinterpret_cast<R (*)[1][TY][32]>(xr), ring, zring);
+        } else if (!skip) {
             bool ok;
             if constexpr (!INIT && sizeof(R) == 4 && STG)
                 ok = slab_pass_f32_staged<RESID, S, CHP>(P, g, ttp, s, sweep_no, Pp, nslab, prog, xr, ring, zring,
@@ -1022,7 +1207,7 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(f
                         }
                     }
                 }
-                fk3tw::st_release(prog[i] + Pp, (s + 1) << SHIFT);
+                fk3tw::st_release(turned_task ? P.done_t + wi[i] : prog[i] + Pp, (s + 1) << SHIFT);
             }
         }
     }
@@ -1080,7 +1265,8 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
      * step's descending sweeps, at least 32, a multiple of 4 */
     const int zring = ((pl->max_nz + 3 > 32 ? pl->max_nz + 3 : 32) + 3) / 4 * 4;
     /* counters hold (sweep << SHIFT) | steps: steps of a slab and sweep numbers must fit */
-    const long long steps = (long long)((pl->max_nx + 31) / 32) * zring + 31 + (DL > DLP ? DL : DLP) * TY;
+    const int zr = zring > pl->max_ny ? zring : pl->max_ny;   /* the turned-axes walk runs along y */
+    const long long steps = (long long)((pl->max_nx + 31) / 32) * (zr + 3) + 31 + (DL > DLP ? DL : DLP) * TY;
     if (steps >= (1LL << SHIFT) || 8 + 8 * (long long)npr + 1 >= (1LL << (31 - SHIFT)))
         return (int)cudaErrorInvalidValue;
     cudaError_t e = cudaSuccess;
@@ -1090,6 +1276,7 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
     if (!e) e = cudaMemsetAsync(pl->resid, 0, sizeof(unsigned long long) * (size_t)nwork * npr, st);
     if (!e) e = cudaMemsetAsync(pl->pass_slabs, 0, sizeof(int) * (size_t)nwork * npr, st);
     if (!e) e = cudaMemsetAsync(pl->conv_pass, 0x3f, sizeof(int) * (size_t)nwork, st);
+    if (!e) e = cudaMemsetAsync(pl->done_t, 0, sizeof(int) * (size_t)nwork, st);
     if (e) return (int)e;
     fk3tw::field_init_kernel<R><<<dim3(64, nwork), 256, 0, st>>>(grids, work, eps);
     fk3tw::corners_kernel<R><<<(nwork * 8 + 127) / 128, 128, 0, st>>>(grids, work, nwork, eps);
@@ -1100,6 +1287,7 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
     P.done_base = pl->done_base;
     P.ntask_sweep = pl->ntask_sweep;
     P.done = pl->done;
+    P.done_t = nullptr;
     P.error = pl->error;
     P.resid = pl->resid;
     P.pass_slabs = pl->pass_slabs;
@@ -1113,6 +1301,14 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
     P.s_end = 8;
     P.ticket = pl->tickets;
     if (fk3tw::g_slab_events) cudaEventRecord(fk3tw::g_slab_events[0], st);
+    /* initialisation with one source per thread: the turned-axes tasks ahead
+     * of the slab tasks; their rings hold a y walk, so they are sized for
+     * the deepest or widest grid */
+    fk3tw::Params Pt = P;
+    Pt.tasks = reinterpret_cast<const int2 *>(pl->tasks_init);
+    Pt.ntask_sweep = pl->ntask_init_sweep;
+    Pt.done_t = pl->done_t;
+    const int zring_t = ((zring > pl->max_ny ? zring : pl->max_ny) + 3) / 4 * 4;
     int rc;
     if constexpr (sizeof(R) == 4) {
         if (pl->init_pairs) { /* two sources per thread over the union of their boxes */
@@ -1121,11 +1317,11 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
             Pi.ntask_sweep = pl->ntask2_sweep;
             rc = launch_init_f32(Pi, zring, st, pl->init_blocks_per_sm, pl->init_pairs);
         } else {
-            rc = launch_init_f32(P, zring, st, pl->init_blocks_per_sm, nullptr);
+            rc = launch_init_f32(Pt, zring_t, st, pl->init_blocks_per_sm, nullptr);
         }
     }
     else
-        rc = launch_slab_kernel<R, true, false, 1>(P, nullptr, zring, st, 0, pl->init_blocks_per_sm);
+        rc = launch_slab_kernel<R, true, false, 1>(Pt, nullptr, zring_t, st, 0, pl->init_blocks_per_sm);
     if (rc) return rc;
     if (fk3tw::g_slab_events) cudaEventRecord(fk3tw::g_slab_events[1], st);
     if (npass > 0) {

@@ -19,6 +19,7 @@ struct Params {
     int ntask_sweep;
     int s_begin, s_end;         /* global sweep numbers: 0..7 init, 8.. Gauss-Seidel */
     int *done;                  /* per slab: (sweep << 20) | steps done */
+    int *done_t;                /* per work item, turned-axes initialisation tasks (or NULL) */
     unsigned long long *ticket;
     int *error;                 /* 0 ok; else the first failure */
     unsigned long long *resid;  /* [nwork][npass]: FP64 max |dt| bits */

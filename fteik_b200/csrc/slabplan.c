@@ -69,6 +69,15 @@ int fk_slabplan_build(fk_slabplan_t *pl, int nwork, const int *nx, const int *ny
                 tasks2[2 * k + 1] = j;
                 k++;
             }
+    /* initialisation sweeps, one source per thread: a turned-axes task per
+     * work item ahead of the slab tasks of each sweep */
+    const long ntask_i = nslab + nwork;
+    int *tasks_i = (int *)malloc(sizeof(int) * 2 * (size_t)ntask_i);
+    for (int w = 0; w < nwork; w++) {
+        tasks_i[2 * w] = w;
+        tasks_i[2 * w + 1] = -1;
+    }
+    memcpy(tasks_i + 2 * (size_t)nwork, tasks, sizeof(int) * 2 * (size_t)nslab);
     const int np = npass > 0 ? npass : 1;
     size_t off_tasks = 0;
     size_t off_base = off_tasks + al(sizeof(int) * 2 * (size_t)nslab);
@@ -80,13 +89,17 @@ int fk_slabplan_build(fk_slabplan_t *pl, int nwork, const int *nx, const int *ny
     size_t off_cp = off_pt + al(sizeof(int) * (size_t)nwork * np);
     size_t off_pairs = off_cp + al(sizeof(int) * (size_t)nwork);
     size_t off_t2 = off_pairs + al(sizeof(int) * 2 * (size_t)npair);
-    size_t total = off_t2 + al(sizeof(int) * 2 * (size_t)ntask2);
+    size_t off_ti = off_t2 + al(sizeof(int) * 2 * (size_t)ntask2);
+    size_t off_dt = off_ti + al(sizeof(int) * 2 * (size_t)ntask_i);
+    size_t total = off_dt + al(sizeof(int) * (size_t)nwork);
     char *m = (char *)fk_dalloc(total, who);
     int e = m ? 0 : 1;
     if (!e) e = fk_check((int)fk_h2d(m + off_tasks, tasks, sizeof(int) * 2 * (size_t)nslab), who);
     if (!e) e = fk_check((int)fk_h2d(m + off_base, base, sizeof(int) * (size_t)nwork), who);
     if (!e) e = fk_check((int)fk_h2d(m + off_pairs, pairs, sizeof(int) * 2 * (size_t)npair), who);
     if (!e) e = fk_check((int)fk_h2d(m + off_t2, tasks2, sizeof(int) * 2 * (size_t)ntask2), who);
+    if (!e) e = fk_check((int)fk_h2d(m + off_ti, tasks_i, sizeof(int) * 2 * (size_t)ntask_i), who);
+    free(tasks_i);
     free(tasks);
     free(tasks2);
     free(pairs);
@@ -114,5 +127,8 @@ int fk_slabplan_build(fk_slabplan_t *pl, int nwork, const int *nx, const int *ny
     pl->dev.pairs = pairing ? pl->pairs_all : NULL;
     pl->dev.tasks2 = (const int *)(m + off_t2);
     pl->dev.ntask2_sweep = (int)ntask2;
+    pl->dev.tasks_init = (const int *)(m + off_ti);
+    pl->dev.ntask_init_sweep = (int)ntask_i;
+    pl->dev.done_t = (int *)(m + off_dt);
     return 0;
 }
