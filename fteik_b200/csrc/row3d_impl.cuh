@@ -868,8 +868,10 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
                 const int ox = (lk == kxl) ? 0 : offX;
                 cpa16(d + 2 * SG_ARR_BYTES, sl + is);
                 cpa16(d + 3 * SG_ARR_BYTES, sl + (is + offY));
-                cpa16(d + 4 * SG_ARR_BYTES, sl + (is + ox));
-                cpa16(d + 5 * SG_ARR_BYTES, sl + (is + ox + offY));
+                if (tx == 31) {   /* the other lanes take their x-downwind cells from lane l + 1 */
+                    cpa16(d + 4 * SG_ARR_BYTES, sl + (is + ox));
+                    cpa16(d + 5 * SG_ARR_BYTES, sl + (is + ox + offY));
+                }
             }
         }
         cpa_commit();
@@ -958,6 +960,12 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
             const Item cur = nxt;
             fetch(nxt, nk, nzq, t0 + u + 1 - c);
             if (++nzq == Zp) { nzq = 0; ++nk; }
+            /* x-downwind cells: lane l + 1's x-upwind ones, its next item being
+             * this lane's current one; lane 31 stages its own, and the last
+             * column (zero x offset) repeats its x-upwind cells */
+            const float dn_uu = __shfl_down_sync(FULL, nxt.duu, 1), dn_ud = __shfl_down_sync(FULL, nxt.dud, 1);
+            const float c_ddu = (tx == 31) ? cur.ddu : (cur.k == kxl) ? cur.duu : dn_uu;
+            const float c_ddd = (tx == 31) ? cur.ddd : (cur.k == kxl) ? cur.dud : dn_ud;
             const bool valid = (unsigned)(cur.zq - zoff) < (unsigned)nz && cur.k < kl;
             const bool upd = valid && cur.zq > zoff && cur.k >= kmin;
             const bool from_ring = tx == 0 && cur.k > 0;   /* then 0 <= zq < Zp */
@@ -976,7 +984,7 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
             const float s4 = fminf(zu_uu, zu_ud), s5 = fminf(zu_uu, zu_du), s6 = fminf(zu_uu, cur.duu);
             const float s1 = fminf(s4, fminf(zu_du, zu_dd));
             const float s2 = fminf(s4, fminf(cur.duu, cur.dud));
-            const float s3 = fminf(s5, fminf(cur.duu, cur.ddu));
+            const float s3 = fminf(s5, fminf(cur.duu, c_ddu));
             const float s7 = zu_uu;
             float res[S], tnv_[S], te[S], ten[S];
 #pragma unroll
@@ -1017,7 +1025,7 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
                 r_last[i] = res[i];
                 tn_last[i] = tnv_[i];
             }
-            zu_uu = cur.duu; zu_ud = cur.dud; zu_du = cur.ddu; zu_dd = cur.ddd;
+            zu_uu = cur.duu; zu_ud = cur.dud; zu_du = c_ddu; zu_dd = c_ddd;
             if (u < DLP - 1) __syncwarp();
         }
         /* (row-pair named barriers instead of the block barrier measured 2 %
