@@ -182,6 +182,8 @@ _SIGS = {
     "fteik_b200_mlp_train": [c_int, _PF, _PF, c_int, c_int, c_double, _PD, _PI],
     "fteik_b200_mlp_setTensorProducts": [c_int, _PI],
     "fteik_b200_mlp_getTensorProducts": [_PI],
+    "fteik_b200_mlp_setTrainGraph": [c_int],
+    "fteik_b200_mlp_getTrainGraph": [_PI],
     "fteik_b200_locate_l2_noalloc": [c_int, c_int, c_int, ctypes.c_void_p, c_int, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, _PI],
@@ -278,6 +280,15 @@ def set_mlp_tensor_products(products):
     ierr = c_int(1)
     lib().fteik_b200_mlp_setTensorProducts(int(products), byref(ierr))
     _check(ierr, "fteik_b200_mlp_setTensorProducts")
+    return old.value
+
+
+def set_mlp_train_graph(on):
+    """Captured (1) or eager (0) training steps of trainSurrogate; returns
+    the previous value."""
+    old = c_int()
+    lib().fteik_b200_mlp_getTrainGraph(byref(old))
+    lib().fteik_b200_mlp_setTrainGraph(int(on))
     return old.value
 
 

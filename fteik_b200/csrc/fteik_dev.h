@@ -249,17 +249,22 @@ int fk_locate_block_tables(int nz, int nx, int ny, int bz, int bx, int by, int n
                            const float *tables, float *out, cudaStream_t s);
 
 /* ---- surrogate network (mlp.c / mlp.cu) ----------------------------------- */
-typedef int (*fk_batch_fn)(void *ctx, long long step, int B, float *x, float *y, cudaStream_t s);
+/* A training batch for step `step`, or, when step_dev is not NULL, for the
+ * step number the device holds there (a batch function that can read it
+ * lets the trainer capture one step in a CUDA graph and replay it). */
+typedef int (*fk_batch_fn)(void *ctx, long long step, const long long *step_dev, int B, float *x, float *y,
+                           cudaStream_t s);
 int fk_mlp_ready(void);
 size_t fk_mlp_flops_per_row(void);
-int fk_mlp_train_device(fk_batch_fn next_batch, void *ctx, long long steps, int B, double lr,
+int fk_mlp_train_device(fk_batch_fn next_batch, void *ctx, int capturable, long long steps, int B, double lr,
                         double *last_loss);
 int fk_mlp_forward_device(long long n, const float *x, float *tau, cudaStream_t s);
 /* Training batch from tables [ntf][ldgrd] on a z-fastest grid and station
  * positions sta [ntf][3] (z, x, y): inputs x [B][6], targets tau [B]. */
 int fk_mlp_sample(int nz, int nx, int ny, double dz, double dx, double dy, int ntf, int ldgrd,
                   double vref, const float *tables, const float *sta, unsigned long long seed,
-                  long long nsamp, long long step, int B, float *x, float *y, cudaStream_t s);
+                  long long nsamp, long long step, const long long *step_dev, int B, float *x, float *y,
+                  cudaStream_t s);
 /* Rows r0 .. r0+nrow-1 of the coarse lattice (row = table * ncoarse + node,
  * node = the centre of its fine block bz x bx x by, clipped to the grid):
  * network inputs and distance / v_ref. */

@@ -615,11 +615,12 @@ typedef struct {
     long long nsamp;
 } table_batch_t;
 
-static int table_batch(void *ctx, long long step, int B, float *x, float *y, cudaStream_t s)
+static int table_batch(void *ctx, long long step, const long long *step_dev, int B, float *x, float *y,
+                       cudaStream_t s)
 {
     table_batch_t *c = (table_batch_t *)ctx;
     return fk_mlp_sample(SP.nz, SP.nx, SP.ny, SP.dz, SP.dx, SP.dy, SL.ntf, SL.ldgrd, SP.vref, SL.tables,
-                         SP.sta_dev, c->seed, c->nsamp, step, B, x, y, s);
+                         SP.sta_dev, c->seed, c->nsamp, step, step_dev, B, x, y, s);
 }
 
 void fteik_b200_locate_trainSurrogate(long long nsamples, int steps, int batch, double lr, double vref,
@@ -642,7 +643,7 @@ void fteik_b200_locate_trainSurrogate(long long nsamples, int steps, int batch, 
     table_batch_t c;
     c.seed = seed;
     c.nsamp = nsamples;
-    if (fk_mlp_train_device(table_batch, &c, steps, batch, lr, loss)) return;
+    if (fk_mlp_train_device(table_batch, &c, 1, steps, batch, lr, loss)) return;
     SP.ready = false;
     *ierr = 0;
 }

@@ -16,11 +16,14 @@
 #include <string.h>
 
 int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta, const float *B, int ldb,
-                int tb, float *C, int ldc, const float *bias, int accumulate, cudaStream_t s);
+                int tb, float *C, int ldc, const float *bias, int accumulate, float *C2, int act, cudaStream_t s);
 int fk_mlp_silu(size_t n, const float *z, float *a, cudaStream_t s);
 int fk_mlp_silu_bwd(size_t n, const float *z, const float *da, float *dz, cudaStream_t s);
 int fk_mlp_colsum(int M, int N, const float *dz, float *db, cudaStream_t s);
 int fk_mlp_mse(int n, const float *pred, const float *y, float *dpred, double *loss, cudaStream_t s);
+int fk_mlp_adam_sched(size_t n, float *w, const float *g, float *m, float *v, const float *sched,
+                      const long long *tdev, float b1, float b2, float eps, cudaStream_t s);
+int fk_mlp_step_inc(long long *tdev, cudaStream_t s);
 int fk_mlp_adam(size_t n, float *w, const float *g, float *m, float *v, float lr, float b1,
                 float b2, float eps, float c1, float c2, cudaStream_t s);
 void fk_mlp_set_tensor(int products);
@@ -194,17 +197,24 @@ static int ensure_batch(int B)
 }
 
 /* Forward pass of B rows already in NN.x[0]; the output lands in
- * NN.x[nlayer] (B values). */
-static int forward(int B, cudaStream_t s)
+ * NN.x[nlayer] (B values).  The SiLU is applied in the GEMM's epilogue;
+ * training (keep_z) also keeps the pre-activations NN.z for the backward
+ * pass. */
+static int forward(int B, bool keep_z, cudaStream_t s)
 {
     int e = 0;
     for (int l = 0; l < NN.nlayer && !e; l++) {
         const int in = NN.din[l], out = NN.dout[l];
         const bool last = l == NN.nlayer - 1;
-        float *dst = last ? NN.x[l + 1] : NN.z[l];
-        e = fk_mlp_gemm(B, out, in, NN.x[l], in, 0, NN.w + NN.woff[l], in, 1, dst, out,
-                        NN.w + NN.boff[l], 0, s);
-        if (!e && !last) e = fk_mlp_silu((size_t)B * out, NN.z[l], NN.x[l + 1], s);
+        if (last)
+            e = fk_mlp_gemm(B, out, in, NN.x[l], in, 0, NN.w + NN.woff[l], in, 1, NN.x[l + 1], out,
+                            NN.w + NN.boff[l], 0, NULL, 0, s);
+        else if (keep_z)
+            e = fk_mlp_gemm(B, out, in, NN.x[l], in, 0, NN.w + NN.woff[l], in, 1, NN.z[l], out,
+                            NN.w + NN.boff[l], 0, NN.x[l + 1], 1, s);
+        else
+            e = fk_mlp_gemm(B, out, in, NN.x[l], in, 0, NN.w + NN.woff[l], in, 1, NN.x[l + 1], out,
+                            NN.w + NN.boff[l], 0, NULL, 2, s);
     }
     return e;
 }
@@ -213,17 +223,18 @@ static int forward(int B, cudaStream_t s)
 static int forward_backward(int B, const float *y, cudaStream_t s)
 {
     int e = cudaMemsetAsync(NN.loss_dev, 0, sizeof(double), s);
-    if (!e) e = forward(B, s);
+    if (!e) e = forward(B, true, s);
     const int L = NN.nlayer;
     /* d loss / d output */
     if (!e) e = fk_mlp_mse(B, NN.x[L], y, NN.dz, NN.loss_dev, s);
     for (int l = L - 1; l >= 0 && !e; l--) {
         const int in = NN.din[l], out = NN.dout[l];
         /* NN.dz holds d loss / d z_l  [B][out] */
-        e = fk_mlp_gemm(out, in, B, NN.dz, out, 1, NN.x[l], in, 0, NN.g + NN.woff[l], in, NULL, 0, s);
+        e = fk_mlp_gemm(out, in, B, NN.dz, out, 1, NN.x[l], in, 0, NN.g + NN.woff[l], in, NULL, 0, NULL, 0, s);
         if (!e) e = fk_mlp_colsum(B, out, NN.dz, NN.g + NN.boff[l], s);
         if (!e && l > 0) {
-            e = fk_mlp_gemm(B, in, out, NN.dz, out, 0, NN.w + NN.woff[l], in, 0, NN.dx, in, NULL, 0, s);
+            e = fk_mlp_gemm(B, in, out, NN.dz, out, 0, NN.w + NN.woff[l], in, 0, NN.dx, in, NULL, 0, NULL, 0,
+                            s);
             if (!e) e = fk_mlp_silu_bwd((size_t)B * in, NN.z[l - 1], NN.dx, NN.dtmp, s);
             if (!e) { float *t = NN.dz; NN.dz = NN.dtmp; NN.dtmp = t; }
         }
@@ -243,7 +254,7 @@ void fteik_b200_mlp_forward(int n, const float x[], float tau[], int *ierr)
         if (ensure_batch(B)) return;
         int e = (int)cudaMemcpyAsync(NN.x[0], x + (size_t)r0 * MLP_IN, sizeof(float) * (size_t)B * MLP_IN,
                                      cudaMemcpyHostToDevice, s);
-        if (!e) e = forward(B, s);
+        if (!e) e = forward(B, false, s);
         if (!e) e = (int)cudaMemcpyAsync(tau + r0, NN.x[NN.nlayer], sizeof(float) * (size_t)B,
                                          cudaMemcpyDeviceToHost, s);
         if (!e) e = (int)cudaStreamSynchronize(s);
@@ -274,9 +285,85 @@ void fteik_b200_mlp_gradient(int n, const float x[], const float y[], double *lo
 }
 
 /* Adam steps over batches produced by next_batch (device x / y).  The
- * learning rate decays by a cosine from lr to lr / 100. */
+ * learning rate decays by a cosine from lr to lr / 100.
+ *
+ * With a capturable batch function one training step (batch, forward,
+ * backward, Adam, step counter) is captured in a CUDA graph after one eager
+ * step and replayed: the step number, learning rate and bias corrections
+ * come from device memory (the schedule computed on the host as the eager
+ * loop does), so the replayed steps are the eager loop's, bit for bit, at a
+ * graph launch per step instead of ~40 kernel launches.  The last 20 steps
+ * read the loss back. */
+static int adam_constants(long long t_adam, long long t, long long steps, double lr, float *lrt, float *c1,
+                          float *c2)
+{
+    const float b1 = 0.9f, b2 = 0.999f;
+    const double frac = (double)t / (double)steps;
+    *lrt = (float)(lr * (0.01 + 0.99 * 0.5 * (1.0 + cos(3.141592653589793 * frac))));
+    *c1 = (float)(1.0 - pow(b1, (double)t_adam));
+    *c2 = (float)(1.0 - pow(b2, (double)t_adam));
+    return 0;
+}
 
-int fk_mlp_train_device(fk_batch_fn next_batch, void *ctx, long long steps, int B, double lr,
+static int train_step_dev(fk_batch_fn next_batch, void *ctx, int B, float *ydev, const float *sched,
+                          long long *tdev, cudaStream_t s)
+{
+    int e = next_batch(ctx, 0, tdev, B, NN.x[0], ydev, s);
+    if (!e) e = forward_backward(B, ydev, s);
+    if (!e) e = fk_mlp_adam_sched(NN.nparam, NN.w, NN.g, NN.m, NN.v, sched, tdev, 0.9f, 0.999f, 1e-8f, s);
+    if (!e) e = fk_mlp_step_inc(tdev, s);
+    return e;
+}
+
+static int train_graph(fk_batch_fn next_batch, void *ctx, long long steps, int B, double lr, float *ydev,
+                       double *lsum, long long *lcount)
+{
+    cudaStream_t s = fk_stream();
+    float *sched_h = (float *)malloc(sizeof(float) * 3 * (size_t)steps);
+    float *sched = (float *)fk_dalloc(sizeof(float) * 3 * (size_t)steps, "mlp");
+    long long *tdev = (long long *)fk_dalloc(sizeof(long long), "mlp");
+    int e = (sched_h && sched && tdev) ? 0 : 1;
+    for (long long t = 0; t < steps && !e; t++)
+        adam_constants(NN.adam_t + 1 + t, t, steps, lr, sched_h + 3 * t, sched_h + 3 * t + 1, sched_h + 3 * t + 2);
+    if (!e) e = (int)fk_h2d(sched, sched_h, sizeof(float) * 3 * (size_t)steps);
+    if (!e) e = (int)cudaMemsetAsync(tdev, 0, sizeof(long long), s);
+    /* step 0 eagerly: every buffer a step uses exists before the capture */
+    if (!e) e = train_step_dev(next_batch, ctx, B, ydev, sched, tdev, s);
+    cudaGraph_t graph = NULL;
+    cudaGraphExec_t exec = NULL;
+    if (!e) e = (int)cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (!e) {
+        const int le = train_step_dev(next_batch, ctx, B, ydev, sched, tdev, s);
+        e = (int)cudaStreamEndCapture(s, &graph);
+        if (!e) e = le;
+    }
+    if (!e) e = (int)cudaGraphInstantiate(&exec, graph, 0);
+    for (long long t = 1; t < steps && !e; t++) {
+        e = (int)cudaGraphLaunch(exec, s);
+        if (!e && t >= steps - 20) {
+            double l = 0.0;
+            e = (int)cudaMemcpyAsync(&l, NN.loss_dev, sizeof(double), cudaMemcpyDeviceToHost, s);
+            if (!e) e = (int)cudaStreamSynchronize(s);
+            *lsum += l;
+            (*lcount)++;
+        }
+    }
+    if (!e) e = (int)cudaStreamSynchronize(s);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    NN.adam_t += steps;
+    fk_dfree(tdev);
+    fk_dfree(sched);
+    free(sched_h);
+    return e;
+}
+
+static int g_train_graph = 1;
+
+void fteik_b200_mlp_setTrainGraph(int on) { g_train_graph = on != 0; }
+void fteik_b200_mlp_getTrainGraph(int *on) { *on = g_train_graph; }
+
+int fk_mlp_train_device(fk_batch_fn next_batch, void *ctx, int capturable, long long steps, int B, double lr,
                         double *last_loss)
 {
     if (!NN.init || steps < 1 || B < 1) return 1;
@@ -288,20 +375,23 @@ int fk_mlp_train_device(fk_batch_fn next_batch, void *ctx, long long steps, int 
     int e = 0;
     double lsum = 0.0;
     long long lcount = 0;
-    for (long long t = 0; t < steps && !e; t++) {
-        e = next_batch(ctx, t, B, NN.x[0], ydev, s);
-        if (!e) e = forward_backward(B, ydev, s);
-        NN.adam_t++;
-        const double frac = (double)t / (double)steps;
-        const float lrt = (float)(lr * (0.01 + 0.99 * 0.5 * (1.0 + cos(3.141592653589793 * frac))));
-        const float c1 = (float)(1.0 - pow(b1, (double)NN.adam_t)), c2 = (float)(1.0 - pow(b2, (double)NN.adam_t));
-        if (!e) e = fk_mlp_adam(NN.nparam, NN.w, NN.g, NN.m, NN.v, lrt, b1, b2, eps, c1, c2, s);
-        if (!e && t >= steps - 20) {
-            double l = 0.0;
-            e = (int)cudaMemcpyAsync(&l, NN.loss_dev, sizeof(double), cudaMemcpyDeviceToHost, s);
-            if (!e) e = (int)cudaStreamSynchronize(s);
-            lsum += l;
-            lcount++;
+    if (capturable && g_train_graph && steps > 21) {
+        e = train_graph(next_batch, ctx, steps, B, lr, ydev, &lsum, &lcount);
+    } else {
+        for (long long t = 0; t < steps && !e; t++) {
+            e = next_batch(ctx, t, NULL, B, NN.x[0], ydev, s);
+            if (!e) e = forward_backward(B, ydev, s);
+            NN.adam_t++;
+            float lrt, c1, c2;
+            adam_constants(NN.adam_t, t, steps, lr, &lrt, &c1, &c2);
+            if (!e) e = fk_mlp_adam(NN.nparam, NN.w, NN.g, NN.m, NN.v, lrt, b1, b2, eps, c1, c2, s);
+            if (!e && t >= steps - 20) {
+                double l = 0.0;
+                e = (int)cudaMemcpyAsync(&l, NN.loss_dev, sizeof(double), cudaMemcpyDeviceToHost, s);
+                if (!e) e = (int)cudaStreamSynchronize(s);
+                lsum += l;
+                lcount++;
+            }
         }
     }
     fk_dfree(ydev);
@@ -315,8 +405,10 @@ typedef struct {
     unsigned long long seed;
 } host_data_t;
 
-static int host_batch(void *ctx, long long step, int B, float *x, float *y, cudaStream_t s)
+static int host_batch(void *ctx, long long step, const long long *step_dev, int B, float *x, float *y,
+                      cudaStream_t s)
 {
+    (void)step_dev;   /* not capturable: the windows are placed by the host */
     /* contiguous windows of a fixed permutation-free ring over the rows */
     host_data_t *d = (host_data_t *)ctx;
     long long start = (step * (long long)B) % d->n;
@@ -354,7 +446,7 @@ void fteik_b200_mlp_train(int n, const float x[], const float y[], int steps, in
     d.x = xd;
     d.y = yd;
     if (!fk_check(e, "fteik_b200_mlp_train"))
-        *ierr = fk_mlp_train_device(host_batch, &d, steps, batch, lr, loss);
+        *ierr = fk_mlp_train_device(host_batch, &d, 0, steps, batch, lr, loss);
     fk_dfree(xd);
     fk_dfree(yd);
 }
@@ -370,7 +462,7 @@ int fk_mlp_forward_device(long long n, const float *x, float *tau, cudaStream_t 
         if (ensure_batch(B)) return 1;
         e = (int)cudaMemcpyAsync(NN.x[0], x + (size_t)r0 * MLP_IN, sizeof(float) * (size_t)B * MLP_IN,
                                  cudaMemcpyDeviceToDevice, s);
-        if (!e) e = forward(B, s);
+        if (!e) e = forward(B, false, s);
         if (!e) e = (int)cudaMemcpyAsync(tau + r0, NN.x[NN.nlayer], sizeof(float) * (size_t)B,
                                          cudaMemcpyDeviceToDevice, s);
     }

@@ -97,7 +97,8 @@ __global__ void __launch_bounds__(NT) gemm_kernel(int M, int N, int K, const flo
 
 /* C[m][n] (+)= sum over the split slices in order + bias[n]. */
 __global__ void splitk_reduce_kernel(int M, int N, int split, const float *__restrict__ ws, float *__restrict__ C,
-                                     int ldc, const float *__restrict__ bias, int accumulate)
+                                     int ldc, const float *__restrict__ bias, int accumulate, float *__restrict__ C2,
+                                     int act)
 {
     const size_t n_el = (size_t)M * N;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n_el; e += (size_t)gridDim.x * blockDim.x) {
@@ -106,7 +107,11 @@ __global__ void splitk_reduce_kernel(int M, int N, int split, const float *__res
         for (int z = 0; z < split; ++z) v += ws[(size_t)z * n_el + e];
         if (bias) v += bias[n];
         float *c = C + (size_t)m * ldc + n;
-        *c = accumulate ? *c + v : v;
+        if (accumulate) v = *c + v;
+        /* act 1: C = z and C2 = silu(z); act 2: C = silu(z) (as silu_kernel) */
+        const float a = act ? v * (1.0f / (1.0f + __expf(-v))) : v;
+        *c = act == 2 ? a : v;
+        if (act == 1) C2[(size_t)m * ldc + n] = a;
     }
 }
 
@@ -116,6 +121,14 @@ __global__ void silu_kernel(size_t n, const float *__restrict__ z, float *__rest
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const float v = z[i];
+        a[i] = v * sigmoid(v);
+    }
+}
+
+__global__ void silu_inplace_kernel(size_t n, float *a)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float v = a[i];
         a[i] = v * sigmoid(v);
     }
 }
@@ -130,13 +143,35 @@ __global__ void silu_bwd_kernel(size_t n, const float *__restrict__ z, const flo
     }
 }
 
-/* db[n] = sum_m dz[m][n] (one thread per column, rows in order) */
-__global__ void colsum_kernel(int M, int N, const float *__restrict__ dz, float *__restrict__ db)
+/* db[n] = sum_m dz[m][n] in a fixed order: block (column group of 32, row
+ * chunk r) sums rows r CR .. r CR + CR - 1, warp w every 8th of them, the
+ * 8 warps' sums added in order into part[r][n]; colsum_final adds the
+ * chunks in order. */
+constexpr int CS_CR = 256;
+__global__ void colsum_kernel(int M, int N, const float *__restrict__ dz, float *__restrict__ part)
+{
+    __shared__ float red[8][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int n = blockIdx.x * 32 + lane;
+    const int m0 = blockIdx.y * CS_CR, m1 = min(M, m0 + CS_CR);
+    float s = 0.0f;
+    if (n < N)
+        for (int m = m0 + w; m < m1; m += 8) s += dz[(size_t)m * N + n];
+    red[w][lane] = s;
+    __syncthreads();
+    if (w == 0 && n < N) {
+        float t = red[0][lane];
+        for (int k = 1; k < 8; ++k) t += red[k][lane];
+        part[(size_t)blockIdx.y * N + n] = t;
+    }
+}
+
+__global__ void colsum_final_kernel(int N, int nchunk, const float *__restrict__ part, float *__restrict__ db)
 {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= N) return;
     float s = 0.0f;
-    for (int m = 0; m < M; ++m) s += dz[(size_t)m * N + n];
+    for (int r = 0; r < nchunk; ++r) s += part[(size_t)r * N + n];
     db[n] = s;
 }
 
@@ -176,6 +211,27 @@ __global__ void adam_kernel(size_t n, float *__restrict__ w, const float *__rest
     }
 }
 
+/* Adam with the step's learning rate and bias corrections read from the
+ * device (sched[3 t .. 3 t + 2] = lr_t, 1 - b1^t, 1 - b2^t, t = *tdev), so
+ * that a captured training step replays with the schedule moving on. */
+__global__ void adam_sched_kernel(size_t n, float *__restrict__ w, const float *__restrict__ g,
+                                  float *__restrict__ m, float *__restrict__ v, const float *__restrict__ sched,
+                                  const long long *__restrict__ tdev, float b1, float b2, float eps)
+{
+    const long long t = *tdev;
+    const float lr = sched[3 * t], c1 = sched[3 * t + 1], c2 = sched[3 * t + 2];
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+__global__ void step_inc_kernel(long long *tdev) { *tdev += 1; }
+
 /* counter-based hash (splitmix64 finaliser) */
 __device__ __forceinline__ uint64_t mix64(uint64_t x)
 {
@@ -209,11 +265,12 @@ __device__ __forceinline__ void norm_inputs(const Geom &G, float zg, float xg, f
  * normalised node and station positions, target tau = T v_ref / distance
  * (distance floored at half a cell). */
 __global__ void sample_kernel(Geom G, const float *__restrict__ tables, const float *__restrict__ sta,
-                              uint64_t seed, long long nsamp, long long t, int B, float *__restrict__ x,
-                              float *__restrict__ y)
+                              uint64_t seed, long long nsamp, long long t, const long long *__restrict__ tdev,
+                              int B, float *__restrict__ x, float *__restrict__ y)
 {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= B) return;
+    if (tdev) t = *tdev;   /* a captured step: the step number from the device */
     const long long ngrd = (long long)G.nz * G.nx * G.ny;
     const uint64_t j = mix64(seed ^ mix64((uint64_t)t * 0x100000001B3ull + (uint64_t)b)) % (uint64_t)nsamp;
     const uint64_t h = mix64(seed * 0x2545F4914F6CDD1Dull + j);
@@ -273,8 +330,8 @@ using namespace fkmlp;
 static int grid1d(size_t n) { size_t b = (n + 255) / 256; return (int)(b < 4096 ? (b ? b : 1) : 4096); }
 
 extern "C" int fk_mlp_gemm_tc(int prod, int M, int N, int K, const float *A, int lda, int ta, const float *B,
-                              int ldb, int tb, float *C, int ldc, const float *bias, int accumulate, int split,
-                              float *ws, int *error, cudaStream_t s);
+                              int ldb, int tb, float *C, int ldc, const float *bias, int accumulate, float *C2,
+                              int act, int split, float *ws, int *error, cudaStream_t s);
 
 /* 0: every GEMM on the CUDA cores in FP32; 1 or 3: GEMMs with N and K of at
  * least 64 (the hidden layers) on the tensor cores with that many BF16
@@ -313,7 +370,8 @@ static int workspace(size_t need, cudaStream_t s)
 }
 
 extern "C" int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta, const float *B, int ldb,
-                           int tb, float *C, int ldc, const float *bias, int accumulate, cudaStream_t s)
+                           int tb, float *C, int ldc, const float *bias, int accumulate, float *C2, int act,
+                           cudaStream_t s)
 {
     if (M <= 0 || N <= 0) return 0;
     if (g_tensor && N >= 64 && N <= 256 && K >= 64 && M >= 64) {
@@ -330,10 +388,11 @@ extern "C" int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta,
             const int e = workspace((size_t)split * M * N, s);
             if (e) return e;
         }
-        int e = fk_mlp_gemm_tc(g_tensor, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate, split, g_ws,
-                               g_tc_error, s);
+        int e = fk_mlp_gemm_tc(g_tensor, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate, C2, act, split,
+                               g_ws, g_tc_error, s);
         if (e || split == 1) return e;
-        splitk_reduce_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>(M, N, split, g_ws, C, ldc, bias, accumulate);
+        splitk_reduce_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>(M, N, split, g_ws, C, ldc, bias, accumulate, C2,
+                                                                   act);
         return (int)cudaGetLastError();
     }
     const int tiles = ((N + TN - 1) / TN) * ((M + TM - 1) / TM);
@@ -343,6 +402,10 @@ extern "C" int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta,
     dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM, split);
     if (split == 1) {
         gemm_kernel<<<grid, NT, 0, s>>>(M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate);
+        if (act == 1 && ldc == N)   /* the activation as a second pass over the contiguous C */
+            silu_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>((size_t)M * N, C, C2);
+        else if (act == 2 && ldc == N)
+            silu_inplace_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>((size_t)M * N, C);
         return (int)cudaGetLastError();
     }
     /* partial tiles into the workspace, then an ordered reduction */
@@ -351,7 +414,8 @@ extern "C" int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta,
     gemm_kernel<<<grid, NT, 0, s>>>(M, N, K, A, lda, ta, B, ldb, tb, g_ws, N, nullptr, 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return (int)e;
-    splitk_reduce_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>(M, N, split, g_ws, C, ldc, bias, accumulate);
+    splitk_reduce_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>(M, N, split, g_ws, C, ldc, bias, accumulate, C2,
+                                                               act);
     return (int)cudaGetLastError();
 }
 
@@ -367,9 +431,24 @@ extern "C" int fk_mlp_silu_bwd(size_t n, const float *z, const float *da, float 
     return (int)cudaGetLastError();
 }
 
+static float *g_colsum = nullptr;
+static size_t g_colsum_cap = 0;
+
 extern "C" int fk_mlp_colsum(int M, int N, const float *dz, float *db, cudaStream_t s)
 {
-    colsum_kernel<<<(N + 127) / 128, 128, 0, s>>>(M, N, dz, db);
+    const int nchunk = (M + CS_CR - 1) / CS_CR;
+    const size_t need = (size_t)nchunk * N;
+    if (need > g_colsum_cap) {   /* grows on the first (eager) step, never during a capture */
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess && g_colsum) e = cudaFree(g_colsum);
+        g_colsum = nullptr;
+        g_colsum_cap = 0;
+        if (e == cudaSuccess) e = cudaMalloc((void **)&g_colsum, sizeof(float) * need);
+        if (e != cudaSuccess) return (int)e;
+        g_colsum_cap = need;
+    }
+    colsum_kernel<<<dim3((N + 31) / 32, nchunk), 256, 0, s>>>(M, N, dz, g_colsum);
+    colsum_final_kernel<<<(N + 127) / 128, 128, 0, s>>>(N, nchunk, g_colsum, db);
     return (int)cudaGetLastError();
 }
 
@@ -386,12 +465,27 @@ extern "C" int fk_mlp_adam(size_t n, float *w, const float *g, float *m, float *
     return (int)cudaGetLastError();
 }
 
+extern "C" int fk_mlp_adam_sched(size_t n, float *w, const float *g, float *m, float *v, const float *sched,
+                                 const long long *tdev, float b1, float b2, float eps, cudaStream_t s)
+{
+    adam_sched_kernel<<<grid1d(n), 256, 0, s>>>(n, w, g, m, v, sched, tdev, b1, b2, eps);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_mlp_step_inc(long long *tdev, cudaStream_t s)
+{
+    step_inc_kernel<<<1, 1, 0, s>>>(tdev);
+    return (int)cudaGetLastError();
+}
+
 extern "C" int fk_mlp_sample(int nz, int nx, int ny, double dz, double dx, double dy, int ntf, int ldgrd,
                              double vref, const float *tables, const float *sta, unsigned long long seed,
-                             long long nsamp, long long step, int B, float *x, float *y, cudaStream_t s)
+                             long long nsamp, long long step, const long long *step_dev, int B, float *x,
+                             float *y, cudaStream_t s)
 {
     Geom G{nz, nx, ny, ntf, ldgrd, (float)dz, (float)dx, (float)dy, (float)vref};
-    sample_kernel<<<(B + 255) / 256, 256, 0, s>>>(G, tables, sta, (uint64_t)seed, nsamp, step, B, x, y);
+    sample_kernel<<<(B + 255) / 256, 256, 0, s>>>(G, tables, sta, (uint64_t)seed, nsamp, step, step_dev, B, x,
+                                                  y);
     return (int)cudaGetLastError();
 }
 

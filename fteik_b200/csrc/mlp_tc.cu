@@ -18,7 +18,8 @@
  * them to the stage's mbarrier; the next stage is staged meanwhile (two
  * stages).  The epilogue reads the accumulators from tensor memory with
  * tcgen05.ld (warp w: lanes 32 (w mod 4) .. +31, columns 128 (w / 4) ..
- * +127) and writes C.  Every mbarrier wait is bounded; on a timeout the CTA
+ * +127) into shared memory and writes C row by row (coalesced), with the
+ * bias, the previous contents and the SiLU activation applied as asked.  Every mbarrier wait is bounded; on a timeout the CTA
  * sets the error word, lets its MMAs drain and frees its tensor memory.
  */
 #include <cuda_bf16.h>
@@ -225,7 +226,7 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
                                                         int ta, const float *__restrict__ B, int ldb, int tb,
                                                         float *__restrict__ C, int ldc,
                                                         const float *__restrict__ bias, int accumulate,
-                                                        int kchunk, int *error)
+                                                        float *__restrict__ C2, int act, int kchunk, int *error)
 {
     using G = Cfg<PROD>;
     extern __shared__ uint8_t smem_raw[];
@@ -290,9 +291,10 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
         const int last = committed - 1;
         if (!mbar_wait(bar0 + 8u * (last & 1), (last >> 1) & 1)) {
             ok = false;
-            if (threadIdx.x == 0) atomicCAS(error, 0, 2);
+            atomicCAS(error, 0, 2);
         }
     }
+    ok = __syncthreads_and(ok) != 0;   /* the epilogue's barriers need every thread on one path */
     tc_fence_after();
     if (ok && committed == 0 && gridDim.z > 1) {
         /* a split-K slice past the end of K: its partial tile is zero */
@@ -302,33 +304,49 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
         }
     }
     if (ok && committed > 0) {
-        /* epilogue: this warp's 32 TMEM lanes, 128 of the 256 columns */
+        /* epilogue through shared memory (the operand stages are free: every
+         * MMA has completed), one 128-column half of the tile at a time: the
+         * warps holding that half read their 32 TMEM lanes x 128 columns
+         * into a [128][129] tile (row stride 129: conflict-free both ways),
+         * then every warp stores whole rows, 32 consecutive columns per
+         * instruction */
+        float *tile = reinterpret_cast<float *>(base);
         const int q = warp & 3, half = warp >> 2;
-        const int m = m0 + q * 32 + lane;
+        for (int p = 0; p < 2; ++p) {
+            if (half == p) {
 #pragma unroll 1
-        for (int c = 0; c < 128; c += 32) {
-            uint32_t r[32];
-            tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(half * 128 + c), r);
-            tmem_wait_ld();
-            if (m < M) {
-                const int nb = n0 + half * 128 + c;
-                if (gridDim.z > 1) {
-                    float *w = C + ((size_t)blockIdx.z * M + m) * N;
+                for (int c = 0; c < 128; c += 32) {
+                    uint32_t r[32];
+                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(p * 128 + c), r);
+                    tmem_wait_ld();
+                    float *trow = tile + (q * 32 + lane) * 129 + c;
 #pragma unroll
-                    for (int j = 0; j < 32; ++j)
-                        if (nb + j < N) w[nb + j] = __uint_as_float(r[j]);
-                } else {
-                    float *crow = C + (size_t)m * ldc;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int n = nb + j;
-                        if (n < N) {
-                            const float v = __uint_as_float(r[j]) + (bias ? bias[n] : 0.0f);
-                            crow[n] = accumulate ? crow[n] + v : v;
-                        }
-                    }
+                    for (int j = 0; j < 32; ++j) trow[j] = __uint_as_float(r[j]);
                 }
             }
+            __syncthreads();
+            for (int rr = warp; rr < BM; rr += NT / 32) {
+                const int m = m0 + rr;
+                if (m >= M) break;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int n = n0 + p * 128 + i * 32 + lane;
+                    if (n >= N) continue;
+                    float v = tile[rr * 129 + i * 32 + lane];
+                    if (gridDim.z > 1) {
+                        C[((size_t)blockIdx.z * M + m) * N + n] = v;   /* split-K partial tile */
+                        continue;
+                    }
+                    float *c = C + (size_t)m * ldc + n;
+                    if (bias) v += bias[n];
+                    if (accumulate) v = *c + v;
+                    /* act 1: C = z and C2 = silu(z); act 2: C = silu(z) */
+                    const float a = act ? v * (1.0f / (1.0f + __expf(-v))) : v;
+                    *c = act == 2 ? a : v;
+                    if (act == 1) C2[(size_t)m * ldc + n] = a;
+                }
+            }
+            __syncthreads();
         }
     }
     tc_fence_before();
@@ -345,8 +363,8 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
  * M N floats, or NULL for split = 1; error: device word set on a wait
  * timeout.  Returns a cudaError_t. */
 extern "C" int fk_mlp_gemm_tc(int prod, int M, int N, int K, const float *A, int lda, int ta, const float *B,
-                              int ldb, int tb, float *C, int ldc, const float *bias, int accumulate, int split,
-                              float *ws, int *error, cudaStream_t s)
+                              int ldb, int tb, float *C, int ldc, const float *bias, int accumulate, float *C2,
+                              int act, int split, float *ws, int *error, cudaStream_t s)
 {
     using namespace fkmtc;
     if (M <= 0 || N <= 0 || K <= 0) return 0;
@@ -360,14 +378,16 @@ extern "C" int fk_mlp_gemm_tc(int prod, int M, int N, int K, const float *A, int
         if (e != cudaSuccess) return (int)e;
         gemm_tc_kernel<3><<<grid, NT, smem, s>>>(M, N, K, A, lda, ta, B, ldb, tb, split > 1 ? ws : C,
                                                  split > 1 ? N : ldc, split > 1 ? nullptr : bias,
-                                                 split > 1 ? 0 : accumulate, kchunk, error);
+                                                 split > 1 ? 0 : accumulate, C2, split > 1 ? 0 : act, kchunk,
+                                                 error);
     } else {
         const int smem = Cfg<1>::SMEM;
         e = cudaFuncSetAttribute(gemm_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return (int)e;
         gemm_tc_kernel<1><<<grid, NT, smem, s>>>(M, N, K, A, lda, ta, B, ldb, tb, split > 1 ? ws : C,
                                                  split > 1 ? N : ldc, split > 1 ? nullptr : bias,
-                                                 split > 1 ? 0 : accumulate, kchunk, error);
+                                                 split > 1 ? 0 : accumulate, C2, split > 1 ? 0 : act, kchunk,
+                                                 error);
     }
     return (int)cudaGetLastError();
 }

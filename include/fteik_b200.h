@@ -492,6 +492,12 @@ void fteik_b200_mlp_train(int n, const float x[], const float y[], int steps, in
  * weights, Adam and losses stay FP32. */
 void fteik_b200_mlp_setTensorProducts(int products, int *ierr);
 void fteik_b200_mlp_getTensorProducts(int *products);
+/* Training on the locator's tables (fteik_b200_locate_trainSurrogate)
+ * captures one step in a CUDA graph and replays it (on = 1, the default);
+ * 0 launches every kernel of every step.  Both give the same weights bit
+ * for bit. */
+void fteik_b200_mlp_setTrainGraph(int on);
+void fteik_b200_mlp_getTrainGraph(int *on);
 
 /* The 2D ray paths of the last fteik_solver2d_traceRaysToPoints /
  * ToReceivers (rays.F90:449-670, which keeps them in module variables no C

@@ -102,6 +102,25 @@ def test_pruned_search_matches_exhaustive(fk):
     loc.finalize()
 
 
+def test_captured_training_steps_match_eager(fk):
+    """trainSurrogate replays one captured step (step number, learning rate
+    and bias corrections from device memory): the same weights and loss as
+    launching every kernel of every step."""
+    loc = _prune_problem(fk, 40)
+    out = []
+    for graph in (1, 0):
+        old = fk.set_mlp_train_graph(graph)
+        try:
+            net = fk.MLP(256, 5, seed=7)
+            loss = loc.trainSurrogate(nsamples=200_000, steps=80, batch=4096, lr=2e-3, vref=3000.0, seed=7)
+            out.append((loss, net.weights()))
+        finally:
+            fk.set_mlp_train_graph(old)
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
+    loc.finalize()
+
+
 def test_training_is_what_makes_pruning_work(fk):
     """Same pipeline with an untrained network (tau = 1 + noise: straight rays
     at v_ref) in a strong gradient (v = 3000 + 2 z m/s, up to ~7600 m/s): its
