@@ -184,6 +184,8 @@ _SIGS = {
     "fteik_b200_mlp_getTensorProducts": [_PI],
     "fteik_b200_mlp_setTrainGraph": [c_int],
     "fteik_b200_mlp_getTrainGraph": [_PI],
+    "fteik_b200_mlp_setFusedForward": [c_int],
+    "fteik_b200_mlp_getFusedForward": [_PI],
     "fteik_b200_locate_l2_noalloc": [c_int, c_int, c_int, ctypes.c_void_p, c_int, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, _PI],
@@ -289,6 +291,15 @@ def set_mlp_train_graph(on):
     old = c_int()
     lib().fteik_b200_mlp_getTrainGraph(byref(old))
     lib().fteik_b200_mlp_setTrainGraph(int(on))
+    return old.value
+
+
+def set_mlp_fused_forward(on):
+    """Fused (1) or layer-by-layer (0) inference of the surrogate; returns
+    the previous value."""
+    old = c_int()
+    lib().fteik_b200_mlp_getFusedForward(byref(old))
+    lib().fteik_b200_mlp_setFusedForward(int(on))
     return old.value
 
 

@@ -29,6 +29,9 @@ int fk_mlp_adam(size_t n, float *w, const float *g, float *m, float *v, float lr
 void fk_mlp_set_tensor(int products);
 int fk_mlp_get_tensor(void);
 int fk_mlp_tc_status(cudaStream_t s);
+int *fk_mlp_tc_error_word(cudaStream_t s);
+int fk_mlp_forward_fused(const float *w, int nh, const long long *woff, const long long *boff, long long n,
+                         const float *x, float *tau, unsigned char *wq, int *error, cudaStream_t s);
 
 void fteik_b200_mlp_setTensorProducts(int products, int *ierr)
 {
@@ -82,9 +85,16 @@ static void mlp_free_buffers(void)
     NN.cap = 0;
 }
 
+static int g_fused = 1;
+static unsigned char *g_wq = NULL;   /* packed BF16 weights of the fused forward pass */
+static size_t g_wq_cap = 0;
+
 void fteik_b200_mlp_finalize(void)
 {
     mlp_free_buffers();
+    fk_dfree(g_wq);
+    g_wq = NULL;
+    g_wq_cap = 0;
     fk_dfree(NN.w); fk_dfree(NN.g); fk_dfree(NN.m); fk_dfree(NN.v); fk_dfree(NN.loss_dev);
     memset(&NN, 0, sizeof(NN));
 }
@@ -242,6 +252,9 @@ static int forward_backward(int B, const float *y, cudaStream_t s)
     return e;
 }
 
+static int fused_ok(long long n);
+static int forward_fused(long long n, const float *x, float *tau, cudaStream_t s);
+
 void fteik_b200_mlp_forward(int n, const float x[], float tau[], int *ierr)
 {
     /* x [n][6] normalised inputs, host; tau [n] host */
@@ -254,7 +267,7 @@ void fteik_b200_mlp_forward(int n, const float x[], float tau[], int *ierr)
         if (ensure_batch(B)) return;
         int e = (int)cudaMemcpyAsync(NN.x[0], x + (size_t)r0 * MLP_IN, sizeof(float) * (size_t)B * MLP_IN,
                                      cudaMemcpyHostToDevice, s);
-        if (!e) e = forward(B, false, s);
+        if (!e) e = fused_ok(B) ? forward_fused(B, NN.x[0], NN.x[NN.nlayer], s) : forward(B, false, s);
         if (!e) e = (int)cudaMemcpyAsync(tau + r0, NN.x[NN.nlayer], sizeof(float) * (size_t)B,
                                          cudaMemcpyDeviceToHost, s);
         if (!e) e = (int)cudaStreamSynchronize(s);
@@ -452,9 +465,38 @@ void fteik_b200_mlp_train(int n, const float x[], const float y[], int steps, in
 }
 
 /* Inference on device rows (x [n][6] device) into tau (device). */
+void fteik_b200_mlp_setFusedForward(int on) { g_fused = on != 0; }
+void fteik_b200_mlp_getFusedForward(int *on) { *on = g_fused; }
+
+/* The fused forward pass applies: BF16 products, width 256, 1 to 8 hidden
+ * layers, at least one full 128-row tile. */
+static int fused_ok(long long n)
+{
+    const int nh = NN.nlayer - 2;
+    return g_fused && fk_mlp_get_tensor() == 1 && NN.width == 256 && nh >= 1 && nh <= 8 && n >= 128;
+}
+
+static int forward_fused(long long n, const float *x, float *tau, cudaStream_t s)
+{
+    const int nh = NN.nlayer - 2;
+    const size_t need = (size_t)nh * 256 * 256 * 2;
+    if (need > g_wq_cap) {
+        fk_dfree(g_wq);
+        g_wq = (unsigned char *)fk_dalloc(need, "mlp");
+        g_wq_cap = g_wq ? need : 0;
+        if (!g_wq) return 1;
+    }
+    int *err = fk_mlp_tc_error_word(s);
+    if (!err) return 1;
+    long long woff[10], boff[10];
+    for (int l = 0; l < nh + 2; l++) { woff[l] = (long long)NN.woff[l]; boff[l] = (long long)NN.boff[l]; }
+    return fk_mlp_forward_fused(NN.w, nh, woff, boff, n, x, tau, g_wq, err, s);
+}
+
 int fk_mlp_forward_device(long long n, const float *x, float *tau, cudaStream_t s)
 {
     if (!NN.init) return 1;
+    if (fused_ok(n)) return forward_fused(n, x, tau, s);
     const int chunk = 65536;
     int e = 0;
     for (long long r0 = 0; r0 < n && !e; r0 += chunk) {

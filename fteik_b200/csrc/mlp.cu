@@ -343,6 +343,17 @@ extern "C" void fk_mlp_set_tensor(int products) { g_tensor = products; }
 extern "C" int fk_mlp_get_tensor(void) { return g_tensor; }
 
 /* the tensor-core kernels' error word (a wait that timed out), read and cleared */
+/* the tensor-core kernels' error word (allocated on first use, outside any capture) */
+extern "C" int *fk_mlp_tc_error_word(cudaStream_t s)
+{
+    if (!g_tc_error) {
+        cudaError_t e = cudaMalloc((void **)&g_tc_error, sizeof(int));
+        if (e == cudaSuccess) e = cudaMemsetAsync(g_tc_error, 0, sizeof(int), s);
+        if (e != cudaSuccess) { g_tc_error = nullptr; return nullptr; }
+    }
+    return g_tc_error;
+}
+
 extern "C" int fk_mlp_tc_status(cudaStream_t s)
 {
     if (!g_tc_error) return 0;
@@ -380,7 +391,8 @@ extern "C" int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta,
             if (e == cudaSuccess) e = cudaMemsetAsync(g_tc_error, 0, sizeof(int), s);
             if (e != cudaSuccess) return (int)e;
         }
-        /* long K with few 128-row tiles (weight gradients): split K over CTAs */
+        /* few 128-row tiles for the 148 SMs (weight gradients, K = the batch;
+         * products of a small batch): split K over CTAs */
         const int mt = (M + 127) / 128;
         int split = 1;
         while (mt * split < 148 && K / (split * 2) >= 128) split *= 2;

@@ -357,6 +357,227 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
     }
 }
 
+/* ---- fused forward pass ----------------------------------------------------
+ * The whole network for 128 rows in one CTA, BF16 operands (products mode
+ * 1), the activations never leaving the SM: layer 0 (6 inputs) on the CUDA
+ * cores into a BF16 A tile in shared memory (128 rows x 256, four 64-wide
+ * K blocks in the MMA's swizzled layout), each hidden layer as 16 MMAs
+ * (128 x 256 x 16) into tensor memory with the layer's BF16 weights
+ * (packed once per call, 128 KB) brought into shared memory by four bulk
+ * copies while the previous layer's epilogue runs, the epilogue adding the
+ * bias, applying SiLU and writing the next A tile, and the last hidden
+ * layer's epilogue forming the output row by row.  Every rounding and sum
+ * is the layer-by-layer path's: the same MMAs in the same K order, the
+ * same BF16 roundings of the FP32 activations, the first and last layers'
+ * multiply-add chains in the same k order (the last one split between the
+ * four warps holding a row's column quarters, each continuing the previous
+ * one's chain), so tau is the same bits.  CTAs loop over row tiles; waits are
+ * bounded. */
+constexpr int FW = 256;                   /* hidden width */
+constexpr int F_ABLK = BM * 64 * 2;       /* 16 KB: one 64-wide K block of the A tile */
+constexpr int F_WBLK = FW * 64 * 2;       /* 32 KB: one K block of a layer's weights */
+constexpr int F_SMEM = 4 * F_ABLK + 4 * F_WBLK + 1024;
+constexpr int F_MAXH = 8;
+constexpr int F_NT = 512;                 /* 16 warps: 4 per TMEM lane quarter, 64 columns each */
+
+struct FusedNet {
+    const float *w;                       /* all weights and biases, FP32 */
+    int nh;                               /* hidden 256 x 256 layers (1 .. F_MAXH) */
+    long long woff[F_MAXH + 2], boff[F_MAXH + 2];   /* layer 0, hidden 1 .. nh, last nh + 1 */
+};
+
+/* wq[l - 1][kb][swz(n, k)]: hidden layer l's W[n][64 kb + k] in BF16 */
+__global__ void fused_pack_kernel(FusedNet net, uint8_t *__restrict__ wq)
+{
+    const long long total = (long long)net.nh * FW * FW;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int l = (int)(e / (FW * FW)), n = (int)((e / FW) % FW), k = (int)(e % FW);
+        const float v = net.w[net.woff[l + 1] + (long long)n * FW + k];
+        uint8_t *blk = wq + ((size_t)l * 4 + (k >> 6)) * F_WBLK;
+        *reinterpret_cast<__nv_bfloat16 *>(blk + swz(n, k & 63)) = __float2bfloat16_rn(v);
+    }
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ float silu_f(float v) { return v * (1.0f / (1.0f + __expf(-v))); }
+
+/* 8 activations of one row as one 16-byte unit of the A tile (k = n0 .. n0 + 7) */
+__device__ __forceinline__ void put_a8(uint8_t *A, int row, int n0, const float (&a)[8])
+{
+    uint32_t h[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const __nv_bfloat162 p = __floats2bfloat162_rn(a[2 * i], a[2 * i + 1]);
+        h[i] = *reinterpret_cast<const uint32_t *>(&p);
+    }
+    *reinterpret_cast<uint4 *>(A + (n0 >> 6) * F_ABLK + swz(row, n0 & 63)) = make_uint4(h[0], h[1], h[2], h[3]);
+}
+
+__global__ void __launch_bounds__(F_NT, 1) mlp_fused_fwd_kernel(FusedNet net, const uint8_t *__restrict__ wq,
+                                                              long long n, const float *__restrict__ x,
+                                                              float *__restrict__ tau, int *error)
+{
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t bars[2];   /* 0: weights landed, 1: MMAs done */
+    __shared__ uint32_t s_tmem;
+    __shared__ float s_part[BM];
+    uint8_t *A = reinterpret_cast<uint8_t *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t *W = A + 4 * F_ABLK;
+    const uint32_t a_s = (uint32_t)__cvta_generic_to_shared(A), w_s = (uint32_t)__cvta_generic_to_shared(W);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t bar_w = (uint32_t)__cvta_generic_to_shared(&bars[0]), bar_m = bar_w + 8;
+    if (tid == 0) {
+        mbar_init(bar_w, 1);
+        mbar_init(bar_m, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(&s_tmem)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const long long ntile = (n + BM - 1) / BM;
+    int nw_done = 0, nm_done = 0;
+    bool w_pending = false;   /* thread 0: a weight load not yet waited for */
+    auto load_w = [&](int l) {   /* hidden layer l's weights (thread 0) */
+        mbar_expect_tx(bar_w, 4 * F_WBLK);
+        const uint8_t *src = wq + (size_t)(l - 1) * 4 * F_WBLK;
+#pragma unroll
+        for (int kb = 0; kb < 4; ++kb) bulk_g2s(w_s + kb * F_WBLK, src + (size_t)kb * F_WBLK, F_WBLK, bar_w);
+    };
+    if (tid == 0 && blockIdx.x < ntile) { load_w(1); w_pending = true; }
+    bool ok = true;
+    for (long long tile = blockIdx.x; tile < ntile && ok; tile += gridDim.x) {
+        const long long row0 = tile * BM;
+        /* layer 0: row tid / 4, columns 64 (tid % 4) .. + 63 */
+        {
+            const int r = tid >> 2, h = tid & 3;
+            const long long m = row0 + r;
+            float xi[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) xi[k] = m < n ? x[m * 6 + k] : 0.0f;
+            const float *w0 = net.w + net.woff[0], *b0 = net.w + net.boff[0];
+#pragma unroll 1
+            for (int c = 0; c < 64; c += 8) {
+                float a[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int col = h * 64 + c + j;
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) acc = fmaf(xi[k], __ldg(w0 + col * 6 + k), acc);
+                    a[j] = silu_f(acc + __ldg(b0 + col));
+                }
+                put_a8(A, r, h * 64 + c, a);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        for (int l = 1; l <= net.nh && ok; ++l) {
+            if (tid == 0) {
+                if (!mbar_wait(bar_w, nw_done & 1)) { atomicCAS(error, 0, 3); ok = false; }
+                else w_pending = false;
+                if (ok) {
+                    tc_fence_after();
+#pragma unroll
+                    for (int kb = 0; kb < 4; ++kb)
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk)
+                            mma_bf16(tmem, sdesc_sw128(a_s + kb * F_ABLK + kk * 32),
+                                     sdesc_sw128(w_s + kb * F_WBLK + kk * 32), (kb | kk) ? 1u : 0u);
+                    mma_commit(bar_m);
+                }
+            }
+            ++nw_done;
+            ok = __syncthreads_and(ok) != 0;
+            if (!ok) break;
+            if (!mbar_wait(bar_m, nm_done & 1)) { atomicCAS(error, 0, 4); ok = false; }
+            ++nm_done;
+            ok = __syncthreads_and(ok) != 0;
+            if (!ok) break;
+            tc_fence_after();
+            /* the MMAs are done with A and W: the next weights come in during the epilogue */
+            const bool more = l < net.nh || tile + gridDim.x < ntile;
+            if (more && tid == 0) { load_w(l < net.nh ? l + 1 : 1); w_pending = true; }
+            /* warp w: TMEM lanes 32 (w mod 4) .. + 31 (rows), columns 64 (w / 4) .. + 63 */
+            const int q = warp & 3, cq = warp >> 2, row = q * 32 + lane;
+            const float *bl = net.w + net.boff[l];
+            if (l < net.nh) {
+#pragma unroll 1
+                for (int c = 0; c < 64; c += 32) {
+                    uint32_t r[32];
+                    tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cq * 64 + c), r);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        float a[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int col = cq * 64 + c + 8 * u + j;
+                            a[j] = silu_f(__uint_as_float(r[8 * u + j]) + __ldg(bl + col));
+                        }
+                        put_a8(A, row, cq * 64 + c + 8 * u, a);
+                    }
+                }
+            } else {
+                /* last hidden layer: the output's multiply-add chain over the 256
+                 * activations in order, each column quarter's warp continuing
+                 * the previous quarter's chain */
+                const float *wl = net.w + net.woff[l + 1];
+                for (int p = 0; p < 4; ++p) {
+                    if (cq == p) {
+                        float acc = p ? s_part[row] : 0.0f;
+#pragma unroll 1
+                        for (int c = 0; c < 64; c += 32) {
+                            uint32_t r[32];
+                            tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(p * 64 + c), r);
+                            tmem_wait_ld();
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) {
+                                const int col = p * 64 + c + j;
+                                const float a = silu_f(__uint_as_float(r[j]) + __ldg(bl + col));
+                                acc = fmaf(a, __ldg(wl + col), acc);
+                            }
+                        }
+                        if (p < 3) s_part[row] = acc;
+                        else if (row0 + row < n) tau[row0 + row] = acc + __ldg(net.w + net.boff[l + 1]);
+                    }
+                    __syncthreads();
+                }
+            }
+            tc_fence_before();
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+        }
+    }
+    /* a weight load still in flight ends before the CTA does */
+    if (tid == 0 && w_pending && !mbar_wait(bar_w, nw_done & 1)) atomicCAS(error, 0, 5);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
 } // namespace fkmtc
 
 /* Launch one tensor-core GEMM (PROD 1 or 3); ws: split-K workspace of split
@@ -389,5 +610,31 @@ extern "C" int fk_mlp_gemm_tc(int prod, int M, int N, int K, const float *A, int
                                                  split > 1 ? 0 : accumulate, C2, split > 1 ? 0 : act, kchunk,
                                                  error);
     }
+    return (int)cudaGetLastError();
+}
+
+/* The fused forward pass of n rows (x [n][6] device, tau [n] device) of a
+ * network with nh hidden 256 x 256 layers; wq: 128 KB per hidden layer of
+ * scratch for the packed weights.  Returns a cudaError_t. */
+extern "C" int fk_mlp_forward_fused(const float *w, int nh, const long long *woff, const long long *boff,
+                                    long long n, const float *x, float *tau, unsigned char *wq, int *error,
+                                    cudaStream_t s)
+{
+    using namespace fkmtc;
+    if (n <= 0) return 0;
+    if (nh < 1 || nh > F_MAXH) return (int)cudaErrorInvalidValue;
+    FusedNet net;
+    net.w = w;
+    net.nh = nh;
+    for (int l = 0; l < nh + 2; ++l) { net.woff[l] = woff[l]; net.boff[l] = boff[l]; }
+    fused_pack_kernel<<<256, 256, 0, s>>>(net, wq);
+    cudaError_t e = cudaFuncSetAttribute(mlp_fused_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, F_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long ntile = (n + BM - 1) / BM;
+    const int grid = (int)(ntile < nsm ? ntile : nsm);
+    mlp_fused_fwd_kernel<<<grid, F_NT, F_SMEM, s>>>(net, wq, n, x, tau, error);
     return (int)cudaGetLastError();
 }

@@ -749,18 +749,27 @@ __device__ __forceinline__ bool slab_pass_f32(const fk3tw::Params &P_, const fk_
  * the batch issued 4 steps before; a lane reads an item from the stage one
  * step before using it.  A group lives in buffer G mod 3: the two groups a
  * lane reads in the next 4 steps and the one in flight.  Stage per warp:
- * [3 buffers][6 arrays: told per source, the 4 slowness values][32 slots]
- * [4 floats] (9 KB); lane l's slot is (l >> 2) | ((l & 3) << 3), so the 32
- * lanes read 32 different banks in every step.  The slab's first row stages
+ * [3 buffers][4 arrays: told per source, the x-upwind slowness cells of
+ * the two y sides][32 slots][4 floats] (6 KB); lane l's slot is
+ * (l >> 2) | ((l & 3) << 3), so the 32 lanes read 32 different banks in
+ * every step.  The x-downwind slowness cells of a lane are lane l + 1's
+ * x-upwind ones (its next item is this lane's current one): only lane 31
+ * stages its own, in a small area after the arrays.  The slab's first row stages
  * its y-upwind values (the upwind slab's last row, final for this sweep)
  * the same way, in a per-block stage [3 buffers][S][32 slots][4 floats];
  * its groups reach SG_AHEAD steps past the batch's step, so the first row
  * waits for the upwind slab to be that much further ahead than a direct
  * load one step ahead would need. */
-constexpr int SG_NARR = 6;
+constexpr int SG_NARR = 4;             /* told per source, the x-upwind slowness cells (y U, D) */
 constexpr int SG_NBUF = 3;
 constexpr int SG_ARR_BYTES = 32 * 16;
-constexpr int SG_WARP_BYTES = SG_NBUF * SG_NARR * SG_ARR_BYTES;   /* 9 KB */
+/* lane 31's x-downwind cells (y U, D): [3 buffers][2][4 floats] after the arrays */
+constexpr int SG_X31_OFF = SG_NBUF * SG_NARR * SG_ARR_BYTES;
+/* 6.1 KB: with the rings and the first row's stage, five blocks of the
+ * two-source staged step fit an SM (registers capped at 102 by the launch
+ * bounds; 95 used): 46.9 ms on 64 sources x 4 grids against 47.4 ms with
+ * the 9 KB stage (six arrays, lane 31's cells among them) at four */
+constexpr int SG_WARP_BYTES = SG_X31_OFF + 128;
 /* the slab's first row also stages its y-upwind values (the upwind slab's
  * last row): [3 buffers][S sources][32 slots][4 floats] per block */
 template <int S> constexpr int sg_tn_bytes() { return SG_NBUF * S * SG_ARR_BYTES; }
@@ -839,6 +848,8 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
     const bool load_tn = oy == 0 && has_yu;               /* first row: stage the upwind slab's last row */
     const uint32_t myt = stage_tn + (uint32_t)(slot * 16);
     const float *const mytf = stage_tn_f + slot * 4;
+    const uint32_t x31 = stage + (uint32_t)SG_X31_OFF;
+    const float *const x31f = stage_f + SG_X31_OFF / 4;
     constexpr int A = SG_ARR_BYTES / 4;                   /* floats per array */
     constexpr int BUFF = SG_NARR * A;                     /* floats per buffer */
     const bool loads_slow = rowupd;                       /* a row that updates reads slowness */
@@ -869,8 +880,8 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
                 cpa16(d + 2 * SG_ARR_BYTES, sl + is);
                 cpa16(d + 3 * SG_ARR_BYTES, sl + (is + offY));
                 if (tx == 31) {   /* the other lanes take their x-downwind cells from lane l + 1 */
-                    cpa16(d + 4 * SG_ARR_BYTES, sl + (is + ox));
-                    cpa16(d + 5 * SG_ARR_BYTES, sl + (is + ox + offY));
+                    cpa16(x31 + (uint32_t)(buf * 32), sl + (is + ox));
+                    cpa16(x31 + (uint32_t)(buf * 32 + 16), sl + (is + ox + offY));
                 }
             }
         }
@@ -897,8 +908,8 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
             if (S == 2) f.told[S - 1] = a[A];
             f.duu = a[2 * A];
             f.dud = a[3 * A];
-            f.ddu = a[4 * A];
-            f.ddd = a[5 * A];
+            f.ddu = x31f[buf * 8 + e];       /* lane 31's (the others' are not used) */
+            f.ddd = x31f[buf * 8 + 4 + e];
             if (oy == 0) {   /* the upwind slab's last row, final for this sweep (invalid items: any value) */
                 const float *b = mytf + buf * (S * A) + e;
                 f.tn[0] = has_yu ? b[0] : HUGEV;
@@ -1049,7 +1060,7 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
  * independent dependency chains.  tasks = {pair, j'} with pairs[2 pair + i]
  * the work items (-1: none) when S = 2, {work, j'} when S = 1. */
 template <typename R, bool INIT, bool RESID, int S, int CHP, bool STG = false>
-__global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : 4)) slab_kernel(fk3tw::Params P, const int *pairs,
+__global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : (STG ? 5 : 4))) slab_kernel(fk3tw::Params P, const int *pairs,
                                                                              int zring)
 {
     __shared__ R xr[(sizeof(R) == 4 && !INIT && STG) ? NBP : NB][S][TY][32];

@@ -498,6 +498,12 @@ void fteik_b200_mlp_getTensorProducts(int *products);
  * for bit. */
 void fteik_b200_mlp_setTrainGraph(int on);
 void fteik_b200_mlp_getTrainGraph(int *on);
+/* Inference (fteik_b200_mlp_forward, the surrogate's coarse tables) with
+ * BF16 products and 256 hidden units runs the whole network in one
+ * tensor-core kernel per 128 rows (on = 1, the default); 0 runs it layer by
+ * layer.  Both give the same bits. */
+void fteik_b200_mlp_setFusedForward(int on);
+void fteik_b200_mlp_getFusedForward(int *on);
 
 /* The 2D ray paths of the last fteik_solver2d_traceRaysToPoints /
  * ToReceivers (rays.F90:449-670, which keeps them in module variables no C

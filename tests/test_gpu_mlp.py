@@ -102,6 +102,31 @@ def test_pruned_search_matches_exhaustive(fk):
     loc.finalize()
 
 
+@pytest.mark.parametrize("n", [20_000, 20_001, 85_537])
+def test_fused_forward_matches_layer_by_layer(fk, n):
+    """The one-kernel forward pass (BF16 products, activations kept on the
+    SM) gives the layer-by-layer path's outputs bit for bit, full and
+    ragged last tiles included (sizes at which the layer-by-layer products
+    are not split over K: at least 148 row tiles per 65,536-row chunk)."""
+    old_p = fk.set_mlp_tensor_products(1)
+    try:
+        net = fk.MLP(256, 5, seed=11)
+        rng = np.random.default_rng(n)
+        net.setWeights(net.weights() * rng.uniform(0.5, 1.5, net.nweights()).astype(np.float32))
+        x = rng.uniform(-1, 1, (n, 6)).astype(np.float32)
+        outs = []
+        for fused in (1, 0):
+            old = fk.set_mlp_fused_forward(fused)
+            try:
+                outs.append(net.forward(x))
+            finally:
+                fk.set_mlp_fused_forward(old)
+        assert np.array_equal(outs[0], outs[1])
+        net.finalize()
+    finally:
+        fk.set_mlp_tensor_products(old_p)
+
+
 def test_captured_training_steps_match_eager(fk):
     """trainSurrogate replays one captured step (step number, learning rate
     and bias corrections from device memory): the same weights and loss as
