@@ -277,4 +277,12 @@ int fk_mlp_coarse_store(long long r0, long long nrow, long long nc, int ldc, con
 #ifdef __cplusplus
 }
 #endif
+#ifdef __CUDACC__
+/* The surrogate's SiLU, z / (1 + e^-z), with the fast exponential and
+ * division (relative error of order 1e-7): one definition for every kernel
+ * that applies it, so the fused and layer-by-layer passes round alike. */
+static __device__ __forceinline__ float fk_sigmoid(float z) { return __fdividef(1.0f, 1.0f + __expf(-z)); }
+static __device__ __forceinline__ float fk_silu(float z) { return z * fk_sigmoid(z); }
+#endif
+
 #endif

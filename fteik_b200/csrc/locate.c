@@ -61,6 +61,7 @@ static struct {
     int bz, bx, by, ncz, ncx, ncy, ngrd_c, ldc;
     float *coarse;           /* device [ntf][ldc] surrogate travel times */
     float *fine_blk;         /* device block-major copy of the exact tables */
+    size_t fine_cap;         /* its size in floats */
     long long blk_gen;       /* table generation fine_blk was built from */
     void *bpack_c;
     int rc, k;
@@ -691,8 +692,12 @@ void fteik_b200_locate_buildSurrogate(int bz, int bx, int by, int *ierr)
         if (!e) e = fk_mlp_coarse_store(r0, m, SP.ngrd_c, SP.ldc, tau, dist, SP.coarse, s);
     }
     if (!e) e = fk_locate_tc_pack_tables(SP.ngrd_c, SP.ldc, SL.ntf, SP.coarse, SP.bpack_c, s);
-    fk_dfree(SP.fine_blk);
-    SP.fine_blk = (float *)fk_dalloc(sizeof(float) * (size_t)SP.ngrd_c * SL.ntf * (size_t)(bz * bx * by), who);
+    const size_t nfine = (size_t)SP.ngrd_c * SL.ntf * (size_t)(bz * bx * by);
+    if (nfine != SP.fine_cap) {   /* a rebuild of the same blocks reuses the copy's memory */
+        fk_dfree(SP.fine_blk);
+        SP.fine_blk = (float *)fk_dalloc(sizeof(float) * nfine, who);
+        SP.fine_cap = SP.fine_blk ? nfine : 0;
+    }
     if (!SP.fine_blk) e = 1;
     if (!e) e = fk_locate_block_tables(SP.nz, SP.nx, SP.ny, bz, bx, by, SL.ntf, SL.ldgrd, SL.tables, SP.fine_blk, s);
     SP.blk_gen = SL.table_gen;

@@ -109,19 +109,19 @@ __global__ void splitk_reduce_kernel(int M, int N, int split, const float *__res
         float *c = C + (size_t)m * ldc + n;
         if (accumulate) v = *c + v;
         /* act 1: C = z and C2 = silu(z); act 2: C = silu(z) (as silu_kernel) */
-        const float a = act ? v * (1.0f / (1.0f + __expf(-v))) : v;
+        const float a = act ? fk_silu(v) : v;
         *c = act == 2 ? a : v;
         if (act == 1) C2[(size_t)m * ldc + n] = a;
     }
 }
 
-__device__ __forceinline__ float sigmoid(float z) { return 1.0f / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float sigmoid(float z) { return fk_sigmoid(z); }
 
 __global__ void silu_kernel(size_t n, const float *__restrict__ z, float *__restrict__ a)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const float v = z[i];
-        a[i] = v * sigmoid(v);
+        a[i] = fk_silu(v);
     }
 }
 
@@ -129,7 +129,7 @@ __global__ void silu_inplace_kernel(size_t n, float *a)
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const float v = a[i];
-        a[i] = v * sigmoid(v);
+        a[i] = fk_silu(v);
     }
 }
 

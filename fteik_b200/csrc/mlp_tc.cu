@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
                     if (bias) v += bias[n];
                     if (accumulate) v = *c + v;
                     /* act 1: C = z and C2 = silu(z); act 2: C = silu(z) */
-                    const float a = act ? v * (1.0f / (1.0f + __expf(-v))) : v;
+                    const float a = act ? fk_silu(v) : v;
                     *c = act == 2 ? a : v;
                     if (act == 1) C2[(size_t)m * ldc + n] = a;
                 }
@@ -411,7 +411,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-__device__ __forceinline__ float silu_f(float v) { return v * (1.0f / (1.0f + __expf(-v))); }
+__device__ __forceinline__ float silu_f(float v) { return fk_silu(v); }
 
 /* 8 activations of one row as one 16-byte unit of the A tile (k = n0 .. n0 + 7) */
 __device__ __forceinline__ void put_a8(uint8_t *A, int row, int n0, const float (&a)[8])

@@ -784,15 +784,16 @@ __device__ __forceinline__ void cpa16(uint32_t saddr, const void *gptr)
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cpa_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-template <bool RESID, int S, int CHP>
+template <bool INIT, bool RESID, int S, int CHP>
 __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, const fk_grid3d_t &g,
                                                      float *const (&ttp)[S], int s, int sweep_no, int P,
                                                      int nslab, int *const (&prog)[S], float (*xr)[S][TY][32],
                                                      float *ring, int zring, int *s_flag, double (&dmax)[S],
                                                      uint32_t stage, const float *stage_f, uint32_t stage_tn,
-                                                     const float *stage_tn_f)
+                                                     const float *stage_tn_f, const Src &q0)
 {
-    constexpr int CH = CHP;
+    static_assert(!INIT || (S == 1 && !RESID), "initialisation sweeps: one source per thread");
+    constexpr int CH = INIT ? CH_INIT : CHP;
     static_assert(CH % DLP == 0 && NBP == 2 * DLP, "windows and progress align");
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const unsigned FULL = 0xffffffffu;
@@ -801,25 +802,34 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
     const int sz = (s0 < 4) ? 1 : -1;
     const int sx = (s0 % 2 == 0) ? 1 : -1;
     const int sy = ((s0 / 2) % 2 == 0) ? 1 : -1;
+    /* the walk's box (solver3D.F90:493-565 in the initialisation sweeps,
+     * logical positions from 1 in the passes) */
+    const int lozb = INIT ? ((sz > 0) ? max(1, q0.zsi - 1) : max(1, nz - q0.zsi - 1)) : 1;
+    const int loxb = INIT ? ((sx > 0) ? max(1, q0.xsi - 1) : max(1, nx - q0.xsi - 1)) : 1;
+    const int loyb = INIT ? ((sy > 0) ? max(1, q0.ysi - 1) : max(1, ny - q0.ysi - 1)) : 1;
     Mesh<float> mesh;
     fk3::make_mesh<float>(mesh, g.dz, g.dx, g.dy);
+    Mesh<double> mesh64;
+    if (INIT) fk3::make_mesh<double>(mesh64, g.dz, g.dx, g.dy);
+    const float eps_r = (float)q0.eps_t;
     const float HUGEV = (float)FK_HUGE;
     const int th = min(TY, ny - TY * P);
     const bool row = ty < th;
     const int y = TY * P + ty;
     const int oy = (sy > 0) ? ty : th - 1 - ty;
     const int yl = (sy > 0) ? y : ny - 1 - y;
-    const bool rowupd = row && yl >= 1;
+    const bool rowupd = row && yl >= loyb;
     const int wy = ty - sy;
     const int zoff = (sz > 0) ? 0 : ((4 - (nz & 3)) & 3);   /* leading dummy items */
     const int Zn = nz + zoff;                               /* items zoff .. Zn - 1 are the nodes */
     const int Zp = ((max(Zn, 32) + 3) >> 2) << 2;
     const int K = (nx + 31) / 32;
-    const int T = K * Zp + 31 + DLP * (TY - 1);
+    const int k0 = (loxb - 1) / 32;                         /* blocks before x' = lox - 1: not walked */
+    const int T = (K - k0) * Zp + 31 + DLP * (TY - 1);
     const int Pu = P - sy;
     const bool has_up = Pu >= 0 && Pu < nslab;
     const int ylast_up = has_up ? ((sy > 0) ? TY * Pu + min(TY, ny - TY * Pu) - 1 : TY * Pu) : 0;
-    const bool wait_up = has_up && (((sy > 0) ? ylast_up : ny - 1 - ylast_up) >= 1);
+    const bool wait_up = has_up && (((sy > 0) ? ylast_up : ny - 1 - ylast_up) >= loyb);
     const int yu = y - sy;
     const bool has_yu = row && yu >= 0 && yu < ny;
     const bool has2 = S == 2 && ttp[S - 1] != nullptr;
@@ -828,7 +838,8 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
 
     const int x0 = (sx > 0) ? tx : nx - 1 - tx;
     const int kl = row ? (nx - tx + 31) / 32 : 0;                  /* blocks with x' < nx */
-    const int kmin = rowupd ? (tx == 0 ? 1 : 0) : 0x7fffffff;       /* updated: x' >= 1, y' >= 1 */
+    /* updated: x' >= lox (1 in the passes), y' >= loy */
+    const int kmin = rowupd ? (loxb > tx ? (loxb - tx + 31) >> 5 : 0) : 0x7fffffff;
     const int kxl = (nx - 1 >= tx && (nx - 1 - tx) % 32 == 0) ? (nx - 1 - tx) / 32 : -1; /* x' = nx - 1 */
     /* node iz of walk position zq: sz > 0: zq; sz < 0: nz - 1 + zoff - zq */
     const int colT = (y * nx + x0) * zp;
@@ -859,7 +870,7 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
      * past the one holding item 4 b + 1 - c, the first read after the batch; G_{b+1} = G_b + 1.
      * Cursor (lk, lzq) = (column block, walk position) of the group's first item. */
     int gl = ((1 - 8 - c) >> 2) + 2;            /* G_{-2}: the prologue issues G_{-2}, G_{-1} */
-    int lk = 0, lzq = 4 * gl;
+    int lk = k0, lzq = 4 * gl;
     while (lzq >= Zp) { lzq -= Zp; ++lk; }
     auto issue = [&]() {
         const int buf = (gl + 3 * 0x2000000) % 3;
@@ -931,7 +942,7 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
     issue();                                    /* G_{-2} */
     issue();                                    /* G_{-1} */
     cpa_wait0();
-    int nk = 0, nzq = -c;                       /* item of the next step */
+    int nk = k0, nzq = -c;                      /* item of the next step */
     Item nxt;
 #pragma unroll
     for (int i = 0; i < S; ++i) nxt.told[i] = nxt.tn[i] = HUGEV;
@@ -978,8 +989,8 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
             const float c_ddu = (tx == 31) ? cur.ddu : (cur.k == kxl) ? cur.duu : dn_uu;
             const float c_ddd = (tx == 31) ? cur.ddd : (cur.k == kxl) ? cur.dud : dn_ud;
             const bool valid = (unsigned)(cur.zq - zoff) < (unsigned)nz && cur.k < kl;
-            const bool upd = valid && cur.zq > zoff && cur.k >= kmin;
-            const bool from_ring = tx == 0 && cur.k > 0;   /* then 0 <= zq < Zp */
+            const bool upd = valid && cur.zq >= zoff + lozb && cur.k >= kmin;
+            const bool from_ring = tx == 0 && cur.k > k0;   /* then 0 <= zq < Zp */
             float rte[S], rten[S];
 #pragma unroll
             for (int i = 0; i < S; ++i) rte[i] = rten[i] = HUGEV;
@@ -1006,8 +1017,28 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
                 res[i] = cur.told[i];
             }
             if (upd) {
-                pass_stencil<S, true>(mesh, r_last, te, tnv_, te_last, ten, tn_last, ten_last, s1, s2, s3, s4, s5, s6,
-                                s7, cur.told, res);
+                if constexpr (INIT) {
+                    /* as in slab_sweep: the plane-wave stencil where the switch
+                     * (compared in FP32) says Cartesian, else the FP64
+                     * spherical one near the source */
+                    const float tv = r_last[0], tn = tnv_[0];
+                    if (rmin(rmin(tv, te[0]), tn) > eps_r) {
+                        res[0] = fk3::noinit_f32(mesh, tv, te[0], tn, te_last[0], ten[0], tn_last[0], ten_last[0], s1,
+                                                 s2, s3, s4, s5, s6, s7, cur.told[0]);
+                    } else {
+                        const int xl = 32 * cur.k + tx;
+                        const int x = (sx > 0) ? xl : nx - 1 - xl;
+                        const int iz = izw + sz * cur.zq;
+                        res[0] = (float)fk3::init_node<double>(
+                            q0, mesh64, false, (double)tv, (double)te[0], (double)tn, (double)te_last[0],
+                            (double)ten[0], (double)tn_last[0], (double)ten_last[0], (double)cur.told[0], (double)s1,
+                            (double)s2, (double)s3, (double)s4, (double)s5, (double)s6, (double)s7, iz + 1, x + 1,
+                            y + 1, sz, sx, sy);
+                    }
+                } else {
+                    pass_stencil<S, true>(mesh, r_last, te, tnv_, te_last, ten, tn_last, ten_last, s1, s2, s3, s4, s5,
+                                          s6, s7, cur.told, res);
+                }
                 const int it = colT + cur.k * dkT + izw + sz * cur.zq;
 #pragma unroll
                 for (int i = 0; i < S; ++i) {
@@ -1063,7 +1094,7 @@ template <typename R, bool INIT, bool RESID, int S, int CHP, bool STG = false>
 __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : (STG ? 5 : 4))) slab_kernel(fk3tw::Params P, const int *pairs,
                                                                              int zring)
 {
-    __shared__ R xr[(sizeof(R) == 4 && !INIT && STG) ? NBP : NB][S][TY][32];
+    __shared__ R xr[(sizeof(R) == 4 && STG) ? NBP : NB][S][TY][32];
     __shared__ long long s_task;
     __shared__ int s_flag[2];
     __shared__ double s_max[S][TY];
@@ -1183,9 +1214,10 @@ __global__ void __launch_bounds__(NT, INIT ? 4 : (S == 1 ? 6 : (STG ? 5 : 4))) s
                                     reinterpret_cast<R (*)[1][TY][32]>(xr), ring, zring);
         } else if (!skip) {
             bool ok;
-            if constexpr (!INIT && sizeof(R) == 4 && STG)
-                ok = slab_pass_f32_staged<RESID, S, CHP>(P, g, ttp, s, sweep_no, Pp, nslab, prog, xr, ring, zring,
-                                                         s_flag, dmax, stage, stage_f, stage_tn, stage_tn_f);
+            if constexpr (sizeof(R) == 4 && STG && (!INIT || S == 1))
+                ok = slab_pass_f32_staged<INIT, RESID, S, CHP>(P, g, ttp, s, sweep_no, Pp, nslab, prog, xr, ring,
+                                                               zring, s_flag, dmax, stage, stage_f, stage_tn,
+                                                               stage_tn_f, qs[0]);
             else if constexpr (!INIT && sizeof(R) == 4)
                 ok = slab_pass_f32<RESID, S, CHP>(P, g, ttp, reinterpret_cast<const float *>(g.slow), s, sweep_no,
                                                   Pp, nslab, prog, xr, ring, zring, s_flag, dmax);
@@ -1269,7 +1301,8 @@ inline int launch_slab_kernel(const fk3tw::Params &P, const int *pairs, int zrin
 /* The FP32 initialisation kernel lives in its own unit (slab_init_f32.cu),
  * compiled without multiply-add contraction: its near-source spherical
  * stencil is FP64 and so rounds as the FP64 CPU algorithm does. */
-int launch_init_f32(const fk3tw::Params &P, int zring, cudaStream_t st, int blocks_per_sm, const int *pairs);
+int launch_init_f32(const fk3tw::Params &P, int zring, cudaStream_t st, int blocks_per_sm, const int *pairs,
+                    bool staged);
 
 template <typename R>
 inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nwork, const fk_slabs3d_t *pl,
@@ -1334,9 +1367,11 @@ inline int launch_rows(const fk_grid3d_t *grids, const fk_work3d_t *work, int nw
             fk3tw::Params Pi = P;
             Pi.tasks = reinterpret_cast<const int2 *>(pl->tasks2);
             Pi.ntask_sweep = pl->ntask2_sweep;
-            rc = launch_init_f32(Pi, zring, st, pl->init_blocks_per_sm, pl->init_pairs);
+            rc = launch_init_f32(Pi, zring, st, pl->init_blocks_per_sm, pl->init_pairs, false);
         } else {
-            rc = launch_init_f32(Pt, zring_t, st, pl->init_blocks_per_sm, nullptr);
+            /* with the staged pass step (the node-indexed slowness built) the
+             * slab tasks take the staged walk too */
+            rc = launch_init_f32(Pt, zring_t, st, pl->init_blocks_per_sm, nullptr, pl->staged != 0);
         }
     }
     else
