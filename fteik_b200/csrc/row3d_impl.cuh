@@ -809,8 +809,6 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
     const int loyb = INIT ? ((sy > 0) ? max(1, q0.ysi - 1) : max(1, ny - q0.ysi - 1)) : 1;
     Mesh<float> mesh;
     fk3::make_mesh<float>(mesh, g.dz, g.dx, g.dy);
-    Mesh<double> mesh64;
-    if (INIT) fk3::make_mesh<double>(mesh64, g.dz, g.dx, g.dy);
     const float eps_r = (float)q0.eps_t;
     const float HUGEV = (float)FK_HUGE;
     const int th = min(TY, ny - TY * P);
@@ -863,6 +861,7 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
     const float *const x31f = stage_f + SG_X31_OFF / 4;
     constexpr int A = SG_ARR_BYTES / 4;                   /* floats per array */
     constexpr int BUFF = SG_NARR * A;                     /* floats per buffer */
+    static_assert(BUFF == 512 && S * A * 4 == S * BUFF, "the cursor's shifts below assume 4 arrays of 128 floats");
     const bool loads_slow = rowupd;                       /* a row that updates reads slowness */
 
     const int c = tx + DLP * oy;                 /* the lane's item at step t is t - c */
@@ -907,26 +906,40 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
         float duu, dud, ddu, ddd;
         int k, zq;
     };
-    /* item jn = (kk, zz) of the walk from the stage (its group is resident) */
-    auto fetch = [&](Item &f, int kk, int zz, int jn) {
+    /* read cursor: the next item jr of the walk, its group's buffer (as a
+     * float offset rb = (jr / 4 mod 3) BUFF) and its place eo in the group,
+     * advanced one item per step */
+    int jr = -c;
+    int rb = (((jr >> 2) + 3 * 0x2000000) % 3) * BUFF;
+    int eo = (sz > 0) ? (jr & 3) : 3 - (jr & 3);
+    auto advance = [&]() {
+        ++jr;
+        if ((jr & 3) == 0) {
+            rb = (rb == 2 * BUFF) ? 0 : rb + BUFF;
+            eo = (sz > 0) ? 0 : 3;
+        } else {
+            eo += sz;
+        }
+    };
+    /* item jr = (kk, zz) of the walk from the stage (its group is resident) */
+    auto fetch = [&](Item &f, int kk, int zz) {
         f.k = kk;
         f.zq = zz;
-        if (jn >= 0) {
-            const int e = (sz > 0) ? (jn & 3) : 3 - (jn & 3);
-            const int buf = ((jn >> 2) + 3 * 0x2000000) % 3;
-            const float *a = myf + buf * BUFF + e;
+        if (jr >= 0) {
+            const float *a = myf + rb + eo;
             f.told[0] = a[0];
             if (S == 2) f.told[S - 1] = a[A];
             f.duu = a[2 * A];
             f.dud = a[3 * A];
-            f.ddu = x31f[buf * 8 + e];       /* lane 31's (the others' are not used) */
-            f.ddd = x31f[buf * 8 + 4 + e];
+            f.ddu = x31f[(rb >> 6) + eo];       /* lane 31's (the others' are not used) */
+            f.ddd = x31f[(rb >> 6) + 4 + eo];
             if (oy == 0) {   /* the upwind slab's last row, final for this sweep (invalid items: any value) */
-                const float *b = mytf + buf * (S * A) + e;
+                const float *b = mytf + ((rb * S) >> 2) + eo;
                 f.tn[0] = has_yu ? b[0] : HUGEV;
                 if (S == 2) f.tn[S - 1] = has_yu ? b[A] : HUGEV;
             }
         }
+        advance();
     };
 
     const int *prog_up = prog[0] + (has_up ? Pu : P);
@@ -947,7 +960,7 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
 #pragma unroll
     for (int i = 0; i < S; ++i) nxt.told[i] = nxt.tn[i] = HUGEV;
     nxt.duu = nxt.dud = nxt.ddu = nxt.ddd = 0.0f;
-    fetch(nxt, nk, nzq, -c);
+    fetch(nxt, nk, nzq);
     if (++nzq == Zp) { nzq = 0; ++nk; }
     float zu_uu = 0.0f, zu_ud = 0.0f, zu_du = 0.0f, zu_dd = 0.0f;
     float r_last[S], te_last[S], tn_last[S], ten_last[S];
@@ -980,7 +993,7 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
                 sh_tn[i] = __shfl_up_sync(FULL, tn_last[i], 1);
             }
             const Item cur = nxt;
-            fetch(nxt, nk, nzq, t0 + u + 1 - c);
+            fetch(nxt, nk, nzq);
             if (++nzq == Zp) { nzq = 0; ++nk; }
             /* x-downwind cells: lane l + 1's x-upwind ones, its next item being
              * this lane's current one; lane 31 stages its own, and the last
@@ -1029,6 +1042,8 @@ __device__ __forceinline__ bool slab_pass_f32_staged(const fk3tw::Params &P_, co
                         const int xl = 32 * cur.k + tx;
                         const int x = (sx > 0) ? xl : nx - 1 - xl;
                         const int iz = izw + sz * cur.zq;
+                        Mesh<double> mesh64;   /* built here: few nodes take this branch */
+                        fk3::make_mesh<double>(mesh64, g.dz, g.dx, g.dy);
                         res[0] = (float)fk3::init_node<double>(
                             q0, mesh64, false, (double)tv, (double)te[0], (double)tn, (double)te_last[0],
                             (double)ten[0], (double)tn_last[0], (double)ten_last[0], (double)cur.told[0], (double)s1,
