@@ -451,7 +451,10 @@ LOC_NEV = 10000
 LOC_EXACT_SAMPLE = 512
 LOC_L1_SAMPLE = 128
 SUR_WIDTH, SUR_DEPTH = 256, 5          # surrogate: 6 -> 5 x 256 SiLU -> tau
-SUR_SAMPLES, SUR_STEPS, SUR_BATCH = 2_000_000, 3000, 4096
+# 12.3e6 sample evaluations either way: 16,384 x 750 (lr 4e-3) keeps the
+# pruning agreement at 100 % with the loss of 4,096 x 3,000 (lr 2e-3) and
+# runs the products 4x larger
+SUR_SAMPLES, SUR_STEPS, SUR_BATCH, SUR_LR = 2_000_000, 750, 16384, 4e-3
 SUR_BLOCK = (4, 4, 4)                  # fine nodes per coarse block (z, x, y)
 
 
@@ -482,7 +485,8 @@ def _mlp_products(fk):
     return v.value
 
 
-def bench_locate(fk, b, grids, stream, steps, nev=LOC_NEV, igrid=LOC_GRID, sur_steps=SUR_STEPS):
+def bench_locate(fk, b, grids, stream, steps, nev=LOC_NEV, igrid=LOC_GRID, sur_steps=SUR_STEPS,
+                 sur_batch=SUR_BATCH, sur_lr=SUR_LR):
     import torch
     g = grids[LOC_GRID - 1]
     ngrd = g["nz"] * g["nx"] * g["ny"]
@@ -518,7 +522,7 @@ def bench_locate(fk, b, grids, stream, steps, nev=LOC_NEV, igrid=LOC_GRID, sur_s
     mlp_products = _mlp_products(fk)
     torch.cuda.synchronize()
     t_tr = time.perf_counter()
-    sur_loss = loc.trainSurrogate(nsamples=SUR_SAMPLES, steps=sur_steps, batch=SUR_BATCH, lr=2e-3,
+    sur_loss = loc.trainSurrogate(nsamples=SUR_SAMPLES, steps=sur_steps, batch=sur_batch, lr=sur_lr,
                                   vref=3000.0, seed=7)
     t_tr = time.perf_counter() - t_tr
     t_bd0 = time.perf_counter()
@@ -575,9 +579,9 @@ def bench_locate(fk, b, grids, stream, steps, nev=LOC_NEV, igrid=LOC_GRID, sur_s
                            "first / last layer, SiLU, Adam on the CUDA cores in FP32" % (
                                SUR_DEPTH, SUR_WIDTH, {0: "off: FP32 CUDA cores", 1: "BF16 operands, FP32 accumulators",
                                                       3: "split-BF16 operands, FP32 accumulators"}[mlp_products]),
-                "training": {"samples": SUR_SAMPLES, "steps": sur_steps, "batch": SUR_BATCH,
+                "training": {"samples": SUR_SAMPLES, "steps": sur_steps, "batch": sur_batch, "lr": sur_lr,
                              "seconds": t_tr, "final_mse_tau": sur_loss,
-                             "tflops": 3.0 * flops_row * sur_steps * SUR_BATCH / t_tr / 1e12},
+                             "tflops": 3.0 * flops_row * sur_steps * sur_batch / t_tr / 1e12},
                 "coarse_build": {"block_zxy": list(SUR_BLOCK), "seconds": t_bd, "seconds_first_build": t_bd0,
                                  "rows": ncoarse * NSRC, "method": "fused forward pass" if mlp_products == 1
                                  else "layer by layer",
@@ -606,6 +610,8 @@ def main():
                     help="solve only the 160x160x96 grid once and run the grid-search section")
     ap.add_argument("--locate-events", type=int, default=LOC_NEV)
     ap.add_argument("--surrogate-steps", type=int, default=SUR_STEPS)
+    ap.add_argument("--surrogate-batch", type=int, default=SUR_BATCH)
+    ap.add_argument("--surrogate-lr", type=float, default=SUR_LR)
     ap.add_argument("--slab-config", default=None,
                     help="staged,pairs,progress,blocks_per_sm for the 3D sweep kernels "
                          "(fteik_b200_setSlabConfig; default: chosen by the library's tuner)")
@@ -643,7 +649,8 @@ def main():
         b.solve()
         stream = torch.cuda.ExternalStream(fk.lib().fteik_b200_stream())
         res = bench_locate(fk, b, grids, stream, args.steps, nev=args.locate_events, igrid=1,
-                           sur_steps=args.surrogate_steps)
+                           sur_steps=args.surrogate_steps,
+                           sur_batch=args.surrogate_batch, sur_lr=args.surrogate_lr)
         print(json.dumps({"locate": res}), flush=True)
         b.finalize()
         return
@@ -757,7 +764,8 @@ def main():
     locate = None
     if not args.no_locate:
         locate = bench_locate(fk, b, grids, stream, args.steps, nev=args.locate_events,
-                              sur_steps=args.surrogate_steps)
+                              sur_steps=args.surrogate_steps,
+                           sur_batch=args.surrogate_batch, sur_lr=args.surrogate_lr)
 
     cpu = None
     batch_err = None

@@ -136,8 +136,6 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
     }
     Mesh<R> mesh;
     fk3::make_mesh<R>(mesh, g.dz, g.dx, g.dy);
-    Mesh<double> mesh64;
-    if (INIT) fk3::make_mesh<double>(mesh64, g.dz, g.dx, g.dy);
     const R HUGEV = (R)FK_HUGE;
     const int th = min(TY, ny - TY * P);             /* rows in this slab */
     const bool row = ty < th;
@@ -288,12 +286,15 @@ __device__ __forceinline__ bool slab_sweep(const fk3tw::Params &P_, const fk_gri
                         else if (lcart || sizeof(R) == 8)
                             r = fk3::init_node<R>(q, mesh, lcart, tv, te, tn, tev, ten, tnv, tnve, told, s1, s2,
                                                   s3, s4, s5, s6, s7, iz + 1, x + 1, y + 1, sz, sx, sy);
-                        else /* near-source spherical stencil in FP64 */
+                        else { /* near-source spherical stencil in FP64 (constants built here: few nodes) */
+                            Mesh<double> mesh64;
+                            fk3::make_mesh<double>(mesh64, g.dz, g.dx, g.dy);
                             r = (R)fk3::init_node<double>(
                                 q, mesh64, lcart, (double)tv, (double)te, (double)tn, (double)tev, (double)ten,
                                 (double)tnv, (double)tnve, (double)told, (double)s1, (double)s2, (double)s3,
                                 (double)s4, (double)s5, (double)s6, (double)s7, iz + 1, x + 1, y + 1, sz, sx,
                                 sy);
+                        }
                     }
                     if (r != told) {
                         ttp[i][cur.addr] = r;
@@ -368,8 +369,6 @@ __device__ __forceinline__ void slab_sweep_zrows(const fk_grid3d_t &g, R *tt, co
     const int loy = (sy > 0) ? max(1, q.ysi - 1) : max(1, ny - q.ysi - 1);
     Mesh<R> mesh;
     fk3::make_mesh<R>(mesh, g.dz, g.dx, g.dy);
-    Mesh<double> mesh64;
-    fk3::make_mesh<double>(mesh64, g.dz, g.dx, g.dy);
     const R HUGEV = (R)FK_HUGE;
     const R eps_r = (R)q.eps_t;
     const int Zr = nz - loz + 1;                     /* rows: logical z loz - 1 .. nz - 1 */
@@ -462,11 +461,14 @@ __device__ __forceinline__ void slab_sweep_zrows(const fk_grid3d_t &g, R *tt, co
                 else if (lcart || sizeof(R) == 8)
                     r = fk3::init_node<R>(q, mesh, lcart, tv, te, tn, tev, ten, tnv, tnve, told, s1, s2, s3, s4, s5,
                                           s6, s7, iz + 1, x + 1, y + 1, sz, sx, sy);
-                else
+                else {   /* near-source spherical stencil in FP64 (constants built here: few nodes) */
+                    Mesh<double> mesh64;
+                    fk3::make_mesh<double>(mesh64, g.dz, g.dx, g.dy);
                     r = (R)fk3::init_node<double>(q, mesh64, lcart, (double)tv, (double)te, (double)tn, (double)tev,
                                                   (double)ten, (double)tnv, (double)tnve, (double)told, (double)s1,
                                                   (double)s2, (double)s3, (double)s4, (double)s5, (double)s6,
                                                   (double)s7, iz + 1, x + 1, y + 1, sz, sx, sy);
+                }
                 if (r != told) tt[cur.addr] = r;
                 result = r;
             }
