@@ -62,6 +62,8 @@ static struct {
     float *coarse;           /* device [ntf][ldc] surrogate travel times */
     float *fine_blk;         /* device block-major copy of the exact tables */
     size_t fine_cap;         /* its size in floats */
+    size_t coarse_cap, bpack_cap;   /* sizes of coarse / bpack_c (floats / bytes) */
+    float *bx_in, *bx_dist, *bx_tau; /* build scratch: inputs, distances, outputs of a chunk */
     long long blk_gen;       /* table generation fine_blk was built from */
     void *bpack_c;
     int rc, k;
@@ -84,6 +86,7 @@ static void surrogate_free(void)
         if (SP.ev[k]) cudaEventDestroy(SP.ev[k]);
     fk_dfree(SP.sta_dev); fk_dfree(SP.coarse); fk_dfree(SP.bpack_c); fk_dfree(SP.flag_dev);
     fk_dfree(SP.fine_blk);
+    fk_dfree(SP.bx_in); fk_dfree(SP.bx_dist); fk_dfree(SP.bx_tau);
     fk_dfree(SP.sub_obs); fk_dfree(SP.sub_w); fk_dfree(SP.sub_elig);
     memset(&SP, 0, sizeof(SP));
 }
@@ -672,15 +675,24 @@ void fteik_b200_locate_buildSurrogate(int bz, int bx, int by, int *ierr)
     SP.ncy = (SP.ny + by - 1) / by;
     SP.ngrd_c = SP.ncz * SP.ncx * SP.ncy;
     SP.ldc = (SP.ngrd_c + 15) / 16 * 16;
-    fk_dfree(SP.coarse);
-    fk_dfree(SP.bpack_c);
-    SP.coarse = (float *)fk_dalloc(sizeof(float) * (size_t)SL.ntf * SP.ldc, who);
-    SP.bpack_c = fk_dalloc(fk_locate_tc_table_bytes(SP.ngrd_c), who);
+    /* a rebuild of the same shape reuses every buffer */
+    const size_t ncoarse = (size_t)SL.ntf * SP.ldc, nbpack = fk_locate_tc_table_bytes(SP.ngrd_c);
+    if (ncoarse != SP.coarse_cap || !SP.coarse) {
+        fk_dfree(SP.coarse);
+        SP.coarse = (float *)fk_dalloc(sizeof(float) * ncoarse, who);
+        SP.coarse_cap = SP.coarse ? ncoarse : 0;
+    }
+    if (nbpack != SP.bpack_cap || !SP.bpack_c) {
+        fk_dfree(SP.bpack_c);
+        SP.bpack_c = fk_dalloc(nbpack, who);
+        SP.bpack_cap = SP.bpack_c ? nbpack : 0;
+    }
     const long long nrow = (long long)SL.ntf * SP.ngrd_c;
     const long long chunk = 1 << 18;
-    float *x = (float *)fk_dalloc(sizeof(float) * 6 * (size_t)chunk, who);
-    float *dist = (float *)fk_dalloc(sizeof(float) * (size_t)chunk, who);
-    float *tau = (float *)fk_dalloc(sizeof(float) * (size_t)chunk, who);
+    if (!SP.bx_in) SP.bx_in = (float *)fk_dalloc(sizeof(float) * 6 * (size_t)chunk, who);
+    if (!SP.bx_dist) SP.bx_dist = (float *)fk_dalloc(sizeof(float) * (size_t)chunk, who);
+    if (!SP.bx_tau) SP.bx_tau = (float *)fk_dalloc(sizeof(float) * (size_t)chunk, who);
+    float *x = SP.bx_in, *dist = SP.bx_dist, *tau = SP.bx_tau;
     int e = (SP.coarse && SP.bpack_c && x && dist && tau) ? 0 : 1;
     cudaStream_t s = fk_stream();
     if (!e) e = (int)cudaMemsetAsync(SP.coarse, 0, sizeof(float) * (size_t)SL.ntf * SP.ldc, s);
@@ -702,7 +714,6 @@ void fteik_b200_locate_buildSurrogate(int bz, int bx, int by, int *ierr)
     if (!e) e = fk_locate_block_tables(SP.nz, SP.nx, SP.ny, bz, bx, by, SL.ntf, SL.ldgrd, SL.tables, SP.fine_blk, s);
     SP.blk_gen = SL.table_gen;
     if (!e) e = (int)cudaStreamSynchronize(s);
-    fk_dfree(x); fk_dfree(dist); fk_dfree(tau);
     if (fk_check(e, who)) return;
     SP.ready = true;
     *ierr = 0;

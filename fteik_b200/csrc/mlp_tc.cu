@@ -376,7 +376,12 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
 constexpr int FW = 256;                   /* hidden width */
 constexpr int F_ABLK = BM * 64 * 2;       /* 16 KB: one 64-wide K block of the A tile */
 constexpr int F_WBLK = FW * 64 * 2;       /* 32 KB: one K block of a layer's weights */
-constexpr int F_SMEM = 4 * F_ABLK + 4 * F_WBLK + 1024;
+/* layer 0's weights and biases in shared memory, [6 + 1][4 column quarters][66]
+ * (a quarter's 64 columns padded to 66 floats: the four quarters a warp
+ * reads fall in different banks) */
+constexpr int F_L0Q = 66;
+constexpr int F_L0 = 7 * 4 * F_L0Q * 4;
+constexpr int F_SMEM = 4 * F_ABLK + 4 * F_WBLK + F_L0 + 1024;
 constexpr int F_MAXH = 8;
 constexpr int F_NT = 512;                 /* 16 warps: 4 per TMEM lane quarter, 64 columns each */
 
@@ -435,6 +440,7 @@ __global__ void __launch_bounds__(F_NT, 1) mlp_fused_fwd_kernel(FusedNet net, co
     __shared__ float s_part[BM];
     uint8_t *A = reinterpret_cast<uint8_t *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t *W = A + 4 * F_ABLK;
+    float *l0 = reinterpret_cast<float *>(W + 4 * F_WBLK);   /* [k (6 weights, then the bias)][quarter][66] */
     const uint32_t a_s = (uint32_t)__cvta_generic_to_shared(A), w_s = (uint32_t)__cvta_generic_to_shared(W);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t bar_w = (uint32_t)__cvta_generic_to_shared(&bars[0]), bar_m = bar_w + 8;
@@ -449,6 +455,13 @@ __global__ void __launch_bounds__(F_NT, 1) mlp_fused_fwd_kernel(FusedNet net, co
                      "r"(TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    {
+        const float *w0 = net.w + net.woff[0], *b0 = net.w + net.boff[0];
+        for (int e = tid; e < 7 * FW; e += F_NT) {
+            const int k = e / FW, col = e % FW;
+            l0[(k * 4 + (col >> 6)) * F_L0Q + (col & 63)] = k < 6 ? w0[col * 6 + k] : b0[col];
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -474,17 +487,23 @@ __global__ void __launch_bounds__(F_NT, 1) mlp_fused_fwd_kernel(FusedNet net, co
             float xi[6];
 #pragma unroll
             for (int k = 0; k < 6; ++k) xi[k] = m < n ? x[m * 6 + k] : 0.0f;
-            const float *w0 = net.w + net.woff[0], *b0 = net.w + net.boff[0];
+            /* two columns per packed multiply-add: each lane of the pair is the
+             * scalar chain fmaf(x_k, w_k, acc) over k = 0 .. 5, as in the
+             * layer-by-layer GEMM */
+            const float *lq = l0 + h * F_L0Q;
 #pragma unroll 1
             for (int c = 0; c < 64; c += 8) {
                 float a[8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int col = h * 64 + c + j;
-                    float acc = 0.0f;
+                for (int j = 0; j < 8; j += 2) {
+                    float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll
-                    for (int k = 0; k < 6; ++k) acc = fmaf(xi[k], __ldg(w0 + col * 6 + k), acc);
-                    a[j] = silu_f(acc + __ldg(b0 + col));
+                    for (int k = 0; k < 6; ++k)
+                        acc = __ffma2_rn(make_float2(xi[k], xi[k]),
+                                         *reinterpret_cast<const float2 *>(lq + k * 4 * F_L0Q + c + j), acc);
+                    const float2 b = *reinterpret_cast<const float2 *>(lq + 6 * 4 * F_L0Q + c + j);
+                    a[j] = silu_f(acc.x + b.x);
+                    a[j + 1] = silu_f(acc.y + b.y);
                 }
                 put_a8(A, r, h * 64 + c, a);
             }
