@@ -186,6 +186,8 @@ _SIGS = {
     "fteik_b200_mlp_getTrainGraph": [_PI],
     "fteik_b200_mlp_setFusedForward": [c_int],
     "fteik_b200_mlp_getFusedForward": [_PI],
+    "fteik_b200_mlp_setAsyncStaging": [c_int],
+    "fteik_b200_mlp_getAsyncStaging": [_PI],
     "fteik_b200_locate_l2_noalloc": [c_int, c_int, c_int, ctypes.c_void_p, c_int, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_void_p, _PI],
@@ -291,6 +293,15 @@ def set_mlp_train_graph(on):
     old = c_int()
     lib().fteik_b200_mlp_getTrainGraph(byref(old))
     lib().fteik_b200_mlp_setTrainGraph(int(on))
+    return old.value
+
+
+def set_mlp_async_staging(on):
+    """Asynchronous (1) or synchronous (0) operand staging of the
+    tensor-core products; returns the previous value."""
+    old = c_int()
+    lib().fteik_b200_mlp_getAsyncStaging(byref(old))
+    lib().fteik_b200_mlp_setAsyncStaging(int(on))
     return old.value
 
 

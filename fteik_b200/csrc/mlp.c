@@ -16,10 +16,8 @@
 #include <string.h>
 
 int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta, const float *B, int ldb,
-                int tb, float *C, int ldc, const float *bias, int accumulate, float *C2, int act, cudaStream_t s);
-int fk_mlp_silu(size_t n, const float *z, float *a, cudaStream_t s);
-int fk_mlp_silu_bwd(size_t n, const float *z, const float *da, float *dz, cudaStream_t s);
-int fk_mlp_colsum(int M, int N, const float *dz, float *db, cudaStream_t s);
+                int tb, float *C, int ldc, const float *bias, int accumulate, float *C2, int act, float *colsum,
+                cudaStream_t s);
 int fk_mlp_mse(int n, const float *pred, const float *y, float *dpred, double *loss, cudaStream_t s);
 int fk_mlp_adam_sched(size_t n, float *w, const float *g, float *m, float *v, const float *sched,
                       const long long *tdev, float b1, float b2, float eps, cudaStream_t s);
@@ -30,6 +28,7 @@ void fk_mlp_set_tensor(int products);
 int fk_mlp_get_tensor(void);
 int fk_mlp_tc_status(cudaStream_t s);
 int *fk_mlp_tc_error_word(cudaStream_t s);
+void fk_mlp_set_async_staging(int on);
 int fk_mlp_forward_fused(const float *w, int nh, const long long *woff, const long long *boff, long long n,
                          const float *x, float *tau, unsigned char *wq, int *error, cudaStream_t s);
 
@@ -72,7 +71,7 @@ static struct {
     int cap;                           /* batch rows the buffers hold */
     float *x[MLP_MAXL + 1];            /* layer inputs; x[nlayer] = output */
     float *z[MLP_MAXL];                /* pre-activations */
-    float *dx, *dz, *dtmp;             /* backward scratch [cap][width] */
+    float *dz, *dtmp;                  /* backward scratch [cap][width] */
     double *loss_dev;
 } NN;
 
@@ -80,8 +79,8 @@ static void mlp_free_buffers(void)
 {
     for (int l = 0; l <= MLP_MAXL; l++) { fk_dfree(NN.x[l]); NN.x[l] = NULL; }
     for (int l = 0; l < MLP_MAXL; l++) { fk_dfree(NN.z[l]); NN.z[l] = NULL; }
-    fk_dfree(NN.dx); fk_dfree(NN.dz); fk_dfree(NN.dtmp);
-    NN.dx = NN.dz = NN.dtmp = NULL;
+    fk_dfree(NN.dz); fk_dfree(NN.dtmp);
+    NN.dz = NN.dtmp = NULL;
     NN.cap = 0;
 }
 
@@ -197,10 +196,9 @@ static int ensure_batch(int B)
         ok &= NN.z[l] != NULL;
     }
     const size_t wd = (size_t)B * (NN.width > MLP_IN ? NN.width : MLP_IN);
-    NN.dx = (float *)fk_dalloc(sizeof(float) * wd, "mlp");
     NN.dz = (float *)fk_dalloc(sizeof(float) * wd, "mlp");
     NN.dtmp = (float *)fk_dalloc(sizeof(float) * wd, "mlp");
-    ok &= NN.dx && NN.dz && NN.dtmp;
+    ok &= NN.dz && NN.dtmp;
     if (!ok) { mlp_free_buffers(); return 1; }
     NN.cap = B;
     return 0;
@@ -218,13 +216,13 @@ static int forward(int B, bool keep_z, cudaStream_t s)
         const bool last = l == NN.nlayer - 1;
         if (last)
             e = fk_mlp_gemm(B, out, in, NN.x[l], in, 0, NN.w + NN.woff[l], in, 1, NN.x[l + 1], out,
-                            NN.w + NN.boff[l], 0, NULL, 0, s);
+                            NN.w + NN.boff[l], 0, NULL, 0, NULL, s);
         else if (keep_z)
             e = fk_mlp_gemm(B, out, in, NN.x[l], in, 0, NN.w + NN.woff[l], in, 1, NN.z[l], out,
-                            NN.w + NN.boff[l], 0, NN.x[l + 1], 1, s);
+                            NN.w + NN.boff[l], 0, NN.x[l + 1], 1, NULL, s);
         else
             e = fk_mlp_gemm(B, out, in, NN.x[l], in, 0, NN.w + NN.woff[l], in, 1, NN.x[l + 1], out,
-                            NN.w + NN.boff[l], 0, NULL, 2, s);
+                            NN.w + NN.boff[l], 0, NULL, 2, NULL, s);
     }
     return e;
 }
@@ -232,20 +230,21 @@ static int forward(int B, bool keep_z, cudaStream_t s)
 /* Loss and gradient (into NN.g) of B rows with targets y (device). */
 static int forward_backward(int B, const float *y, cudaStream_t s)
 {
-    int e = cudaMemsetAsync(NN.loss_dev, 0, sizeof(double), s);
-    if (!e) e = forward(B, true, s);
+    int e = forward(B, true, s);
     const int L = NN.nlayer;
     /* d loss / d output */
     if (!e) e = fk_mlp_mse(B, NN.x[L], y, NN.dz, NN.loss_dev, s);
     for (int l = L - 1; l >= 0 && !e; l--) {
         const int in = NN.din[l], out = NN.dout[l];
-        /* NN.dz holds d loss / d z_l  [B][out] */
-        e = fk_mlp_gemm(out, in, B, NN.dz, out, 1, NN.x[l], in, 0, NN.g + NN.woff[l], in, NULL, 0, NULL, 0, s);
-        if (!e) e = fk_mlp_colsum(B, out, NN.dz, NN.g + NN.boff[l], s);
+        /* NN.dz holds d loss / d z_l  [B][out]: dW_l = dz^T x_l, and the
+         * bias gradient (the column sums of dz) from the same pass */
+        e = fk_mlp_gemm(out, in, B, NN.dz, out, 1, NN.x[l], in, 0, NN.g + NN.woff[l], in, NULL, 0, NULL, 0,
+                        NN.g + NN.boff[l], s);
         if (!e && l > 0) {
-            e = fk_mlp_gemm(B, in, out, NN.dz, out, 0, NN.w + NN.woff[l], in, 0, NN.dx, in, NULL, 0, NULL, 0,
-                            s);
-            if (!e) e = fk_mlp_silu_bwd((size_t)B * in, NN.z[l - 1], NN.dx, NN.dtmp, s);
+            /* d loss / d z_{l-1} = (dz W_l) silu'(z_{l-1}), the derivative
+             * applied in the product's epilogue */
+            e = fk_mlp_gemm(B, in, out, NN.dz, out, 0, NN.w + NN.woff[l], in, 0, NN.dtmp, in, NULL, 0, NN.z[l - 1],
+                            3, NULL, s);
             if (!e) { float *t = NN.dz; NN.dz = NN.dtmp; NN.dtmp = t; }
         }
     }
@@ -467,6 +466,14 @@ void fteik_b200_mlp_train(int n, const float x[], const float y[], int steps, in
 /* Inference on device rows (x [n][6] device) into tau (device). */
 void fteik_b200_mlp_setFusedForward(int on) { g_fused = on != 0; }
 void fteik_b200_mlp_getFusedForward(int *on) { *on = g_fused; }
+
+static int g_async_staging = 1;
+void fteik_b200_mlp_setAsyncStaging(int on)
+{
+    g_async_staging = on != 0;
+    fk_mlp_set_async_staging(g_async_staging);
+}
+void fteik_b200_mlp_getAsyncStaging(int *on) { *on = g_async_staging; }
 
 /* The fused forward pass applies: BF16 products, width 256, 1 to 8 hidden
  * layers, at least one full 128-row tile. */

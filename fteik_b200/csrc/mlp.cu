@@ -95,23 +95,203 @@ __global__ void __launch_bounds__(NT) gemm_kernel(int M, int N, int K, const flo
     }
 }
 
-/* C[m][n] (+)= sum over the split slices in order + bias[n]. */
+/* The output value v of element (m, n) of C, the activation applied as asked:
+ * act 0: C = v; act 1: C = v and C2 = silu(v) (the forward pass keeping the
+ * pre-activation); act 2: C = silu(v); act 3: C = v silu'(z) with z = C2
+ * (the backward pass: dz = da s (1 + z (1 - s)), s = sigmoid(z), as
+ * silu_bwd_kernel). */
+__device__ __forceinline__ void store_act(float *__restrict__ C, float *__restrict__ C2, size_t off, float v,
+                                          int act)
+{
+    if (act == 3) {
+        const float z = C2[off], s = fk_sigmoid(z);
+        C[off] = v * s * (1.0f + z * (1.0f - s));
+        return;
+    }
+    const float a = act ? fk_silu(v) : v;
+    C[off] = act == 2 ? a : v;
+    if (act == 1) C2[off] = a;
+}
+
+/* C[m][n] (+)= sum over the split slices in order + bias[n], activation as
+ * store_act; with db, also db[m] = sum over the slices in order of the
+ * column sums cs[z][m]. */
 __global__ void splitk_reduce_kernel(int M, int N, int split, const float *__restrict__ ws, float *__restrict__ C,
                                      int ldc, const float *__restrict__ bias, int accumulate, float *__restrict__ C2,
-                                     int act)
+                                     int act, const float *__restrict__ cs, float *__restrict__ db)
 {
-    const size_t n_el = (size_t)M * N;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n_el; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t n_el = (size_t)M * N, n_all = n_el + (db ? (size_t)M : 0);
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n_all; e += (size_t)gridDim.x * blockDim.x) {
+        if (e >= n_el) {
+            const int m = (int)(e - n_el);
+            float v = 0.0f;
+#pragma unroll 16
+            for (int z = 0; z < split; ++z) v += cs[(size_t)z * M + m];
+            db[m] = v;
+            continue;
+        }
         const int m = (int)(e / N), n = (int)(e % N);
         float v = 0.0f;
+#pragma unroll 16
         for (int z = 0; z < split; ++z) v += ws[(size_t)z * n_el + e];
         if (bias) v += bias[n];
-        float *c = C + (size_t)m * ldc + n;
-        if (accumulate) v = *c + v;
-        /* act 1: C = z and C2 = silu(z); act 2: C = silu(z) (as silu_kernel) */
-        const float a = act ? fk_silu(v) : v;
-        *c = act == 2 ? a : v;
-        if (act == 1) C2[(size_t)m * ldc + n] = a;
+        const size_t off = (size_t)m * ldc + n;
+        if (accumulate) v = C[off] + v;
+        store_act(C, C2, off, v, act);
+    }
+}
+
+/* The same sums for few outputs and many slices (the thin layers' weight
+ * gradients): one warp per output, lane l adding slices l, l + 32, ... in
+ * order, then a fixed butterfly over the lanes (the same order on every
+ * run).  No bias, accumulation or activation. */
+__global__ void splitk_reduce_warp_kernel(int M, int N, int split, const float *__restrict__ ws,
+                                          float *__restrict__ C, int ldc, const float *__restrict__ cs,
+                                          float *__restrict__ db)
+{
+    const size_t n_el = (size_t)M * N, n_all = n_el + (db ? (size_t)M : 0);
+    const size_t e = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (e >= n_all) return;
+    const bool is_db = e >= n_el;
+    const float *src = is_db ? cs + (e - n_el) : ws + e;
+    const size_t stride = is_db ? (size_t)M : n_el;
+    float v = 0.0f;
+#pragma unroll 4
+    for (int z = lane; z < split; z += 32) v += src[(size_t)z * stride];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) {
+        if (is_db) db[e - n_el] = v;
+        else C[(e / N) * ldc + e % N] = v;
+    }
+}
+
+/* Products with K <= 8 (the first layer, 6 inputs; the output layer's
+ * input gradient, K = 1), A[m][k]: thread n of a block of SK_N columns
+ * keeps B(., n) in registers and runs over SK_R rows, the multiply-adds in
+ * k order from zero as gemm_kernel, then the bias and the activation
+ * (store_act); stores are coalesced along n. */
+constexpr int SK_N = 128, SK_R = 32, SK_KMAX = 8;
+__global__ void __launch_bounds__(SK_N, 4) smallk_kernel(int M, int N, int K, const float *__restrict__ A, int lda,
+                                                      const float *__restrict__ B, int ldb, int tb,
+                                                      float *__restrict__ C, int ldc, const float *__restrict__ bias,
+                                                      int accumulate, float *__restrict__ C2, int act)
+{
+    const int n = blockIdx.x * SK_N + threadIdx.x;
+    if (n >= N) return;
+    float b[SK_KMAX];
+#pragma unroll
+    for (int k = 0; k < SK_KMAX; ++k) b[k] = k < K ? (tb ? B[(size_t)n * ldb + k] : B[(size_t)k * ldb + n]) : 0.0f;
+    const float bn = bias ? bias[n] : 0.0f;
+    for (int m0 = blockIdx.y * SK_R; m0 < M; m0 += gridDim.y * SK_R) {
+        const int m1 = min(M, m0 + SK_R);
+#pragma unroll 4
+        for (int m = m0; m < m1; ++m) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < SK_KMAX; ++k)
+                if (k < K) acc = fmaf(A[(size_t)m * lda + k], b[k], acc);
+            float v = acc + bn;
+            const size_t off = (size_t)m * ldc + n;
+            if (accumulate) v = C[off] + v;
+            store_act(C, C2, off, v, act);
+        }
+    }
+}
+
+/* Products with N = 1 (the output layer), A[m][k]: one thread per row, the
+ * multiply-adds in k order from zero as gemm_kernel; a block of 256
+ * threads brings 64 rows x 64 k of A into a [64][65] tile by coalesced
+ * loads (16 per thread, all in flight), then 64 of them run the rows'
+ * chains; B(k, 0) = B[k bs]. */
+constexpr int GV_R = 64, GV_K = 64, GV_NT = 256;
+__global__ void __launch_bounds__(GV_NT) gemv_kernel(int M, int K, const float *__restrict__ A, int lda,
+                                                     const float *__restrict__ B, int bs, float *__restrict__ C,
+                                                     int ldc, const float *__restrict__ bias, int accumulate)
+{
+    __shared__ float tile[GV_R][GV_K + 1];
+    __shared__ float sb[GV_K];
+    const int m0 = blockIdx.x * GV_R, t = threadIdx.x, c = t & (GV_K - 1), r0 = t / GV_K;
+    float acc = 0.0f;
+    for (int k0 = 0; k0 < K; k0 += GV_K) {
+        const int kn = min(GV_K, K - k0);
+        float v[GV_R * GV_K / GV_NT];
+#pragma unroll
+        for (int i = 0; i < GV_R * GV_K / GV_NT; ++i) {
+            const int m = m0 + r0 + i * (GV_NT / GV_K);
+            v[i] = (m < M && c < kn) ? A[(size_t)m * lda + k0 + c] : 0.0f;
+        }
+#pragma unroll
+        for (int i = 0; i < GV_R * GV_K / GV_NT; ++i) tile[r0 + i * (GV_NT / GV_K)][c] = v[i];
+        if (t < kn) sb[t] = B[(size_t)(k0 + t) * bs];
+        __syncthreads();
+        if (t < GV_R)
+            for (int k = 0; k < kn; ++k) acc = fmaf(tile[t][k], sb[k], acc);
+        __syncthreads();
+    }
+    const int m = m0 + t;
+    if (t < GV_R && m < M) {
+        const float v = acc + (bias ? bias[0] : 0.0f);
+        float *cp = C + (size_t)m * ldc;
+        *cp = accumulate ? *cp + v : v;
+    }
+}
+
+/* Weight gradients of the thin layers: C[m][n] = sum_k A[k lda + m]
+ * B[k ldb + n] with N <= 8 (BIG_M: one thread per m, B's row broadcast) or
+ * M <= 8 (one thread per n, A's row broadcast), K in slices of kchunk (one
+ * per blockIdx.y): the partial products go to ws[slice][M][N] and the
+ * column sums of A over the slice to cs[slice][M] (the bias gradient),
+ * each in k order; a reduction adds the slices in order.  SC: the small
+ * dimension when known at compile time (the surrogate's 6 inputs and 1
+ * output), else 0 (read from M or N). */
+constexpr int TS_MAX = 8;
+template <bool BIG_M, int SC>
+__global__ void __launch_bounds__(256) tn_small_kernel(int M, int N, int K, int kchunk, const float *__restrict__ A,
+                                                       int lda, const float *__restrict__ B, int ldb,
+                                                       float *__restrict__ ws, float *__restrict__ cs)
+{
+    constexpr int SM_ = SC ? SC : TS_MAX;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;   /* m (BIG_M) or n */
+    const int S = SC ? SC : (BIG_M ? N : M);
+    if (i >= (BIG_M ? M : N)) return;
+    const int kb = blockIdx.y * kchunk, ke = min(K, kb + kchunk);
+    float acc[SM_], sum[SM_];
+#pragma unroll
+    for (int j = 0; j < SM_; ++j) acc[j] = sum[j] = 0.0f;
+#pragma unroll 8
+    for (int k = kb; k < ke; ++k) {
+        if (BIG_M) {
+            const float a = A[(size_t)k * lda + i];
+            sum[0] += a;
+#pragma unroll
+            for (int j = 0; j < SM_; ++j)
+                if (j < S) acc[j] = fmaf(a, B[(size_t)k * ldb + j], acc[j]);
+        } else {
+            const float b = B[(size_t)k * ldb + i];
+#pragma unroll
+            for (int j = 0; j < SM_; ++j)
+                if (j < S) {
+                    const float a = A[(size_t)k * lda + j];
+                    acc[j] = fmaf(a, b, acc[j]);
+                    sum[j] += a;
+                }
+        }
+    }
+    float *w = ws + (size_t)blockIdx.y * M * N;
+#pragma unroll
+    for (int j = 0; j < SM_; ++j)
+        if (j < S) {
+            if (BIG_M) w[(size_t)i * N + j] = acc[j];
+            else w[(size_t)j * N + i] = acc[j];
+        }
+    if (cs) {
+        if (BIG_M) cs[(size_t)blockIdx.y * M + i] = sum[0];
+        else if (i == 0)
+#pragma unroll
+            for (int j = 0; j < SM_; ++j)
+                if (j < S) cs[(size_t)blockIdx.y * M + j] = sum[j];
     }
 }
 
@@ -140,6 +320,14 @@ __global__ void silu_bwd_kernel(size_t n, const float *__restrict__ z, const flo
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const float v = z[i], s = sigmoid(v);
         dz[i] = da[i] * s * (1.0f + v * (1.0f - s));
+    }
+}
+
+__global__ void silu_bwd_inplace_kernel(size_t n, const float *__restrict__ z, float *d)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float v = z[i], s = sigmoid(v);
+        d[i] = d[i] * s * (1.0f + v * (1.0f - s));
     }
 }
 
@@ -175,12 +363,14 @@ __global__ void colsum_final_kernel(int N, int nchunk, const float *__restrict__
     db[n] = s;
 }
 
-/* mean squared error over n outputs: dpred = 2 (pred - y) / n; loss sums
- * into a double by blocks */
+/* mean squared error over n outputs: dpred = 2 (pred - y) / n; the loss in
+ * a fixed order: block sums into part[], and the block that finishes last
+ * (a counter, reset by it) adds them in block order into *loss */
 __global__ void mse_kernel(int n, const float *__restrict__ pred, const float *__restrict__ y,
-                           float *__restrict__ dpred, double *__restrict__ loss)
+                           float *__restrict__ dpred, double *__restrict__ loss, double *part, unsigned *count)
 {
     __shared__ double red[256];
+    __shared__ bool last;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double l = 0.0;
     if (i < n) {
@@ -194,7 +384,20 @@ __global__ void mse_kernel(int n, const float *__restrict__ pred, const float *_
         if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x == 0) atomicAdd(loss, red[0]);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = red[0];
+        __threadfence();
+        last = atomicAdd(count, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double t = 0.0;
+#pragma unroll 8
+        for (unsigned b = 0; b < gridDim.x; ++b) t += reinterpret_cast<volatile double *>(part)[b];
+        *loss = t;
+        *count = 0;
+    }
 }
 
 __global__ void adam_kernel(size_t n, float *__restrict__ w, const float *__restrict__ g,
@@ -331,7 +534,7 @@ static int grid1d(size_t n) { size_t b = (n + 255) / 256; return (int)(b < 4096 
 
 extern "C" int fk_mlp_gemm_tc(int prod, int M, int N, int K, const float *A, int lda, int ta, const float *B,
                               int ldb, int tb, float *C, int ldc, const float *bias, int accumulate, float *C2,
-                              int act, int split, float *ws, int *error, cudaStream_t s);
+                              int act, int split, float *ws, float *colsum, int *error, cudaStream_t s);
 
 /* 0: every GEMM on the CUDA cores in FP32; 1 or 3: GEMMs with N and K of at
  * least 64 (the hidden layers) on the tensor cores with that many BF16
@@ -342,7 +545,6 @@ static int *g_tc_error = nullptr;
 extern "C" void fk_mlp_set_tensor(int products) { g_tensor = products; }
 extern "C" int fk_mlp_get_tensor(void) { return g_tensor; }
 
-/* the tensor-core kernels' error word (a wait that timed out), read and cleared */
 /* the tensor-core kernels' error word (allocated on first use, outside any capture) */
 extern "C" int *fk_mlp_tc_error_word(cudaStream_t s)
 {
@@ -354,6 +556,7 @@ extern "C" int *fk_mlp_tc_error_word(cudaStream_t s)
     return g_tc_error;
 }
 
+/* the tensor-core kernels' error word (a wait that timed out), read and cleared */
 extern "C" int fk_mlp_tc_status(cudaStream_t s)
 {
     if (!g_tc_error) return 0;
@@ -367,6 +570,8 @@ extern "C" int fk_mlp_tc_status(cudaStream_t s)
 static float *g_ws = nullptr;
 static size_t g_ws_cap = 0;
 
+/* split-K / slice workspace; grows on a training run's first (eager) step,
+ * never during a capture */
 static int workspace(size_t need, cudaStream_t s)
 {
     if (need <= g_ws_cap) return 0;
@@ -380,55 +585,116 @@ static int workspace(size_t need, cudaStream_t s)
     return 0;
 }
 
+extern "C" int fk_mlp_colsum(int M, int N, const float *dz, float *db, cudaStream_t s);
+
+/* C = A B (+ bias) with the activation act (store_act) and, with colsum
+ * (weight gradients, ta = 1 and lda = M only), colsum[m] = sum_k A(m, k)
+ * (the bias gradient).  Thin products go to their own CUDA-core kernels
+ * (K <= 8; N = 1; weight gradients with M or N <= 8), the hidden layers'
+ * to the tensor cores (g_tensor), the rest to gemm_kernel; K is split
+ * over CTAs only when it is long (the weight gradients, K = the batch),
+ * the slices added in a fixed order, so every result is reproducible. */
 extern "C" int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta, const float *B, int ldb,
                            int tb, float *C, int ldc, const float *bias, int accumulate, float *C2, int act,
-                           cudaStream_t s)
+                           float *colsum, cudaStream_t s)
 {
     if (M <= 0 || N <= 0) return 0;
-    if (g_tensor && N >= 64 && N <= 256 && K >= 64 && M >= 64) {
-        if (!g_tc_error) {
-            cudaError_t e = cudaMalloc((void **)&g_tc_error, sizeof(int));
-            if (e == cudaSuccess) e = cudaMemsetAsync(g_tc_error, 0, sizeof(int), s);
-            if (e != cudaSuccess) return (int)e;
-        }
-        /* few 128-row tiles for the 148 SMs (weight gradients, K = the batch;
-         * products of a small batch): split K over CTAs */
-        const int mt = (M + 127) / 128;
-        int split = 1;
-        while (mt * split < 148 && K / (split * 2) >= 128) split *= 2;
-        if (split > 1) {
-            const int e = workspace((size_t)split * M * N, s);
-            if (e) return e;
-        }
-        int e = fk_mlp_gemm_tc(g_tensor, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate, C2, act, split,
-                               g_ws, g_tc_error, s);
-        if (e || split == 1) return e;
-        splitk_reduce_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>(M, N, split, g_ws, C, ldc, bias, accumulate, C2,
-                                                                   act);
+    if ((colsum && (!ta || lda != M)) || (act && !C2 && act != 2) || act < 0 || act > 3)
+        return (int)cudaErrorInvalidValue;
+    if (!ta && N == 1 && act == 0) {
+        gemv_kernel<<<(M + GV_R - 1) / GV_R, GV_NT, 0, s>>>(M, K, A, lda, B, tb ? 1 : ldb, C, ldc, bias,
+                                                            accumulate);
         return (int)cudaGetLastError();
     }
+    if (!ta && K <= SK_KMAX) {
+        const int rb = (M + SK_R - 1) / SK_R;
+        smallk_kernel<<<dim3((N + SK_N - 1) / SK_N, rb < 65535 ? rb : 65535), SK_N, 0, s>>>(
+            M, N, K, A, lda, B, ldb, tb, C, ldc, bias, accumulate, C2, act);
+        return (int)cudaGetLastError();
+    }
+    if (ta && !tb && (N <= TS_MAX || M <= TS_MAX)) {
+        const bool big_m = N <= TS_MAX;
+        const int nb = ((big_m ? M : N) + 255) / 256;
+        int nchunk = 1;
+        while (nb * nchunk < 148 && K / (nchunk * 2) >= 64) nchunk *= 2;
+        const int kchunk = (K + nchunk - 1) / nchunk;
+        const int e = workspace((size_t)nchunk * M * N + (size_t)nchunk * M, s);
+        if (e) return e;
+        float *cs = g_ws + (size_t)nchunk * M * N;
+        const dim3 grid(nb, nchunk);
+        if (big_m && N == 6)
+            tn_small_kernel<true, 6><<<grid, 256, 0, s>>>(M, N, K, kchunk, A, lda, B, ldb, g_ws, cs);
+        else if (big_m)
+            tn_small_kernel<true, 0><<<grid, 256, 0, s>>>(M, N, K, kchunk, A, lda, B, ldb, g_ws, cs);
+        else if (M == 1)
+            tn_small_kernel<false, 1><<<grid, 256, 0, s>>>(M, N, K, kchunk, A, lda, B, ldb, g_ws, cs);
+        else
+            tn_small_kernel<false, 0><<<grid, 256, 0, s>>>(M, N, K, kchunk, A, lda, B, ldb, g_ws, cs);
+        const size_t nout = (size_t)M * N + M;
+        if (!bias && !accumulate && !act && ldc >= N)
+            splitk_reduce_warp_kernel<<<(unsigned)((nout * 32 + 255) / 256), 256, 0, s>>>(M, N, nchunk, g_ws, C, ldc,
+                                                                                          cs, colsum);
+        else
+            splitk_reduce_kernel<<<grid1d(nout), 256, 0, s>>>(M, N, nchunk, g_ws, C, ldc, bias, accumulate, C2, act,
+                                                              cs, colsum);
+        return (int)cudaGetLastError();
+    }
+    if (g_tensor && N >= 64 && N <= 256 && K >= 64 && M >= 64) {
+        if (!fk_mlp_tc_error_word(s)) return (int)cudaErrorMemoryAllocation;
+        /* long K with few 128-row tiles for the 148 SMs (the weight
+         * gradients, K = the batch): split K, each slice 256 or more */
+        const int mt = (M + 127) / 128;
+        int split = 1;
+        while (mt * split < 148 && K / (split * 2) >= 256) split *= 2;
+        const bool cs_fused = colsum && K % 64 == 0;
+        float *cs = nullptr;
+        if (split > 1) {
+            const int e = workspace((size_t)split * M * N + (cs_fused ? (size_t)split * M : 0), s);
+            if (e) return e;
+            if (cs_fused) cs = g_ws + (size_t)split * M * N;
+        } else if (cs_fused) {
+            cs = colsum;
+        }
+        int e = fk_mlp_gemm_tc(g_tensor, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate, C2, act, split,
+                               g_ws, cs, g_tc_error, s);
+        if (!e && split > 1) {
+            splitk_reduce_kernel<<<grid1d((size_t)M * N + (cs_fused ? M : 0)), 256, 0, s>>>(
+                M, N, split, g_ws, C, ldc, bias, accumulate, C2, act, cs, cs_fused ? colsum : nullptr);
+            e = (int)cudaGetLastError();
+        }
+        if (!e && colsum && !cs_fused) e = fk_mlp_colsum(K, M, A, colsum, s);
+        return e;
+    }
+    if (act && ldc != N) return (int)cudaErrorInvalidValue;   /* the activation pass needs a contiguous C */
     const int tiles = ((N + TN - 1) / TN) * ((M + TM - 1) / TM);
     /* long K with few output tiles (weight gradients): split K over CTAs */
     int split = 1;
     while (tiles * split < 128 && K / (split * 2) >= 256) split *= 2;
     dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM, split);
+    cudaError_t e;
     if (split == 1) {
         gemm_kernel<<<grid, NT, 0, s>>>(M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate);
-        if (act == 1 && ldc == N)   /* the activation as a second pass over the contiguous C */
+        /* the activation as a second pass over the contiguous C */
+        if (act == 1)
             silu_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>((size_t)M * N, C, C2);
-        else if (act == 2 && ldc == N)
+        else if (act == 2)
             silu_inplace_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>((size_t)M * N, C);
-        return (int)cudaGetLastError();
+        else if (act == 3)
+            silu_bwd_inplace_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>((size_t)M * N, C2, C);
+        e = cudaGetLastError();
+    } else {
+        /* partial tiles into the workspace, then an ordered reduction */
+        const int ew = workspace((size_t)split * M * N, s);
+        if (ew) return ew;
+        gemm_kernel<<<grid, NT, 0, s>>>(M, N, K, A, lda, ta, B, ldb, tb, g_ws, N, nullptr, 0);
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            splitk_reduce_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>(M, N, split, g_ws, C, ldc, bias, accumulate,
+                                                                       C2, act, nullptr, nullptr);
+        e = cudaGetLastError();
     }
-    /* partial tiles into the workspace, then an ordered reduction */
-    const int ew = workspace((size_t)split * M * N, s);
-    if (ew) return ew;
-    gemm_kernel<<<grid, NT, 0, s>>>(M, N, K, A, lda, ta, B, ldb, tb, g_ws, N, nullptr, 0);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return (int)e;
-    splitk_reduce_kernel<<<grid1d((size_t)M * N), 256, 0, s>>>(M, N, split, g_ws, C, ldc, bias, accumulate, C2,
-                                                               act);
-    return (int)cudaGetLastError();
+    if (e == cudaSuccess && colsum) return fk_mlp_colsum(K, M, A, colsum, s);
+    return (int)e;
 }
 
 extern "C" int fk_mlp_silu(size_t n, const float *z, float *a, cudaStream_t s)
@@ -464,9 +730,28 @@ extern "C" int fk_mlp_colsum(int M, int N, const float *dz, float *db, cudaStrea
     return (int)cudaGetLastError();
 }
 
+static double *g_mse_part = nullptr;
+static unsigned *g_mse_count = nullptr;
+static int g_mse_cap = 0;
+
+/* *loss = the mean squared error (written, not added) */
 extern "C" int fk_mlp_mse(int n, const float *pred, const float *y, float *dpred, double *loss, cudaStream_t s)
 {
-    mse_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, pred, y, dpred, loss);
+    const int nb = (n + 255) / 256;
+    if (nb > g_mse_cap) {   /* grows on a training run's first (eager) step, never during a capture */
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess && g_mse_part) e = cudaFree(g_mse_part);
+        g_mse_part = nullptr;
+        g_mse_cap = 0;
+        if (e == cudaSuccess) e = cudaMalloc((void **)&g_mse_part, sizeof(double) * nb);
+        if (e == cudaSuccess && !g_mse_count) {
+            e = cudaMalloc((void **)&g_mse_count, sizeof(unsigned));
+            if (e == cudaSuccess) e = cudaMemsetAsync(g_mse_count, 0, sizeof(unsigned), s);
+        }
+        if (e != cudaSuccess) return (int)e;
+        g_mse_cap = nb;
+    }
+    mse_kernel<<<nb, 256, 0, s>>>(n, pred, y, dpred, loss, g_mse_part, g_mse_count);
     return (int)cudaGetLastError();
 }
 

@@ -32,6 +32,7 @@ namespace fkmtc {
 
 constexpr int BM = 128, BN = 256, BK = 64;
 constexpr int NT = 256;
+static_assert(NT == BN && NT == 2 * BM, "the staging maps a thread to one B row and half an A row");
 constexpr int A_TILE = BM * BK * 2;   /* 16 KB of BF16 */
 constexpr int B_TILE = BN * BK * 2;   /* 32 KB */
 constexpr uint32_t TMEM_COLS = 256;
@@ -42,12 +43,23 @@ constexpr long long WAIT_LIMIT = 1ll << 24;
 constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                            ((uint32_t)(BM >> 4) << 24);
 
+/* FP32 half-stages of the asynchronous staging: 32 k of A (128 rows) and
+ * B (256 columns) as copied from global memory */
+constexpr int HK = 32;
+constexpr int FA_BYTES = BM * HK * 4;   /* 16 KB */
+constexpr int FB_BYTES = BN * HK * 4;   /* 32 KB */
+constexpr int FSTAGE = FA_BYTES + FB_BYTES;
+
 template <int PROD>
 struct Cfg {
     static constexpr int NP = PROD == 3 ? 2 : 1;          /* hi (+ lo) copies */
     static constexpr int STAGE = NP * (A_TILE + B_TILE);
     static constexpr int SMEM = 2 * STAGE + 1024;         /* + alignment slack */
+    /* asynchronous staging: a ring of NS FP32 half-stages and one BF16 stage */
+    static constexpr int NS = PROD == 3 ? 2 : 3;
+    static constexpr int SMEM_ASYNC = NS * FSTAGE + STAGE + 1024;
 };
+static_assert(BM * 129 * 4 <= 2 * FSTAGE && BM * 129 * 4 <= 2 * Cfg<1>::STAGE, "the epilogue tile fits the stages");
 
 /* byte offset of element (row, k) in a swizzled K-major tile (rows of 128 B) */
 __device__ __forceinline__ uint32_t swz(int row, int k)
@@ -152,11 +164,17 @@ __device__ __forceinline__ void put8(uint8_t *hi, uint8_t *lo, uint32_t off, flo
 
 /* Stage the K block [k0, k0 + 64) of A (rows m0 ..) and B (columns n0 ..);
  * out-of-range elements are zero.  Rows with k contiguous in memory move in
- * 16-byte loads when the whole block is in range and aligned. */
+ * 16-byte loads when the whole block is in range and aligned.  Operands
+ * with m (n) contiguous move, when the whole block is in range, in units
+ * of one row and 8 consecutive k: a warp's 32 units are 32 consecutive
+ * rows, so each of a unit's 8 loads is one coalesced 128-byte segment and
+ * the 8 values fill one 16-byte swizzle unit.  cs (A with m contiguous and
+ * a full block only): the thread's A values are added to *cs, k in order
+ * (the thread's row is t mod 128 in every block). */
 template <int PROD>
 __device__ __forceinline__ void stage(uint8_t *sA, uint8_t *sB, int M, int N, int K, const float *__restrict__ A,
                                       int lda, int ta, const float *__restrict__ B, int ldb, int tb, int m0, int n0,
-                                      int k0, int k1)
+                                      int k0, int k1, float *cs)
 {
     uint8_t *aLo = sA + A_TILE, *bLo = sB + B_TILE;
     const int t = threadIdx.x;
@@ -169,6 +187,21 @@ __device__ __forceinline__ void stage(uint8_t *sA, uint8_t *sB, int M, int N, in
             float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
             if (m < M) { a = src[2 * c]; b = src[2 * c + 1]; }
             put8<PROD>(sA, aLo, swz(row, kb + 8 * c), a, b);
+        }
+    } else if (ta && kfull) {
+        const int row = t & (BM - 1), m = m0 + row;
+#pragma unroll
+        for (int j = 0; j < BM * (BK / 8) / NT; ++j) {
+            const int g = (t >> 7) + 2 * j;
+            const float *src = A + (size_t)(k0 + 8 * g) * lda + m;
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = m < M ? src[(size_t)i * lda] : 0.0f;
+            if (cs)
+#pragma unroll
+                for (int i = 0; i < 8; ++i) *cs += v[i];
+            put8<PROD>(sA, aLo, swz(row, 8 * g), make_float4(v[0], v[1], v[2], v[3]),
+                       make_float4(v[4], v[5], v[6], v[7]));
         }
     } else if (!ta) {
         /* A[m][k], k contiguous: thread -> row t / 2, 32 consecutive k */
@@ -198,6 +231,17 @@ __device__ __forceinline__ void stage(uint8_t *sA, uint8_t *sB, int M, int N, in
             if (n < N) { a = src[2 * c]; b = src[2 * c + 1]; }
             put8<PROD>(sB, bLo, swz(t, 8 * c), a, b);
         }
+    } else if (!tb && kfull) {
+        const int n = n0 + t;
+#pragma unroll 2
+        for (int g = 0; g < BK / 8; ++g) {
+            const float *src = B + (size_t)(k0 + 8 * g) * ldb + n;
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = n < N ? src[(size_t)i * ldb] : 0.0f;
+            put8<PROD>(sB, bLo, swz(t, 8 * g), make_float4(v[0], v[1], v[2], v[3]),
+                       make_float4(v[4], v[5], v[6], v[7]));
+        }
     } else if (tb) {
         /* B[n][k], k contiguous: thread -> row n = t, 64 consecutive k */
         const int n = n0 + t;
@@ -221,18 +265,136 @@ __device__ __forceinline__ void stage(uint8_t *sA, uint8_t *sB, int M, int N, in
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+/* ---- asynchronous staging ---------------------------------------------
+ * The FP32 operands come in by 16-byte cp.async copies (zero-filled outside
+ * the matrices) into a ring of NS half-stages of 32 k, NS - 1 of them in
+ * flight ahead of the one being converted, so global-memory latency is
+ * hidden behind the conversion and the MMAs; every thread then converts a
+ * landed half-stage into the BF16 stage exactly as stage() would (same
+ * roundings, same swizzled layout, same order of the column sums).
+ * Layouts of a half-stage: a k-contiguous operand as rows of 32 values
+ * (128 B), chunk c of row r at chunk c ^ (r mod 8) (conflict-free 16-byte
+ * reads of 8 consecutive rows); an m- (n-) contiguous operand as 32 rows of
+ * k, 128 (256) values each.  Needs 16-byte aligned operands, leading
+ * dimensions and contiguous extents that are multiples of 4. */
+__device__ __forceinline__ void cp16(uint32_t dst, const float *src, bool ok)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(ok ? 16 : 0) : "memory");
+}
+
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N_>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N_) : "memory"); }
+
+/* copies of the half-stage k in [k0, k0 + 32) into the ring slot at f */
+__device__ __forceinline__ void issue_half(uint32_t f, int M, int N, const float *__restrict__ A, int lda, int ta,
+                                           const float *__restrict__ B, int ldb, int tb, int m0, int n0, int k0,
+                                           int k1)
+{
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int j = 0; j < FA_BYTES / 16 / NT; ++j) {
+        const int q = t + NT * j;
+        if (!ta) {
+            const int r = q >> 3, c = q & 7, m = m0 + r, k = k0 + 4 * c;
+            const bool ok = m < M && k < k1;
+            cp16(f + r * 128 + ((c ^ (r & 7)) << 4), ok ? A + (size_t)m * lda + k : A, ok);
+        } else {
+            const int r = q >> 5, c = q & 31, m = m0 + 4 * c, k = k0 + r;
+            const bool ok = m < M && k < k1;
+            cp16(f + r * 512 + c * 16, ok ? A + (size_t)k * lda + m : A, ok);
+        }
+    }
+    f += FA_BYTES;
+#pragma unroll
+    for (int j = 0; j < FB_BYTES / 16 / NT; ++j) {
+        const int q = t + NT * j;
+        if (tb) {
+            const int r = q >> 3, c = q & 7, n = n0 + r, k = k0 + 4 * c;
+            const bool ok = n < N && k < k1;
+            cp16(f + r * 128 + ((c ^ (r & 7)) << 4), ok ? B + (size_t)n * ldb + k : B, ok);
+        } else {
+            const int r = q >> 6, c = q & 63, n = n0 + 4 * c, k = k0 + r;
+            const bool ok = n < N && k < k1;
+            cp16(f + r * 1024 + c * 16, ok ? B + (size_t)k * ldb + n : B, ok);
+        }
+    }
+}
+
+/* a landed half-stage (slot f) into half hh (k 32 hh ..) of the BF16 stage */
 template <int PROD>
+__device__ __forceinline__ void convert_half(const uint8_t *f, uint8_t *sA, uint8_t *sB, int ta, int tb, int hh,
+                                             float *cs)
+{
+    uint8_t *aLo = sA + A_TILE, *bLo = sB + B_TILE;
+    const float *fA = reinterpret_cast<const float *>(f), *fB = reinterpret_cast<const float *>(f + FA_BYTES);
+    const int t = threadIdx.x, row = t & (BM - 1);
+#pragma unroll
+    for (int j = 0; j < BM * (HK / 8) / NT; ++j) {
+        const int g = (t >> 7) + 2 * j;
+        float v[8];
+        if (!ta) {
+            const float4 a = *reinterpret_cast<const float4 *>(fA + row * 32 + (((2 * g) ^ (row & 7)) << 2));
+            const float4 b = *reinterpret_cast<const float4 *>(fA + row * 32 + (((2 * g + 1) ^ (row & 7)) << 2));
+            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = fA[(8 * g + i) * BM + row];
+            if (cs)
+#pragma unroll
+                for (int i = 0; i < 8; ++i) *cs += v[i];
+        }
+        put8<PROD>(sA, aLo, swz(row, HK * hh + 8 * g), make_float4(v[0], v[1], v[2], v[3]),
+                   make_float4(v[4], v[5], v[6], v[7]));
+    }
+#pragma unroll
+    for (int g = 0; g < HK / 8; ++g) {
+        float v[8];
+        if (tb) {
+            const float4 a = *reinterpret_cast<const float4 *>(fB + t * 32 + (((2 * g) ^ (t & 7)) << 2));
+            const float4 b = *reinterpret_cast<const float4 *>(fB + t * 32 + (((2 * g + 1) ^ (t & 7)) << 2));
+            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = fB[(8 * g + i) * BN + t];
+        }
+        put8<PROD>(sB, bLo, swz(t, HK * hh + 8 * g), make_float4(v[0], v[1], v[2], v[3]),
+                   make_float4(v[4], v[5], v[6], v[7]));
+    }
+}
+
+/* the MMAs of one BF16 stage (K 64), accumulating unless first */
+template <int PROD>
+__device__ __forceinline__ void issue_mmas(uint32_t tmem, const uint8_t *sA, const uint8_t *sB, bool first)
+{
+    const uint32_t a_hi = (uint32_t)__cvta_generic_to_shared(sA), a_lo = a_hi + A_TILE;
+    const uint32_t b_hi = (uint32_t)__cvta_generic_to_shared(sB), b_lo = b_hi + B_TILE;
+#pragma unroll
+    for (int kk = 0; kk < BK / 16; ++kk) {
+        const uint32_t ko = (uint32_t)kk * 32u;
+        mma_bf16(tmem, sdesc_sw128(a_hi + ko), sdesc_sw128(b_hi + ko), (!first || kk > 0) ? 1u : 0u);
+        if (PROD == 3) {
+            mma_bf16(tmem, sdesc_sw128(a_hi + ko), sdesc_sw128(b_lo + ko), 1u);
+            mma_bf16(tmem, sdesc_sw128(a_lo + ko), sdesc_sw128(b_hi + ko), 1u);
+        }
+    }
+}
+
+template <int PROD, bool ASYNC>
 __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, const float *__restrict__ A, int lda,
                                                         int ta, const float *__restrict__ B, int ldb, int tb,
                                                         float *__restrict__ C, int ldc,
                                                         const float *__restrict__ bias, int accumulate,
-                                                        float *__restrict__ C2, int act, int kchunk, int *error)
+                                                        float *__restrict__ C2, int act, int kchunk,
+                                                        float *__restrict__ colsum, int *error)
 {
     using G = Cfg<PROD>;
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
+    __shared__ float s_cs[BM];
     uint8_t *base = reinterpret_cast<uint8_t *>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int kb = blockIdx.z * kchunk, ke = min(K, kb + kchunk);
@@ -257,45 +419,82 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
     tc_fence_after();
     const uint32_t tmem = s_tmem;
     int committed = 0;
-    for (int b = 0; b < nkb; ++b) {
-        const int buf = b & 1;
-        uint8_t *sA = base + buf * G::STAGE;
-        uint8_t *sB = sA + G::NP * A_TILE;
-        if (b >= 2 && !mbar_wait(bar0 + 8u * buf, ((b - 2) >> 1) & 1)) {   /* the MMAs of b - 2 read this stage */
-            if (threadIdx.x == 0) { atomicCAS(error, 0, 1); s_fail = 1; }
-        }
-        __syncthreads();
-        if (s_fail) break;
-        stage<PROD>(sA, sB, M, N, K, A, lda, ta, B, ldb, tb, m0, n0, kb + b * BK, ke);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            tc_fence_after();
-            const uint32_t a_hi = (uint32_t)__cvta_generic_to_shared(sA), a_lo = a_hi + A_TILE;
-            const uint32_t b_hi = (uint32_t)__cvta_generic_to_shared(sB), b_lo = b_hi + B_TILE;
+    uint32_t last_bar = bar0, last_par = 0;   /* the barrier and parity of the last commit */
+    float cs = 0.0f;   /* colsum: this thread's A values (row t mod 128) */
+    if constexpr (ASYNC) {
+        const uint32_t ring = (uint32_t)__cvta_generic_to_shared(base);
+        uint8_t *sA = base + G::NS * FSTAGE, *sB = sA + G::NP * A_TILE;
+        const int nh = 2 * nkb;
 #pragma unroll
-            for (int kk = 0; kk < BK / 16; ++kk) {
-                const uint32_t ko = (uint32_t)kk * 32u;
-                mma_bf16(tmem, sdesc_sw128(a_hi + ko), sdesc_sw128(b_hi + ko), (b > 0 || kk > 0) ? 1u : 0u);
-                if (PROD == 3) {
-                    mma_bf16(tmem, sdesc_sw128(a_hi + ko), sdesc_sw128(b_lo + ko), 1u);
-                    mma_bf16(tmem, sdesc_sw128(a_lo + ko), sdesc_sw128(b_hi + ko), 1u);
-                }
-            }
-            mma_commit(bar0 + 8u * buf);
+        for (int h = 0; h < G::NS - 1; ++h) {
+            if (h < nh) issue_half(ring + h * FSTAGE, M, N, A, lda, ta, B, ldb, tb, m0, n0, kb + h * HK, ke);
+            cp_commit();
         }
-        committed = b + 1;
+        for (int h = 0; h < nh; ++h) {
+            const int b = h >> 1, hh = h & 1;
+            cp_wait<G::NS - 2>();   /* this thread's copies of half-stage h have landed */
+            __syncthreads();        /* everyone's have; slot (h - 1) mod NS is converted */
+            if (s_fail) break;
+            {
+                const int hn = h + G::NS - 1;
+                if (hn < nh)
+                    issue_half(ring + (hn % G::NS) * FSTAGE, M, N, A, lda, ta, B, ldb, tb, m0, n0, kb + hn * HK, ke);
+                cp_commit();
+            }
+            /* the MMAs of stage b - 1 read the BF16 stage */
+            if (hh == 0 && b > 0 && !mbar_wait(bar0, (b - 1) & 1)) {
+                atomicCAS(error, 0, 1);
+                s_fail = 1;
+                continue;
+            }
+            convert_half<PROD>(base + (h % G::NS) * FSTAGE, sA, sB, ta, tb, hh, colsum ? &cs : nullptr);
+            if (hh == 1) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncthreads();
+                if (s_fail) break;
+                if (threadIdx.x == 0) {
+                    tc_fence_after();
+                    issue_mmas<PROD>(tmem, sA, sB, b == 0);
+                    mma_commit(bar0);
+                }
+                committed = b + 1;
+                last_par = (uint32_t)(b & 1);
+            }
+        }
+        cp_wait<0>();
+    } else {
+        for (int b = 0; b < nkb; ++b) {
+            const int buf = b & 1;
+            uint8_t *sA = base + buf * G::STAGE;
+            uint8_t *sB = sA + G::NP * A_TILE;
+            if (b >= 2 && !mbar_wait(bar0 + 8u * buf, ((b - 2) >> 1) & 1)) {   /* the MMAs of b - 2 read this stage */
+                if (threadIdx.x == 0) { atomicCAS(error, 0, 1); s_fail = 1; }
+            }
+            __syncthreads();
+            if (s_fail) break;
+            stage<PROD>(sA, sB, M, N, K, A, lda, ta, B, ldb, tb, m0, n0, kb + b * BK, ke, colsum ? &cs : nullptr);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                tc_fence_after();
+                issue_mmas<PROD>(tmem, sA, sB, b == 0);
+                mma_commit(bar0 + 8u * buf);
+            }
+            committed = b + 1;
+            last_bar = bar0 + 8u * buf;
+            last_par = (uint32_t)((b >> 1) & 1);
+        }
     }
     /* every MMA of this CTA has completed: the last commit covers them all */
     bool ok = !s_fail;
-    if (committed > 0) {
-        const int last = committed - 1;
-        if (!mbar_wait(bar0 + 8u * (last & 1), (last >> 1) & 1)) {
-            ok = false;
-            atomicCAS(error, 0, 2);
-        }
+    if (committed > 0 && !mbar_wait(last_bar, last_par)) {
+        ok = false;
+        atomicCAS(error, 0, 2);
     }
+    if (colsum && threadIdx.x >= BM) s_cs[threadIdx.x - BM] = cs;
     ok = __syncthreads_and(ok) != 0;   /* the epilogue's barriers need every thread on one path */
     tc_fence_after();
+    if (colsum && threadIdx.x < BM && m0 + (int)threadIdx.x < M)
+        colsum[(size_t)blockIdx.z * M + m0 + threadIdx.x] = cs + s_cs[threadIdx.x];
     if (ok && committed == 0 && gridDim.z > 1) {
         /* a split-K slice past the end of K: its partial tile is zero */
         for (int e = threadIdx.x; e < BM * BN; e += NT) {
@@ -325,25 +524,46 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
                 }
             }
             __syncthreads();
-            for (int rr = warp; rr < BM; rr += NT / 32) {
-                const int m = m0 + rr;
-                if (m >= M) break;
+            /* a warp stores rows warp + 8 j; four of them at a time, their
+             * act-3 inputs z loaded first (16 loads in flight) */
+            for (int r0 = warp; r0 < BM; r0 += 4 * (NT / 32)) {
+                float zv[4][4];
+                if (act == 3) {
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int n = n0 + p * 128 + i * 32 + lane;
-                    if (n >= N) continue;
-                    float v = tile[rr * 129 + i * 32 + lane];
-                    if (gridDim.z > 1) {
-                        C[((size_t)blockIdx.z * M + m) * N + n] = v;   /* split-K partial tile */
-                        continue;
+                    for (int j = 0; j < 4; ++j)
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const int m = m0 + r0 + j * (NT / 32), n = n0 + p * 128 + i * 32 + lane;
+                            zv[j][i] = (m < M && n < N) ? C2[(size_t)m * ldc + n] : 0.0f;
+                        }
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int rr = r0 + j * (NT / 32), m = m0 + rr;
+                    if (m >= M) break;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const int n = n0 + p * 128 + i * 32 + lane;
+                        if (n >= N) continue;
+                        float v = tile[rr * 129 + i * 32 + lane];
+                        if (gridDim.z > 1) {
+                            C[((size_t)blockIdx.z * M + m) * N + n] = v;   /* split-K partial tile */
+                            continue;
+                        }
+                        float *c = C + (size_t)m * ldc + n;
+                        if (bias) v += bias[n];
+                        if (accumulate) v = *c + v;
+                        if (act == 3) {
+                            /* C = v silu'(z), z = C2 (the backward pass's dz) */
+                            const float z = zv[j][i], sg = fk_sigmoid(z);
+                            *c = v * sg * (1.0f + z * (1.0f - sg));
+                            continue;
+                        }
+                        /* act 1: C = z and C2 = silu(z); act 2: C = silu(z) */
+                        const float a = act ? fk_silu(v) : v;
+                        *c = act == 2 ? a : v;
+                        if (act == 1) C2[(size_t)m * ldc + n] = a;
                     }
-                    float *c = C + (size_t)m * ldc + n;
-                    if (bias) v += bias[n];
-                    if (accumulate) v = *c + v;
-                    /* act 1: C = z and C2 = silu(z); act 2: C = silu(z) */
-                    const float a = act ? fk_silu(v) : v;
-                    *c = act == 2 ? a : v;
-                    if (act == 1) C2[(size_t)m * ldc + n] = a;
                 }
             }
             __syncthreads();
@@ -599,37 +819,58 @@ __global__ void __launch_bounds__(F_NT, 1) mlp_fused_fwd_kernel(FusedNet net, co
 
 } // namespace fkmtc
 
+/* 1: stage the operands asynchronously where their alignment allows (the
+ * default); 0: always synchronously.  Both give the same bits. */
+static int g_async = 1;
+extern "C" void fk_mlp_set_async_staging(int on) { g_async = on != 0; }
+
+template <int PROD, bool ASYNC>
+static cudaError_t launch_tc(dim3 grid, cudaStream_t s, int M, int N, int K, const float *A, int lda, int ta,
+                             const float *B, int ldb, int tb, float *C, int ldc, const float *bias, int accumulate,
+                             float *C2, int act, int kchunk, float *colsum, int *error)
+{
+    using namespace fkmtc;
+    const int smem = ASYNC ? Cfg<PROD>::SMEM_ASYNC : Cfg<PROD>::SMEM;
+    cudaError_t e = cudaFuncSetAttribute(gemm_tc_kernel<PROD, ASYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         smem);
+    if (e != cudaSuccess) return e;
+    gemm_tc_kernel<PROD, ASYNC><<<grid, NT, smem, s>>>(M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate, C2,
+                                                       act, kchunk, colsum, error);
+    return cudaGetLastError();
+}
+
 /* Launch one tensor-core GEMM (PROD 1 or 3); ws: split-K workspace of split
- * M N floats, or NULL for split = 1; error: device word set on a wait
- * timeout.  Returns a cudaError_t. */
+ * M N floats, or NULL for split = 1; colsum (A[k][m] with K a multiple of
+ * 64, or NULL): [split][M] sums over each slice's k of A(m, k); error:
+ * device word set on a wait timeout.  Returns a cudaError_t. */
 extern "C" int fk_mlp_gemm_tc(int prod, int M, int N, int K, const float *A, int lda, int ta, const float *B,
                               int ldb, int tb, float *C, int ldc, const float *bias, int accumulate, float *C2,
-                              int act, int split, float *ws, int *error, cudaStream_t s)
+                              int act, int split, float *ws, float *colsum, int *error, cudaStream_t s)
 {
     using namespace fkmtc;
     if (M <= 0 || N <= 0 || K <= 0) return 0;
     if (N > BN || (prod != 1 && prod != 3) || (split > 1 && !ws)) return (int)cudaErrorInvalidValue;
+    if (colsum && (!ta || K % BK)) return (int)cudaErrorInvalidValue;   /* only full blocks of A[k][m] */
     const int kchunk = ((K + split * BK - 1) / (split * BK)) * BK;
     const dim3 grid(1, (M + BM - 1) / BM, split);
+    float *Cw = split > 1 ? ws : C;
+    const int ldw = split > 1 ? N : ldc, accw = split > 1 ? 0 : accumulate, actw = split > 1 ? 0 : act;
+    const float *bw = split > 1 ? nullptr : bias;
+    /* 16-byte copies: aligned operands, leading dimensions and contiguous extents in fours */
+    const bool async = g_async && ((uintptr_t)A & 15) == 0 && ((uintptr_t)B & 15) == 0 && lda % 4 == 0 &&
+                       ldb % 4 == 0 && K % 4 == 0 && (!ta || M % 4 == 0) && (tb || N % 4 == 0);
     cudaError_t e;
-    if (prod == 3) {
-        const int smem = Cfg<3>::SMEM;
-        e = cudaFuncSetAttribute(gemm_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return (int)e;
-        gemm_tc_kernel<3><<<grid, NT, smem, s>>>(M, N, K, A, lda, ta, B, ldb, tb, split > 1 ? ws : C,
-                                                 split > 1 ? N : ldc, split > 1 ? nullptr : bias,
-                                                 split > 1 ? 0 : accumulate, C2, split > 1 ? 0 : act, kchunk,
-                                                 error);
-    } else {
-        const int smem = Cfg<1>::SMEM;
-        e = cudaFuncSetAttribute(gemm_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return (int)e;
-        gemm_tc_kernel<1><<<grid, NT, smem, s>>>(M, N, K, A, lda, ta, B, ldb, tb, split > 1 ? ws : C,
-                                                 split > 1 ? N : ldc, split > 1 ? nullptr : bias,
-                                                 split > 1 ? 0 : accumulate, C2, split > 1 ? 0 : act, kchunk,
-                                                 error);
-    }
-    return (int)cudaGetLastError();
+    if (prod == 3)
+        e = async ? launch_tc<3, true>(grid, s, M, N, K, A, lda, ta, B, ldb, tb, Cw, ldw, bw, accw, C2, actw, kchunk,
+                                       colsum, error)
+                  : launch_tc<3, false>(grid, s, M, N, K, A, lda, ta, B, ldb, tb, Cw, ldw, bw, accw, C2, actw, kchunk,
+                                        colsum, error);
+    else
+        e = async ? launch_tc<1, true>(grid, s, M, N, K, A, lda, ta, B, ldb, tb, Cw, ldw, bw, accw, C2, actw, kchunk,
+                                       colsum, error)
+                  : launch_tc<1, false>(grid, s, M, N, K, A, lda, ta, B, ldb, tb, Cw, ldw, bw, accw, C2, actw, kchunk,
+                                        colsum, error);
+    return (int)e;
 }
 
 /* The fused forward pass of n rows (x [n][6] device, tau [n] device) of a

@@ -504,6 +504,12 @@ void fteik_b200_mlp_getTrainGraph(int *on);
  * layer.  Both give the same bits. */
 void fteik_b200_mlp_setFusedForward(int on);
 void fteik_b200_mlp_getFusedForward(int *on);
+/* The tensor-core products stage their FP32 operands into shared memory by
+ * asynchronous copies, several K blocks ahead, where the operands are
+ * 16-byte aligned (on = 1, the default); 0 stages every K block with plain
+ * loads.  Both give the same bits. */
+void fteik_b200_mlp_setAsyncStaging(int on);
+void fteik_b200_mlp_getAsyncStaging(int *on);
 
 /* The 2D ray paths of the last fteik_solver2d_traceRaysToPoints /
  * ToReceivers (rays.F90:449-670, which keeps them in module variables no C

@@ -22,7 +22,7 @@ PRODUCTS = [(0, 2e-4, 1e-5), (3, 2e-4, 1e-5), (1, 2e-2, 5e-3)]
 
 
 @pytest.mark.parametrize("products,gtol,ftol", PRODUCTS)
-@pytest.mark.parametrize("width,depth,n", [(32, 3, 64), (256, 5, 300), (256, 5, 4096)])
+@pytest.mark.parametrize("width,depth,n", [(32, 3, 64), (256, 5, 300), (256, 5, 4096), (256, 5, 16384)])
 def test_gradient_matches_oracle(fk, width, depth, n, products, gtol, ftol):
     """The hidden layers reach the tensor cores when their width is 64 or
     more (width 256); the width-32 network checks the CUDA-core path."""
@@ -122,6 +122,41 @@ def test_fused_forward_matches_layer_by_layer(fk, n):
             finally:
                 fk.set_mlp_fused_forward(old)
         assert np.array_equal(outs[0], outs[1])
+        net.finalize()
+    finally:
+        fk.set_mlp_tensor_products(old_p)
+
+
+@pytest.mark.parametrize("products", [1, 3])
+@pytest.mark.parametrize("n", [300, 4096, 16384])
+def test_async_staging_matches_synchronous(fk, products, n):
+    """The tensor-core products staged by asynchronous copies (FP32 ring,
+    then BF16 conversion) give the synchronous staging's loss, gradient and
+    outputs bit for bit: forward, input-gradient and split-K weight-gradient
+    products with their fused column sums."""
+    old_p = fk.set_mlp_tensor_products(products)
+    try:
+        net = fk.MLP(256, 5, seed=13)
+        rng = np.random.default_rng(n + products)
+        x = rng.uniform(-1, 1, (n, 6)).astype(np.float32)
+        y = rng.uniform(0.6, 1.1, n).astype(np.float32)
+        out = []
+        for on in (1, 0):
+            old = fk.set_mlp_async_staging(on)
+            try:
+                old_f = fk.set_mlp_fused_forward(0)
+                try:
+                    loss, g = net.gradient(x, y)
+                    out.append((loss, g, net.forward(x)))
+                finally:
+                    fk.set_mlp_fused_forward(old_f)
+            finally:
+                fk.set_mlp_async_staging(old)
+        gd = np.flatnonzero(out[0][1] != out[1][1])
+        fd = np.flatnonzero(out[0][2] != out[1][2])
+        assert out[0][0] == out[1][0], (out[0][0], out[1][0])
+        assert gd.size == 0, ("gradient entries differ", gd[:10], gd.size)
+        assert fd.size == 0, ("outputs differ", fd[:10], fd.size)
         net.finalize()
     finally:
         fk.set_mlp_tensor_products(old_p)
