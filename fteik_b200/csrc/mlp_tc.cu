@@ -59,7 +59,6 @@ struct Cfg {
     static constexpr int NS = PROD == 3 ? 2 : 3;
     static constexpr int SMEM_ASYNC = NS * FSTAGE + STAGE + 1024;
 };
-static_assert(BM * 129 * 4 <= 2 * FSTAGE && BM * 129 * 4 <= 2 * Cfg<1>::STAGE, "the epilogue tile fits the stages");
 
 /* byte offset of element (row, k) in a swizzled K-major tile (rows of 128 B) */
 __device__ __forceinline__ uint32_t swz(int row, int k)
@@ -287,40 +286,76 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N_>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N_) : "memory"); }
 
-/* copies of the half-stage k in [k0, k0 + 32) into the ring slot at f */
-__device__ __forceinline__ void issue_half(uint32_t f, int M, int N, const float *__restrict__ A, int lda, int ta,
-                                           const float *__restrict__ B, int ldb, int tb, int m0, int n0, int k0,
-                                           int k1)
-{
-    const int t = threadIdx.x;
+/* The copies of one thread: 4 chunks of A and 8 of B per half-stage.
+ * Pointers run along k (advance() moves them one half-stage on); the
+ * destinations and the in-range tests follow from the thread index. */
+template <int TA, int TB>
+struct Copier {
+    const float *pa[FA_BYTES / 16 / NT], *pb[FB_BYTES / 16 / NT];
+    size_t sa, sb;   /* pointer step per half-stage */
+
+    __device__ __forceinline__ Copier(const float *A, int lda, const float *B, int ldb, int m0, int n0, int k0)
+    {
+        const int t = threadIdx.x;
 #pragma unroll
-    for (int j = 0; j < FA_BYTES / 16 / NT; ++j) {
-        const int q = t + NT * j;
-        if (!ta) {
-            const int r = q >> 3, c = q & 7, m = m0 + r, k = k0 + 4 * c;
-            const bool ok = m < M && k < k1;
-            cp16(f + r * 128 + ((c ^ (r & 7)) << 4), ok ? A + (size_t)m * lda + k : A, ok);
-        } else {
-            const int r = q >> 5, c = q & 31, m = m0 + 4 * c, k = k0 + r;
-            const bool ok = m < M && k < k1;
-            cp16(f + r * 512 + c * 16, ok ? A + (size_t)k * lda + m : A, ok);
+        for (int j = 0; j < FA_BYTES / 16 / NT; ++j) {
+            const int q = t + NT * j;
+            pa[j] = TA ? A + (size_t)(k0 + (q >> 5)) * lda + m0 + 4 * (q & 31)
+                       : A + (size_t)(m0 + (q >> 3)) * lda + k0 + 4 * (q & 7);
+        }
+#pragma unroll
+        for (int j = 0; j < FB_BYTES / 16 / NT; ++j) {
+            const int q = t + NT * j;
+            pb[j] = TB ? B + (size_t)(n0 + (q >> 3)) * ldb + k0 + 4 * (q & 7)
+                       : B + (size_t)(k0 + (q >> 6)) * ldb + n0 + 4 * (q & 63);
+        }
+        sa = TA ? (size_t)HK * lda : HK;
+        sb = TB ? HK : (size_t)HK * ldb;
+    }
+
+    /* the half-stage k in [k0, k0 + 32) into the ring slot at f (zero
+     * outside the matrices, k1 = the end of this CTA's K range) */
+    __device__ __forceinline__ void issue(uint32_t f, const float *A, const float *B, int M, int N, int m0, int n0,
+                                          int k0, int k1) const
+    {
+        const int t = threadIdx.x;
+#pragma unroll
+        for (int j = 0; j < FA_BYTES / 16 / NT; ++j) {
+            const int q = t + NT * j;
+            if (!TA) {
+                const int r = q >> 3, c = q & 7;
+                const bool ok = m0 + r < M && k0 + 4 * c < k1;
+                cp16(f + r * 128 + ((c ^ (r & 7)) << 4), ok ? pa[j] : A, ok);
+            } else {
+                const int r = q >> 5, c = q & 31;
+                const bool ok = m0 + 4 * c < M && k0 + r < k1;
+                cp16(f + r * 512 + c * 16, ok ? pa[j] : A, ok);
+            }
+        }
+        f += FA_BYTES;
+#pragma unroll
+        for (int j = 0; j < FB_BYTES / 16 / NT; ++j) {
+            const int q = t + NT * j;
+            if (TB) {
+                const int r = q >> 3, c = q & 7;
+                const bool ok = n0 + r < N && k0 + 4 * c < k1;
+                cp16(f + r * 128 + ((c ^ (r & 7)) << 4), ok ? pb[j] : B, ok);
+            } else {
+                const int r = q >> 6, c = q & 63;
+                const bool ok = n0 + 4 * c < N && k0 + r < k1;
+                cp16(f + r * 1024 + c * 16, ok ? pb[j] : B, ok);
+            }
         }
     }
-    f += FA_BYTES;
+
+    __device__ __forceinline__ void advance()
+    {
 #pragma unroll
-    for (int j = 0; j < FB_BYTES / 16 / NT; ++j) {
-        const int q = t + NT * j;
-        if (tb) {
-            const int r = q >> 3, c = q & 7, n = n0 + r, k = k0 + 4 * c;
-            const bool ok = n < N && k < k1;
-            cp16(f + r * 128 + ((c ^ (r & 7)) << 4), ok ? B + (size_t)n * ldb + k : B, ok);
-        } else {
-            const int r = q >> 6, c = q & 63, n = n0 + 4 * c, k = k0 + r;
-            const bool ok = n < N && k < k1;
-            cp16(f + r * 1024 + c * 16, ok ? B + (size_t)k * ldb + n : B, ok);
-        }
+        for (int j = 0; j < FA_BYTES / 16 / NT; ++j) pa[j] += sa;
+#pragma unroll
+        for (int j = 0; j < FB_BYTES / 16 / NT; ++j) pb[j] += sb;
     }
-}
+};
 
 /* a landed half-stage (slot f) into half hh (k 32 hh ..) of the BF16 stage */
 template <int PROD>
@@ -381,14 +416,104 @@ __device__ __forceinline__ void issue_mmas(uint32_t tmem, const uint8_t *sA, con
     }
 }
 
-template <int PROD, bool ASYNC>
+/* ---- epilogue ----------------------------------------------------------
+ * The accumulators go through a [128][TS] FP32 tile in shared memory (row
+ * stride 132: 16-byte rows; the float4 writes of 8 consecutive rows and
+ * the float4 reads of one row are both conflict-free), one 128-column half
+ * at a time, then out by rows: lane l of a warp holds columns 4 l .. 4 l + 3
+ * of the half, so a row is one 512-byte store.  MODE: 0 C = v; 1 C = v and
+ * C2 = silu(v); 2 C = silu(v); 3 C = v silu'(z), z = C2; 4 split-K partial
+ * tile (C = the workspace slice, no bias).  The bias and the previous
+ * contents are added first where asked (modes 0-3). */
+constexpr int TS = 132;
+static_assert(BM * TS * 4 <= 2 * FSTAGE && BM * TS * 4 <= 2 * Cfg<1>::STAGE, "the epilogue tile fits the stages");
+
+__device__ __forceinline__ float silu_bwd1(float v, float z)
+{
+    const float sg = fk_sigmoid(z);
+    return v * sg * (1.0f + z * (1.0f - sg));
+}
+
+template <int MODE>
+__device__ __forceinline__ void epi_rows_vec(const float *tile, int warp, int lane, int m0, int M, int N, int nc0,
+                                             float *__restrict__ C, size_t ldc, const float *__restrict__ bias,
+                                             int accumulate, float *__restrict__ C2)
+{
+    const int n = nc0 + 4 * lane;
+    if (n >= N) return;   /* N is a multiple of 4: a lane's columns are all in or all out */
+    float4 bv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (MODE != 4 && bias) bv = make_float4(bias[n], bias[n + 1], bias[n + 2], bias[n + 3]);
+    for (int r0 = warp; r0 < BM; r0 += 4 * (NT / 32)) {
+        float4 zv[4];
+        if (MODE == 3) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int m = m0 + r0 + j * (NT / 32);
+                zv[j] = m < M ? *reinterpret_cast<const float4 *>(C2 + (size_t)m * ldc + n) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int rr = r0 + j * (NT / 32), m = m0 + rr;
+            if (m >= M) break;
+            float4 v = *reinterpret_cast<const float4 *>(tile + rr * TS + 4 * lane);
+            float4 *c = reinterpret_cast<float4 *>(C + (size_t)m * ldc + n);
+            if (MODE == 4) { *c = v; continue; }
+            if (bias) { v.x += bv.x; v.y += bv.y; v.z += bv.z; v.w += bv.w; }
+            if (accumulate) {
+                const float4 o = *c;
+                v.x = o.x + v.x; v.y = o.y + v.y; v.z = o.z + v.z; v.w = o.w + v.w;
+            }
+            if (MODE == 0) *c = v;
+            if (MODE == 1) {
+                *c = v;
+                *reinterpret_cast<float4 *>(C2 + (size_t)m * ldc + n) =
+                    make_float4(fk_silu(v.x), fk_silu(v.y), fk_silu(v.z), fk_silu(v.w));
+            }
+            if (MODE == 2) *c = make_float4(fk_silu(v.x), fk_silu(v.y), fk_silu(v.z), fk_silu(v.w));
+            if (MODE == 3)
+                *c = make_float4(silu_bwd1(v.x, zv[j].x), silu_bwd1(v.y, zv[j].y), silu_bwd1(v.z, zv[j].z),
+                                 silu_bwd1(v.w, zv[j].w));
+        }
+    }
+}
+
+/* the same for any alignment: lane l holds columns l, l + 32, l + 64, l + 96 */
+__device__ __forceinline__ void epi_rows_scalar(const float *tile, int warp, int lane, int m0, int M, int N, int nc0,
+                                                float *__restrict__ C, size_t ldc, const float *__restrict__ bias,
+                                                int accumulate, float *__restrict__ C2, int mode)
+{
+    for (int rr = warp; rr < BM; rr += NT / 32) {
+        const int m = m0 + rr;
+        if (m >= M) break;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int n = nc0 + i * 32 + lane;
+            if (n >= N) continue;
+            float v = tile[rr * TS + i * 32 + lane];
+            float *c = C + (size_t)m * ldc + n;
+            if (mode == 4) { *c = v; continue; }
+            if (bias) v += bias[n];
+            if (accumulate) v = *c + v;
+            if (mode == 3) *c = silu_bwd1(v, C2[(size_t)m * ldc + n]);
+            else if (mode == 2) *c = fk_silu(v);
+            else {
+                *c = v;
+                if (mode == 1) C2[(size_t)m * ldc + n] = fk_silu(v);
+            }
+        }
+    }
+}
+
+template <int PROD, bool ASYNC, int TA, int TB>
 __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, const float *__restrict__ A, int lda,
-                                                        int ta, const float *__restrict__ B, int ldb, int tb,
+                                                        const float *__restrict__ B, int ldb,
                                                         float *__restrict__ C, int ldc,
                                                         const float *__restrict__ bias, int accumulate,
                                                         float *__restrict__ C2, int act, int kchunk,
                                                         float *__restrict__ colsum, int *error)
 {
+    constexpr int ta = TA, tb = TB;
     using G = Cfg<PROD>;
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t bars[2];
@@ -425,9 +550,13 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
         const uint32_t ring = (uint32_t)__cvta_generic_to_shared(base);
         uint8_t *sA = base + G::NS * FSTAGE, *sB = sA + G::NP * A_TILE;
         const int nh = 2 * nkb;
+        Copier<TA, TB> cp(A, lda, B, ldb, m0, n0, kb);
 #pragma unroll
         for (int h = 0; h < G::NS - 1; ++h) {
-            if (h < nh) issue_half(ring + h * FSTAGE, M, N, A, lda, ta, B, ldb, tb, m0, n0, kb + h * HK, ke);
+            if (h < nh) {
+                cp.issue(ring + h * FSTAGE, A, B, M, N, m0, n0, kb + h * HK, ke);
+                cp.advance();
+            }
             cp_commit();
         }
         for (int h = 0; h < nh; ++h) {
@@ -437,8 +566,10 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
             if (s_fail) break;
             {
                 const int hn = h + G::NS - 1;
-                if (hn < nh)
-                    issue_half(ring + (hn % G::NS) * FSTAGE, M, N, A, lda, ta, B, ldb, tb, m0, n0, kb + hn * HK, ke);
+                if (hn < nh) {
+                    cp.issue(ring + (hn % G::NS) * FSTAGE, A, B, M, N, m0, n0, kb + hn * HK, ke);
+                    cp.advance();
+                }
                 cp_commit();
             }
             /* the MMAs of stage b - 1 read the BF16 stage */
@@ -503,14 +634,16 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
         }
     }
     if (ok && committed > 0) {
-        /* epilogue through shared memory (the operand stages are free: every
-         * MMA has completed), one 128-column half of the tile at a time: the
-         * warps holding that half read their 32 TMEM lanes x 128 columns
-         * into a [128][129] tile (row stride 129: conflict-free both ways),
-         * then every warp stores whole rows, 32 consecutive columns per
-         * instruction */
+        /* the operand stages are free (every MMA has completed): the warps
+         * holding a 128-column half read their 32 TMEM lanes into the tile,
+         * then every warp stores rows */
         float *tile = reinterpret_cast<float *>(base);
         const int q = warp & 3, half = warp >> 2;
+        const int mode = gridDim.z > 1 ? 4 : act;
+        float *Cb = gridDim.z > 1 ? C + (size_t)blockIdx.z * M * N : C;
+        const size_t ldo = gridDim.z > 1 ? (size_t)N : (size_t)ldc;
+        const bool vec = (N & 3) == 0 && (ldo & 3) == 0 && ((uintptr_t)Cb & 15) == 0 &&
+                         (!(mode == 1 || mode == 3) || ((uintptr_t)C2 & 15) == 0);
         for (int p = 0; p < 2; ++p) {
             if (half == p) {
 #pragma unroll 1
@@ -518,54 +651,27 @@ __global__ void __launch_bounds__(NT, 1) gemm_tc_kernel(int M, int N, int K, con
                     uint32_t r[32];
                     tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(p * 128 + c), r);
                     tmem_wait_ld();
-                    float *trow = tile + (q * 32 + lane) * 129 + c;
+                    float4 *trow = reinterpret_cast<float4 *>(tile + (q * 32 + lane) * TS + c);
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) trow[j] = __uint_as_float(r[j]);
+                    for (int j = 0; j < 8; ++j)
+                        trow[j] = make_float4(__uint_as_float(r[4 * j]), __uint_as_float(r[4 * j + 1]),
+                                              __uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3]));
                 }
             }
             __syncthreads();
-            /* a warp stores rows warp + 8 j; four of them at a time, their
-             * act-3 inputs z loaded first (16 loads in flight) */
-            for (int r0 = warp; r0 < BM; r0 += 4 * (NT / 32)) {
-                float zv[4][4];
-                if (act == 3) {
-#pragma unroll
-                    for (int j = 0; j < 4; ++j)
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) {
-                            const int m = m0 + r0 + j * (NT / 32), n = n0 + p * 128 + i * 32 + lane;
-                            zv[j][i] = (m < M && n < N) ? C2[(size_t)m * ldc + n] : 0.0f;
-                        }
-                }
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int rr = r0 + j * (NT / 32), m = m0 + rr;
-                    if (m >= M) break;
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        const int n = n0 + p * 128 + i * 32 + lane;
-                        if (n >= N) continue;
-                        float v = tile[rr * 129 + i * 32 + lane];
-                        if (gridDim.z > 1) {
-                            C[((size_t)blockIdx.z * M + m) * N + n] = v;   /* split-K partial tile */
-                            continue;
-                        }
-                        float *c = C + (size_t)m * ldc + n;
-                        if (bias) v += bias[n];
-                        if (accumulate) v = *c + v;
-                        if (act == 3) {
-                            /* C = v silu'(z), z = C2 (the backward pass's dz) */
-                            const float z = zv[j][i], sg = fk_sigmoid(z);
-                            *c = v * sg * (1.0f + z * (1.0f - sg));
-                            continue;
-                        }
-                        /* act 1: C = z and C2 = silu(z); act 2: C = silu(z) */
-                        const float a = act ? fk_silu(v) : v;
-                        *c = act == 2 ? a : v;
-                        if (act == 1) C2[(size_t)m * ldc + n] = a;
-                    }
-                }
-            }
+            const int nc0 = n0 + p * 128;
+            if (!vec)
+                epi_rows_scalar(tile, warp, lane, m0, M, N, nc0, Cb, ldo, bias, accumulate, C2, mode);
+            else if (mode == 4)
+                epi_rows_vec<4>(tile, warp, lane, m0, M, N, nc0, Cb, ldo, nullptr, 0, nullptr);
+            else if (mode == 1)
+                epi_rows_vec<1>(tile, warp, lane, m0, M, N, nc0, Cb, ldo, bias, accumulate, C2);
+            else if (mode == 2)
+                epi_rows_vec<2>(tile, warp, lane, m0, M, N, nc0, Cb, ldo, bias, accumulate, C2);
+            else if (mode == 3)
+                epi_rows_vec<3>(tile, warp, lane, m0, M, N, nc0, Cb, ldo, bias, accumulate, C2);
+            else
+                epi_rows_vec<0>(tile, warp, lane, m0, M, N, nc0, Cb, ldo, bias, accumulate, C2);
             __syncthreads();
         }
     }
@@ -824,19 +930,37 @@ __global__ void __launch_bounds__(F_NT, 1) mlp_fused_fwd_kernel(FusedNet net, co
 static int g_async = 1;
 extern "C" void fk_mlp_set_async_staging(int on) { g_async = on != 0; }
 
-template <int PROD, bool ASYNC>
-static cudaError_t launch_tc(dim3 grid, cudaStream_t s, int M, int N, int K, const float *A, int lda, int ta,
-                             const float *B, int ldb, int tb, float *C, int ldc, const float *bias, int accumulate,
+template <int PROD, bool ASYNC, int TA, int TB>
+static cudaError_t launch_tc(dim3 grid, cudaStream_t s, int M, int N, int K, const float *A, int lda,
+                             const float *B, int ldb, float *C, int ldc, const float *bias, int accumulate,
                              float *C2, int act, int kchunk, float *colsum, int *error)
 {
     using namespace fkmtc;
     const int smem = ASYNC ? Cfg<PROD>::SMEM_ASYNC : Cfg<PROD>::SMEM;
-    cudaError_t e = cudaFuncSetAttribute(gemm_tc_kernel<PROD, ASYNC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         smem);
+    cudaError_t e = cudaFuncSetAttribute(gemm_tc_kernel<PROD, ASYNC, TA, TB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    gemm_tc_kernel<PROD, ASYNC><<<grid, NT, smem, s>>>(M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate, C2,
-                                                       act, kchunk, colsum, error);
+    gemm_tc_kernel<PROD, ASYNC, TA, TB><<<grid, NT, smem, s>>>(M, N, K, A, lda, B, ldb, C, ldc, bias, accumulate,
+                                                               C2, act, kchunk, colsum, error);
     return cudaGetLastError();
+}
+
+template <int PROD, bool ASYNC>
+static cudaError_t launch_tc_layout(int ta, int tb, dim3 grid, cudaStream_t s, int M, int N, int K, const float *A,
+                                    int lda, const float *B, int ldb, float *C, int ldc, const float *bias,
+                                    int accumulate, float *C2, int act, int kchunk, float *colsum, int *error)
+{
+    if (!ta && tb)
+        return launch_tc<PROD, ASYNC, 0, 1>(grid, s, M, N, K, A, lda, B, ldb, C, ldc, bias, accumulate, C2, act,
+                                            kchunk, colsum, error);
+    if (!ta && !tb)
+        return launch_tc<PROD, ASYNC, 0, 0>(grid, s, M, N, K, A, lda, B, ldb, C, ldc, bias, accumulate, C2, act,
+                                            kchunk, colsum, error);
+    if (ta && !tb)
+        return launch_tc<PROD, ASYNC, 1, 0>(grid, s, M, N, K, A, lda, B, ldb, C, ldc, bias, accumulate, C2, act,
+                                            kchunk, colsum, error);
+    return launch_tc<PROD, ASYNC, 1, 1>(grid, s, M, N, K, A, lda, B, ldb, C, ldc, bias, accumulate, C2, act, kchunk,
+                                        colsum, error);
 }
 
 /* Launch one tensor-core GEMM (PROD 1 or 3); ws: split-K workspace of split
@@ -861,15 +985,15 @@ extern "C" int fk_mlp_gemm_tc(int prod, int M, int N, int K, const float *A, int
                        ldb % 4 == 0 && K % 4 == 0 && (!ta || M % 4 == 0) && (tb || N % 4 == 0);
     cudaError_t e;
     if (prod == 3)
-        e = async ? launch_tc<3, true>(grid, s, M, N, K, A, lda, ta, B, ldb, tb, Cw, ldw, bw, accw, C2, actw, kchunk,
-                                       colsum, error)
-                  : launch_tc<3, false>(grid, s, M, N, K, A, lda, ta, B, ldb, tb, Cw, ldw, bw, accw, C2, actw, kchunk,
-                                        colsum, error);
+        e = async ? launch_tc_layout<3, true>(ta, tb, grid, s, M, N, K, A, lda, B, ldb, Cw, ldw, bw, accw, C2, actw,
+                                              kchunk, colsum, error)
+                  : launch_tc_layout<3, false>(ta, tb, grid, s, M, N, K, A, lda, B, ldb, Cw, ldw, bw, accw, C2, actw,
+                                               kchunk, colsum, error);
     else
-        e = async ? launch_tc<1, true>(grid, s, M, N, K, A, lda, ta, B, ldb, tb, Cw, ldw, bw, accw, C2, actw, kchunk,
-                                       colsum, error)
-                  : launch_tc<1, false>(grid, s, M, N, K, A, lda, ta, B, ldb, tb, Cw, ldw, bw, accw, C2, actw, kchunk,
-                                        colsum, error);
+        e = async ? launch_tc_layout<1, true>(ta, tb, grid, s, M, N, K, A, lda, B, ldb, Cw, ldw, bw, accw, C2, actw,
+                                              kchunk, colsum, error)
+                  : launch_tc_layout<1, false>(ta, tb, grid, s, M, N, K, A, lda, B, ldb, Cw, ldw, bw, accw, C2, actw,
+                                               kchunk, colsum, error);
     return (int)e;
 }
 
