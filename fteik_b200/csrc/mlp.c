@@ -22,6 +22,8 @@ int fk_mlp_mse(int n, const float *pred, const float *y, float *dpred, double *l
 int fk_mlp_adam_sched(size_t n, float *w, const float *g, float *m, float *v, const float *sched,
                       const long long *tdev, float b1, float b2, float eps, cudaStream_t s);
 int fk_mlp_step_inc(long long *tdev, cudaStream_t s);
+int fk_mlp_transpose_layers(int n, const long long *off, const int *in, const int *out, const float *w, float *wt,
+                            cudaStream_t s);
 int fk_mlp_adam(size_t n, float *w, const float *g, float *m, float *v, float lr, float b1,
                 float b2, float eps, float c1, float c2, cudaStream_t s);
 void fk_mlp_set_tensor(int products);
@@ -67,6 +69,7 @@ static struct {
     int din[MLP_MAXL], dout[MLP_MAXL];
     size_t woff[MLP_MAXL], boff[MLP_MAXL], nparam;
     float *w, *g, *m, *v;              /* device [nparam] */
+    float *wt;                         /* device [nparam]: transposed hidden weights (backward pass) */
     long long adam_t;
     int cap;                           /* batch rows the buffers hold */
     float *x[MLP_MAXL + 1];            /* layer inputs; x[nlayer] = output */
@@ -94,7 +97,7 @@ void fteik_b200_mlp_finalize(void)
     fk_dfree(g_wq);
     g_wq = NULL;
     g_wq_cap = 0;
-    fk_dfree(NN.w); fk_dfree(NN.g); fk_dfree(NN.m); fk_dfree(NN.v); fk_dfree(NN.loss_dev);
+    fk_dfree(NN.w); fk_dfree(NN.g); fk_dfree(NN.m); fk_dfree(NN.v); fk_dfree(NN.wt); fk_dfree(NN.loss_dev);
     memset(&NN, 0, sizeof(NN));
 }
 
@@ -145,8 +148,9 @@ void fteik_b200_mlp_initialize(int width, int depth, unsigned long long seed, in
     NN.g = (float *)fk_dalloc(sizeof(float) * off, "mlp");
     NN.m = (float *)fk_dalloc(sizeof(float) * off, "mlp");
     NN.v = (float *)fk_dalloc(sizeof(float) * off, "mlp");
+    NN.wt = (float *)fk_dalloc(sizeof(float) * off, "mlp");
     NN.loss_dev = (double *)fk_dalloc(sizeof(double), "mlp");
-    int e = (NN.w && NN.g && NN.m && NN.v && NN.loss_dev) ? 0 : 1;
+    int e = (NN.w && NN.g && NN.m && NN.v && NN.wt && NN.loss_dev) ? 0 : 1;
     if (!e) e = (int)fk_h2d(NN.w, h, sizeof(float) * off);
     if (!e) e = (int)fk_zero(NN.m, sizeof(float) * off);
     if (!e) e = (int)fk_zero(NN.v, sizeof(float) * off);
@@ -232,6 +236,20 @@ static int forward_backward(int B, const float *y, cudaStream_t s)
 {
     int e = forward(B, true, s);
     const int L = NN.nlayer;
+    /* the input-gradient products of the layers with more than 8 outputs
+     * read W^T (k-contiguous rows), transposed once per pass */
+    long long toff[MLP_MAXL];
+    int tin[MLP_MAXL], tout[MLP_MAXL], nt = 0;
+    bool trans[MLP_MAXL] = {false};
+    for (int l = 1; l < L; l++)
+        if (NN.dout[l] > 8) {
+            toff[nt] = (long long)NN.woff[l];
+            tin[nt] = NN.din[l];
+            tout[nt] = NN.dout[l];
+            trans[l] = true;
+            nt++;
+        }
+    if (!e) e = fk_mlp_transpose_layers(nt, toff, tin, tout, NN.w, NN.wt, s);
     /* d loss / d output */
     if (!e) e = fk_mlp_mse(B, NN.x[L], y, NN.dz, NN.loss_dev, s);
     for (int l = L - 1; l >= 0 && !e; l--) {
@@ -243,8 +261,12 @@ static int forward_backward(int B, const float *y, cudaStream_t s)
         if (!e && l > 0) {
             /* d loss / d z_{l-1} = (dz W_l) silu'(z_{l-1}), the derivative
              * applied in the product's epilogue */
-            e = fk_mlp_gemm(B, in, out, NN.dz, out, 0, NN.w + NN.woff[l], in, 0, NN.dtmp, in, NULL, 0, NN.z[l - 1],
-                            3, NULL, s);
+            if (trans[l])
+                e = fk_mlp_gemm(B, in, out, NN.dz, out, 0, NN.wt + NN.woff[l], out, 1, NN.dtmp, in, NULL, 0,
+                                NN.z[l - 1], 3, NULL, s);
+            else
+                e = fk_mlp_gemm(B, in, out, NN.dz, out, 0, NN.w + NN.woff[l], in, 0, NN.dtmp, in, NULL, 0,
+                                NN.z[l - 1], 3, NULL, s);
             if (!e) { float *t = NN.dz; NN.dz = NN.dtmp; NN.dtmp = t; }
         }
     }

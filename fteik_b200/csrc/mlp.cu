@@ -141,6 +141,48 @@ __global__ void splitk_reduce_kernel(int M, int N, int split, const float *__res
     }
 }
 
+/* The same plain sums (no bias, accumulation or activation) four outputs
+ * per group of 4 threads with 16-byte loads and stores (N and ldc
+ * multiples of 4, 16-byte aligned buffers): thread u of a group adds
+ * slices u, u + 4, ... in order, and the group's 4 sums are added in
+ * thread order (a fixed order).  The column sums as splitk_reduce_kernel. */
+__global__ void splitk_reduce_vec_kernel(int M, int N, int split, const float *__restrict__ ws, float *__restrict__ C,
+                                         int ldc, const float *__restrict__ cs, float *__restrict__ db)
+{
+    const size_t n4 = (size_t)M * N / 4, n_all = n4 + (db ? (size_t)M : 0);
+    const size_t e = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 2;
+    const int u = threadIdx.x & 3;
+    /* every lane reaches the shuffles below (no early exit) */
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (e < n4) {
+#pragma unroll 4
+        for (int z = u; z < split; z += 4) {
+            const float4 w = reinterpret_cast<const float4 *>(ws)[(size_t)z * n4 + e];
+            v.x += w.x; v.y += w.y; v.z += w.z; v.w += w.w;
+        }
+    }
+    /* lanes 4 g .. 4 g + 3 hold one output's partial sums: ((s0 + s1) + s2) + s3 */
+    float4 r;
+    r.x = __shfl_sync(0xffffffffu, v.x, 0, 4); r.y = __shfl_sync(0xffffffffu, v.y, 0, 4);
+    r.z = __shfl_sync(0xffffffffu, v.z, 0, 4); r.w = __shfl_sync(0xffffffffu, v.w, 0, 4);
+#pragma unroll
+    for (int i = 1; i < 4; ++i) {
+        r.x += __shfl_sync(0xffffffffu, v.x, i, 4); r.y += __shfl_sync(0xffffffffu, v.y, i, 4);
+        r.z += __shfl_sync(0xffffffffu, v.z, i, 4); r.w += __shfl_sync(0xffffffffu, v.w, i, 4);
+    }
+    if (u != 0 || e >= n_all) return;
+    if (e < n4) {
+        const int m = (int)(4 * e / N), n = (int)(4 * e % N);
+        *reinterpret_cast<float4 *>(C + (size_t)m * ldc + n) = r;
+    } else {
+        const int m = (int)(e - n4);
+        float t = 0.0f;
+#pragma unroll 16
+        for (int z = 0; z < split; ++z) t += cs[(size_t)z * M + m];
+        db[m] = t;
+    }
+}
+
 /* The same sums for few outputs and many slices (the thin layers' weight
  * gradients): one warp per output, lane l adding slices l, l + 32, ... in
  * order, then a fixed butterfly over the lanes (the same order on every
@@ -200,6 +242,70 @@ __global__ void __launch_bounds__(SK_N, 4) smallk_kernel(int M, int N, int K, co
     }
 }
 
+/* The same products four columns per thread (N, ldc multiples of 4,
+ * 16-byte aligned C and C2): 64 column quads x 4 row groups per block,
+ * float4 stores (and float4 loads of z for act 3); the same arithmetic per
+ * element as smallk_kernel. */
+constexpr int SKQ_R = 32;
+__global__ void __launch_bounds__(256) smallk_quad_kernel(int M, int N, int K, const float *__restrict__ A, int lda,
+                                                          const float *__restrict__ B, int ldb, int tb,
+                                                          float *__restrict__ C, int ldc,
+                                                          const float *__restrict__ bias, int accumulate,
+                                                          float *__restrict__ C2, int act)
+{
+    const int t = threadIdx.x, n = blockIdx.x * 256 + 4 * (t & 63), rs = t >> 6;
+    if (n >= N) return;
+    float b[SK_KMAX][4];
+#pragma unroll
+    for (int k = 0; k < SK_KMAX; ++k)
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            b[k][c] = k < K ? (tb ? B[(size_t)(n + c) * ldb + k] : B[(size_t)k * ldb + n + c]) : 0.0f;
+    float bn[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) bn[c] = bias ? bias[n + c] : 0.0f;
+    for (int m0 = blockIdx.y * SKQ_R; m0 < M; m0 += gridDim.y * SKQ_R) {
+#pragma unroll 2
+        for (int i = rs; i < SKQ_R; i += 4) {
+            const int m = m0 + i;
+            if (m >= M) break;
+            float v[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int k = 0; k < SK_KMAX; ++k)
+                if (k < K) {
+                    const float a = A[(size_t)m * lda + k];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) v[c] = fmaf(a, b[k][c], v[c]);
+                }
+#pragma unroll
+            for (int c = 0; c < 4; ++c) v[c] = v[c] + bn[c];
+            const size_t off = (size_t)m * ldc + n;
+            float4 *cp = reinterpret_cast<float4 *>(C + off);
+            if (accumulate) {
+                const float4 o = *cp;
+                v[0] = o.x + v[0]; v[1] = o.y + v[1]; v[2] = o.z + v[2]; v[3] = o.w + v[3];
+            }
+            if (act == 3) {
+                const float4 z = *reinterpret_cast<const float4 *>(C2 + off);
+                const float zs[4] = {z.x, z.y, z.z, z.w};
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const float sg = fk_sigmoid(zs[c]);
+                    v[c] = v[c] * sg * (1.0f + zs[c] * (1.0f - sg));
+                }
+                *cp = make_float4(v[0], v[1], v[2], v[3]);
+            } else if (act == 2) {
+                *cp = make_float4(fk_silu(v[0]), fk_silu(v[1]), fk_silu(v[2]), fk_silu(v[3]));
+            } else {
+                *cp = make_float4(v[0], v[1], v[2], v[3]);
+                if (act == 1)
+                    *reinterpret_cast<float4 *>(C2 + off) =
+                        make_float4(fk_silu(v[0]), fk_silu(v[1]), fk_silu(v[2]), fk_silu(v[3]));
+            }
+        }
+    }
+}
+
 /* Products with N = 1 (the output layer), A[m][k]: one thread per row, the
  * multiply-adds in k order from zero as gemm_kernel; a block of 256
  * threads brings 64 rows x 64 k of A into a [64][65] tile by coalesced
@@ -247,6 +353,86 @@ __global__ void __launch_bounds__(GV_NT) gemv_kernel(int M, int K, const float *
  * dimension when known at compile time (the surrogate's 6 inputs and 1
  * output), else 0 (read from M or N). */
 constexpr int TS_MAX = 8;
+
+/* The same products with 16-byte loads along the wide dimension D (M when
+ * BIG_M, else N; D and its leading dimension multiples of 4, 16-byte
+ * aligned): a block covers 256 of D (64 quads) and one K slice; its 4
+ * row groups (threads t / 64) take rows kb + g, kb + g + 4, ... of the
+ * slice, the narrow operand's rows of the slice (S values each) staged in
+ * shared memory; the groups' sums are added in group order.  Same outputs
+ * and layout as tn_small_kernel; the order of the k sums differs, fixed. */
+constexpr int TQ_K = 64;   /* rows per slice */
+template <bool BIG_M, int S>
+__global__ void __launch_bounds__(256) tn_quad_kernel(int M, int N, int K, const float *__restrict__ A, int lda,
+                                                      const float *__restrict__ B, int ldb, float *__restrict__ ws,
+                                                      float *__restrict__ cs)
+{
+    static_assert(BIG_M || S <= 4, "narrow A: its column sums ride in the first 4 sums");
+    __shared__ float nar[TQ_K * S];
+    __shared__ float red[4][256][S + 1];
+    const int t = threadIdx.x, g = t >> 6, dq = t & 63;
+    const int D = BIG_M ? M : N;
+    const int d = blockIdx.x * 256 + 4 * dq;
+    const int kb = blockIdx.y * TQ_K, ke = min(K, kb + TQ_K);
+    for (int i = t; i < (ke - kb) * S; i += 256) {
+        const int k = kb + i / S, j = i % S;
+        nar[i] = BIG_M ? B[(size_t)k * ldb + j] : A[(size_t)k * lda + j];
+    }
+    __syncthreads();
+    float acc[4][S], sum[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        sum[c] = 0.0f;
+#pragma unroll
+        for (int j = 0; j < S; ++j) acc[c][j] = 0.0f;
+    }
+    if (d < D) {
+        const float *wide = BIG_M ? A + d : B + d;
+        const size_t ld = BIG_M ? (size_t)lda : (size_t)ldb;
+#pragma unroll 4
+        for (int k = kb + g; k < ke; k += 4) {
+            const float4 w = *reinterpret_cast<const float4 *>(wide + (size_t)k * ld);
+            const float wv[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+                const float nv = nar[(k - kb) * S + j];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[c][j] = fmaf(wv[c], nv, acc[c][j]);
+                if (!BIG_M) sum[j < 4 ? j : 0] += (j < 4) ? nv : 0.0f;
+            }
+            if (BIG_M)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) sum[c] += wv[c];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+#pragma unroll
+        for (int j = 0; j < S; ++j) red[g][4 * dq + c][j] = acc[c][j];
+        red[g][4 * dq + c][S] = sum[c];
+    }
+    __syncthreads();
+    const int dl = blockIdx.x * 256 + t;
+    if (dl >= D) return;
+    float *w = ws + (size_t)blockIdx.y * M * N;
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+        const float v = ((red[0][t][j] + red[1][t][j]) + red[2][t][j]) + red[3][t][j];
+        if (BIG_M) w[(size_t)dl * N + j] = v;
+        else w[(size_t)j * N + dl] = v;
+    }
+    if (!cs) return;
+    if (BIG_M) {
+        cs[(size_t)blockIdx.y * M + dl] = ((red[0][t][S] + red[1][t][S]) + red[2][t][S]) + red[3][t][S];
+    } else if (dl == 0) {
+        /* the narrow operand's column sums: thread 4 dq + c of group g kept
+         * sum[c] = its group's sum of A(c, k) (c < S <= 4) */
+#pragma unroll
+        for (int j = 0; j < S; ++j)
+            cs[(size_t)blockIdx.y * M + j] = ((red[0][j][S] + red[1][j][S]) + red[2][j][S]) + red[3][j][S];
+    }
+}
+
 template <bool BIG_M, int SC>
 __global__ void __launch_bounds__(256) tn_small_kernel(int M, int N, int K, int kchunk, const float *__restrict__ A,
                                                        int lda, const float *__restrict__ B, int ldb,
@@ -435,6 +621,29 @@ __global__ void adam_sched_kernel(size_t n, float *__restrict__ w, const float *
 
 __global__ void step_inc_kernel(long long *tdev) { *tdev += 1; }
 
+/* wt = the transposes of the listed layers' weights: W [out][in] at off
+ * becomes W^T [in][out] at the same offset (the input-gradient products
+ * then read k-contiguous rows); blockIdx.y = the layer */
+constexpr int TL_MAX = 16;
+struct TLayers {
+    int n;
+    long long off[TL_MAX];
+    int in[TL_MAX], out[TL_MAX];
+};
+
+__global__ void transpose_layers_kernel(TLayers L, const float *__restrict__ w, float *__restrict__ wt)
+{
+    const int l = blockIdx.y;
+    if (l >= L.n) return;
+    const int in = L.in[l], out = L.out[l];
+    const long long off = L.off[l];
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < (size_t)in * out;
+         e += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)(e / out), o = (int)(e % out);
+        wt[off + e] = w[off + (size_t)o * in + j];
+    }
+}
+
 /* counter-based hash (splitmix64 finaliser) */
 __device__ __forceinline__ uint64_t mix64(uint64_t x)
 {
@@ -606,10 +815,39 @@ extern "C" int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta,
                                                             accumulate);
         return (int)cudaGetLastError();
     }
+    const bool al16 = ((uintptr_t)C & 15) == 0 && (!C2 || ((uintptr_t)C2 & 15) == 0);
+    if (!ta && K <= SK_KMAX && N % 4 == 0 && ldc % 4 == 0 && al16) {
+        const int rb = (M + SKQ_R - 1) / SKQ_R;
+        smallk_quad_kernel<<<dim3((N + 255) / 256, rb < 65535 ? rb : 65535), 256, 0, s>>>(
+            M, N, K, A, lda, B, ldb, tb, C, ldc, bias, accumulate, C2, act);
+        return (int)cudaGetLastError();
+    }
     if (!ta && K <= SK_KMAX) {
         const int rb = (M + SK_R - 1) / SK_R;
         smallk_kernel<<<dim3((N + SK_N - 1) / SK_N, rb < 65535 ? rb : 65535), SK_N, 0, s>>>(
             M, N, K, A, lda, B, ldb, tb, C, ldc, bias, accumulate, C2, act);
+        return (int)cudaGetLastError();
+    }
+    if (ta && !tb && ((N == 6 && M % 4 == 0 && lda % 4 == 0 && ((uintptr_t)A & 15) == 0) ||
+                      (M == 1 && N % 4 == 0 && ldb % 4 == 0 && ((uintptr_t)B & 15) == 0))) {
+        /* the surrogate's first and last layers: 16-byte loads along the wide side */
+        const bool big_m = N == 6;
+        const int nchunk = (K + TQ_K - 1) / TQ_K;
+        const int e = workspace((size_t)nchunk * M * N + (size_t)nchunk * M, s);
+        if (e) return e;
+        float *cs = g_ws + (size_t)nchunk * M * N;
+        const dim3 grid(((big_m ? M : N) + 255) / 256, nchunk);
+        if (big_m)
+            tn_quad_kernel<true, 6><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, g_ws, cs);
+        else
+            tn_quad_kernel<false, 1><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, g_ws, cs);
+        const size_t nout = (size_t)M * N + M;
+        if (!bias && !accumulate && !act && ldc >= N)
+            splitk_reduce_warp_kernel<<<(unsigned)((nout * 32 + 255) / 256), 256, 0, s>>>(M, N, nchunk, g_ws, C, ldc,
+                                                                                          cs, colsum);
+        else
+            splitk_reduce_kernel<<<grid1d(nout), 256, 0, s>>>(M, N, nchunk, g_ws, C, ldc, bias, accumulate, C2, act,
+                                                              cs, colsum);
         return (int)cudaGetLastError();
     }
     if (ta && !tb && (N <= TS_MAX || M <= TS_MAX)) {
@@ -658,8 +896,13 @@ extern "C" int fk_mlp_gemm(int M, int N, int K, const float *A, int lda, int ta,
         int e = fk_mlp_gemm_tc(g_tensor, M, N, K, A, lda, ta, B, ldb, tb, C, ldc, bias, accumulate, C2, act, split,
                                g_ws, cs, g_tc_error, s);
         if (!e && split > 1) {
-            splitk_reduce_kernel<<<grid1d((size_t)M * N + (cs_fused ? M : 0)), 256, 0, s>>>(
-                M, N, split, g_ws, C, ldc, bias, accumulate, C2, act, cs, cs_fused ? colsum : nullptr);
+            const size_t nout = (size_t)M * N + (cs_fused ? M : 0);
+            if (!bias && !accumulate && !act && N % 4 == 0 && ldc % 4 == 0 && ((uintptr_t)C & 15) == 0)
+                splitk_reduce_vec_kernel<<<(unsigned)((4 * ((size_t)M * N / 4 + (cs_fused ? M : 0)) + 255) / 256), 256, 0,
+                                           s>>>(M, N, split, g_ws, C, ldc, cs, cs_fused ? colsum : nullptr);
+            else
+                splitk_reduce_kernel<<<grid1d(nout), 256, 0, s>>>(M, N, split, g_ws, C, ldc, bias, accumulate, C2, act,
+                                                                  cs, cs_fused ? colsum : nullptr);
             e = (int)cudaGetLastError();
         }
         if (!e && colsum && !cs_fused) e = fk_mlp_colsum(K, M, A, colsum, s);
@@ -766,6 +1009,18 @@ extern "C" int fk_mlp_adam_sched(size_t n, float *w, const float *g, float *m, f
                                  const long long *tdev, float b1, float b2, float eps, cudaStream_t s)
 {
     adam_sched_kernel<<<grid1d(n), 256, 0, s>>>(n, w, g, m, v, sched, tdev, b1, b2, eps);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int fk_mlp_transpose_layers(int n, const long long *off, const int *in, const int *out, const float *w,
+                                       float *wt, cudaStream_t s)
+{
+    if (n <= 0) return 0;
+    if (n > TL_MAX) return (int)cudaErrorInvalidValue;
+    TLayers L;
+    L.n = n;
+    for (int i = 0; i < n; ++i) { L.off[i] = off[i]; L.in[i] = in[i]; L.out[i] = out[i]; }
+    transpose_layers_kernel<<<dim3(64, n), 256, 0, s>>>(L, w, wt);
     return (int)cudaGetLastError();
 }
 
