@@ -451,10 +451,10 @@ LOC_NEV = 10000
 LOC_EXACT_SAMPLE = 512
 LOC_L1_SAMPLE = 128
 SUR_WIDTH, SUR_DEPTH = 256, 5          # surrogate: 6 -> 5 x 256 SiLU -> tau
-# 12.3e6 sample evaluations either way: 16,384 x 750 (lr 4e-3) keeps the
-# pruning agreement at 100 % with the loss of 4,096 x 3,000 (lr 2e-3) and
-# runs the products 4x larger
-SUR_SAMPLES, SUR_STEPS, SUR_BATCH, SUR_LR = 2_000_000, 750, 16384, 4e-3
+# 65,536 rows x 375 steps (lr 4e-3, 24.6e6 sample evaluations) keeps the
+# pruning agreement at 100 % (as 16,384 x 750 and 4,096 x 3,000 at lr
+# 2e-3 do) with products large enough for the tensor cores' throughput
+SUR_SAMPLES, SUR_STEPS, SUR_BATCH, SUR_LR = 2_000_000, 375, 65536, 4e-3
 SUR_BLOCK = (4, 4, 4)                  # fine nodes per coarse block (z, x, y)
 
 

@@ -10,16 +10,18 @@
  * range of K (split K: partial tiles go to a workspace that a second kernel
  * adds in a fixed order).
  *
- * Each K block of 64 is staged by all 256 threads: FP32 values from global
- * memory, rounded to BF16 (PROD = 1) or split into BF16 hi + lo parts
- * (PROD = 3: products hi hi + hi lo + lo hi, about FP32 accuracy), written
- * into shared memory in the 128-byte-swizzled K-major layout the MMA reads.
- * One thread issues the MMAs (kind::f16, 128 x 256 x 16 each) and commits
- * them to the stage's mbarrier; the next stage is staged meanwhile (two
- * stages).  The epilogue reads the accumulators from tensor memory with
- * tcgen05.ld (warp w: lanes 32 (w mod 4) .. +31, columns 128 (w / 4) ..
- * +127) into shared memory and writes C row by row (coalesced), with the
- * bias, the previous contents and the SiLU activation applied as asked.  Every mbarrier wait is bounded; on a timeout the CTA
+ * Each K block of 64 reaches shared memory as BF16 in the 128-byte-swizzled
+ * K-major layout the MMA reads: FP32 values rounded to BF16 (PROD = 1) or
+ * split into BF16 hi + lo parts (PROD = 3: products hi hi + hi lo + lo hi,
+ * about FP32 accuracy).  With 16-byte aligned operands the FP32 values
+ * arrive by cp.async copies into a ring of half-stages several blocks
+ * ahead and are converted from shared memory (ASYNC); otherwise every
+ * thread loads and converts each block directly (two stages).  One thread
+ * issues the MMAs (kind::f16, 128 x 256 x 16 each) and commits them to an
+ * mbarrier.  The epilogue reads the accumulators from tensor memory with
+ * tcgen05.ld into a shared-memory tile and writes C row by row, with the
+ * bias, the previous contents and the SiLU activation (or its derivative)
+ * applied as asked.  Every mbarrier wait is bounded; on a timeout the CTA
  * sets the error word, lets its MMAs drain and frees its tensor memory.
  */
 #include <cuda_bf16.h>
