@@ -22,10 +22,14 @@ PRODUCTS = [(0, 2e-4, 1e-5), (3, 2e-4, 1e-5), (1, 2e-2, 5e-3)]
 
 
 @pytest.mark.parametrize("products,gtol,ftol", PRODUCTS)
-@pytest.mark.parametrize("width,depth,n", [(32, 3, 64), (256, 5, 300), (256, 5, 4096), (256, 5, 16384)])
+@pytest.mark.parametrize("width,depth,n", [(32, 3, 64), (256, 5, 300), (256, 5, 4096), (256, 5, 16384),
+                                           (102, 3, 301)])
 def test_gradient_matches_oracle(fk, width, depth, n, products, gtol, ftol):
     """The hidden layers reach the tensor cores when their width is 64 or
-    more (width 256); the width-32 network checks the CUDA-core path."""
+    more (width 256); the width-32 network checks the CUDA-core path; width
+    102 with 301 rows (extents not multiples of 4 or 64) the fallbacks:
+    plain-load staging with ragged K blocks, the scalar epilogue, the
+    one-column thin-layer kernels and the separate column sums."""
     old = fk.set_mlp_tensor_products(products)
     try:
         _gradient_case(fk, width, depth, n, gtol, ftol)
@@ -160,6 +164,24 @@ def test_async_staging_matches_synchronous(fk, products, n):
         net.finalize()
     finally:
         fk.set_mlp_tensor_products(old_p)
+
+
+def test_retraining_from_restored_weights_is_reproducible(fk):
+    """setWeights restores a network's starting state (weights, Adam
+    moments and step count): training again from the initial weights gives
+    the first run's weights and loss bit for bit (the bench times a run
+    after an untimed warm-up run this way)."""
+    loc = _prune_problem(fk, 40)
+    net = fk.MLP(256, 5, seed=7)
+    w0 = net.weights()
+    loss_a = loc.trainSurrogate(nsamples=200_000, steps=30, batch=4096, lr=2e-3, vref=3000.0, seed=7)
+    wa = net.weights()
+    net.setWeights(w0)
+    loss_b = loc.trainSurrogate(nsamples=200_000, steps=30, batch=4096, lr=2e-3, vref=3000.0, seed=7)
+    assert loss_a == loss_b
+    assert np.array_equal(wa, net.weights())
+    assert not np.array_equal(wa, w0)
+    loc.finalize()
 
 
 def test_captured_training_steps_match_eager(fk):
