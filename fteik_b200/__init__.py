@@ -159,6 +159,8 @@ _SIGS = {
     "fteik_b200_batch3d_getSlabConfig": [_PI, _PI, _PI, _PI, _PI, _PI, POINTER(c_float), POINTER(c_float), _PI, _PI],
     "fteik_b200_locate_locateEvents": [c_int, _PI, _PI, _PD, _PD, _PI],
     "fteik_b200_locate_setMethod": [c_int, _PI],
+    "fteik_b200_locate_setRankingProducts": [c_int, _PI],
+    "fteik_b200_locate_getRankingProducts": [_PI],
     "fteik_b200_locate_setNorm": [c_int, _PI],
     "fteik_b200_locate_setRescoreCandidates": [c_int, _PI],
     "fteik_b200_locate_debugAccumulators": [c_int, _PF, _PI],
@@ -625,6 +627,15 @@ class Locator:
         ierr = c_int(1)
         self.lib.fteik_b200_locate_setMethod(int(method), byref(ierr))
         _check(ierr, "fteik_b200_locate_setMethod")
+
+    def setRankingProducts(self, nprod):
+        """BF16 products of the tensor-core ranking: 3 (hi+lo both sides)
+        or 2 (the event side rounded once); returns the previous value."""
+        old, ierr = c_int(), c_int(1)
+        self.lib.fteik_b200_locate_getRankingProducts(byref(old))
+        self.lib.fteik_b200_locate_setRankingProducts(int(nprod), byref(ierr))
+        _check(ierr, "fteik_b200_locate_setRankingProducts")
+        return old.value
 
     def setNorm(self, norm):
         """2: the reference's L2 misfit; 1: L1 with median origin time."""

@@ -447,6 +447,22 @@ void fteik_b200_locate_setMethod(int method, int *ierr)
     SL.method = method;
 }
 
+void fk_locate_tc_set_products(int n);
+int fk_locate_tc_get_products(void);
+
+void fteik_b200_locate_setRankingProducts(int nprod, int *ierr)
+{
+    *ierr = 0;
+    if (nprod != 2 && nprod != 3) {
+        FK_ERR("fteik_b200_locate_setRankingProducts: nprod=%d must be 2 or 3", nprod);
+        *ierr = 1;
+        return;
+    }
+    fk_locate_tc_set_products(nprod);
+}
+
+void fteik_b200_locate_getRankingProducts(int *nprod) { *nprod = fk_locate_tc_get_products(); }
+
 void fteik_b200_locate_setRescoreCandidates(int ncand, int *ierr)
 {
     *ierr = 0;

@@ -14,7 +14,9 @@
  * so ranking grid points by s needs one events x stations by stations x points
  * product.  It runs on tcgen05 in BF16 with FP32 accumulation:
  *   - each operand is split as x = hi + lo (hi = bf16(x), lo = bf16(x - hi));
- *     the product is hi*hi + hi*lo + lo*hi (relative error about 2^-16);
+ *     the product is hi*hi + hi*lo (the default: the event side's rounding,
+ *     o_lo . T(g), varies smoothly over the grid and the FP64 re-score
+ *     decides) or hi*hi + hi*lo + lo*hi (relative error about 2^-16);
  *   - the event operand carries -2 o' (an exact scaling of the split);
  *   - q(g) enters as one more K step: the event side holds 1, 1, 1 and the
  *     table side q's three-way bf16 split (about 2^-24 relative), so the
@@ -43,7 +45,7 @@
  *   warp 0, one lane   bulk copies: two event tiles per work item, then a
  *                      4-stage ring of table tiles
  *   warp 1, one lane   tcgen05.mma: per table tile, 2 event tiles x (4 k-steps
- *                      x 3 products + the q step) into a 128 x 128 FP32
+ *                      x 2 or 3 products + the q step) into a 128 x 128 FP32
  *                      accumulator each; two accumulator sets (512 TMEM
  *                      columns) alternate
  *   warps 2-9          tcgen05.ld of the accumulators, run minima, top 4 runs
@@ -227,6 +229,10 @@ __device__ __forceinline__ void set_abort(volatile int *abort, int *error, int c
     atomicCAS(error, 0, code);
 }
 
+/* NPROD: 3 = hi*hi + hi*lo + lo*hi; 2 = hi*hi + hi*lo (the event operand
+ * rounded to BF16 once: its rounding error o_lo . T(g) varies smoothly over
+ * the grid, unlike the tables' rounding, which both forms keep) */
+template <int NPROD>
 __global__ void __launch_bounds__(NTHREADS, 1) l2_tc_kernel(Params P)
 {
     extern __shared__ uint8_t smem_raw[];
@@ -346,7 +352,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) l2_tc_kernel(Params P)
                         const uint32_t ko = (uint32_t)k * 32u;
                         mma_bf16(d, sdesc_sw128(a_hi + ko), sdesc_sw128(b_hi + ko), 1u);
                         mma_bf16(d, sdesc_sw128(a_hi + ko), sdesc_sw128(b_lo + ko), 1u);
-                        mma_bf16(d, sdesc_sw128(a_lo + ko), sdesc_sw128(b_hi + ko), 1u);
+                        if (NPROD == 3) mma_bf16(d, sdesc_sw128(a_lo + ko), sdesc_sw128(b_hi + ko), 1u);
                     }
                 }
                 mma_commit(EMPTY(stage));
@@ -914,6 +920,11 @@ static int pick_npart(int nmg, int ntile, int nsm)
     return best;
 }
 
+/* products of the ranking, 2 (the default) or 3 (l2_tc_kernel<NPROD>) */
+static int g_nprod = 2;
+extern "C" void fk_locate_tc_set_products(int n) { g_nprod = n == 2 ? 2 : 3; }
+extern "C" int fk_locate_tc_get_products(void) { return g_nprod; }
+
 extern "C" int fk_locate_tc_npart(int nev, int ngrd)
 {
     int dev = 0, nsm = 148;
@@ -941,8 +952,10 @@ extern "C" int fk_locate_tc(int ngrd, int ldgrd, int ntf, const float *tables, c
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(s, &cs);
     if (!attr_done && cs == cudaStreamCaptureStatusNone) {
-        cudaError_t e = cudaFuncSetAttribute(l2_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(l2_tc_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              SMEM_BYTES);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(l2_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
         if (e != cudaSuccess) return (int)e;
         attr_done = 1;
     }
@@ -963,7 +976,10 @@ extern "C" int fk_locate_tc(int ngrd, int ldgrd, int ntf, const float *tables, c
     P.dbg = dbg;
     P.spin_limit = 1ll << 22;
     const int grid = P.nitems < nsm ? P.nitems : nsm;
-    l2_tc_kernel<<<grid, NTHREADS, SMEM_BYTES, s>>>(P);
+    if (g_nprod == 2)
+        l2_tc_kernel<2><<<grid, NTHREADS, SMEM_BYTES, s>>>(P);
+    else
+        l2_tc_kernel<3><<<grid, NTHREADS, SMEM_BYTES, s>>>(P);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return (int)e;
     if (rescore > 0) {

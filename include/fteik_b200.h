@@ -421,6 +421,12 @@ void fteik_b200_locate_locateEvents(int n, const int ev[], int optIndx[],
  *      Events whose picks do not cover every table with one common weight
  *      fall back to method 0. */
 void fteik_b200_locate_setMethod(int method, int *ierr);
+/* BF16 products of the tensor-core ranking (methods 1 and 2): 2 (default)
+ * = hi*hi + hi*lo, the event operand rounded to BF16 once (its rounding
+ * error varies smoothly over the grid, and the FP64 re-score of the best
+ * candidates decides); 3 = hi*hi + hi*lo + lo*hi of both split operands. */
+void fteik_b200_locate_setRankingProducts(int nprod, int *ierr);
+void fteik_b200_locate_getRankingProducts(int *nprod);
 /* Misfit norm of every method (no counterpart in the reference, which has
  * L2 only): 2 (default) = locate.F90:620-744; 1 = L1 with origin-time
  * removal, obj(g) = w sum_i |o_i - T_i(g) - t0(g)|, t0(g) = the median of the
