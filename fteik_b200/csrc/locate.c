@@ -720,7 +720,8 @@ void fteik_b200_locate_buildSurrogate(int bz, int bx, int by, int *ierr)
         if (!e) e = fk_mlp_coarse_store(r0, m, SP.ngrd_c, SP.ldc, tau, dist, SP.coarse, s);
     }
     if (!e) e = fk_locate_tc_pack_tables(SP.ngrd_c, SP.ldc, SL.ntf, SP.coarse, SP.bpack_c, s);
-    const size_t nfine = (size_t)SP.ngrd_c * SL.ntf * (size_t)(bz * bx * by);
+    /* node-major block copy: each node's tables padded to a multiple of 4 */
+    const size_t nfine = (size_t)SP.ngrd_c * (size_t)((SL.ntf + 3) & ~3) * (size_t)(bz * bx * by);
     if (nfine != SP.fine_cap) {   /* a rebuild of the same blocks reuses the copy's memory */
         fk_dfree(SP.fine_blk);
         SP.fine_blk = (float *)fk_dalloc(sizeof(float) * nfine, who);

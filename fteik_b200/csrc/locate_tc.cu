@@ -668,6 +668,54 @@ __global__ void rescore_kernel(int nev, int npart, int ngrd, int ntf, int ldgrd,
 }
 
 
+/* a node's stations rounded up to 4 in the node-major block copy */
+__host__ __device__ __forceinline__ int ntf_pad(int ntf) { return (ntf + 3) & ~3; }
+
+/* misfit64 of NP nodes whose tables are 16-byte aligned runs (node-major
+ * block copy): the same operations in the same station order as
+ * misfit64_n, four stations per load; row[j] == nullptr skips node j. */
+template <int NP>
+__device__ __forceinline__ void misfit64_rows(const float *const (&row)[NP], const float *dummy, int ntf,
+                                              const double *o, const double *w, double sw, double sw2,
+                                              double (&ob)[NP], double (&t0)[NP])
+{
+    double a[NP], b[NP], c[NP];
+    const float4 *r4[NP];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+        a[j] = b[j] = c[j] = 0.0;
+        r4[j] = reinterpret_cast<const float4 *>(row[j] ? row[j] : dummy);
+    }
+    const int nq = ntf_pad(ntf) / 4;
+#pragma unroll 4
+    for (int q = 0; q < nq; ++q) {
+        float4 v[NP];
+#pragma unroll
+        for (int j = 0; j < NP; ++j) v[j] = __ldg(r4[j] + q);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = 4 * q + u;
+            if (i < ntf) {
+                const double wi = w[i], oi = o[i];
+#pragma unroll
+                for (int j = 0; j < NP; ++j) {
+                    const float tv = u == 0 ? v[j].x : u == 1 ? v[j].y : u == 2 ? v[j].z : v[j].w;
+                    const double d = oi - (double)tv;
+                    const double w2d = wi * wi * d;
+                    a[j] += wi * d;
+                    b[j] += w2d;
+                    c[j] += w2d * d;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+        t0[j] = a[j] / sw;
+        ob[j] = row[j] ? 0.5 * (c[j] - 2.0 * t0[j] * b[j] + t0[j] * t0[j] * sw2) : 1.0e300;
+    }
+}
+
 /* ---- pruned search (surrogate coarse lattice) ---------------------------- */
 
 struct PruneGeom {
@@ -684,7 +732,8 @@ struct PruneGeom {
  *  2. every fine node of the K coarse nodes' blocks (coarse node c owns the
  *     fine nodes f with floor(f / b) = c on every axis: bz bx by per block,
  *     bz bx by K in all) scored in FP64 on the exact tables, read from their
- *     block-major copy (one contiguous run per table and block); the minimum
+ *     node-major block copy (each node's tables one 16-byte aligned run,
+ *     read four stations per load); the minimum
  *     returned (first index among equal misfits);
  *  3. while a node next to that minimum (26-neighbourhood) lies in a block
  *     not yet examined, that block is examined too (a descent over blocks on
@@ -780,7 +829,7 @@ __global__ void __launch_bounds__(256, 3) prune_kernel(int nev, int npart, int R
     }
     __syncwarp();
     /* 2. fine nodes of the selected blocks */
-    const int nb = G.bz * G.bx * G.by;
+    const int nb = G.bz * G.bx * G.by, ntp = ntf_pad(G.ntf);
     double best = 1.0e300, bt0 = 0.0;
     int bg = 0x7fffffff, bk = -1;
     auto scan_block = [&](int k) {
@@ -796,12 +845,15 @@ __global__ void __launch_bounds__(256, 3) prune_kernel(int nev, int npart, int R
                 g2[j] = (p < nb && fz < G.nz && fx < G.nx && fy < G.ny)
                             ? fz + (long long)G.nz * (fx + (long long)G.nx * fy) : -1;
             }
-            /* the block's nodes are contiguous per table in the block-major copy */
+            /* each node's tables are one 16-byte aligned run in the node-major block copy */
             long long q2[2];
 #pragma unroll
             for (int j = 0; j < 2; ++j) q2[j] = g2[j] >= 0 ? p0 + 32 * j : -1;
             double ob[2], t0[2];
-            misfit64_n<2>(fine + (size_t)c * G.ntf * nb, (size_t)nb, q2, G.ntf, o, w, sw, sw2, ob, t0);
+            const float *rows[2];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) rows[j] = q2[j] >= 0 ? fine + ((size_t)c * nb + q2[j]) * ntp : nullptr;
+            misfit64_rows<2>(rows, fine, G.ntf, o, w, sw, sw2, ob, t0);
 #pragma unroll
             for (int j = 0; j < 2; ++j)
                 if (g2[j] >= 0 && lex_lt_d(ob[j], (int)g2[j], best, bg)) {
@@ -856,14 +908,15 @@ __global__ void __launch_bounds__(256, 3) prune_kernel(int nev, int npart, int R
     flag[e] = fb ? (unsigned char)0xFF : (unsigned char)nsel;
 }
 
-/* Block-major copy of the exact tables for the pruned search:
- * out[((c * ntf) + i) * nb + p] = T_i(node p of block c), p = pz + bz (px + bx py);
- * nodes outside the grid hold 0 (never read). */
+/* Block-major, node-major copy of the exact tables for the pruned search:
+ * out[(c nb + p) ntp + i] = T_i(node p of block c), p = pz + bz (px + bx py),
+ * ntp = ntf rounded up to 4 (a node's tables are one 16-byte aligned run);
+ * padding and nodes outside the grid hold 0 (never read). */
 __global__ void block_tables_kernel(int nz, int nx, int ny, int bz, int bx, int by, int ncz, int ncx, int ntf,
                                     int ldgrd, long long nblk, const float *__restrict__ tables,
                                     float *__restrict__ out)
 {
-    const int nb = bz * bx * by;
+    const int nb = bz * bx * by, ntp = ntf_pad(ntf);
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= nblk * nb) return;
     const long long c = t / nb;
@@ -872,9 +925,18 @@ __global__ void block_tables_kernel(int nz, int nx, int ny, int bz, int bx, int 
     const int fz = bz * cz + p % bz, fx = bx * cx + (p / bz) % bx, fy = by * cy + p / (bz * bx);
     const bool in = fz < nz && fx < nx && fy < ny;
     const long long g = in ? fz + (long long)nz * (fx + (long long)nx * fy) : 0;
-    float *dst = out + (size_t)c * ntf * nb + p;
-    for (int i = 0; i < ntf; ++i) dst[(size_t)i * nb] = in ? __ldg(tables + (size_t)i * ldgrd + g) : 0.0f;
+    float4 *dst = reinterpret_cast<float4 *>(out + (size_t)t * ntp);
+    for (int q = 0; q < ntp / 4; ++q) {
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = 4 * q + u;
+            v[u] = (in && i < ntf) ? __ldg(tables + (size_t)i * ldgrd + g) : 0.0f;
+        }
+        dst[q] = make_float4(v[0], v[1], v[2], v[3]);
+    }
 }
+
 } // namespace fktc
 
 using namespace fktc;
