@@ -332,12 +332,19 @@ def bench_single_3d(fk, torch, steps):
     ms = ev0.elapsed_time(ev1) / steps
     init_ms, pass_ms = b.kernelTimes()
     out = np.empty(n[0] * n[1] * n[2], np.float32)
+
+    def e2e_once():
+        """model and source up, solve, field down (the drop-in call sequence)"""
+        b.setVelocityModel(1, vel)
+        b.setSources(1, [src[0]], [src[1]], [src[2]])
+        b.solve()
+        b.fields32(1, out)
+
+    e2e_once()                               # untimed: the download's staging buffer, first copies
     t0 = time.perf_counter()
-    b.setVelocityModel(1, vel)
-    b.setSources(1, [src[0]], [src[1]], [src[2]])
-    b.solve()
-    b.fields32(1, out)
-    e2e_ms = (time.perf_counter() - t0) * 1e3
+    for _ in range(max(1, steps)):
+        e2e_once()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / max(1, steps)
     res, npass = b.solveInfo(1, 1)
     b.finalize()
     si = (snap1(n[0], h, src[0]), snap1(n[1], h, src[1]), snap1(n[2], h, src[2]))
