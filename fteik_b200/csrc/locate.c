@@ -65,6 +65,7 @@ static struct {
     size_t coarse_cap, bpack_cap;   /* sizes of coarse / bpack_c (floats / bytes) */
     float *bx_in, *bx_dist, *bx_tau; /* build scratch: inputs, distances, outputs of a chunk */
     long long blk_gen;       /* table generation fine_blk was built from */
+    int blk_shape[3];        /* and its block shape (bz, bx, by) */
     void *bpack_c;
     int rc, k;
     unsigned char *flag_dev;
@@ -728,9 +729,21 @@ void fteik_b200_locate_buildSurrogate(int bz, int bx, int by, int *ierr)
         SP.fine_cap = SP.fine_blk ? nfine : 0;
     }
     if (!SP.fine_blk) e = 1;
-    if (!e) e = fk_locate_block_tables(SP.nz, SP.nx, SP.ny, bz, bx, by, SL.ntf, SL.ldgrd, SL.tables, SP.fine_blk, s);
-    SP.blk_gen = SL.table_gen;
+    /* the block copy depends on the exact tables and the block shape only:
+     * a rebuild for a retrained network keeps it */
+    const bool blk_fresh = SP.blk_gen == SL.table_gen && SP.blk_shape[0] == bz && SP.blk_shape[1] == bx &&
+                           SP.blk_shape[2] == by;
+    if (!e && !blk_fresh)
+        e = fk_locate_block_tables(SP.nz, SP.nx, SP.ny, bz, bx, by, SL.ntf, SL.ldgrd, SL.tables, SP.fine_blk, s);
     if (!e) e = (int)cudaStreamSynchronize(s);
+    if (!e) {
+        SP.blk_shape[0] = bz;
+        SP.blk_shape[1] = bx;
+        SP.blk_shape[2] = by;
+        SP.blk_gen = SL.table_gen;
+    } else {
+        SP.blk_shape[0] = 0;   /* the copy is not known to be complete */
+    }
     if (fk_check(e, who)) return;
     SP.ready = true;
     *ierr = 0;
@@ -818,6 +831,9 @@ static int locate_range_pruned(int e0, int n, int *idx, double *t0, double *obj)
                                         SP.fine_blk, fk_stream());
         if (fk_check(eb, "locate (surrogate-pruned): block copy")) return 1;
         SP.blk_gen = SL.table_gen;
+        SP.blk_shape[0] = SP.bz;
+        SP.blk_shape[1] = SP.bx;
+        SP.blk_shape[2] = SP.by;
     }
     const int npart = fk_locate_tc_npart(n, SP.ngrd_c);
     if (upload_obs64() || ensure_tc(n, npart)) return 1;
