@@ -106,6 +106,37 @@ def test_pruned_search_matches_exhaustive(fk):
     loc.finalize()
 
 
+def test_rebuild_keeps_block_copy_only_while_tables_unchanged(fk):
+    """buildSurrogate keeps the exact tables' block copy across rebuilds
+    with the same tables and block shape (the same located events), and
+    rebuilds it when a table changes (the pruned search then follows the
+    new tables: it agrees with the exhaustive search on them)."""
+    nev = 300
+    loc = _prune_problem(fk, nev)
+    ev = np.arange(1, nev + 1)
+    fk.MLP(256, 5, seed=7)
+    loc.trainSurrogate(nsamples=400_000, steps=600, batch=4096, lr=2e-3, vref=3000.0, seed=7)
+    loc.setMethod(2)
+    loc.buildSurrogate((4, 4, 4))
+    first = loc.locateEvents(ev)
+    loc.buildSurrogate((4, 4, 4))                    # same tables and shape: the copy is kept
+    again = loc.locateEvents(ev)
+    assert np.array_equal(first[0], again[0]) and np.array_equal(first[2], again[2])
+    # move one station's table: the copy must follow it
+    nz, nx, ny, h = 24, 40, 36, 100.0
+    tables, _ = linear_gradient_tables(nz, nx, ny, h, 64, grad=0.5, seed=20)
+    shifted = tables[5] + np.float32(0.35)
+    loc.setTravelTimeField32f(6, shifted)
+    loc.buildSurrogate((4, 4, 4))
+    got = loc.locateEvents(ev)
+    loc.setMethod(1)
+    ref = loc.locateEvents(ev)
+    assert np.mean(got[0] == ref[0]) >= 0.995
+    same = got[0] == ref[0]
+    assert np.all(np.abs(got[2][same] - ref[2][same]) <= 1e-9 * np.abs(ref[2][same]) + 1e-12)
+    loc.finalize()
+
+
 @pytest.mark.parametrize("n", [20_000, 20_001, 85_537])
 def test_fused_forward_matches_layer_by_layer(fk, n):
     """The one-kernel forward pass (BF16 products, activations kept on the
