@@ -6,12 +6,21 @@
  * The network has no counterpart in the reference; it ranks grid points for
  * the pruned grid search and is checked against the exhaustive search.
  *
- * GEMM: C[M][N] = sum_k A(m,k) B(k,n) (+ bias[n]) in FP32 on the CUDA cores,
- * 128 x 64 output tiles, K in steps of 16 through shared memory, 8 x 4
- * outputs per thread.  A(m,k) = A[m*lda + k] (ta = 0) or A[k*lda + m]
- * (ta = 1); B(k,n) = B[k*ldb + n] (tb = 0) or B[n*ldb + k] (tb = 1).
- * Forward Z = X W^T + b is (ta, tb) = (0, 1); dX = dZ W is (0, 0);
- * dW = dZ^T X is (1, 0).
+ * Products C[M][N] = sum_k A(m,k) B(k,n) (+ bias[n]), A(m,k) = A[m*lda + k]
+ * (ta = 0) or A[k*lda + m] (ta = 1); B(k,n) = B[k*ldb + n] (tb = 0) or
+ * B[n*ldb + k] (tb = 1).  Forward Z = X W^T + b is (ta, tb) = (0, 1); the
+ * input gradient dZ W is (0, 1) on the transposed weights; the weight
+ * gradient dZ^T X is (1, 0).  fk_mlp_gemm sends each product to:
+ *   - the thin-layer kernels (FP32): K <= 8 (the 6-input first layer, the
+ *     1-output layer's input gradient), N = 1 (the output layer), and the
+ *     weight gradients with M or N <= 8 (first and last layers), the bias
+ *     gradient from the same pass;
+ *   - the tensor cores (mlp_tc.cu) for the hidden layers (N, K >= 64);
+ *   - otherwise the FP32 tiled GEMM below (128 x 64 output tiles, K in
+ *     steps of 16 through shared memory, 8 x 4 outputs per thread).
+ * K is split over CTAs only for long K (the weight gradients); slices are
+ * added in a fixed order, and every reduction here (slices, column sums,
+ * the loss) has a fixed order, so training is reproducible run to run.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
