@@ -198,3 +198,36 @@ def test_archive_levels_and_velocities(fk, tmp_path):
     geo = (d / "Geometry.txt").read_text().split()
     assert [int(v) for v in geo[:3]] == [nz, nx, ny]
     L.fteik_model_free()
+
+
+def test_host_switches_validate_and_round_trip(fk):
+    """The speed switches of the grid search and the surrogate (host-side
+    state only): invalid values are refused with ierr = 1 and leave the
+    setting unchanged; valid ones read back."""
+    from ctypes import byref, c_int
+    L = fk.lib()
+    old, ierr = c_int(), c_int(0)
+    L.fteik_b200_locate_getRankingProducts(byref(old))
+    assert old.value == 2                       # the default: tables split, events rounded once
+    for bad in (0, 1, 4):
+        L.fteik_b200_locate_setRankingProducts(bad, byref(ierr))
+        assert ierr.value == 1
+        v = c_int()
+        L.fteik_b200_locate_getRankingProducts(byref(v))
+        assert v.value == old.value
+    for good in (3, 2):
+        L.fteik_b200_locate_setRankingProducts(good, byref(ierr))
+        assert ierr.value == 0
+        v = c_int()
+        L.fteik_b200_locate_getRankingProducts(byref(v))
+        assert v.value == good
+    for name in ("AsyncStaging", "FusedForward", "TrainGraph"):
+        get, put = getattr(L, "fteik_b200_mlp_get" + name), getattr(L, "fteik_b200_mlp_set" + name)
+        was = c_int()
+        get(byref(was))
+        assert was.value == 1                   # every speed path on by default
+        put(0)
+        v = c_int()
+        get(byref(v))
+        assert v.value == 0
+        put(was.value)
