@@ -560,7 +560,7 @@ __global__ void colsum_final_kernel(int N, int nchunk, const float *__restrict__
 
 /* mean squared error over n outputs: dpred = 2 (pred - y) / n; the loss in
  * a fixed order: block sums into part[], and the block that finishes last
- * (a counter, reset by it) adds them in block order into *loss */
+ * (a counter, reset by it) adds them in a fixed order into *loss */
 __global__ void mse_kernel(int n, const float *__restrict__ pred, const float *__restrict__ y,
                            float *__restrict__ dpred, double *__restrict__ loss, double *part, unsigned *count)
 {
@@ -585,12 +585,21 @@ __global__ void mse_kernel(int n, const float *__restrict__ pred, const float *_
         last = atomicAdd(count, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        double t = 0.0;
-#pragma unroll 8
-        for (unsigned b = 0; b < gridDim.x; ++b) t += reinterpret_cast<volatile double *>(part)[b];
-        *loss = t;
+    if (!last) return;   /* block-uniform: read after the barrier */
+    /* the last block adds the block sums in a fixed order: thread i the
+     * sums i, i + 256, ... in order, then a fixed tree */
+    __threadfence();
+    double t = 0.0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+        t += reinterpret_cast<volatile double *>(part)[b];
+    red[threadIdx.x] = t;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        *loss = red[0];
         *count = 0;
     }
 }
